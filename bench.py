@@ -1,0 +1,401 @@
+#!/usr/bin/env python3
+"""Benchmark: trajectory steps/s and DTM Mpx/s of the trace + fields stages.
+
+One step = the reference's Trace stage on one synthetic DTM: record the
+trajectory-seed subsample down and up (Trajectories), then trace every pixel's
+d*d jittered sub-pixel trajectories down and up accumulating slc/slt
+(Fields).  Default workload: 2048^2 @ 2 m, d=2, jitter +-0.5 px, RK4, step
+0.1 px, max 10000 steps (16.8 M field trajectories per direction).
+
+  value  steps/s with inputs resident in HBM (CUDA events around each step;
+         a 256 MiB buffer is written between steps to flush L2)
+  e2e    the same metric through the public API (Trajectories + Fields) with
+         the inputs in pinned host memory and the results read back per step
+  roofline  the field kernel: algorithmic bytes per RK step (RK2 75 B, RK4
+         139 B) x steps / kernel time, against the measured HBM copy peak
+  cpu_baseline  the reference's CPU path timed on this host's cores on a
+         bounded stride of the same seeds
+
+N>1 (torchrun): the field seeds are split into contiguous ranges per rank,
+each rank accumulates its own uint64 slc/slt, then one NCCL all-reduce (sum)
+combines them (integer sums: identical to one GPU).  Total work is fixed
+(strong scaling).
+
+`--impl reference` times the reference's own CPU implementation instead
+(rank 0 only): the reference's OpenCL C kernels compiled for the host
+(oracle/_ref) with OpenMP on all cores when the workload uses the
+reference's RK2, else (RK4 has no counterpart in the reference) the oracle's
+C restatement.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [ROOT, os.path.join(ROOT, "oracle")]
+
+BYTES_PER_STEP = {2: 75, 4: 139}
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fp:
+            pk = json.load(fp)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.QUERY,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _cpu_sample(wl, stride, sign, cores):
+    """Fields pass over every stride-th shuffled seed on the host cores.
+
+    The sampled seeds form their own list (their RNG streams follow their
+    position in it).  The oracle's restatement counts the RK steps of that
+    list; with the reference's RK2 the timed run is the reference's own kernel
+    on the same list (bit-identical trajectories), otherwise the restatement.
+    Returns (steps, seconds, kind)."""
+    import oracle as O
+    from slm_b200 import params as P
+    integ = wl.spec.integrator
+    sub = np.ascontiguousarray(wl.seeds[::stride])
+    prm = P.kernel_params(wl.info, "INTEGRATE_FIELDS", sign)
+    prm.n_seed_points = sub.shape[0]
+    t0 = time.perf_counter()
+    _, _, steps, _ = O.integrate_fields(prm, sub, wl.mask, wl.uv, integ, n_threads=cores)
+    t = time.perf_counter() - t0
+    if integ == 2 and O.ref_available("integrate_fields"):
+        t0 = time.perf_counter()
+        O.ref_integrate_fields(prm, sub, wl.mask, wl.uv, n_threads=cores)
+        return steps, time.perf_counter() - t0, "reference"
+    return steps, t, "port"
+
+
+def _cpu_stride(wl, cores, target_s):
+    n = int(wl.info.n_seed_points)
+    probe = max(1, n // 512)
+    _, t, _ = _cpu_sample(wl, probe, 1.0, cores)
+    return max(1, int(probe * max(t, 1e-3) / target_s))
+
+
+def run_reference(args):
+    """The reference's CPU implementation on this host, a bounded sample per step."""
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    from slm_b200.workloads import Workload
+    wl = Workload(args.workload)
+    cores = os.cpu_count() or 1
+    stride = _cpu_stride(wl, cores, 3.0)
+    for _ in range(args.warmup):
+        _cpu_sample(wl, stride * 16, 1.0, cores)
+    tot_steps, tot_t, kind = 0, 0.0, "port"
+    for _ in range(args.steps):
+        for sign in (1.0, -1.0):
+            s, t, kind = _cpu_sample(wl, stride, sign, cores)
+            tot_steps += s
+            tot_t += t
+    v = tot_steps / tot_t
+    sample = "fields down+up over every {}th shuffled seed ({} of {} seeds)".format(
+        stride, (int(wl.info.n_seed_points) + stride - 1) // stride, int(wl.info.n_seed_points))
+    line = {
+        "impl": "reference", "metric": "trajectory steps/s (trace+fields)", "value": v,
+        "unit": "steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * tot_t / max(args.steps, 1), "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": wl.spec.name, "sample": sample},
+        "cpu_baseline": {"value": v, "unit": "steps/s", "cores": cores, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    from slm_b200 import kernels
+    from slm_b200.params import kernel_params
+    from slm_b200.workloads import Workload
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if ws > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    wl = Workload(args.workload)
+    spec = wl.spec
+    info = wl.info
+    integrator = spec.integrator
+    n_seeds = int(info.n_seed_points)
+    begin = (n_seeds * rank) // ws
+    end = (n_seeds * (rank + 1)) // ws
+    nxy = int(info.nx_padded * info.ny_padded)
+
+    seeds_d = torch.from_numpy(wl.seeds).to(dev)
+    mask_d = torch.from_numpy(wl.mask.view(np.uint8)).to(dev)
+    uv_d = torch.from_numpy(wl.uv).to(dev)
+    acc = torch.zeros((2, 2, nxy), dtype=torch.uint64, device=dev)
+    work = [kernels.workspace(dev) for _ in range(2)]
+    n_traj = wl.n_traj
+    nl = int(info.max_n_steps)
+    traj_d = torch.zeros(n_traj * nl * 2, dtype=torch.int8, device=dev)
+    nsteps_d = torch.zeros((2, n_traj), dtype=torch.uint16, device=dev)
+    length_d = torch.zeros((2, n_traj), dtype=torch.float32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+
+    field_prm = []
+    for sign in (1.0, -1.0):
+        prm = kernel_params(info, "INTEGRATE_FIELDS", sign)
+        prm.seeds_chunk_offset = begin
+        prm.n_seed_points = end
+        field_prm.append(prm)
+    tinfo = wl.fresh_info()
+    tinfo.n_seed_points = n_traj
+    traj_prm = [kernel_params(tinfo, "INTEGRATE_TRAJECTORY", np.float32(s)) for s in (1.0, -1.0)]
+    stream = torch.cuda.current_stream()
+
+    def device_step(ev=None):
+        acc.zero_()
+        for d in range(2):
+            kernels.integrate_trajectory(traj_prm[d], n_traj, seeds_d, mask_d, uv_d, traj_d,
+                                         nsteps_d[d], length_d[d], integrator)
+        if ev is not None:
+            ev[0].record(stream)
+        for d in range(2):
+            kernels.integrate_fields(field_prm[d], seeds_d, mask_d, uv_d, acc[d, 0], acc[d, 1],
+                                     work[d], schedule=args.schedule, integrator=integrator)
+        if ev is not None:
+            ev[1].record(stream)
+        if ws > 1:
+            dist.all_reduce(acc.view(torch.int64), op=dist.ReduceOp.SUM)
+
+    def count_steps():
+        f = sum(int(w[1].view(torch.int64).item()) for w in work)
+        t = int(nsteps_d.to(torch.int32).sum().item())
+        return f, t
+
+    for _ in range(args.warmup):
+        device_step()
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    field_steps_rank, traj_steps = count_steps()
+    times, ktimes = [], []
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            if ws > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            e0.record(stream)
+            device_step((k0, k1))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+            ktimes.append(k0.elapsed_time(k1) / 1e3)
+    step_t = float(np.sum(times))
+    kern_t = float(np.sum(ktimes))
+    if ws > 1:
+        t = torch.tensor([step_t, kern_t], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_t, kern_t = float(t[0]), float(t[1])
+        fs = torch.tensor([field_steps_rank], dtype=torch.int64, device=dev)
+        dist.all_reduce(fs, op=dist.ReduceOp.SUM)
+        field_steps = int(fs.item())
+    else:
+        field_steps = field_steps_rank
+    steps_per_step = field_steps + traj_steps
+    value = steps_per_step * args.steps / step_t
+    ms = 1e3 * step_t / args.steps
+
+    # e2e through the public API (pinned host inputs, results back on the host)
+    e2e = None
+    if ws == 1 and not args.no_e2e:
+        e2e = run_e2e(args, wl, dev)
+
+    peak, peak_kind = _peaks()
+    bps = BYTES_PER_STEP[integrator]
+    achieved = field_steps_rank * args.steps * bps / kern_t / 1e9
+    line = {
+        "metric": "trajectory steps/s (trace+fields)", "value": value, "unit": "steps/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded DTM; no dataset)",
+        "config": {"workload": spec.name, "schedule": args.schedule,
+                   "field_trajectories_per_direction": n_seeds * spec.density ** 2,
+                   "trajectory_seeds": n_traj, "l2": "256 MiB buffer written between steps",
+                   "mpx_per_s": wl.n_pixels / (step_t / args.steps) / 1e6,
+                   "rk_steps_per_step": steps_per_step,
+                   "parallelism": "seed shards + NCCL all-reduce" if ws > 1 else "1 GPU"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_source": peak_kind,
+                     "kernel": "k_fields_{}<{}>".format(args.schedule, integrator),
+                     "bytes_per_step": bps},
+        "clocks": clocks.summary(),
+        "gpu_launches": args.steps * 4,
+    }
+    if e2e is not None:
+        line["e2e"] = e2e
+    if rank == 0 and not args.no_cpu and ws == 1:
+        line["cpu_baseline"] = cpu_baseline(wl, args)
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_e2e(args, wl, dev):
+    """Public-API step: Trajectories then Fields on pinned host arrays."""
+    import torch
+
+    from slm_b200.device import pinned_empty
+    from slm_b200.fields import Fields
+    from slm_b200.trajectories import Trajectories
+    from slm_b200.useful import Data
+
+    uv_h = pinned_empty(wl.uv.shape, np.float32)
+    uv_h[...] = wl.uv
+    mask_h = pinned_empty(wl.mask.shape, np.bool_)
+    mask_h[...] = wl.mask
+    integ = wl.spec.integrator
+
+    def step():
+        info = wl.fresh_info()
+        data = Data(info=info, mask_array=mask_h, uv_array=uv_h,
+                    mapping_array=np.zeros(mask_h.shape, np.uint32))
+        tr = Trajectories(0, dev.index, info=info, data=data, integrator=integ)
+        tr.integrate()
+        info2 = wl.fresh_info()
+        data2 = Data(info=info2, mask_array=mask_h, uv_array=uv_h,
+                     mapping_array=np.zeros(mask_h.shape, np.uint32),
+                     traj_stats_df=tr.data.traj_stats_df)
+        f = Fields(0, dev.index, info=info2, data=data2, schedule=args.schedule, integrator=integ)
+        f.integrate()
+        return tr.n_steps + sum(f.n_steps)
+
+    step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    n = 0
+    k = max(1, min(args.steps, 3))
+    for _ in range(k):
+        n += step()
+    torch.cuda.synchronize()
+    t = time.perf_counter() - t0
+    nxy = wl.mask.size
+    h2d = wl.uv.nbytes * 2 + wl.mask.nbytes * 2 + wl.seeds.nbytes + wl.traj_seeds.nbytes
+    d2h = nxy * 4 * 4 + wl.n_traj * 2 * (2 + 4)
+    return {"value": n / t, "unit": "steps/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "steps": k,
+            "note": "Trajectories.integrate + Fields.integrate incl. seed shuffle and host post-processing"}
+
+
+def cpu_baseline(wl, args):
+    """The reference's CPU path on a bounded seed stride (same metric, ~10 s)."""
+    cores = os.cpu_count() or 1
+    stride = _cpu_stride(wl, cores, 10.0)
+    steps, t, kind = _cpu_sample(wl, stride, 1.0, cores)
+    n = int(wl.info.n_seed_points)
+    return {"value": steps / t, "unit": "steps/s", "cores": cores, "kind": kind,
+            "sample": "downstream fields over every {}th shuffled seed ({} of {} seeds), {:.1f} s".format(
+                stride, (n + stride - 1) // stride, n, t)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="config2")
+    ap.add_argument("--schedule", default="persistent", choices=["plain", "persistent"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

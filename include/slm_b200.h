@@ -1,0 +1,133 @@
+/* slm_b200.h -- C ABI of the B200 streamline tracer (libslm_b200.so).
+ *
+ * Drop-in boundary for the OpenCL kernels of atthecodeface/slm's `streamlines`
+ * package.  The reference builds one OpenCL program per launch with every
+ * scalar as a -D macro (python/streamlines/pocl.py:178-299) and passes only
+ * __global buffers, in the insertion order of each wrapper's array_dict
+ * (pocl.py:538-539).  Each entry point here takes:
+ *   - `const slm_params*`: the macro values as a host struct (field = macro name
+ *     in lower case; built by slm_b200/params.py exactly as the reference
+ *     formats its macros);
+ *   - the same buffers as the reference kernel, in the same order, as DEVICE
+ *     pointers owned by the caller (nothing here allocates device memory);
+ *   - a CUDA stream (`void*`, cudaStream_t; NULL = legacy default stream).
+ * Calls are asynchronous and stream-ordered.  They return 0 on success or an
+ * SLM_ERR_* code; slm_last_error() gives the message of the calling thread's
+ * last failure.  No exception or device trap crosses this boundary.
+ *
+ * Accumulators that the reference keeps as wrapping uint32 (slt, slc) are
+ * uint64 here; the low 32 bits equal the reference's values.
+ */
+#ifndef SLM_B200_H
+#define SLM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SLM_OK 0
+#define SLM_ERR_ARGS 1          /* bad pointer, size or parameter */
+#define SLM_ERR_CUDA 2          /* a CUDA runtime call failed */
+#define SLM_ERR_CAPACITY 3      /* a buffer or work queue is too small */
+#define SLM_ERR_ITERATION_CAP 4 /* a bounded device loop hit its cap (see message) */
+#define SLM_ERR_UNSUPPORTED 5   /* option not built into this library */
+
+/* Kernel parameters: one field per -D macro of pocl.set_compile_options
+ * (pocl.py:197-277); the last two carry the DO_MEASURE_HSL_FROM_RIDGES flag
+ * and the KDF_IS_<shape> selector (0 tophat, 1 triangle, 2 epanechnikov,
+ * 3 cosine, 4 gaussian). */
+typedef struct slm_params {
+    uint32_t n_seed_points, downup_sign;
+    float integrator_step_factor, max_integration_step_error, adjusted_max_error,
+          integration_halt_threshold, max_length, pixel_size;
+    uint32_t pad_width;
+    float pad_width_pp5;
+    uint32_t nx_padded, ny_padded, nxy_padded;
+    float nxf_mp5, nyf_mp5, grid_scale, combo_factor, dt_max;
+    uint32_t max_n_steps, trajectory_resolution, seeds_chunk_offset,
+             subpixel_seed_point_density;
+    float subpixel_seed_halfspan, subpixel_seed_step, jitter_magnitude;
+    uint32_t interchannel_max_n_steps, left_flank_addition;
+    uint32_t is_channel, is_thinchannel, is_interchannel, is_channelhead,
+             is_channeltail, is_majorconfluence, is_minorconfluence,
+             is_majorinflow, is_minorinflow, is_leftflank, is_rightflank,
+             is_midslope, is_ridge, was_channelhead, is_subsegmenthead, is_loop,
+             is_blockage;
+    uint32_t segmentation_threshold;
+    float bandwidth;
+    uint32_t n_data, n_hist_bins, n_pdf_points;
+    float logx_min, logx_max, logx_range, bin_dx, pdf_dx, kdf_width_x;
+    uint32_t n_kdf_part_points_x;
+    float logy_min, logy_max, logy_range, bin_dy, pdf_dy, kdf_width_y;
+    uint32_t n_kdf_part_points_y;
+    uint32_t do_measure_hsl_from_ridges, kdf_kind;
+} slm_params;
+
+/* Integrator order used by the tracing entry points. */
+#define SLM_RK2 2   /* the reference's integrator (opencl/computestep.cl:42-106) */
+#define SLM_RK4 4   /* classical 4-stage extension; same quantisation and dt rule */
+
+/* Launch shape of the field tracer. */
+#define SLM_SCHED_PLAIN 0       /* one thread per (seed, sub-pixel) trajectory */
+#define SLM_SCHED_PERSISTENT 1  /* persistent warps refilled from a work queue */
+
+typedef struct slm_launch {
+    int32_t schedule;        /* SLM_SCHED_* */
+    int32_t integrator;      /* SLM_RK2 or SLM_RK4 */
+    int32_t block_threads;   /* threads per block (multiple of 32); 0 = default */
+    int32_t blocks_per_sm;   /* persistent schedule: resident blocks per SM; 0 = default */
+    int32_t chunk;           /* persistent schedule: items taken per queue grab per lane */
+    int32_t reserved[3];
+} slm_launch;
+
+const char* slm_version(void);
+const char* slm_last_error(void);
+int slm_device_count(void);
+
+/* Words of device scratch the field tracer needs (queue head and counters);
+ * the caller allocates slm_fields_workspace_words() uint64 words. */
+size_t slm_fields_workspace_words(void);
+
+/* integrate_fields: d*d jittered sub-pixel trajectories per seed, downstream
+ * or upstream (sign carried in combo_factor / downup_sign), accumulating per
+ * pixel the streamline count slc (+1 per visit) and the rounded running length
+ * slt (+ (uint)(l+0.5)).  Replaces kernel integrate_fields
+ * (opencl/integratefields.cl:60-114, jittertrajectory.cl:42-88) bound by
+ * Fields.gpu_integrate (python/streamlines/fields.py:217-260).
+ *   seed_point [n_seed_points] float2 (x,y) in unpadded pixel units
+ *   mask       [nxy_padded] uint8 (nonzero = masked)
+ *   uv         [nxy_padded] float2, x-major (idx = ny_padded*x + y)
+ *   mapping    unused by the kernel (kept for argument-order parity); may be NULL
+ *   slc, slt   [nxy_padded] uint64 accumulators (added to, not cleared)
+ *   workspace  [slm_fields_workspace_words()] uint64; on return word 1 holds
+ *              the number of RK steps and word 2 the number of trajectories
+ *              traced by this call (stream-ordered).
+ * Seeds seeds_chunk_offset .. n_seed_points-1 are traced (the whole list when
+ * seeds_chunk_offset is 0). */
+int slm_integrate_fields(const slm_params* p, const slm_launch* launch,
+                         const float* seed_point, const uint8_t* mask, const float* uv,
+                         uint32_t* mapping, uint64_t* slc, uint64_t* slt,
+                         uint64_t* workspace, void* stream);
+
+/* integrate_trajectory: one un-jittered trajectory per seed of the chunk
+ * seeds_chunk_offset .. seeds_chunk_offset+n_chunk-1 (clipped to
+ * n_seed_points), recording each step as a char2 at 1/trajectory_resolution
+ * px, the step count (uint16) and the length in px (float).  Replaces kernel
+ * integrate_trajectory (opencl/integratetraj.cl:54-97, trajectory.cl:41-80)
+ * bound by Trajectories.gpu_compute_trajectories
+ * (python/streamlines/trajectories.py:196-317).
+ *   trajectories [n_chunk * max_n_steps] int8x2, row g = chunk-local seed g
+ *   nsteps       [n_chunk] uint16
+ *   length       [n_chunk] float */
+int slm_integrate_trajectory(const slm_params* p, int32_t integrator, uint32_t n_chunk,
+                             const float* seed_point, const uint8_t* mask, const float* uv,
+                             uint32_t* mapping, int8_t* trajectories, uint16_t* nsteps,
+                             float* length, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SLM_B200_H */

@@ -1,0 +1,91 @@
+"""ctypes binding of ``libslm_b200.so`` (the C ABI declared in ``include/slm_b200.h``).
+
+There is no fallback: if the library is missing or no CUDA device is visible,
+every product call raises.  Build it with ``python -m slm_b200.build``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libslm_b200.so")
+
+SLM_OK = 0
+SLM_ERR_ARGS = 1
+SLM_ERR_CUDA = 2
+SLM_ERR_CAPACITY = 3
+SLM_ERR_ITERATION_CAP = 4
+SLM_ERR_UNSUPPORTED = 5
+
+SLM_RK2 = 2
+SLM_RK4 = 4
+SLM_SCHED_PLAIN = 0
+SLM_SCHED_PERSISTENT = 1
+
+
+class SlmLaunch(ctypes.Structure):
+    _fields_ = [("schedule", ctypes.c_int32), ("integrator", ctypes.c_int32),
+                ("block_threads", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
+                ("chunk", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3)]
+
+
+class SlmError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__("slm_b200 error {}: {}".format(code, message))
+        self.code = code
+
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int32
+_U = ctypes.c_uint32
+
+# name -> (restype, argtypes); every symbol of include/slm_b200.h
+SIGNATURES = {
+    "slm_version": (ctypes.c_char_p, []),
+    "slm_last_error": (ctypes.c_char_p, []),
+    "slm_device_count": (ctypes.c_int, []),
+    "slm_fields_workspace_words": (ctypes.c_size_t, []),
+    "slm_integrate_fields": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "slm_integrate_trajectory": (ctypes.c_int, [_P, _I, _U, _P, _P, _P, _P, _P, _P, _P, _P]),
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+def load():
+    """Load the library and bind every entry point (raises if it is missing)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(
+                    "{} is not built; run `python -m slm_b200.build` (nvcc, sm_100a)".format(LIB_PATH))
+            L = ctypes.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(L, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = L
+        return _lib
+
+
+def check(rc):
+    if rc != SLM_OK:
+        msg = load().slm_last_error()
+        raise SlmError(rc, msg.decode() if msg else "")
+
+
+def ptr(t):
+    """Device (or host) address of a torch tensor / numpy array, or None."""
+    if t is None:
+        return None
+    if hasattr(t, "data_ptr"):
+        return ctypes.c_void_p(t.data_ptr())
+    return ctypes.c_void_p(t.ctypes.data)
+
+
+def sref(struct):
+    return ctypes.cast(ctypes.byref(struct), ctypes.c_void_p)

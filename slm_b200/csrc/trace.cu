@@ -1,0 +1,378 @@
+// trace.cu -- streamline tracing kernels and their C ABI.
+//
+//   k_fields_plain       one thread per (seed, sub-pixel) trajectory
+//   k_fields_persistent  persistent warps; a lane whose trajectory ends takes
+//                        the next one from a global work queue, so warps stay
+//                        full however uneven the trajectory lengths are
+//   k_trajectory         one thread per seed, records char2 steps
+//
+// Both field kernels produce identical slc/slt: every trajectory is computed
+// bit-exactly as the reference's jittered_trajectory
+// (opencl/jittertrajectory.cl:42-88) and the per-pixel sums are integer sums,
+// independent of order.  Each lane merges consecutive visits to the same pixel
+// (a step is at most integrator_step_factor px, so a trajectory usually visits
+// a pixel several times in a row) and adds the merged count and length sum
+// with one 64-bit atomic each when it moves to another pixel.
+#include "capi_util.cuh"
+#include "trace_common.cuh"
+
+namespace slm {
+
+// Run-length merge of pixel visits for one lane.
+struct Acc {
+    uint32_t idx, cnt;
+    u64 sum;
+};
+
+__device__ __forceinline__ void acc_flush(Acc& a, u64* __restrict__ slc, u64* __restrict__ slt) {
+    if (a.cnt) {
+        atomicAdd(slt + a.idx, a.sum);
+        atomicAdd(slc + a.idx, (u64)a.cnt);
+        a.cnt = 0;
+    }
+}
+
+// writearray.cl:31-40: slt += (uint)(l+0.5), slc += 1
+__device__ __forceinline__ void acc_visit(Acc& a, uint32_t idx, float l, u64* __restrict__ slc,
+                                          u64* __restrict__ slt) {
+    const u64 v = __float2uint_rz(l + 0.5f);
+    if (idx == a.idx && a.cnt) {
+        a.cnt += 1;
+        a.sum += v;
+    } else {
+        acc_flush(a, slc, slt);
+        a.idx = idx;
+        a.cnt = 1;
+        a.sum = v;
+    }
+}
+
+// State of one jittered field trajectory between steps.
+struct FieldLane {
+    Vec2 a;
+    float l, dt;
+    uint32_t n, rng;
+    bool alive;
+};
+
+// Start trajectory `item` = (seed - seed_begin) * d*d + j*d + i
+// (integratefields.cl:83-113; jittertrajectory.cl:56-62).
+__device__ __forceinline__ void field_start(FieldLane& s, u64 item, uint32_t seed_begin,
+                                            const float2* __restrict__ seeds,
+                                            const uint8_t* __restrict__ mask, const slm_params& p,
+                                            Acc& acc, u64* __restrict__ slc, u64* __restrict__ slt) {
+    const uint32_t d = p.subpixel_seed_point_density;
+    const uint32_t dd = d * d;
+    const uint32_t seed_idx = seed_begin + (uint32_t)(item / dd);
+    const uint32_t sub = (uint32_t)(item % dd);
+    const uint32_t j = sub / d, i = sub % d;
+    const float2 c = __ldg(seeds + seed_idx);
+    s.a.x = c.x + ((float)i * p.subpixel_seed_step - p.subpixel_seed_halfspan);
+    s.a.y = c.y + ((float)j * p.subpixel_seed_step - p.subpixel_seed_halfspan);
+    s.rng = seed_rng(seed_idx);
+    s.l = 0.0f;
+    s.dt = p.dt_max;
+    s.n = 0;
+    const uint32_t idx = pixel_of(s.a, p);
+    const bool masked = __ldg(mask + idx) != 0;
+    if (!masked) acc_visit(acc, idx, 0.0f, slc, slt);
+    s.alive = !masked && (0.0f < p.max_length) && (0u < p.max_n_steps);
+}
+
+// One pass of the while loop of jittered_trajectory with
+// runge_kutta_step_write_sl_data (rungekutta.cl:163-186).  The Euler branch
+// of that loop is unreachable (get_array_idx clamps into the grid).
+template <int ORDER>
+__device__ __forceinline__ void field_step(FieldLane& s, const uint8_t* __restrict__ mask,
+                                           const float2* __restrict__ uv, const slm_params& p,
+                                           Acc& acc, u64* __restrict__ slc, u64* __restrict__ slt) {
+    const Step st = rk_step<ORDER, true>(s.a, s.dt, s.rng, uv, p);
+    if (__ldg(mask + st.idx)) {
+        s.alive = false;
+        return;
+    }
+    const float err = vlen(__fdiv_rn(st.d2.x - st.d1.x, p.grid_scale),
+                           __fdiv_rn(st.d2.y - st.d1.y, p.grid_scale));
+    const float dl = vlen(st.d2.x, st.d2.y);
+    s.a = st.next;
+    if (dl < p.integration_halt_threshold) {
+        s.l = s.l + dl;
+        s.n += 1;
+        acc_visit(acc, st.idx, s.l, slc, slt);
+        s.alive = false;
+        return;
+    }
+    s.dt = next_dt(s.dt, err, p);
+    s.l = s.l + dl;
+    s.n += 1;
+    acc_visit(acc, st.idx, s.l, slc, slt);
+    s.alive = (s.l < p.max_length) && (s.n < p.max_n_steps);
+}
+
+__device__ __forceinline__ void warp_add_counters(u64 steps, u64 ntraj, u64* work) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        steps += __shfl_xor_sync(0xffffffffu, steps, o);
+        ntraj += __shfl_xor_sync(0xffffffffu, ntraj, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(work + 1, steps);
+        atomicAdd(work + 2, ntraj);
+    }
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(256)
+k_fields_plain(const slm_params p, const float2* __restrict__ seeds, uint32_t seed_begin,
+               u64 n_items, const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
+               u64* __restrict__ slc, u64* __restrict__ slt, u64* __restrict__ work) {
+    const u64 item = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    u64 steps = 0, ntraj = 0;
+    Acc acc{0u, 0u, 0ull};
+    if (item < n_items) {
+        FieldLane s;
+        field_start(s, item, seed_begin, seeds, mask, p, acc, slc, slt);
+        ntraj = 1;
+        while (s.alive) {
+            field_step<ORDER>(s, mask, uv, p, acc, slc, slt);
+            steps++;
+        }
+        acc_flush(acc, slc, slt);
+    }
+    warp_add_counters(steps, ntraj, work);
+}
+
+// Persistent form: the queue head work[0] must be 0 at launch.  Every loop
+// pass either hands queue items to idle lanes or advances every live
+// trajectory by one step, and each trajectory ends within max_n_steps steps,
+// so the loop ends; the exit test is warp-uniform.
+template <int ORDER>
+__global__ void __launch_bounds__(256)
+k_fields_persistent(const slm_params p, const float2* __restrict__ seeds, uint32_t seed_begin,
+                    u64 n_items, const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
+                    u64* __restrict__ slc, u64* __restrict__ slt, u64* __restrict__ work) {
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    FieldLane s;
+    s.alive = false;
+    Acc acc{0u, 0u, 0ull};
+    u64 steps = 0, ntraj = 0;
+    bool drained = false;
+    while (true) {
+        if (!drained) {
+            const unsigned idle = __ballot_sync(FULL, !s.alive);
+            if (idle) {
+                const int leader = __ffs(idle) - 1;
+                const unsigned n_idle = __popc(idle);
+                u64 base = 0;
+                if ((int)lane == leader) base = atomicAdd(work, (u64)n_idle);
+                base = __shfl_sync(FULL, base, leader);
+                if (base + n_idle >= n_items) drained = true;
+                if (!s.alive) {
+                    const u64 item = base + __popc(idle & ((1u << lane) - 1u));
+                    if (item < n_items) {
+                        field_start(s, item, seed_begin, seeds, mask, p, acc, slc, slt);
+                        ntraj++;
+                    }
+                }
+            }
+        }
+        if (!__any_sync(FULL, s.alive)) {
+            if (drained) break;
+            continue;
+        }
+        if (s.alive) {
+            field_step<ORDER>(s, mask, uv, p, acc, slc, slt);
+            steps++;
+        }
+    }
+    acc_flush(acc, slc, slt);
+    warp_add_counters(steps, ntraj, work);
+}
+
+// ------------------------------------------------------------------ trajectories
+__device__ __forceinline__ float edge_dt(float x, float u) {
+    float dt = 0.0f;
+    const float right = __fdiv_rn((float)__float2int_rz(x + 1.5f) - (x + 0.5f), u);
+    const float left = __fdiv_rn(-((x + 0.5f) - (float)__float2int_rz(x + 0.5f)), u);
+    if (u > 0.0f) dt = right;
+    if (u < 0.0f) dt = left;
+    return dt;
+}
+
+__device__ __forceinline__ float min_mag(float x, float y) {
+    if (fabsf(x) < fabsf(y)) return x;
+    if (fabsf(y) < fabsf(x)) return y;
+    return fminf(x, y);
+}
+
+__device__ __forceinline__ void put_step(int8_t* rec, uint32_t n, float dx, float dy, float res) {
+    const uint32_t lo = (uint8_t)cvt_i8(dx * res), hi = (uint8_t)cvt_i8(dy * res);
+    reinterpret_cast<uint16_t*>(rec)[n] = (uint16_t)(lo | (hi << 8));
+}
+
+// trajectory_record (trajectory.cl:41-80) with runge_kutta_step_record and
+// euler_step_record (rungekutta.cl:49-120)
+template <int ORDER>
+__global__ void __launch_bounds__(128)
+k_trajectory(const slm_params p, uint32_t n_chunk, const float2* __restrict__ seeds,
+             const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
+             int8_t* __restrict__ traj, uint16_t* __restrict__ nsteps_out,
+             float* __restrict__ length_out) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_chunk) return;
+    const uint32_t seed_idx = p.seeds_chunk_offset + g;
+    if (seed_idx >= p.n_seed_points) return;
+    int8_t* rec = traj + 2ull * g * p.max_n_steps;
+    const float res = (float)p.trajectory_resolution;
+    const float2 c = __ldg(seeds + seed_idx);
+    Vec2 a{c.x, c.y}, prev = a;
+    uint32_t n = 0, rng = 0;
+    float l = 0.0f, dt = p.dt_max;
+    uint32_t idx = pixel_of(a, p);
+    while (!__ldg(mask + idx) && (l < p.max_length && n < p.max_n_steps)) {
+        const Step st = rk_step<ORDER, false>(a, dt, rng, uv, p);
+        idx = st.idx;
+        if (!__ldg(mask + idx)) {
+            const float err = vlen(__fdiv_rn(st.d2.x - st.d1.x, p.grid_scale),
+                                   __fdiv_rn(st.d2.y - st.d1.y, p.grid_scale));
+            Vec2 next = st.next;
+            float dl = vlen(st.d2.x, st.d2.y);
+            if (dl < p.integration_halt_threshold) {
+                next.x = a.x + st.d1.x;
+                next.y = a.y + st.d1.y;
+                dl = vlen(st.d1.x, st.d1.y);
+            }
+            a = next;
+            idx = pixel_of(next, p);
+            const bool stuck = dl < p.integration_halt_threshold;
+            if (!stuck) dt = next_dt(dt, err, p);
+            l = l + dl;
+            put_step(rec, n, a.x - prev.x, a.y - prev.y, res);
+            n++;
+            if (stuck) break;
+            prev = a;
+        } else {
+            // DOWNUP_SIGN is an unsigned literal: upstream it widens to 4294967296.0f
+            const float sg = __uint2float_rn(p.downup_sign);
+            const float sx = st.u1.x * sg, sy = st.u1.y * sg;
+            const float dtx = edge_dt(a.x, sx), dty = edge_dt(a.y, sy);
+            dt = min_mag(dtx, dty);
+            a.x = a.x + sx * dt;
+            a.y = a.y + sy * dt;
+            a.x = quant(a.x, res);
+            a.y = quant(a.y, res);
+            a.x = fminf(fmaxf(a.x, -0.5f), p.nxf_mp5);
+            a.y = fminf(fmaxf(a.y, -0.5f), p.nyf_mp5);
+            const float dl = vlen(a.x - prev.x, a.y - prev.y);
+            l = l + dl;
+            put_step(rec, n, a.x - prev.x, a.y - prev.y, res);
+            n++;
+            break;
+        }
+    }
+    nsteps_out[g] = (uint16_t)n;
+    length_out[g] = l;
+}
+
+}  // namespace slm
+
+using namespace slm;
+
+static int check_grid(const slm_params* p) {
+    SLM_REQUIRE(p != nullptr, "params is NULL");
+    SLM_REQUIRE(p->nx_padded >= 2 && p->ny_padded >= 2, "grid too small: %u x %u",
+                p->nx_padded, p->ny_padded);
+    SLM_REQUIRE((u64)p->nx_padded * p->ny_padded == p->nxy_padded,
+                "nxy_padded %u != nx_padded*ny_padded", p->nxy_padded);
+    SLM_REQUIRE(p->trajectory_resolution > 0, "trajectory_resolution is 0");
+    return SLM_OK;
+}
+
+extern "C" {
+
+size_t slm_fields_workspace_words(void) { return 4; }
+
+int slm_integrate_fields(const slm_params* p, const slm_launch* launch, const float* seed_point,
+                         const uint8_t* mask, const float* uv, uint32_t* mapping, uint64_t* slc,
+                         uint64_t* slt, uint64_t* workspace, void* stream) {
+    (void)mapping;
+    clear_error();
+    int rc = check_grid(p);
+    if (rc) return rc;
+    SLM_REQUIRE(seed_point && mask && uv && slc && slt && workspace, "NULL buffer");
+    SLM_REQUIRE(aligned(uv, 8) && aligned(seed_point, 8), "uv/seed_point must be 8-byte aligned");
+    SLM_REQUIRE(aligned(slc, 8) && aligned(slt, 8) && aligned(workspace, 8),
+                "slc/slt/workspace must be 8-byte aligned");
+    SLM_REQUIRE(p->subpixel_seed_point_density >= 1, "subpixel_seed_point_density is 0");
+    slm_launch def{SLM_SCHED_PERSISTENT, SLM_RK2, 256, 0, 1, {0, 0, 0}};
+    const slm_launch& L = launch ? *launch : def;
+    SLM_REQUIRE(L.integrator == SLM_RK2 || L.integrator == SLM_RK4, "integrator must be 2 or 4");
+    const int block = L.block_threads > 0 ? L.block_threads : 256;
+    SLM_REQUIRE(block % 32 == 0 && block <= 256, "block_threads must be a multiple of 32, <= 256");
+    cudaStream_t s = (cudaStream_t)stream;
+    SLM_CUDA(cudaMemsetAsync(workspace, 0, slm_fields_workspace_words() * sizeof(uint64_t), s));
+    const uint32_t begin = p->seeds_chunk_offset;
+    if (begin >= p->n_seed_points) return SLM_OK;
+    const u64 dd = (u64)p->subpixel_seed_point_density * p->subpixel_seed_point_density;
+    const u64 n_items = (u64)(p->n_seed_points - begin) * dd;
+    const float2* sp = reinterpret_cast<const float2*>(seed_point);
+    const float2* u2 = reinterpret_cast<const float2*>(uv);
+    if (L.schedule == SLM_SCHED_PLAIN) {
+        const u64 grid = (n_items + block - 1) / block;
+        SLM_REQUIRE(grid < (1ull << 31), "too many trajectories for one launch");
+        if (L.integrator == SLM_RK4)
+            k_fields_plain<4><<<(unsigned)grid, block, 0, s>>>(*p, sp, begin, n_items, mask, u2, (u64*)slc, (u64*)slt, (u64*)workspace);
+        else
+            k_fields_plain<2><<<(unsigned)grid, block, 0, s>>>(*p, sp, begin, n_items, mask, u2, (u64*)slc, (u64*)slt, (u64*)workspace);
+        SLM_LAUNCHED("k_fields_plain");
+    } else if (L.schedule == SLM_SCHED_PERSISTENT) {
+        int per_sm = L.blocks_per_sm;
+        if (per_sm <= 0) {
+            int occ = 0;
+            if (L.integrator == SLM_RK4)
+                SLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fields_persistent<4>, block, 0));
+            else
+                SLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fields_persistent<2>, block, 0));
+            per_sm = occ > 0 ? occ : 1;
+        }
+        const unsigned grid = (unsigned)(num_sms() * per_sm);
+        if (L.integrator == SLM_RK4)
+            k_fields_persistent<4><<<grid, block, 0, s>>>(*p, sp, begin, n_items, mask, u2, (u64*)slc, (u64*)slt, (u64*)workspace);
+        else
+            k_fields_persistent<2><<<grid, block, 0, s>>>(*p, sp, begin, n_items, mask, u2, (u64*)slc, (u64*)slt, (u64*)workspace);
+        SLM_LAUNCHED("k_fields_persistent");
+    } else {
+        set_error("unknown schedule %d", L.schedule);
+        return SLM_ERR_ARGS;
+    }
+    return SLM_OK;
+}
+
+int slm_integrate_trajectory(const slm_params* p, int32_t integrator, uint32_t n_chunk,
+                             const float* seed_point, const uint8_t* mask, const float* uv,
+                             uint32_t* mapping, int8_t* trajectories, uint16_t* nsteps,
+                             float* length, void* stream) {
+    (void)mapping;
+    clear_error();
+    int rc = check_grid(p);
+    if (rc) return rc;
+    SLM_REQUIRE(integrator == SLM_RK2 || integrator == SLM_RK4, "integrator must be 2 or 4");
+    if (n_chunk == 0) return SLM_OK;
+    SLM_REQUIRE(seed_point && mask && uv && trajectories && nsteps && length, "NULL buffer");
+    SLM_REQUIRE(aligned(uv, 8) && aligned(seed_point, 8), "uv/seed_point must be 8-byte aligned");
+    SLM_REQUIRE(aligned(trajectories, 2) && aligned(nsteps, 2) && aligned(length, 4),
+                "trajectory buffers misaligned");
+    cudaStream_t s = (cudaStream_t)stream;
+    const unsigned block = 128, grid = (n_chunk + block - 1) / block;
+    const float2* sp = reinterpret_cast<const float2*>(seed_point);
+    const float2* u2 = reinterpret_cast<const float2*>(uv);
+    if (integrator == SLM_RK4)
+        k_trajectory<4><<<grid, block, 0, s>>>(*p, n_chunk, sp, mask, u2, trajectories, nsteps, length);
+    else
+        k_trajectory<2><<<grid, block, 0, s>>>(*p, n_chunk, sp, mask, u2, trajectories, nsteps, length);
+    SLM_LAUNCHED("k_trajectory");
+    return SLM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,163 @@
+// trace_common.cuh -- device arithmetic shared by every tracing kernel.
+//
+// Bit-exact restatement of the reference's per-step arithmetic on sm_100a.
+// The translation units that include this are compiled with --fmad=false and
+// IEEE division / square root (no fast-math), so each expression below is a
+// sequence of separately rounded binary32 operations in the order written,
+// the same order as the reference's OpenCL C:
+//   speed_interpolator   opencl/essentials.cl:24-45
+//   get_array_idx        opencl/essentials.cl:56-59
+//   approximate          opencl/essentials.cl:104-109
+//   lehmer_rand_*        opencl/rng.cl:37-67
+//   compute_step_vec[_jittered]  opencl/computestep.cl:42-57, 86-106
+// Conventions fixed where OpenCL leaves them open (shared with the oracle):
+//   fast_length = IEEE sqrt(x*x+y*y); fast_normalize divides by it;
+//   float->char = x86 truncation (out of range / NaN -> INT32_MIN) low byte;
+//   the two variates of lehmer_rand_vec are drawn x first, then y.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "slm_b200.h"
+
+namespace slm {
+
+typedef unsigned long long u64;
+
+struct Vec2 { float x, y; };
+
+// float -> char the way x86 converts (cvttss2si, keep the low byte)
+__device__ __forceinline__ int8_t cvt_i8(float v) {
+    const int32_t i = (v >= -2147483648.0f && v < 2147483648.0f) ? __float2int_rz(v)
+                                                                 : (int32_t)0x80000000;
+    return (int8_t)(i & 0xff);
+}
+
+// clamped axis index: min(n-1, (uint)max(0, c + pad + 0.5))
+__device__ __forceinline__ uint32_t axis_index(float c, float pp5, uint32_t n) {
+    const float v = c + pp5;
+    const float m = (0.0f < v) ? v : 0.0f;
+    const uint32_t i = __float2uint_rz(m);
+    return (i < n - 1u) ? i : n - 1u;
+}
+
+__device__ __forceinline__ uint32_t pixel_of(Vec2 a, const slm_params& p) {
+    return axis_index(a.y, p.pad_width_pp5, p.ny_padded)
+         + p.ny_padded * axis_index(a.x, p.pad_width_pp5, p.nx_padded);
+}
+
+// Bilinear, renormalised flow vector at a (essentials.cl:24-45).
+__device__ __forceinline__ Vec2 sample_uv(Vec2 a, const float2* __restrict__ uv,
+                                          const slm_params& p) {
+    const uint32_t nyp = p.ny_padded;
+    const uint32_t xl = axis_index(a.x, p.pad_width_pp5, p.nx_padded);
+    const uint32_t yd = axis_index(a.y, p.pad_width_pp5, p.ny_padded);
+    const uint32_t xr = (xl + 1u < p.nx_padded - 1u) ? xl + 1u : p.nx_padded - 1u;
+    const uint32_t yu = (yd + 1u < nyp - 1u) ? yd + 1u : nyp - 1u;
+    const float wr = a.x - (float)xl + (float)p.pad_width;
+    const float wl = 1.0f - wr;
+    const float wu = a.y - (float)yd + (float)p.pad_width;
+    const float wd = 1.0f - wu;
+    const float2 q00 = __ldg(uv + (nyp * xl + yd));
+    const float2 q10 = __ldg(uv + (nyp * xr + yd));
+    const float2 q01 = __ldg(uv + (nyp * xl + yu));
+    const float2 q11 = __ldg(uv + (nyp * xr + yu));
+    const float bx = q00.x * wl + q10.x * wr, by = q00.y * wl + q10.y * wr;
+    const float tx = q01.x * wl + q11.x * wr, ty = q01.y * wl + q11.y * wr;
+    const float vx = bx * wd + tx * wu, vy = by * wd + ty * wu;
+    const float len = __fsqrt_rn(vx * vx + vy * vy);
+    return Vec2{__fdiv_rn(vx, len), __fdiv_rn(vy, len)};
+}
+
+__device__ __forceinline__ float quant(float v, float res) {
+    return __fdiv_rn((float)cvt_i8(v * res), res);
+}
+
+// Lehmer step s <- ((u64)(s+1) * 279470273) mod (2^32 - 5) (rng.cl:37-45),
+// reduced with 2^32 == 5 (mod 2^32-5): two folds and one conditional subtract.
+__device__ __forceinline__ uint32_t lehmer_next(uint32_t s) {
+    const u64 x = (u64)(uint32_t)(s + 1u) * 279470273ull;
+    const u64 y = (x >> 32) * 5ull + (x & 0xffffffffull);
+    const u64 z = (y >> 32) * 5ull + (y & 0xffffffffull);
+    return (uint32_t)(z >= 0xfffffffbull ? z - 0xfffffffbull : z);
+}
+
+// initial_rng_state of a seed: byte-reverse, one Lehmer step, byte-reverse
+// (integratefields.cl:24-28, 96-99)
+__device__ __forceinline__ uint32_t seed_rng(uint32_t seed_idx) {
+    return __byte_perm(lehmer_next(__byte_perm(seed_idx, 0, 0x0123)), 0, 0x0123);
+}
+
+__device__ __forceinline__ Vec2 jitter(Vec2 u, uint32_t& rng, float mag) {
+    rng = lehmer_next(rng);
+    const float rx = __fdiv_rn(__uint2float_rn(rng), 4294967296.0f) - 0.5f;
+    rng = lehmer_next(rng);
+    const float ry = __fdiv_rn(__uint2float_rn(rng), 4294967296.0f) - 0.5f;
+    u.x = u.x + rx * mag;
+    u.y = u.y + ry * mag;
+    const float len = __fsqrt_rn(u.x * u.x + u.y * u.y);
+    u.x = __fdiv_rn(u.x, len);
+    u.y = __fdiv_rn(u.y, len);
+    return u;
+}
+
+struct Step {
+    Vec2 d1, d2;   // first-order and final quantised steps
+    Vec2 u1;       // flow vector at the start point
+    Vec2 next;     // start + d2
+    uint32_t idx;  // pixel of next
+};
+
+// RK2 (computestep.cl:42-57 / 86-106), or the RK4 extension (same
+// quantisation; d1 = approx(h k1) for the error estimate).
+template <int ORDER, bool JITTER>
+__device__ __forceinline__ Step rk_step(Vec2 a, float dt, uint32_t& rng,
+                                        const float2* __restrict__ uv, const slm_params& p) {
+    Step s;
+    const float cf = p.combo_factor;
+    const float res = (float)p.trajectory_resolution;
+    Vec2 k1 = sample_uv(a, uv, p);
+    if (JITTER) k1 = jitter(k1, rng, p.jitter_magnitude);
+    s.u1 = k1;
+    if (ORDER == 2) {
+        s.d1.x = quant(k1.x * cf * dt, res);
+        s.d1.y = quant(k1.y * cf * dt, res);
+        const Vec2 b{a.x + s.d1.x, a.y + s.d1.y};
+        Vec2 k2 = sample_uv(b, uv, p);
+        if (JITTER) k2 = jitter(k2, rng, p.jitter_magnitude);
+        s.d2.x = quant(0.5f * (s.d1.x + k2.x * cf * dt), res);
+        s.d2.y = quant(0.5f * (s.d1.y + k2.y * cf * dt), res);
+    } else {
+        const float h1x = k1.x * cf * dt, h1y = k1.y * cf * dt;
+        s.d1.x = quant(h1x, res);
+        s.d1.y = quant(h1y, res);
+        const Vec2 b{a.x + 0.5f * h1x, a.y + 0.5f * h1y};
+        Vec2 k2 = sample_uv(b, uv, p);
+        if (JITTER) k2 = jitter(k2, rng, p.jitter_magnitude);
+        const float h2x = k2.x * cf * dt, h2y = k2.y * cf * dt;
+        const Vec2 c{a.x + 0.5f * h2x, a.y + 0.5f * h2y};
+        Vec2 k3 = sample_uv(c, uv, p);
+        if (JITTER) k3 = jitter(k3, rng, p.jitter_magnitude);
+        const float h3x = k3.x * cf * dt, h3y = k3.y * cf * dt;
+        const Vec2 d{a.x + h3x, a.y + h3y};
+        Vec2 k4 = sample_uv(d, uv, p);
+        if (JITTER) k4 = jitter(k4, rng, p.jitter_magnitude);
+        const float h4x = k4.x * cf * dt, h4y = k4.y * cf * dt;
+        s.d2.x = quant(__fdiv_rn(h1x + 2.0f * h2x + 2.0f * h3x + h4x, 6.0f), res);
+        s.d2.y = quant(__fdiv_rn(h1y + 2.0f * h2y + 2.0f * h3y + h4y, 6.0f), res);
+    }
+    s.next.x = a.x + s.d2.x;
+    s.next.y = a.y + s.d2.y;
+    s.idx = pixel_of(s.next, p);
+    return s;
+}
+
+__device__ __forceinline__ float vlen(float x, float y) { return __fsqrt_rn(x * x + y * y); }
+
+// adaptive dt (rungekutta.cl:70-71): DT_MAX when the error is 0, else
+// fmin(DT_MAX, ADJUSTED_MAX_ERROR*dt/err)
+__device__ __forceinline__ float next_dt(float dt, float err, const slm_params& p) {
+    const float cand = fminf(p.dt_max, __fdiv_rn(p.adjusted_max_error * dt, err));
+    return (err == 0.0f) ? p.dt_max : cand;
+}
+
+}  // namespace slm

@@ -1,0 +1,46 @@
+"""Device selection and host<->device staging for the stage wrappers."""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+
+
+def cuda_device(cl_platform=0, cl_device=0):
+    """CUDA device standing in for the reference's (cl_platform, cl_device) pair.
+
+    The reference picks an OpenCL device by index (pocl.py:76-93); here the
+    index selects a CUDA device modulo the number present.  Raises if none is.
+    """
+    _lib.load()
+    n = torch.cuda.device_count()
+    if n == 0 or not torch.cuda.is_available():
+        raise RuntimeError("slm_b200 needs a CUDA device (B200, sm_100a); none is visible")
+    idx = int(cl_device or 0) % n
+    return torch.device("cuda", idx)
+
+
+def to_device(array, device, dtype=None):
+    """Copy a NumPy array to the device; pinned-memory arrays go by async DMA."""
+    a = np.ascontiguousarray(array)
+    if a.dtype == np.bool_:
+        a = a.view(np.uint8)
+    t = torch.from_numpy(a)
+    if dtype is not None and t.dtype != dtype:
+        t = t.to(dtype)
+    return t.to(device, non_blocking=t.is_pinned())
+
+
+def pinned_empty(shape, dtype):
+    """A NumPy array backed by page-locked host memory (fast DMA both ways)."""
+    tdt = {np.dtype(np.float32): torch.float32, np.dtype(np.uint8): torch.uint8,
+           np.dtype(np.uint32): torch.uint32, np.dtype(np.uint16): torch.uint16,
+           np.dtype(np.int8): torch.int8, np.dtype(np.uint64): torch.uint64,
+           np.dtype(np.bool_): torch.bool}[np.dtype(dtype)]
+    return torch.empty(shape, dtype=tdt, pin_memory=True).numpy()
+
+
+def low32(t_u64):
+    """Low 32 bits of a uint64 device tensor, as uint32 (the reference's wrap-around)."""
+    return t_u64.view(torch.int32).view(-1, 2)[:, 0].contiguous().view(torch.uint32)

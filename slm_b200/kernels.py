@@ -1,0 +1,78 @@
+"""Tensor-level calls into the C ABI (device tensors in, device tensors out).
+
+Each function checks dtypes, devices, contiguity and sizes on the host, then
+calls the ``extern "C"`` entry point on the current CUDA stream (or the one
+given).  Nothing here falls back to the CPU.
+"""
+from __future__ import annotations
+
+import torch
+
+from . import _lib
+from ._lib import SlmLaunch, check, ptr, sref
+
+SCHEDULES = {"plain": _lib.SLM_SCHED_PLAIN, "persistent": _lib.SLM_SCHED_PERSISTENT}
+
+
+def _need(t, dtype, numel, name):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise ValueError("{} must be a CUDA tensor".format(name))
+    if t.dtype != dtype:
+        raise ValueError("{} must be {}, got {}".format(name, dtype, t.dtype))
+    if not t.is_contiguous():
+        raise ValueError("{} must be contiguous".format(name))
+    if numel is not None and t.numel() < numel:
+        raise ValueError("{} has {} elements, needs {}".format(name, t.numel(), numel))
+
+
+def _stream(stream):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return __import__("ctypes").c_void_p(s.cuda_stream)
+
+
+def workspace(device=None):
+    """Scratch words the field tracer needs (queue head, step/trajectory counters)."""
+    n = _lib.load().slm_fields_workspace_words()
+    return torch.zeros(n, dtype=torch.uint64, device=device or "cuda")
+
+
+def launch_config(schedule="persistent", integrator=2, block_threads=0, blocks_per_sm=0, chunk=1):
+    L = SlmLaunch()
+    L.schedule = SCHEDULES[schedule] if isinstance(schedule, str) else int(schedule)
+    L.integrator = int(integrator)
+    L.block_threads = int(block_threads)
+    L.blocks_per_sm = int(blocks_per_sm)
+    L.chunk = int(chunk)
+    return L
+
+
+def integrate_fields(params, seeds, mask, uv, slc, slt, work, schedule="persistent",
+                     integrator=2, block_threads=0, blocks_per_sm=0, stream=None):
+    """Trace every seed's d*d jittered trajectories, adding into slc/slt (uint64)."""
+    lib = _lib.load()
+    nxy = params.nxy_padded
+    _need(seeds, torch.float32, 2 * params.n_seed_points, "seeds")
+    _need(mask, torch.uint8, nxy, "mask")
+    _need(uv, torch.float32, 2 * nxy, "uv")
+    _need(slc, torch.uint64, nxy, "slc")
+    _need(slt, torch.uint64, nxy, "slt")
+    _need(work, torch.uint64, lib.slm_fields_workspace_words(), "workspace")
+    L = launch_config(schedule, integrator, block_threads, blocks_per_sm)
+    check(lib.slm_integrate_fields(sref(params), sref(L), ptr(seeds), ptr(mask), ptr(uv), None,
+                                   ptr(slc), ptr(slt), ptr(work), _stream(stream)))
+
+
+def integrate_trajectory(params, n_chunk, seeds, mask, uv, traj, nsteps, length,
+                         integrator=2, stream=None):
+    """Record one trajectory per seed of the chunk starting at params.seeds_chunk_offset."""
+    lib = _lib.load()
+    nxy = params.nxy_padded
+    _need(seeds, torch.float32, 2 * params.n_seed_points, "seeds")
+    _need(mask, torch.uint8, nxy, "mask")
+    _need(uv, torch.float32, 2 * nxy, "uv")
+    _need(traj, torch.int8, 2 * n_chunk * params.max_n_steps, "trajectories")
+    _need(nsteps, torch.uint16, n_chunk, "nsteps")
+    _need(length, torch.float32, n_chunk, "length")
+    check(lib.slm_integrate_trajectory(sref(params), int(integrator), int(n_chunk), ptr(seeds),
+                                       ptr(mask), ptr(uv), None, ptr(traj), ptr(nsteps),
+                                       ptr(length), _stream(stream)))

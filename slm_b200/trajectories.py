@@ -1,0 +1,114 @@
+"""Recorded streamline trajectories: drop-in for the reference's ``Trajectories``.
+
+Mirrors ``python/streamlines/trajectories.py`` (class ``Trajectories``,
+:40-346): same constructor and ``integrate()`` contract -- fills
+``data.seed_point_array``, ``data.streamline_arrays_list`` (per direction, one
+int8 ``(n_steps, 2)`` array of steps in 1/trajectory_resolution px per seed),
+``data.traj_nsteps_array`` uint16 ``[N, 2]``, ``data.traj_length_array``
+float32 ``[N, 2]`` and ``data.traj_stats_df`` -- with the tracing done by the
+CUDA kernel ``k_trajectory``.  Chunking by device memory follows
+``Trajectories.choose_chunks`` (:166-194) with the device's total memory.
+The per-direction lists are NumPy object arrays of the per-seed step arrays.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import kernels
+from .device import cuda_device, to_device
+from .params import kernel_params
+from .useful import compute_stats, create_seeds, vprint
+
+
+class Trajectories:
+    def __init__(self, cl_platform, cl_device, cl_src_path=None, info=None, data=None,
+                 do_trace_downstream=True, do_trace_upstream=True, verbose=False,
+                 gpu_verbose=False, integrator=2):
+        self.device = cuda_device(cl_platform, cl_device)
+        self.cl_src_path = cl_src_path
+        self.info = info
+        self.data = data
+        self.do_trace_downstream = do_trace_downstream
+        self.do_trace_upstream = do_trace_upstream
+        self.verbose = verbose
+        self.gpu_verbose = gpu_verbose
+        self.integrator = integrator
+        self.n_steps = 0
+
+    def integrate(self):
+        vprint(self.verbose, "Integrating trajectories...")
+        info = self.info
+        mask_array = self.data.mask_array
+        self.data.seed_point_array, n_seed_points, n_padded_seed_points = create_seeds(
+            mask_array, info.pad_width, info.n_work_items,
+            n_seed_points=info.n_trajectory_seed_points, do_shuffle=info.do_shuffle,
+            rng_seed=info.shuffle_rng_seed, verbose=self.verbose)
+        info.n_seed_points = n_seed_points
+        info.n_padded_seed_points = n_padded_seed_points
+        if self.data.mapping_array is None:
+            self.data.mapping_array = np.zeros_like(mask_array, dtype=np.uint32)
+        total = torch.cuda.get_device_properties(self.device).total_memory
+        limit = (total * int(info.gpu_memory_limit_pc)) // 100
+        request = n_seed_points * np.dtype(np.uint8).itemsize * int(info.max_n_steps) * 2
+        n_chunks = max(1, int(np.ceil(request / limit)))
+        self.choose_chunks(n_chunks)
+        self.gpu_compute_trajectories()
+        self.data.traj_stats_df = compute_stats(self.data.traj_length_array,
+                                                self.data.traj_nsteps_array,
+                                                info.pixel_size, self.verbose)
+        vprint(self.verbose, "...done")
+
+    def choose_chunks(self, n_chunks):
+        ns = int(self.info.n_seed_points)
+        npad = int(self.info.n_padded_seed_points)
+        self.chunk_size = int(np.round(npad / n_chunks))
+        chunk_list = [[i, c, min(ns, c + self.chunk_size) - c, self.chunk_size]
+                      for i, c in enumerate(range(0, npad, self.chunk_size))]
+        trace_do_list = [[self.do_trace_downstream, "Downstream:", 0, np.float32(+1.0)],
+                         [self.do_trace_upstream, "Upstream:  ", 1, np.float32(-1.0)]]
+        self.trace_do_chunks = [td + chunk for td in trace_do_list for chunk in chunk_list]
+
+    def gpu_compute_trajectories(self):
+        info = self.info
+        dev = self.device
+        ns = int(info.n_seed_points)
+        nl = int(info.max_n_steps)
+        streamline_arrays_list = [[], []]
+        traj_nsteps_array = np.zeros([ns, 2], dtype=np.uint16)
+        traj_length_array = np.zeros([ns, 2], dtype=np.float32)
+        with torch.cuda.device(dev):
+            seeds_d = to_device(self.data.seed_point_array, dev, torch.float32)
+            mask_d = to_device(self.data.mask_array, dev)
+            uv_d = to_device(self.data.uv_array, dev, torch.float32)
+            traj_d = torch.zeros(self.chunk_size * nl * 2, dtype=torch.int8, device=dev)
+            nsteps_d = torch.zeros(self.chunk_size, dtype=torch.uint16, device=dev)
+            length_d = torch.zeros(self.chunk_size, dtype=torch.float32, device=dev)
+            for (_, downup_idx, downup_sign, _chunk_idx, seeds_chunk_offset, n_chunk_seeds,
+                 n_chunk_ki) in [td[1:] for td in self.trace_do_chunks if td[0]]:
+                info.downup_sign = downup_sign
+                info.seeds_chunk_offset = seeds_chunk_offset
+                prm = kernel_params(info, "INTEGRATE_TRAJECTORY", downup_sign)
+                kernels.integrate_trajectory(prm, n_chunk_ki, seeds_d, mask_d, uv_d, traj_d,
+                                             nsteps_d, length_d, integrator=self.integrator)
+                n = max(n_chunk_seeds, 0)
+                chunk_nsteps = nsteps_d[:n].cpu().numpy()
+                chunk_length = length_d[:n].cpu().numpy()
+                # copy back only the recorded prefix of each seed's row
+                rows = traj_d.view(self.chunk_size, nl, 2)[:n]
+                maxn = int(chunk_nsteps.max()) if n else 0
+                chunk_traj = rows[:, :maxn].cpu().numpy()
+                for k in range(n):
+                    streamline_arrays_list[downup_idx].append(chunk_traj[k, :chunk_nsteps[k]].copy())
+                traj_nsteps_array[seeds_chunk_offset:seeds_chunk_offset + n, downup_idx] = chunk_nsteps
+                traj_length_array[seeds_chunk_offset:seeds_chunk_offset + n, downup_idx] = chunk_length
+                self.n_steps += int(chunk_nsteps.astype(np.int64).sum())
+            info.seeds_chunk_offset = np.uint32(0)
+        for downup_idx in (0, 1):
+            arr = np.empty(len(streamline_arrays_list[downup_idx]), dtype=object)
+            for k, a in enumerate(streamline_arrays_list[downup_idx]):
+                arr[k] = a
+            streamline_arrays_list[downup_idx] = arr
+        self.data.streamline_arrays_list = streamline_arrays_list
+        self.data.traj_nsteps_array = traj_nsteps_array[0:ns].copy()
+        self.data.traj_length_array = traj_length_array[0:ns].copy()

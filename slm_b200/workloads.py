@@ -1,0 +1,89 @@
+"""Named synthetic workloads (DTM recipe + trace parameters) for the bench and tests.
+
+Each workload is one of the configurations the tracer is measured on; the
+DTMs are seeded synthetic stand-ins (slm_b200.synth) for lidar DTMs.
+"step" is ``integrator_step_factor`` (the maximum step in px) and the step cap
+is set the way the reference derives it, ``max_n_steps = max_length / step``
+(useful.py:159), with ``max_length = cap * step`` in metres.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import synth
+from .useful import Info, create_seeds, default_parameters
+
+
+@dataclass
+class WorkloadSpec:
+    name: str
+    n: int
+    pixel_size: float
+    density: int
+    jitter: float
+    integrator: int
+    step: float
+    max_steps: int
+    dtm: str
+    n_traj_seeds: int = 1000
+
+
+SPECS = {
+    "config1": WorkloadSpec("512x512 @1m, d=1, no jitter, RK2, step 0.1 px, max 2000 steps",
+                            512, 1.0, 1, 0.0, 2, 0.1, 2000, "config1"),
+    "config2": WorkloadSpec("2048x2048 @2m, d=2, jitter +-0.5, RK4, step 0.1 px, max 10000 steps",
+                            2048, 2.0, 2, 1.0, 4, 0.1, 10000, "config2"),
+    "config2_rk2": WorkloadSpec("2048x2048 @2m, d=2, jitter +-0.5, RK2, step 0.1 px, max 10000 steps",
+                                2048, 2.0, 2, 1.0, 2, 0.1, 10000, "config2"),
+    "config5": WorkloadSpec("8192x8192 @1m, d=2, jitter +-0.5, RK4, step 0.1 px, max 20000 steps",
+                            8192, 1.0, 2, 1.0, 4, 0.1, 20000, "config5"),
+    "small": WorkloadSpec("256x256 @1m, d=2, jitter +-0.5, RK2, step 0.1 px, max 2000 steps",
+                          256, 1.0, 2, 1.0, 2, 0.1, 2000, "tile"),
+}
+
+
+def make_dtm(spec, seed=None):
+    if spec.dtm == "config1":
+        return synth.config1_dtm(spec.n, seed or 1)
+    if spec.dtm == "config2":
+        return synth.config2_dtm(spec.n, seed or 2)
+    if spec.dtm == "config5":
+        return synth.config5_dtm(spec.n, seed or 5)
+    return synth.tile_dtm(spec.n, spec.n, seed or 9)
+
+
+class Workload:
+    """DTM, uv, mask, Info and the shuffled seed lists of one configuration."""
+
+    def __init__(self, key, seed=None):
+        spec = SPECS[key]
+        self.key = key
+        self.spec = spec
+        self.dtm = make_dtm(spec, seed)
+        self.uv, self.mask = synth.uv_from_dtm(self.dtm, spec.pixel_size, 2)
+        d = default_parameters()
+        d.trace.subpixel_seed_point_density = spec.density
+        d.trace.jitter_magnitude = spec.jitter
+        d.trace.integrator_step_factor = spec.step
+        d.trace.max_length = spec.max_steps * spec.step
+        d.trace.n_trajectory_seed_points = spec.n_traj_seeds
+        self.defaults = d
+        self.info = Info(d.state, d.trace, spec.pixel_size)
+        self.info.set_xy(spec.n, spec.n, 2)
+        self.seeds, ns, npad = create_seeds(self.mask, 2, self.info.n_work_items,
+                                            do_shuffle=True, rng_seed=1)
+        self.info.n_seed_points = ns
+        self.info.n_padded_seed_points = npad
+        self.traj_seeds = np.ascontiguousarray(self.seeds[:spec.n_traj_seeds])
+        self.n_traj = min(spec.n_traj_seeds, ns)
+
+    @property
+    def n_pixels(self):
+        return self.spec.n * self.spec.n
+
+    def fresh_info(self):
+        i = Info(self.defaults.state, self.defaults.trace, self.spec.pixel_size)
+        i.set_xy(self.spec.n, self.spec.n, 2)
+        return i
