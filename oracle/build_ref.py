@@ -186,6 +186,7 @@ def build_one(kernel, reference, force=False):
         raise RuntimeError("g++ failed for {}:\n{}".format(kernel, r.stderr[-4000:]))
     with open(stamp, "w") as fp:
         fp.write(digest)
+    os.remove(cpp)  # the generated source embeds the reference's; keep only the library
     return kernel, "built"
 
 
