@@ -196,6 +196,44 @@ def vprint(verbose, *args, **kwargs):
         sys.stdout.flush()
 
 
+_SEED_CACHE = {}
+_SEED_CACHE_MAX = 4
+
+
+def _shuffled_seeds(mask, pad, do_shuffle, rng_seed):
+    """argwhere(~mask) - pad, shuffled as the reference shuffles it.
+
+    The reference seeds NumPy's global legacy generator and shuffles the
+    (N, 2) array in place (useful.py:496-501).  Shuffling the rows of an
+    array and ``permutation(N)`` draw the same Fisher-Yates indices from the
+    same stream, so ``rows[permutation(N)]`` is the same array and leaves the
+    global generator in the same state -- ten times faster.  Results are
+    cached by mask content; a cache hit restores the global generator to the
+    state the shuffle leaves, so the side effect is the reference's too.
+    """
+    import hashlib
+    m = np.ascontiguousarray(mask)
+    if m.dtype != np.bool_:
+        m = m.astype(np.bool_)
+    key = None
+    if do_shuffle:
+        key = (m.shape, int(pad), int(rng_seed),
+               hashlib.blake2b(m.view(np.uint8).data, digest_size=16).hexdigest())
+        hit = _SEED_CACHE.get(key)
+        if hit is not None:
+            np.random.set_state(hit[1])
+            return hit[0].copy()
+    seed_point_array = (np.argwhere(~m).astype(np.float32) - pad)
+    if do_shuffle:
+        np.random.seed(rng_seed)
+        perm = np.random.permutation(seed_point_array.shape[0])
+        seed_point_array = seed_point_array[perm]
+        if len(_SEED_CACHE) >= _SEED_CACHE_MAX:
+            _SEED_CACHE.pop(next(iter(_SEED_CACHE)))
+        _SEED_CACHE[key] = (seed_point_array.copy(), np.random.get_state())
+    return seed_point_array
+
+
 def create_seeds(mask, pad, n_work_items, n_seed_points=None, do_shuffle=True,
                  rng_seed=1, verbose=False):
     """Seed coordinates of the unmasked pixels (unpadded frame), optionally shuffled.
@@ -206,10 +244,7 @@ def create_seeds(mask, pad, n_work_items, n_seed_points=None, do_shuffle=True,
     Returns ``(seed_point_array, n_seed_points, n_padded_seed_points)``.
     """
     vprint(verbose, "Generating seed points...", end="")
-    seed_point_array = (np.argwhere(~mask).astype(np.float32) - pad)
-    if do_shuffle:
-        np.random.seed(rng_seed)
-        np.random.shuffle(seed_point_array)
+    seed_point_array = _shuffled_seeds(mask, pad, do_shuffle, rng_seed)
     if n_seed_points is not None and n_seed_points > 0:
         seed_point_array = seed_point_array[:n_seed_points].astype(np.float32)
     else:

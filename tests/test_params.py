@@ -149,3 +149,23 @@ def _header_struct_fields():
 def test_struct_layout_matches_header():
     assert _header_struct_fields() == P.FIELDS
     assert len(P.FIELDS) == len(set(P.FIELD_NAMES))
+
+
+@pytest.mark.parametrize("shape,holes", [((30, 40), 0), ((257, 129), 40), ((64, 64), 4000)])
+def test_create_seeds_matches_reference(ref_modules, shape, holes):
+    from slm_b200.useful import create_seeds
+    rng = np.random.default_rng(holes)
+    mask = np.zeros(shape, dtype=bool)
+    mask[:2, :] = mask[-2:, :] = mask[:, :2] = mask[:, -2:] = True
+    if holes:
+        mask[rng.integers(0, shape[0], holes), rng.integers(0, shape[1], holes)] = True
+    for n_seed_points in (None, 17):
+        for rng_seed in (1, 7):
+            ref = ref_modules["useful"].create_seeds(mask, 2, 32, n_seed_points=n_seed_points,
+                                                     do_shuffle=True, rng_seed=rng_seed)
+            st_ref = np.random.get_state()[1].copy()
+            for _ in range(2):  # second call is served from the cache
+                mine = create_seeds(mask, 2, 32, n_seed_points=n_seed_points,
+                                    do_shuffle=True, rng_seed=rng_seed)
+                assert np.array_equal(ref[0], mine[0]) and ref[1:] == mine[1:]
+                assert np.array_equal(np.random.get_state()[1], st_ref)
