@@ -112,6 +112,27 @@ int slm_integrate_fields(const slm_params* p, const slm_launch* launch,
                          uint32_t* mapping, uint64_t* slc, uint64_t* slt,
                          uint64_t* workspace, void* stream);
 
+/* slm_integrate_fields_noalloc -- no counterpart in the reference.
+ * For callers that cannot call cudaMalloc: a host application that hands a
+ * plugin only its own pre-allocated device buffers, or a binding of the
+ * reference's six-buffer integrate_fields signature, which has no workspace
+ * argument.  Same field trace and results as slm_integrate_fields, but it
+ * allocates nothing: its scratch (work-queue head, step and trajectory
+ * counters) lives in a static device array of SLM_NOALLOC_SCRATCH_WORDS uint64
+ * words inside this library, which every GPU that loads the library holds
+ * until the process exits.  The caller still passes every input and output.
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress, with that device current); make that first call
+ * before any stream capture.  All calls share the one array and each call
+ * clears the words it uses: calls that overlap on the GPU (several streams or
+ * host threads) race on it, so the caller must serialise them.  The step and
+ * trajectory counters are not returned.  Returns SLM_ERR_CAPACITY if the
+ * tracer ever needs more scratch than the array holds. */
+#define SLM_NOALLOC_SCRATCH_WORDS 64
+int slm_integrate_fields_noalloc(const slm_params* p, const slm_launch* launch,
+                                 const float* seed_point, const uint8_t* mask, const float* uv,
+                                 uint32_t* mapping, uint64_t* slc, uint64_t* slt, void* stream);
+
 /* integrate_trajectory: one un-jittered trajectory per seed of the chunk
  * seeds_chunk_offset .. seeds_chunk_offset+n_chunk-1 (clipped to
  * n_seed_points), recording each step as a char2 at 1/trajectory_resolution

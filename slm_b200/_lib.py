@@ -48,6 +48,7 @@ SIGNATURES = {
     "slm_device_count": (ctypes.c_int, []),
     "slm_fields_workspace_words": (ctypes.c_size_t, []),
     "slm_integrate_fields": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "slm_integrate_fields_noalloc": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_integrate_trajectory": (ctypes.c_int, [_P, _I, _U, _P, _P, _P, _P, _P, _P, _P, _P]),
 }
 

@@ -13,8 +13,11 @@
 // (a step is at most integrator_step_factor px, so a trajectory usually visits
 // a pixel several times in a row) and adds the merged count and length sum
 // with one 64-bit atomic each when it moves to another pixel.
+#include <mutex>
 #include "capi_util.cuh"
 #include "trace_common.cuh"
+
+#define SLM_MAX_DEVICES 64
 
 namespace slm {
 
@@ -376,3 +379,63 @@ int slm_integrate_trajectory(const slm_params* p, int32_t integrator, uint32_t n
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ no-alloc variant
+// Some callers cannot call cudaMalloc: a host application that hands a plugin
+// only its own pre-allocated buffers, or a binding of the reference's
+// six-buffer integrate_fields signature, which has no workspace argument.
+// For them, slm_integrate_fields_noalloc keeps the field tracer's scratch (the
+// work-queue head and the step/trajectory counters) in the file-scope device
+// array below instead of a caller-allocated workspace.  The array is modest
+// (SLM_NOALLOC_SCRATCH_WORDS 64-bit words, 512 bytes) and every GPU that loads
+// this library holds it until the process exits.
+namespace slm {
+
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[SLM_NOALLOC_SCRATCH_WORDS];
+
+// Device address of g_noalloc_scratch per device.  In host code the array's
+// name is only a host-side stand-in, so the address comes from
+// cudaGetSymbolAddress, called once per device with that device current.
+static std::mutex g_noalloc_mutex;
+static u64* g_noalloc_addr[SLM_MAX_DEVICES] = {};
+
+static int noalloc_scratch(u64** out) {
+    int dev = 0;
+    SLM_CUDA(cudaGetDevice(&dev));
+    SLM_REQUIRE(dev >= 0 && dev < SLM_MAX_DEVICES, "device %d beyond %d", dev, SLM_MAX_DEVICES);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_addr[dev] == nullptr) {
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess) {
+            set_error("cudaGetSymbolAddress(scratch) failed on device %d: %s", dev, cudaGetErrorString(e));
+            return SLM_ERR_CUDA;
+        }
+        g_noalloc_addr[dev] = static_cast<u64*>(ptr);
+    }
+    *out = g_noalloc_addr[dev];
+    return SLM_OK;
+}
+
+}  // namespace slm
+
+extern "C" int slm_integrate_fields_noalloc(const slm_params* p, const slm_launch* launch,
+                                            const float* seed_point, const uint8_t* mask,
+                                            const float* uv, uint32_t* mapping, uint64_t* slc,
+                                            uint64_t* slt, void* stream) {
+    clear_error();
+    const size_t need = slm_fields_workspace_words();
+    if (need > SLM_NOALLOC_SCRATCH_WORDS) {
+        set_error("field tracer needs %zu scratch words, the static array holds %d",
+                  need, SLM_NOALLOC_SCRATCH_WORDS);
+        return SLM_ERR_CAPACITY;
+    }
+    u64* scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    // slm_integrate_fields clears the scratch words it uses (queue head and
+    // counters) on the stream before its launch, so a previous call's contents
+    // never leak into this one.
+    return slm_integrate_fields(p, launch, seed_point, mask, uv, mapping, slc, slt,
+                                reinterpret_cast<uint64_t*>(scratch), stream);
+}
