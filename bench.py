@@ -228,12 +228,22 @@ def run_b200(args):
     tinfo.n_seed_points = n_traj
     traj_prm = [kernel_params(tinfo, "INTEGRATE_TRAJECTORY", np.float32(s)) for s in (1.0, -1.0)]
     stream = torch.cuda.current_stream()
+    side = torch.cuda.Stream()
+    traj_d2 = torch.zeros_like(traj_d)
 
     def device_step(ev=None):
+        # the trajectory recorder (1000 seeds, latency-bound) runs on a side
+        # stream concurrently with the field passes
         acc.zero_()
+        fork = torch.cuda.Event()
+        fork.record(stream)
+        side.wait_event(fork)
         for d in range(2):
-            kernels.integrate_trajectory(traj_prm[d], n_traj, seeds_d, mask_d, uv_d, traj_d,
-                                         nsteps_d[d], length_d[d], integrator)
+            kernels.integrate_trajectory(traj_prm[d], n_traj, seeds_d, mask_d, uv_d,
+                                         traj_d if d == 0 else traj_d2, nsteps_d[d],
+                                         length_d[d], integrator, stream=side)
+        join = torch.cuda.Event()
+        join.record(side)
         if ev is not None:
             ev[0].record(stream)
         for d in range(2):
@@ -241,6 +251,7 @@ def run_b200(args):
                                      work[d], schedule=args.schedule, integrator=integrator)
         if ev is not None:
             ev[1].record(stream)
+        stream.wait_event(join)
         if ws > 1:
             dist.all_reduce(acc.view(torch.int64), op=dist.ReduceOp.SUM)
 

@@ -66,8 +66,16 @@ __device__ __forceinline__ void field_start(FieldLane& s, u64 item, uint32_t see
                                             Acc& acc, u64* __restrict__ slc, u64* __restrict__ slt) {
     const uint32_t d = p.subpixel_seed_point_density;
     const uint32_t dd = d * d;
-    const uint32_t seed_idx = seed_begin + (uint32_t)(item / dd);
-    const uint32_t sub = (uint32_t)(item % dd);
+    uint32_t seed_off, sub;
+    if (item < 0x100000000ull) {  // 32-bit division unless the queue is huge
+        const uint32_t it = (uint32_t)item;
+        seed_off = it / dd;
+        sub = it - seed_off * dd;
+    } else {
+        seed_off = (uint32_t)(item / dd);
+        sub = (uint32_t)(item - (u64)seed_off * dd);
+    }
+    const uint32_t seed_idx = seed_begin + seed_off;
     const uint32_t j = sub / d, i = sub % d;
     const float2 c = __ldg(seeds + seed_idx);
     s.a.x = c.x + ((float)i * p.subpixel_seed_step - p.subpixel_seed_halfspan);

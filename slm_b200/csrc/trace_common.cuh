@@ -68,17 +68,35 @@ __device__ __forceinline__ Vec2 sample_uv(Vec2 a, const float2* __restrict__ uv,
     return Vec2{__fdiv_rn(vx, len), __fdiv_rn(vy, len)};
 }
 
+// Quantisation scale.  When trajectory_resolution is a power of two (128 by
+// default) dividing by it is exactly a multiplication by its reciprocal.
+struct Quant {
+    float res, inv;
+    bool pow2;
+    __device__ __forceinline__ explicit Quant(uint32_t r)
+        : res((float)r), inv(__fdiv_rn(1.0f, (float)r)), pow2(r != 0u && (r & (r - 1u)) == 0u) {}
+    __device__ __forceinline__ float operator()(float v) const {
+        const float c = (float)cvt_i8(v * res);
+        return pow2 ? c * inv : __fdiv_rn(c, res);
+    }
+};
+
 __device__ __forceinline__ float quant(float v, float res) {
     return __fdiv_rn((float)cvt_i8(v * res), res);
 }
 
 // Lehmer step s <- ((u64)(s+1) * 279470273) mod (2^32 - 5) (rng.cl:37-45),
 // reduced with 2^32 == 5 (mod 2^32-5): two folds and one conditional subtract.
+// With x = hi*2^32 + lo (hi < 2^28.1): lo + 5*hi < 2^32 + 2^31, so one carry
+// c folds it to (lo + 5*hi mod 2^32) + 5c < 2^32, then one conditional subtract.
 __device__ __forceinline__ uint32_t lehmer_next(uint32_t s) {
-    const u64 x = (u64)(uint32_t)(s + 1u) * 279470273ull;
-    const u64 y = (x >> 32) * 5ull + (x & 0xffffffffull);
-    const u64 z = (y >> 32) * 5ull + (y & 0xffffffffull);
-    return (uint32_t)(z >= 0xfffffffbull ? z - 0xfffffffbull : z);
+    const uint32_t t = s + 1u;
+    const uint32_t lo = t * 279470273u;
+    const uint32_t hi = __umulhi(t, 279470273u);
+    const uint32_t h5 = hi * 5u;
+    const uint32_t y = lo + h5;
+    const uint32_t z = y + ((y < lo) ? 5u : 0u);
+    return z >= 0xfffffffbu ? z - 0xfffffffbu : z;
 }
 
 // initial_rng_state of a seed: byte-reverse, one Lehmer step, byte-reverse
@@ -88,10 +106,12 @@ __device__ __forceinline__ uint32_t seed_rng(uint32_t seed_idx) {
 }
 
 __device__ __forceinline__ Vec2 jitter(Vec2 u, uint32_t& rng, float mag) {
+    // (float)r / (float)0xfffffffb: the divisor rounds to 2^32, and dividing
+    // by a power of two is exactly a multiplication by 2^-32.
     rng = lehmer_next(rng);
-    const float rx = __fdiv_rn(__uint2float_rn(rng), 4294967296.0f) - 0.5f;
+    const float rx = __uint2float_rn(rng) * 2.3283064365386963e-10f - 0.5f;
     rng = lehmer_next(rng);
-    const float ry = __fdiv_rn(__uint2float_rn(rng), 4294967296.0f) - 0.5f;
+    const float ry = __uint2float_rn(rng) * 2.3283064365386963e-10f - 0.5f;
     u.x = u.x + rx * mag;
     u.y = u.y + ry * mag;
     const float len = __fsqrt_rn(u.x * u.x + u.y * u.y);
@@ -114,22 +134,22 @@ __device__ __forceinline__ Step rk_step(Vec2 a, float dt, uint32_t& rng,
                                         const float2* __restrict__ uv, const slm_params& p) {
     Step s;
     const float cf = p.combo_factor;
-    const float res = (float)p.trajectory_resolution;
+    const Quant quant(p.trajectory_resolution);
     Vec2 k1 = sample_uv(a, uv, p);
     if (JITTER) k1 = jitter(k1, rng, p.jitter_magnitude);
     s.u1 = k1;
     if (ORDER == 2) {
-        s.d1.x = quant(k1.x * cf * dt, res);
-        s.d1.y = quant(k1.y * cf * dt, res);
+        s.d1.x = quant(k1.x * cf * dt);
+        s.d1.y = quant(k1.y * cf * dt);
         const Vec2 b{a.x + s.d1.x, a.y + s.d1.y};
         Vec2 k2 = sample_uv(b, uv, p);
         if (JITTER) k2 = jitter(k2, rng, p.jitter_magnitude);
-        s.d2.x = quant(0.5f * (s.d1.x + k2.x * cf * dt), res);
-        s.d2.y = quant(0.5f * (s.d1.y + k2.y * cf * dt), res);
+        s.d2.x = quant(0.5f * (s.d1.x + k2.x * cf * dt));
+        s.d2.y = quant(0.5f * (s.d1.y + k2.y * cf * dt));
     } else {
         const float h1x = k1.x * cf * dt, h1y = k1.y * cf * dt;
-        s.d1.x = quant(h1x, res);
-        s.d1.y = quant(h1y, res);
+        s.d1.x = quant(h1x);
+        s.d1.y = quant(h1y);
         const Vec2 b{a.x + 0.5f * h1x, a.y + 0.5f * h1y};
         Vec2 k2 = sample_uv(b, uv, p);
         if (JITTER) k2 = jitter(k2, rng, p.jitter_magnitude);
@@ -142,8 +162,8 @@ __device__ __forceinline__ Step rk_step(Vec2 a, float dt, uint32_t& rng,
         Vec2 k4 = sample_uv(d, uv, p);
         if (JITTER) k4 = jitter(k4, rng, p.jitter_magnitude);
         const float h4x = k4.x * cf * dt, h4y = k4.y * cf * dt;
-        s.d2.x = quant(__fdiv_rn(h1x + 2.0f * h2x + 2.0f * h3x + h4x, 6.0f), res);
-        s.d2.y = quant(__fdiv_rn(h1y + 2.0f * h2y + 2.0f * h3y + h4y, 6.0f), res);
+        s.d2.x = quant(__fdiv_rn(h1x + 2.0f * h2x + 2.0f * h3x + h4x, 6.0f));
+        s.d2.y = quant(__fdiv_rn(h1y + 2.0f * h2y + 2.0f * h3y + h4y, 6.0f));
     }
     s.next.x = a.x + s.d2.x;
     s.next.y = a.y + s.d2.y;
