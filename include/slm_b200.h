@@ -148,6 +148,32 @@ int slm_integrate_trajectory(const slm_params* p, int32_t integrator, uint32_t n
                              uint32_t* mapping, int8_t* trajectories, uint16_t* nsteps,
                              float* length, void* stream);
 
+
+/* ---- kernel-density estimation (log-distributions) ----
+ * Histograms are added to (zero them first); the smoothing passes overwrite.
+ * kdf_kind selects the kernel shape (KDF_IS_<shape>); n_hist_bins must be a
+ * multiple of n_pdf_points (the reference assumes so, opencl/kde.cl:438). */
+
+/* histogram_univariate (opencl/kde.cl:383-394) as run by kde.gpu_compute
+ * (python/streamlines/kde.py:196-293) for estimate_univariate_pdf (kde.py:116-194).
+ *   sl [n_data] float log-values; hist [n_hist_bins] uint32 */
+int slm_histogram_univariate(const slm_params* p, const float* sl, uint32_t n_data,
+                             uint32_t* hist, void* stream);
+
+/* pdf_univariate (opencl/kde.cl:426-526): hist [n_hist_bins] -> pdf [n_pdf_points] */
+int slm_pdf_univariate(const slm_params* p, const uint32_t* hist, float* pdf, void* stream);
+
+/* histogram_bivariate (opencl/kde.cl:109-123) for estimate_bivariate_pdf (kde.py:35-114).
+ *   sl [n_data] float2 (x,y); hist [n_hist_bins^2] uint32, index y + n_hist_bins*x */
+int slm_histogram_bivariate(const slm_params* p, const float* sl, uint32_t n_data,
+                            uint32_t* hist, void* stream);
+
+/* pdf_bivariate_rows (opencl/kde.cl:144-228): hist -> partial [n_hist_bins^2] float */
+int slm_pdf_bivariate_rows(const slm_params* p, const uint32_t* hist, float* partial, void* stream);
+
+/* pdf_bivariate_cols (opencl/kde.cl:249-361): partial -> pdf [n_pdf_points^2] float */
+int slm_pdf_bivariate_cols(const slm_params* p, const float* partial, float* pdf, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -26,7 +26,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB_PATH = os.path.join(HERE, "liboracle_slm.so")
-SOURCES = ["slm_oracle_trace.c"]
+SOURCES = ["slm_oracle_trace.c", "slm_oracle_kde.c"]
 REF_DIR = os.path.join(HERE, "_ref")
 
 _lock = threading.Lock()
@@ -40,7 +40,7 @@ def build(force=False):
     if (not force and os.path.exists(LIB_PATH)
             and os.path.getmtime(LIB_PATH) >= max(os.path.getmtime(f) for f in srcs + [hdr])):
         return LIB_PATH
-    cmd = ["gcc", "-std=c11", "-O2", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
+    cmd = ["gcc", "-std=gnu11", "-O2", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
            "-fno-fast-math", "-I", os.path.join(ROOT, "include")] + srcs + ["-o", LIB_PATH, "-lm"]
     subprocess.run(cmd, check=True)
     return LIB_PATH
@@ -59,6 +59,13 @@ def lib():
             L.oracle_integrate_fields.argtypes = [P, i32, P, u32, u32, u32, P, P, P, P, P, i32]
             L.oracle_integrate_trajectory.restype = u64
             L.oracle_integrate_trajectory.argtypes = [P, i32, u32, P, P, P, P, P, P, i32]
+            for name in ("oracle_histogram_univariate", "oracle_histogram_bivariate"):
+                getattr(L, name).restype = None
+                getattr(L, name).argtypes = [P, P, u32, P]
+            for name in ("oracle_pdf_univariate", "oracle_pdf_bivariate_rows",
+                         "oracle_pdf_bivariate_cols"):
+                getattr(L, name).restype = None
+                getattr(L, name).argtypes = [P, P, P]
             _lib = L
         return _lib
 
@@ -167,3 +174,51 @@ def ref_integrate_trajectory(params, n_chunk, seeds, mask, uv, n_threads=1):
     RefKernel.get("integrate_trajectory").run(
         params, [seeds, mask, uv, mapping, traj, nsteps, length], n_chunk, 0, n_threads)
     return traj, nsteps, length
+
+
+# ------------------------------------------------------------------ KDE
+KDF_SHAPES = ["tophat", "triangle", "epanechnikov", "cosine", "gaussian"]
+
+
+def histogram_univariate(params, data):
+    data = np.ascontiguousarray(data, dtype=np.float32).reshape(-1)
+    hist = np.zeros(params.n_hist_bins, dtype=np.uint32)
+    lib().oracle_histogram_univariate(_params_ptr(params), _ptr(data), data.size, _ptr(hist))
+    return hist
+
+
+def histogram_bivariate(params, data):
+    data = np.ascontiguousarray(data, dtype=np.float32).reshape(-1, 2)
+    hist = np.zeros(params.n_hist_bins * params.n_hist_bins, dtype=np.uint32)
+    lib().oracle_histogram_bivariate(_params_ptr(params), _ptr(data), data.shape[0], _ptr(hist))
+    return hist
+
+
+def pdf_univariate(params, hist):
+    hist = np.ascontiguousarray(hist, dtype=np.uint32).reshape(-1)
+    pdf = np.zeros(params.n_pdf_points, dtype=np.float32)
+    lib().oracle_pdf_univariate(_params_ptr(params), _ptr(hist), _ptr(pdf))
+    return pdf
+
+
+def pdf_bivariate_rows(params, hist):
+    hist = np.ascontiguousarray(hist, dtype=np.uint32).reshape(-1)
+    out = np.zeros(params.n_hist_bins * params.n_hist_bins, dtype=np.float32)
+    lib().oracle_pdf_bivariate_rows(_params_ptr(params), _ptr(hist), _ptr(out))
+    return out
+
+
+def pdf_bivariate_cols(params, partial):
+    partial = np.ascontiguousarray(partial, dtype=np.float32).reshape(-1)
+    out = np.zeros(params.n_pdf_points * params.n_pdf_points, dtype=np.float32)
+    lib().oracle_pdf_bivariate_cols(_params_ptr(params), _ptr(partial), _ptr(out))
+    return out
+
+
+def ref_kde(name, params, inp, out_size, out_dtype, n_global):
+    """Run one reference KDE kernel (pdf kernels pick the KDF_IS_<shape> build)."""
+    if name.startswith("pdf_"):
+        name = "{}__{}".format(name, KDF_SHAPES[params.kdf_kind])
+    out = np.zeros(out_size, dtype=out_dtype)
+    RefKernel.get(name).run(params, [np.ascontiguousarray(inp), out], n_global, 0, 1)
+    return out

@@ -50,6 +50,11 @@ SIGNATURES = {
     "slm_integrate_fields": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_integrate_fields_noalloc": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_integrate_trajectory": (ctypes.c_int, [_P, _I, _U, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "slm_histogram_univariate": (ctypes.c_int, [_P, _P, _U, _P, _P]),
+    "slm_histogram_bivariate": (ctypes.c_int, [_P, _P, _U, _P, _P]),
+    "slm_pdf_univariate": (ctypes.c_int, [_P, _P, _P, _P]),
+    "slm_pdf_bivariate_rows": (ctypes.c_int, [_P, _P, _P, _P]),
+    "slm_pdf_bivariate_cols": (ctypes.c_int, [_P, _P, _P, _P]),
 }
 
 _lock = threading.Lock()

@@ -73,13 +73,19 @@ __device__ __forceinline__ Vec2 sample_uv(Vec2 a, const float2* __restrict__ uv,
 struct Quant {
     float res, inv;
     bool pow2;
-    __device__ __forceinline__ explicit Quant(uint32_t r)
-        : res((float)r), inv(__fdiv_rn(1.0f, (float)r)), pow2(r != 0u && (r & (r - 1u)) == 0u) {}
     __device__ __forceinline__ float operator()(float v) const {
         const float c = (float)cvt_i8(v * res);
         return pow2 ? c * inv : __fdiv_rn(c, res);
     }
 };
+
+__device__ __forceinline__ Quant make_quant(uint32_t r) {
+    Quant q;
+    q.res = (float)r;
+    q.inv = __fdiv_rn(1.0f, (float)r);
+    q.pow2 = r != 0u && (r & (r - 1u)) == 0u;
+    return q;
+}
 
 __device__ __forceinline__ float quant(float v, float res) {
     return __fdiv_rn((float)cvt_i8(v * res), res);
@@ -134,7 +140,7 @@ __device__ __forceinline__ Step rk_step(Vec2 a, float dt, uint32_t& rng,
                                         const float2* __restrict__ uv, const slm_params& p) {
     Step s;
     const float cf = p.combo_factor;
-    const Quant quant(p.trajectory_resolution);
+    const Quant quant = make_quant(p.trajectory_resolution);
     Vec2 k1 = sample_uv(a, uv, p);
     if (JITTER) k1 = jitter(k1, rng, p.jitter_magnitude);
     s.u1 = k1;

@@ -76,3 +76,39 @@ def integrate_trajectory(params, n_chunk, seeds, mask, uv, traj, nsteps, length,
     check(lib.slm_integrate_trajectory(sref(params), int(integrator), int(n_chunk), ptr(seeds),
                                        ptr(mask), ptr(uv), None, ptr(traj), ptr(nsteps),
                                        ptr(length), _stream(stream)))
+
+
+# ------------------------------------------------------------------ KDE
+def histogram_univariate(params, data, hist, stream=None):
+    _need(data, torch.float32, None, "data")
+    _need(hist, torch.uint32, int(params.n_hist_bins), "histogram")
+    check(_lib.load().slm_histogram_univariate(sref(params), ptr(data), int(data.numel()),
+                                                ptr(hist), _stream(stream)))
+
+
+def histogram_bivariate(params, data, hist, stream=None):
+    _need(data, torch.float32, None, "data")
+    nb = int(params.n_hist_bins)
+    _need(hist, torch.uint32, nb * nb, "histogram")
+    check(_lib.load().slm_histogram_bivariate(sref(params), ptr(data), int(data.numel() // 2),
+                                               ptr(hist), _stream(stream)))
+
+
+def pdf_univariate(params, hist, pdf, stream=None):
+    _need(hist, torch.uint32, int(params.n_hist_bins), "histogram")
+    _need(pdf, torch.float32, int(params.n_pdf_points), "pdf")
+    check(_lib.load().slm_pdf_univariate(sref(params), ptr(hist), ptr(pdf), _stream(stream)))
+
+
+def pdf_bivariate_rows(params, hist, partial, stream=None):
+    nb = int(params.n_hist_bins)
+    _need(hist, torch.uint32, nb * nb, "histogram")
+    _need(partial, torch.float32, nb * nb, "partial pdf")
+    check(_lib.load().slm_pdf_bivariate_rows(sref(params), ptr(hist), ptr(partial), _stream(stream)))
+
+
+def pdf_bivariate_cols(params, partial, pdf, stream=None):
+    nb, np_ = int(params.n_hist_bins), int(params.n_pdf_points)
+    _need(partial, torch.float32, nb * nb, "partial pdf")
+    _need(pdf, torch.float32, np_ * np_, "pdf")
+    check(_lib.load().slm_pdf_bivariate_cols(sref(params), ptr(partial), ptr(pdf), _stream(stream)))
