@@ -202,8 +202,6 @@ def run_b200(args):
     info = wl.info
     integrator = spec.integrator
     n_seeds = int(info.n_seed_points)
-    begin = (n_seeds * rank) // ws
-    end = (n_seeds * (rank + 1)) // ws
     nxy = int(info.nx_padded * info.ny_padded)
 
     seeds_d = torch.from_numpy(wl.seeds).to(dev)
@@ -218,12 +216,9 @@ def run_b200(args):
     length_d = torch.zeros((2, n_traj), dtype=torch.float32, device=dev)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
 
-    field_prm = []
-    for sign in (1.0, -1.0):
-        prm = kernel_params(info, "INTEGRATE_FIELDS", sign)
-        prm.seeds_chunk_offset = begin
-        prm.n_seed_points = end
-        field_prm.append(prm)
+    from slm_b200.distributed import allreduce_counts, shard_params
+    field_prm = [shard_params(kernel_params(info, "INTEGRATE_FIELDS", s), rank, ws)
+                 for s in (1.0, -1.0)]
     tinfo = wl.fresh_info()
     tinfo.n_seed_points = n_traj
     traj_prm = [kernel_params(tinfo, "INTEGRATE_TRAJECTORY", np.float32(s)) for s in (1.0, -1.0)]
@@ -253,7 +248,7 @@ def run_b200(args):
             ev[1].record(stream)
         stream.wait_event(join)
         if ws > 1:
-            dist.all_reduce(acc.view(torch.int64), op=dist.ReduceOp.SUM)
+            allreduce_counts(acc)
 
     def count_steps():
         f = sum(int(w[1].view(torch.int64).item()) for w in work)

@@ -13,7 +13,10 @@ Differences from the reference (none changes a result):
   direction; ``max_time_per_kernel`` is not used;
 * device accumulators are uint64; ``slc``/``slt`` returned to the caller are
   the low 32 bits (what the reference's uint32 atomics hold) unless
-  ``exact=True``, which keeps the full sums.
+  ``exact=True``, which keeps the full sums;
+* with ``process_group`` (one process per GPU) each rank traces its shard of
+  the seed list and the uint64 accumulators are summed with one all-reduce
+  (slm_b200.distributed); every rank then holds the full fields.
 """
 from __future__ import annotations
 
@@ -22,6 +25,7 @@ import torch
 
 from . import kernels
 from .device import cuda_device, low32, to_device
+from .distributed import sharded_field_pass
 from .params import kernel_params
 from .useful import create_seeds, vprint
 
@@ -29,7 +33,7 @@ from .useful import create_seeds, vprint
 class Fields:
     def __init__(self, cl_platform, cl_device, cl_src_path=None, info=None, data=None,
                  verbose=False, gpu_verbose=False, schedule="persistent", integrator=2,
-                 exact=False):
+                 exact=False, process_group=None):
         self.device = cuda_device(cl_platform, cl_device)
         self.cl_src_path = cl_src_path  # unused: kernels are prebuilt
         self.info = info
@@ -40,6 +44,7 @@ class Fields:
         self.schedule = schedule
         self.integrator = integrator
         self.exact = exact
+        self.process_group = process_group
         self.n_steps = [0, 0]
         self.n_trajectories = [0, 0]
 
@@ -80,12 +85,18 @@ class Fields:
             for downup_idx, downup_sign in ((0, +1.0), (1, -1.0)):
                 info.downup_sign = downup_sign
                 prm = kernel_params(info, "INTEGRATE_FIELDS", downup_sign)
-                kernels.integrate_fields(prm, seeds_d, mask_d, uv_d, acc[downup_idx, 0],
-                                         acc[downup_idx, 1], work, schedule=self.schedule,
-                                         integrator=self.integrator)
-                counters = work[1:3].view(torch.int64).cpu()
-                self.n_steps[downup_idx] = int(counters[0])
-                self.n_trajectories[downup_idx] = int(counters[1])
+
+                def trace(p, slc, slt):
+                    kernels.integrate_fields(p, seeds_d, mask_d, uv_d, slc, slt, work,
+                                             schedule=self.schedule, integrator=self.integrator)
+                    return int(work[1].view(torch.int64).item())
+
+                if self.process_group is None:
+                    self.n_steps[downup_idx] = trace(prm, acc[downup_idx, 0], acc[downup_idx, 1])
+                else:
+                    _, self.n_steps[downup_idx] = sharded_field_pass(
+                        prm, trace, acc[downup_idx, 0], acc[downup_idx, 1], self.process_group)
+                self.n_trajectories[downup_idx] = int(prm.n_seed_points) * int(prm.subpixel_seed_point_density) ** 2
             if self.exact:
                 raw = acc.cpu().numpy()
                 slc_raw = raw[:, 0].astype(np.float64)

@@ -1,0 +1,62 @@
+"""The drop-in stage wrappers (Trajectories, Fields) on the GPU against the oracle."""
+import numpy as np
+import pytest
+
+import oracle as O
+from cases import Case
+from slm_b200.fields import Fields
+from slm_b200.trajectories import Trajectories
+from slm_b200.useful import Data, compute_stats, create_seeds
+
+pytestmark = pytest.mark.gpu
+
+
+def _data(c, stats=None):
+    return Data(info=c.info, mask_array=c.mask, uv_array=c.uv,
+                mapping_array=np.zeros(c.mask.shape, np.uint32), traj_stats_df=stats)
+
+
+@pytest.mark.parametrize("integrator", [2, 4])
+def test_trajectories_stage(integrator):
+    c = Case(nx=64, ny=48, seed=81, step=0.25, max_length=80.0, n_traj_seeds=300)
+    tr = Trajectories(0, 0, info=c.info, data=_data(c), integrator=integrator)
+    tr.integrate()
+    n = int(c.info.n_seed_points)
+    for d, sign in ((0, np.float32(1.0)), (1, np.float32(-1.0))):
+        c.info.seeds_chunk_offset = np.uint32(0)
+        prm = c.params("INTEGRATE_TRAJECTORY", sign)
+        ot, on, ol, _ = O.integrate_trajectory(prm, n, c.seeds, c.mask, c.uv, integrator=integrator)
+        assert np.array_equal(tr.data.traj_nsteps_array[:, d], on)
+        assert np.array_equal(tr.data.traj_length_array[:, d].view(np.uint32), ol.view(np.uint32))
+        for k in range(n):
+            assert np.array_equal(tr.data.streamline_arrays_list[d][k], ot[k, :on[k]])
+    ref_stats = compute_stats(tr.data.traj_length_array, tr.data.traj_nsteps_array, c.info.pixel_size)
+    assert np.array_equal(tr.data.traj_stats_df.values, ref_stats.values)
+
+
+def test_fields_stage_raw_and_postprocessed():
+    c = Case(nx=56, ny=60, seed=82, density=2, step=0.25, max_length=60.0, n_traj_seeds=200)
+    tr = Trajectories(0, 0, info=c.info, data=_data(c))
+    tr.integrate()
+    stats = tr.data.traj_stats_df
+    c2 = Case(nx=56, ny=60, seed=82, density=2, step=0.25, max_length=60.0)
+    f = Fields(0, 0, info=c2.info, data=_data(c2, stats))
+    seeds, ns, npad = create_seeds(c2.mask, 2, 32)
+    f.data.seed_point_array = seeds
+    c2.info.n_seed_points, c2.info.n_padded_seed_points = ns, npad
+    f.gpu_integrate()
+    nxp, nyp = c2.mask.shape
+    raw_slc = f.data.slc_array.copy()
+    for d, sign in ((0, 1.0), (1, -1.0)):
+        prm = c2.params("INTEGRATE_FIELDS", sign)
+        oslc, oslt, osteps, _ = O.integrate_fields(prm, seeds, c2.mask, c2.uv, n_threads=4)
+        assert np.array_equal(raw_slc[:, :, d], oslc.astype(np.uint32).reshape(nxp, nyp))
+        assert f.n_steps[d] == osteps
+    # full integrate(): the reference's post-processing on the same raw sums
+    c3 = Case(nx=56, ny=60, seed=82, density=2, step=0.25, max_length=60.0)
+    f2 = Fields(0, 0, info=c3.info, data=_data(c3, stats))
+    f2.integrate()
+    assert f2.data.slc_array.shape == (nxp, nyp, 2) and f2.data.slt_array.dtype == np.float32
+    expect_slc = np.sqrt(2.0) * np.power(raw_slc / 4, 2 / 3)
+    assert np.array_equal(f2.data.slc_array, expect_slc)
+    assert np.isfinite(f2.data.sla_array).all()
