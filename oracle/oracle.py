@@ -26,8 +26,17 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB_PATH = os.path.join(HERE, "liboracle_slm.so")
-SOURCES = ["slm_oracle_trace.c", "slm_oracle_kde.c"]
+SOURCES = ["slm_oracle_trace.c", "slm_oracle_kde.c", "slm_oracle_map.c"]
 REF_DIR = os.path.join(HERE, "_ref")
+
+# mapping kernel -> number of buffer arguments after (params, seeds, n)
+MAP_KERNELS = {
+    "connect_channels": 3, "map_channel_heads": 3, "prune_channel_heads": 3,
+    "count_downchannels": 5, "flag_downchannels": 5, "label_confluences": 6,
+    "segment_downchannels": 6, "segment_hillslopes": 6, "subsegment_channel_edges": 6,
+    "subsegment_flanks": 6, "fix_right_flanks": 6, "fix_left_flanks": 6,
+    "hillslopes": 5, "hillslope_lengths": 5,
+}
 
 _lock = threading.Lock()
 _lib = None
@@ -66,6 +75,10 @@ def lib():
                          "oracle_pdf_bivariate_cols"):
                 getattr(L, name).restype = None
                 getattr(L, name).argtypes = [P, P, P]
+            for name, nargs in MAP_KERNELS.items():
+                fn = getattr(L, "oracle_" + name)
+                fn.restype = u32
+                fn.argtypes = [P, P, u32] + [P] * nargs
             _lib = L
         return _lib
 
@@ -222,3 +235,25 @@ def ref_kde(name, params, inp, out_size, out_dtype, n_global):
     out = np.zeros(out_size, dtype=out_dtype)
     RefKernel.get(name).run(params, [np.ascontiguousarray(inp), out], n_global, 0, 1)
     return out
+
+
+# ------------------------------------------------------------------ mapping
+def map_kernel(name, params, seeds, arrays):
+    """Run one mapping kernel of the restatement in place on ``arrays`` (the
+    reference kernel's buffers after seed_point, in order); returns the status
+    word (bit 0 loop cap hit, bit 1 out-of-grid access skipped)."""
+    seeds = np.ascontiguousarray(seeds, dtype=np.float32)
+    fn = getattr(lib(), "oracle_" + name)
+    ptrs = []
+    for a in arrays:
+        assert a.flags["C_CONTIGUOUS"], name
+        ptrs.append(ctypes.c_void_p(a.ctypes.data))
+    return int(fn(_params_ptr(params), _ptr(seeds), seeds.shape[0], *ptrs))
+
+
+def ref_map_kernel(name, params, seeds, arrays):
+    """The reference's own mapping kernel, sequential ascending global id, in place."""
+    seeds = np.ascontiguousarray(seeds, dtype=np.float32)
+    p = params.copy()
+    p.n_seed_points = seeds.shape[0]
+    RefKernel.get(name).run(p, [seeds] + list(arrays), seeds.shape[0], 0, 1)

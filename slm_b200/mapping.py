@@ -1,0 +1,275 @@
+"""Channel, segment and hillslope mapping: drop-ins for the reference's mapping
+wrappers and the kernel sequence of ``Mapping.map_channels_segments``.
+
+Each function mirrors one reference wrapper -- same signature
+``fn(cl_state, info, data, verbose)``, same seed selection, same in-place
+updates of ``data.mapping_array`` / ``count_array`` / ``link_array`` /
+``label_array`` / ``channel_label_array`` / ``subsegment_hsl_array``, same
+return value (``False``/``0`` on an empty seed list):
+
+  connect_channel_pixels   connect.py:32-79        kernel connect_channels
+  map_channel_heads        channelheads.py:33-80   kernel map_channel_heads
+  prune_channel_heads      channelheads.py:82-118  kernel prune_channel_heads
+  count_downchannels       countlink.py:36-81      kernel count_downchannels
+  flag_downchannels        countlink.py:83-130     kernel flag_downchannels
+  label_confluences        label.py:33-78          kernel label_confluences
+  segment_channels         segment.py:34-93        kernel segment_downchannels
+  segment_hillslopes       segment.py:95-146       kernel segment_hillslopes
+  subsegment_flanks        segment.py:148-243      kernels subsegment_channel_edges,
+                                                   subsegment_flanks, fix_right_flanks,
+                                                   fix_left_flanks
+  link_hillslopes          hillslopes.py:32-80     kernel hillslopes
+  hsl                      lengths.py:33-92        kernel hillslope_lengths
+
+``map_channels_segments`` follows mapping.py:627-677 (with the helpers
+:695-775).  The host thinning step uses this project's Zhang-Suen thinning
+(slm_b200.skeleton) in place of scikit-image's medial axis + skeletonize.
+
+Kernels run through ``runner(name, params, seeds, arrays)``, which updates the
+NumPy ``arrays`` (the reference kernel's buffers after ``seed_point``, in its
+order) in place.  The default runner is the CUDA library (``DeviceRunner``).
+Host relabelling keeps the reference's results where NumPy 2 would reject its
+expressions: segment relabelling is a rank map (the reference's loop over
+sorted labels gives the same values) and the left-flank sign fix-up is done in
+64-bit arithmetic.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .params import kernel_params
+from .skeleton import zhang_suen
+from .useful import pick_seeds, vprint
+
+
+class DeviceRunner:
+    """Runs one mapping kernel on the GPU: uploads the buffers, calls the C
+    ABI entry point, copies the written buffers back into the arrays."""
+
+    def __init__(self, device=None):
+        self.device = device
+
+    def __call__(self, name, params, seeds, arrays):
+        from . import map_kernels
+        return map_kernels.run(name, params, seeds, arrays, self.device)
+
+
+_default_runner = None
+
+
+def _runner(runner):
+    global _default_runner
+    if runner is not None:
+        return runner
+    if _default_runner is None:
+        _default_runner = DeviceRunner()
+    return _default_runner
+
+
+def _u32(a):
+    """uint32 view of a label array (the kernels treat int32 labels as uint)."""
+    return a.view(np.uint32) if a.dtype == np.int32 else a
+
+
+def _run(runner, kernel, info, seeds, arrays):
+    info.n_seed_points = np.uint32(seeds.shape[0])
+    prm = kernel_params(info, kernel.upper())
+    return _runner(runner)(kernel, prm, seeds, arrays)
+
+
+def connect_channel_pixels(cl_state, info, data, verbose=False, runner=None):
+    seeds = pick_seeds(map=data.mapping_array, flag=info.is_channel, pad=info.pad_width)
+    if seeds.shape[0] == 0:
+        return None
+    _run(runner, "connect_channels", info, seeds,
+         [data.mask_array, data.uv_array, data.mapping_array])
+    return True
+
+
+def map_channel_heads(cl_state, info, data, verbose=False, runner=None):
+    m = data.mapping_array
+    m[(m & info.is_thinchannel) == info.is_thinchannel] |= info.is_channelhead
+    seeds = pick_seeds(mask=data.mask_array, flag=info.is_channel, pad=info.pad_width)
+    if seeds.shape[0] == 0:
+        return False
+    _run(runner, "map_channel_heads", info, seeds, [data.mask_array, data.uv_array, m])
+    return True
+
+
+def prune_channel_heads(cl_state, info, data, verbose=False, runner=None):
+    seeds = pick_seeds(mask=data.mask_array, map=data.mapping_array,
+                       flag=info.is_channelhead, pad=info.pad_width)
+    if seeds.shape[0] == 0:
+        return None
+    _run(runner, "prune_channel_heads", info, seeds,
+         [data.mask_array, data.uv_array, data.mapping_array])
+
+
+def count_downchannels(cl_state, info, data, verbose=False, runner=None):
+    m = data.mapping_array
+    m[(m & info.is_thinchannel) != 0] ^= info.is_thinchannel
+    seeds = pick_seeds(mask=data.mask_array, map=m, flag=info.is_channelhead, pad=info.pad_width)
+    if seeds.shape[0] == 0:
+        return False
+    _run(runner, "count_downchannels", info, seeds,
+         [data.mask_array, data.uv_array, m, data.count_array, data.link_array])
+    return True
+
+
+def flag_downchannels(cl_state, info, data, verbose=False, do_reset_count=True, runner=None):
+    m = data.mapping_array
+    m[(m & info.is_thinchannel) != 0] ^= info.is_thinchannel
+    if do_reset_count:
+        data.count_array *= 0
+    seeds = pick_seeds(mask=data.mask_array, map=m, flag=info.is_channelhead, pad=info.pad_width)
+    if seeds.shape[0] == 0:
+        return False
+    _run(runner, "flag_downchannels", info, seeds,
+         [data.mask_array, data.uv_array, m, data.count_array, data.link_array])
+    return True
+
+
+def label_confluences(cl_state, info, data, verbose=False, runner=None):
+    seeds = pick_seeds(mask=data.mask_array, map=data.mapping_array,
+                       flag=info.is_thinchannel, pad=info.pad_width)
+    if seeds.shape[0] == 0:
+        return False
+    dn_slt = np.ascontiguousarray(data.slt_array[:, :, 0], dtype=np.float32)
+    _run(runner, "label_confluences", info, seeds,
+         [data.mask_array, data.uv_array, dn_slt, data.mapping_array, data.count_array,
+          data.link_array])
+    return True
+
+
+def segment_channels(cl_state, info, data, verbose=False, runner=None):
+    seeds = pick_seeds(mask=data.mask_array, map=data.mapping_array,
+                       flag=info.is_channelhead, pad=info.pad_width)
+    if seeds.shape[0] == 0:
+        return 0
+    _run(runner, "segment_downchannels", info, seeds,
+         [data.mask_array, data.uv_array, data.mapping_array, data.count_array,
+          data.link_array, _u32(data.label_array)])
+    # relabel channel segments 1,2,3,... in label order (segment.py:83-88)
+    lab = data.label_array
+    pos = lab > 0
+    labels = np.unique(lab[pos].ravel())
+    if labels.size == 0:
+        return 0
+    lab[pos] = (np.searchsorted(labels, lab[pos]) + 1).astype(lab.dtype)
+    return int(labels.size)
+
+
+def link_hillslopes(cl_state, info, data, verbose=False, runner=None):
+    seeds = pick_seeds(mask=data.mask_array, map=~data.mapping_array,
+                       flag=info.is_thinchannel, pad=info.pad_width)
+    if seeds.shape[0] == 0:
+        return False
+    _run(runner, "hillslopes", info, seeds,
+         [data.mask_array, data.uv_array, data.mapping_array, data.count_array, data.link_array])
+    return True
+
+
+def segment_hillslopes(cl_state, info, data, verbose=False, runner=None):
+    seeds = pick_seeds(mask=data.mask_array, map=~data.mapping_array,
+                       flag=info.is_thinchannel, pad=info.pad_width)
+    if seeds.shape[0] == 0:
+        return False
+    _run(runner, "segment_hillslopes", info, seeds,
+         [data.mask_array, data.uv_array, data.mapping_array, data.count_array,
+          data.link_array, _u32(data.label_array)])
+    return True
+
+
+def subsegment_flanks(cl_state, info, data, verbose=False, runner=None):
+    pad = info.pad_width
+    arrays = [data.mask_array, data.uv_array, data.mapping_array, data.channel_label_array,
+              data.link_array, _u32(data.label_array)]
+    seeds = pick_seeds(mask=data.mask_array, map=data.mapping_array,
+                       flag=info.is_subsegmenthead, pad=pad)
+    if seeds.shape[0] == 0:
+        return False
+    _run(runner, "subsegment_channel_edges", info, seeds, arrays)
+    flag = info.is_leftflank | info.is_thinchannel
+    for kernel in ("subsegment_flanks", "fix_right_flanks"):
+        seeds = pick_seeds(mask=data.mask_array, map=~data.mapping_array, flag=flag, pad=pad)
+        if seeds.shape[0] == 0:
+            return False
+        _run(runner, kernel, info, seeds, arrays)
+    seeds = pick_seeds(mask=data.mask_array, map=data.mapping_array, flag=info.is_leftflank, pad=pad)
+    if seeds.shape[0] == 0:
+        return False
+    _run(runner, "fix_left_flanks", info, seeds, arrays)
+    return True
+
+
+def hsl(cl_state, info, data, do_use_ridges, verbose=False, runner=None):
+    flag = info.is_ridge if do_use_ridges else info.is_midslope
+    seeds = pick_seeds(mask=data.mask_array, map=data.mapping_array, flag=flag, pad=info.pad_width)
+    if seeds.shape[0] != data.subsegment_hsl_array.shape[0]:
+        raise ValueError("Mismatched midslope/ridge point arrays: seed pts={0} traj len={1}"
+                         .format(seeds.shape, data.subsegment_hsl_array.shape))
+    if seeds.shape[0] == 0:
+        return False
+    _run(runner, "hillslope_lengths", info, seeds,
+         [data.mask_array, data.uv_array, data.mapping_array, _u32(data.label_array),
+          data.subsegment_hsl_array])
+    if not do_use_ridges:
+        data.subsegment_hsl_array *= 2.0
+    return True
+
+
+# ------------------------------------------------------------------ sequence
+def map_channels(info, data):
+    """Channel pixels from the downstream fields (mapping.py:695-702)."""
+    slt = data.slt_array[:, :, 0]
+    slc = data.slc_array[:, :, 0]
+    data.mapping_array[(slt >= info.channel_threshold) & (slt * 2 >= slc)] = info.is_channel
+
+
+def thin_channels(info, data):
+    """Thin channel + inter-channel pixels to a skeleton (mapping.py:707-719)."""
+    m = data.mapping_array
+    channel = (((m & info.is_channel) == info.is_channel)
+               | ((m & info.is_interchannel) == info.is_interchannel))
+    m[zhang_suen(channel)] |= info.is_thinchannel
+
+
+def map_channels_segments(cl_state, info, data, do_map_channels_from_scratch=True,
+                          do_map_segments=True, verbose=False, runner=None):
+    """The kernel sequence of mapping.py:627-677 (with :695-775)."""
+    nxp, nyp = data.mask_array.shape
+    if do_map_channels_from_scratch:
+        map_channels(info, data)
+    if not connect_channel_pixels(cl_state, info, data, verbose, runner):
+        return False
+    thin_channels(info, data)
+    if not map_channel_heads(cl_state, info, data, verbose, runner):
+        return False
+    data.count_array = np.zeros((nxp, nyp), dtype=np.uint32)
+    data.link_array = np.zeros((nxp, nyp), dtype=np.uint32)
+    if not count_downchannels(cl_state, info, data, verbose, runner):
+        return False
+    if not flag_downchannels(cl_state, info, data, verbose, runner=runner):
+        return False
+    if not do_map_segments:
+        return True
+    if (not label_confluences(cl_state, info, data, verbose, runner)
+            or not flag_downchannels(cl_state, info, data, verbose, runner=runner)
+            or not flag_downchannels(cl_state, info, data, verbose, do_reset_count=False, runner=runner)
+            or not flag_downchannels(cl_state, info, data, verbose, do_reset_count=False, runner=runner)):
+        return False
+    data.label_array = np.zeros((nxp, nyp), dtype=np.int32)
+    if segment_channels(cl_state, info, data, verbose, runner) == 0:
+        return False
+    data.channel_label_array = data.label_array.copy().astype(np.uint32)
+    if not link_hillslopes(cl_state, info, data, verbose, runner):
+        return False
+    if not segment_hillslopes(cl_state, info, data, verbose, runner):
+        return False
+    if not subsegment_flanks(cl_state, info, data, verbose, runner):
+        return False
+    lab = data.label_array
+    neg = lab < 0
+    lab[neg] = (-(lab[neg].astype(np.int64) + int(info.left_flank_addition))).astype(np.int32)
+    vprint(verbose, "mapped channels and segments")
+    return True
