@@ -174,6 +174,86 @@ int slm_pdf_bivariate_rows(const slm_params* p, const uint32_t* hist, float* par
 /* pdf_bivariate_cols (opencl/kde.cl:249-361): partial -> pdf [n_pdf_points^2] float */
 int slm_pdf_bivariate_cols(const slm_params* p, const float* partial, float* pdf, void* stream);
 
+/* ---- channel / segment / hillslope mapping ----
+ * One entry point per reference mapping kernel, same buffers in the same
+ * order after (params, n_seeds, seed_point).  Results equal the reference's
+ * work-items run one after another in ascending global id (the reference
+ * races in count_downchannels, flag_downchannels, segment_downchannels,
+ * prune_channel_heads and fix_*_flanks; this is the schedule its results are
+ * pinned to).  `status` is a device word cleared by the call: bit 0 = a loop
+ * cap the reference would exceed was hit, bit 1 = an out-of-grid neighbour
+ * was skipped.  Entry points with a workspace run a counting pass first: with
+ * too small a workspace they return SLM_ERR_CAPACITY and write the bytes
+ * needed to *required_bytes (host pointer); fix_*_flanks and
+ * count_downchannels synchronise the stream. */
+
+/* connect_channels (opencl/connect.cl:26-108; connect.py:32-79);
+ * interchannel_max_n_steps must be <= 256 */
+int slm_connect_channels(const slm_params* p, uint32_t n_seeds, const float* seed_point,
+                         const uint8_t* mask, const float* uv, uint32_t* mapping,
+                         uint32_t* status, void* stream);
+/* map_channel_heads (opencl/channelheads.cl:32-93; channelheads.py:33-80) */
+int slm_map_channel_heads(const slm_params* p, uint32_t n_seeds, const float* seed_point,
+                          const uint8_t* mask, const float* uv, uint32_t* mapping, void* stream);
+/* prune_channel_heads (opencl/channelheads.cl:143-199; channelheads.py:82-118) */
+int slm_prune_channel_heads(const slm_params* p, uint32_t n_seeds, const float* seed_point,
+                            const uint8_t* mask, const float* uv, uint32_t* mapping, void* stream);
+/* count_downchannels (opencl/countlink.cl:34-114; countlink.py:36-81) */
+size_t slm_count_downchannels_workspace(uint32_t n_seeds, uint64_t n_path_events);
+int slm_count_downchannels(const slm_params* p, uint32_t n_seeds, const float* seed_point,
+                           const uint8_t* mask, const float* uv, uint32_t* mapping, uint32_t* count,
+                           uint32_t* link, void* workspace, size_t workspace_bytes,
+                           uint64_t* required_bytes, void* stream);
+/* flag_downchannels (opencl/countlink.cl:134-210; countlink.py:83-130) */
+int slm_flag_downchannels(const slm_params* p, uint32_t n_seeds, const float* seed_point,
+                          const uint8_t* mask, const float* uv, uint32_t* mapping, uint32_t* count,
+                          const uint32_t* link, void* stream);
+/* label_confluences (opencl/label.cl:49-134; label.py:33-78); slt = downstream slt, float */
+int slm_label_confluences(const slm_params* p, uint32_t n_seeds, const float* seed_point,
+                          const uint8_t* mask, const float* uv, const float* slt, uint32_t* mapping,
+                          const uint32_t* count, const uint32_t* link, void* stream);
+/* segment_downchannels (opencl/segment.cl:38-107; segment.py:34-93) */
+int slm_segment_downchannels(const slm_params* p, uint32_t n_seeds, const float* seed_point,
+                             const uint8_t* mask, const float* uv, uint32_t* mapping,
+                             const uint32_t* count, const uint32_t* link, uint32_t* label,
+                             uint32_t* status, void* stream);
+/* segment_hillslopes (opencl/segment.cl:133-188; segment.py:95-146) */
+int slm_segment_hillslopes(const slm_params* p, uint32_t n_seeds, const float* seed_point,
+                           const uint8_t* mask, const float* uv, const uint32_t* mapping,
+                           const uint32_t* count, const uint32_t* link, uint32_t* label, void* stream);
+/* subsegment_channel_edges (opencl/segment.cl:195-334; segment.py:148-195) */
+int slm_subsegment_channel_edges(const slm_params* p, uint32_t n_seeds, const float* seed_point,
+                                 const uint8_t* mask, const float* uv, uint32_t* mapping,
+                                 const uint32_t* channel_label, const uint32_t* link,
+                                 uint32_t* label, uint32_t* status, void* stream);
+/* subsegment_flanks (opencl/segment.cl:360-414; segment.py:197-208) */
+int slm_subsegment_flanks(const slm_params* p, uint32_t n_seeds, const float* seed_point,
+                          const uint8_t* mask, const float* uv, const uint32_t* mapping,
+                          const uint32_t* channel_label, const uint32_t* link, uint32_t* label,
+                          void* stream);
+/* fix_right_flanks / fix_left_flanks (opencl/segment.cl:441-504, 530-594;
+ * segment.py:210-232) */
+size_t slm_fix_flanks_workspace(uint32_t n_seeds, uint32_t nxy_padded, uint64_t n_path_steps);
+int slm_fix_right_flanks(const slm_params* p, uint32_t n_seeds, const float* seed_point,
+                         const uint8_t* mask, const float* uv, const uint32_t* mapping,
+                         const uint32_t* channel_label, const uint32_t* link, uint32_t* label,
+                         void* workspace, size_t workspace_bytes, uint64_t* required_bytes,
+                         void* stream);
+int slm_fix_left_flanks(const slm_params* p, uint32_t n_seeds, const float* seed_point,
+                        const uint8_t* mask, const float* uv, const uint32_t* mapping,
+                        const uint32_t* channel_label, const uint32_t* link, uint32_t* label,
+                        void* workspace, size_t workspace_bytes, uint64_t* required_bytes,
+                        void* stream);
+/* hillslopes (opencl/hillslopes.cl:31-91; hillslopes.py:32-80) */
+int slm_hillslopes(const slm_params* p, uint32_t n_seeds, const float* seed_point,
+                   const uint8_t* mask, const float* uv, const uint32_t* mapping,
+                   const uint32_t* count, uint32_t* link, void* stream);
+/* hillslope_lengths (opencl/lengths.cl:37-116; lengths.py:33-92);
+ * traj_length [n_seeds] float, written only where a channel is reached */
+int slm_hillslope_lengths(const slm_params* p, uint32_t n_seeds, const float* seed_point,
+                          const uint8_t* mask, const float* uv, const uint32_t* mapping,
+                          const uint32_t* label, float* traj_length, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

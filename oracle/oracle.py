@@ -79,6 +79,8 @@ def lib():
                 fn = getattr(L, "oracle_" + name)
                 fn.restype = u32
                 fn.argtypes = [P, P, u32] + [P] * nargs
+            L.oracle_flank_paths.restype = u64
+            L.oracle_flank_paths.argtypes = [P, P, u32, P, P, P, u32, P, P]
             _lib = L
         return _lib
 
@@ -257,3 +259,15 @@ def ref_map_kernel(name, params, seeds, arrays):
     p = params.copy()
     p.n_seed_points = seeds.shape[0]
     RefKernel.get(name).run(p, [seeds] + list(arrays), seeds.shape[0], 0, 1)
+
+
+def flank_paths(params, seeds, mask, uv, mapping, cap=4096):
+    """(counts [n], pairs [n, cap, 2]) of the flank walks (tests only)."""
+    seeds = np.ascontiguousarray(seeds, dtype=np.float32)
+    n = seeds.shape[0]
+    counts = np.zeros(n, dtype=np.uint32)
+    pairs = np.zeros((n, cap, 2), dtype=np.uint32)
+    lib().oracle_flank_paths(_params_ptr(params), _ptr(seeds), n,
+                             _ptr(np.ascontiguousarray(mask).view(np.uint8)), _ptr(uv),
+                             _ptr(mapping), cap, _ptr(counts), _ptr(pairs))
+    return counts, pairs

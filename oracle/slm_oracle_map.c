@@ -571,3 +571,32 @@ uint32_t oracle_hillslope_lengths(const slm_params* p, const float* seeds, uint3
     }
     return 0;
 }
+
+/* Per-item flank walk steps up to the label-independent end, as (compute
+ * pixel, moved-to pixel) pairs with consecutive duplicates merged; used by
+ * tests to check the dependency-round formulation of fix_*_flanks.  Writes at
+ * most cap pairs per item; returns the total number of pairs. */
+uint64_t oracle_flank_paths(const slm_params* p, const float* seeds, uint32_t n,
+                            const uint8_t* mask, const float* uv, const uint32_t* mapping,
+                            uint32_t cap, uint32_t* counts, uint32_t* pairs) {
+    uint64_t total = 0;
+    for (uint32_t g = 0; g < n; ++g) {
+        v2 vec = seed_at(seeds, g);
+        uint32_t idx = pixel_of(vec, p), n_steps = 0, k = 0, lq = 0xffffffffu, lr = 0xffffffffu;
+        float dt = p->dt_max;
+        while (!mask[idx] && ((~mapping[idx]) & p->is_thinchannel) && n_steps < p->max_n_steps) {
+            rk_t s = rk_compute(vec, dt, uv, p, &idx);
+            const uint32_t q = idx;
+            const int stuck = seg_step(&vec, &idx, &dt, &n_steps, uv, p, 0, &s);
+            if (q != lq || idx != lr) {
+                lq = q; lr = idx;
+                if (k < cap) { pairs[2 * ((size_t)g * cap + k)] = q; pairs[2 * ((size_t)g * cap + k) + 1] = idx; }
+                k++;
+            }
+            if (stuck) break;
+        }
+        counts[g] = k;
+        total += k;
+    }
+    return total;
+}

@@ -55,6 +55,22 @@ SIGNATURES = {
     "slm_pdf_univariate": (ctypes.c_int, [_P, _P, _P, _P]),
     "slm_pdf_bivariate_rows": (ctypes.c_int, [_P, _P, _P, _P]),
     "slm_pdf_bivariate_cols": (ctypes.c_int, [_P, _P, _P, _P]),
+    "slm_connect_channels": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P]),
+    "slm_map_channel_heads": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P]),
+    "slm_prune_channel_heads": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P]),
+    "slm_count_downchannels_workspace": (ctypes.c_size_t, [_U, ctypes.c_uint64]),
+    "slm_count_downchannels": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P, ctypes.c_size_t, _P, _P]),
+    "slm_flag_downchannels": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P]),
+    "slm_label_confluences": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "slm_segment_downchannels": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "slm_segment_hillslopes": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "slm_subsegment_channel_edges": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "slm_subsegment_flanks": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "slm_fix_flanks_workspace": (ctypes.c_size_t, [_U, _U, ctypes.c_uint64]),
+    "slm_fix_right_flanks": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P, _P, ctypes.c_size_t, _P, _P]),
+    "slm_fix_left_flanks": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P, _P, ctypes.c_size_t, _P, _P]),
+    "slm_hillslopes": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P]),
+    "slm_hillslope_lengths": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P]),
 }
 
 _lock = threading.Lock()

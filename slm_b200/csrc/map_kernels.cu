@@ -1,0 +1,912 @@
+// map_kernels.cu -- channel, segment and hillslope mapping kernels.
+//
+// Each reference mapping kernel (opencl/connect.cl, channelheads.cl,
+// countlink.cl, label.cl, segment.cl, hillslopes.cl, lengths.cl) becomes one
+// entry point computing the same result as the reference's work-items run one
+// after another in ascending global id -- the pinned schedule, since several
+// reference kernels race (atomic_xchg last-writer-wins, reads of values other
+// work-items write) and have no other defined result.
+//
+// Order-independent kernels (every cross-item read is of bits the kernel never
+// writes, or every write is an idempotent atomic OR/AND) run one thread per
+// seed: connect_channels, map_channel_heads, label_confluences, hillslopes,
+// segment_hillslopes, subsegment_channel_edges, subsegment_flanks,
+// hillslope_lengths.
+//
+// Order-dependent kernels:
+//   count_downchannels  the RK walk from each head is independent of the
+//       shared state except for where it stops, so every head's sequence of
+//       newly entered pixels is traced in parallel (k_count_paths), then one
+//       thread replays the integer updates (count, link, flags) head by head
+//       with the reference's early stop (k_count_replay);
+//   flag_downchannels, segment_downchannels, prune_channel_heads  link walks
+//       and neighbour checks with no RK arithmetic, replayed in seed order by
+//       one thread;
+//   fix_right_flanks, fix_left_flanks  every work-item writes only its own
+//       pixel's label and reads labels along its RK path, so its result depends
+//       only on the final labels of lower-index items owning pixels on that
+//       path.  Paths are traced in parallel (k_flank_paths, compressed to the
+//       steps whose (compute pixel, moved-to pixel) pair changes), then items
+//       are resolved in rounds (k_flank_round): an item resolves once every
+//       lower-index owner it reads has resolved in an earlier round.  The
+//       lowest unresolved item always can, so the rounds end.
+//
+// Every loop is bounded; a cap that the reference would exceed (it would loop
+// on) or a neighbour index outside the grid sets a bit in the caller's status
+// word instead of trapping.
+#include <cstring>
+#include "capi_util.cuh"
+#include "trace_common.cuh"
+
+#define MAP_ST_CAP 1u
+#define MAP_ST_OOB 2u
+#define MAP_LOOP_CAP (1u << 26)
+#define CONNECT_REC_MAX 256
+#define NO_OWNER 0xffffffffu
+
+namespace slm {
+
+__device__ __forceinline__ Vec2 seed_vec(const float2* __restrict__ seeds, uint32_t g) {
+    const float2 s = seeds[g];
+    return Vec2{s.x, s.y};
+}
+
+struct Move { float err, dl; bool stuck; };
+
+// the shared tail of every *_runge_kutta_step (rungekutta.cl:289-296 ...):
+// error, length, first-order fallback when stuck, move to the new point
+__device__ __forceinline__ Move rk_move(const Step& s, Vec2& vec, uint32_t& idx, const slm_params& p) {
+    Move m;
+    m.err = vlen(__fdiv_rn(s.d2.x - s.d1.x, p.grid_scale), __fdiv_rn(s.d2.y - s.d1.y, p.grid_scale));
+    Vec2 next = s.next;
+    m.dl = vlen(s.d2.x, s.d2.y);
+    if (m.dl < p.integration_halt_threshold) {
+        next.x = vec.x + s.d1.x;
+        next.y = vec.y + s.d1.y;
+        m.dl = vlen(s.d1.x, s.d1.y);
+    }
+    vec = next;
+    idx = pixel_of(next, p);
+    m.stuck = m.dl < p.integration_halt_threshold;
+    return m;
+}
+
+__device__ __forceinline__ Step rk_plain(Vec2 a, float dt, const float2* __restrict__ uv,
+                                         const slm_params& p) {
+    uint32_t rng = 0;
+    return rk_step<2, false>(a, dt, rng, uv, p);
+}
+
+// ------------------------------------------------------------------ connect
+__global__ void k_connect_channels(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
+                                   const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
+                                   uint32_t* mapping, uint32_t* status) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    int8_t rec[2 * CONNECT_REC_MAX];
+    const uint32_t cap_rec = p.interchannel_max_n_steps;
+    const float res = (float)p.trajectory_resolution;
+    const Vec2 start = seed_vec(seeds, g);
+    Vec2 vec = start, prev = start;
+    float dt = p.dt_max;
+    uint32_t idx = pixel_of(vec, p), prev_idx = idx, n_steps = 0, guard = 0;
+    while (prev_idx == idx && !mask[idx] && n_steps != p.max_n_steps) {
+        if (++guard > MAP_LOOP_CAP) { atomicOr(status, MAP_ST_CAP); break; }
+        const Step s = rk_plain(vec, dt, uv, p);
+        idx = s.idx;
+        if (!mask[idx]) {
+            const Move m = rk_move(s, vec, idx, p);
+            if (!m.stuck) dt = next_dt(dt, m.err, p);
+            if (n_steps < cap_rec) {
+                rec[2 * n_steps] = cvt_i8((vec.x - prev.x) * res);
+                rec[2 * n_steps + 1] = cvt_i8((vec.y - prev.y) * res);
+            }
+            n_steps++;
+            if (!m.stuck) prev = vec;
+        }
+    }
+    guard = 0;
+    while ((mapping[idx] & p.is_channel) == 0 && !mask[idx] && n_steps != p.interchannel_max_n_steps) {
+        if (++guard > MAP_LOOP_CAP) { atomicOr(status, MAP_ST_CAP); break; }
+        const Step s = rk_plain(vec, dt, uv, p);
+        idx = s.idx;
+        if (!mask[idx]) {
+            const Move m = rk_move(s, vec, idx, p);
+            if (!m.stuck) dt = next_dt(dt, m.err, p);
+            if (n_steps < cap_rec) {
+                rec[2 * n_steps] = cvt_i8((vec.x - prev.x) * res);
+                rec[2 * n_steps + 1] = cvt_i8((vec.y - prev.y) * res);
+            }
+            n_steps++;
+            if (!m.stuck) prev = vec;
+        }
+    }
+    if (n_steps > 2 && n_steps < p.interchannel_max_n_steps) {
+        vec = start;
+        idx = pixel_of(vec, p);
+        uint32_t step = 0;
+        while (!mask[idx] && step < n_steps - 1) {
+            if (*(volatile uint32_t*)(mapping + idx) == 0u) atomicOr(mapping + idx, p.is_interchannel);
+            vec.x = vec.x + __fdiv_rn((float)rec[2 * step], res);
+            vec.y = vec.y + __fdiv_rn((float)rec[2 * step + 1], res);
+            idx = pixel_of(vec, p);
+            step++;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ channel heads
+__global__ void k_map_channel_heads(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
+                                    const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
+                                    uint32_t* mapping) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    Vec2 vec = seed_vec(seeds, g);
+    float dt = p.dt_max;
+    uint32_t idx = pixel_of(vec, p), prev_idx = idx, n_steps = 0;
+    while (prev_idx == idx && !mask[idx] && n_steps < p.max_n_steps) {
+        const Step s = rk_plain(vec, dt, uv, p);
+        idx = s.idx;
+        const Move m = rk_move(s, vec, idx, p);
+        n_steps++;
+        dt = next_dt(dt, m.err, p);
+    }
+    if (n_steps >= p.max_n_steps) return;
+    if (!mask[idx]) {
+        idx = pixel_of(vec, p);
+        const uint32_t here = *(volatile uint32_t*)(mapping + idx);
+        const uint32_t before = *(volatile uint32_t*)(mapping + prev_idx);
+        if (((~here) & p.is_thinchannel) || (before & p.is_thinchannel))
+            atomicAnd(mapping + idx, ~p.is_channelhead);
+    }
+}
+
+// neighbour offsets in the reference's check order N, S, E, W, NE, SE, NW, SW
+__constant__ float c_nbr[8][2] = {{0, 1}, {0, -1}, {1, 0}, {-1, 0}, {1, 1}, {1, -1}, {-1, 1}, {-1, -1}};
+
+__global__ void k_prune_channel_heads(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
+                                      uint32_t* mapping) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    for (uint32_t g = 0; g < n; ++g) {
+        const Vec2 vec = seed_vec(seeds, g);
+        uint32_t flag = 0;
+        for (int k = 0; k < 8; ++k) {
+            const Vec2 nb{vec.x + c_nbr[k][0], vec.y + c_nbr[k][1]};
+            flag += (mapping[pixel_of(nb, p)] & p.is_thinchannel) != 0u;
+        }
+        if (flag != 1u) {
+            const uint32_t idx = pixel_of(vec, p);
+            mapping[idx] &= ~p.is_channelhead;
+            if (flag == 0u) mapping[idx] &= ~(p.is_thinchannel | p.is_channel);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ count / flag
+// Phase A of count_downchannels: the pixels each head's walk enters, in order,
+// up to the walk's state-independent end; with events == nullptr only counts.
+__global__ void k_count_paths(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
+                              const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
+                              u64* __restrict__ n_events, const u64* __restrict__ offsets,
+                              uint32_t* __restrict__ events, uint32_t* __restrict__ tail_idx) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    Vec2 vec = seed_vec(seeds, g);
+    float dt = p.dt_max;
+    uint32_t idx = pixel_of(vec, p), prev_idx = idx, n_steps = 0;
+    const uint32_t lim = 1000u * p.max_n_steps;
+    u64 k = 0;
+    uint32_t* out = events ? events + offsets[g] : nullptr;
+    while (!mask[idx] && n_steps < lim) {
+        const Step s = rk_plain(vec, dt, uv, p);
+        idx = s.idx;
+        const Move m = rk_move(s, vec, idx, p);
+        if (m.stuck) break;
+        dt = next_dt(dt, m.err, p);
+        n_steps++;
+        if (prev_idx != idx) {
+            if (out) out[k] = idx;
+            k++;
+            prev_idx = idx;
+        }
+    }
+    if (events) tail_idx[g] = idx;
+    else n_events[g] = k;
+}
+
+// Phase B: the integer updates in seed order (countlink.cl:56-112).
+__global__ void k_count_replay(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
+                               const u64* __restrict__ offsets, const uint32_t* __restrict__ events,
+                               const uint32_t* __restrict__ tail_idx, uint32_t* mapping,
+                               uint32_t* count, uint32_t* link) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    for (uint32_t g = 0; g < n; ++g) {
+        const uint32_t head = pixel_of(seed_vec(seeds, g), p);
+        uint32_t counter = 1, prev = head, last = tail_idx[g];
+        count[head] = counter++;
+        for (u64 k = offsets[g]; k < offsets[g + 1]; ++k) {
+            const uint32_t e = events[k];
+            mapping[e] &= ~p.is_channelhead;
+            mapping[e] |= p.is_thinchannel;
+            link[prev] = e;
+            if (++counter < count[e]) { last = e; break; }
+            count[e] = counter;
+            prev = e;
+        }
+        link[prev] = last;
+    }
+}
+
+__global__ void k_flag_downchannels(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
+                                    const uint8_t* __restrict__ mask, uint32_t* mapping,
+                                    uint32_t* count, const uint32_t* __restrict__ link) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const uint32_t lim = 1000u * p.max_n_steps;
+    for (uint32_t g = 0; g < n; ++g) {
+        const uint32_t head = pixel_of(seed_vec(seeds, g), p);
+        uint32_t idx = head, prev_idx = idx + 1u, counter = 1;
+        count[idx] = counter;
+        mapping[idx] |= p.is_thinchannel;
+        while (!mask[idx] && prev_idx != idx && counter < lim) {
+            prev_idx = idx;
+            idx = link[idx];
+            counter++;
+            if (!mask[idx]) {
+                if (((mapping[idx] & p.is_minorinflow) > 0u || (counter == 2u && count[idx] > 2u))
+                    && counter < 20u)
+                    mapping[head] &= ~p.is_channelhead;
+                mapping[idx] |= p.is_thinchannel;
+                if (counter >= count[idx]) count[idx] = counter;
+            } else {
+                break;
+            }
+        }
+        if (!mask[prev_idx] && counter < lim) mapping[prev_idx] |= p.is_channeltail;
+    }
+}
+
+// ------------------------------------------------------------------ label
+__global__ void k_label_confluences(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
+                                    const uint8_t* __restrict__ mask, const float* __restrict__ slt,
+                                    uint32_t* mapping, const uint32_t* __restrict__ count,
+                                    const uint32_t* __restrict__ link) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const Vec2 vec = seed_vec(seeds, g);
+    const uint32_t idx = pixel_of(vec, p);
+    uint32_t inflows[8], equal_dom[8], n_in = 0, n_eq = 0, dom_idx = 0;
+    float dom_slt = -3.40282347e+38f;
+    for (int k = 0; k < 8; ++k) {
+        const Vec2 nb{vec.x + c_nbr[k][0], vec.y + c_nbr[k][1]};
+        const uint32_t ni = pixel_of(nb, p);
+        if (!mask[ni] && (*(volatile uint32_t*)(mapping + ni) & p.is_thinchannel) && link[ni] == idx)
+            inflows[n_in++] = ni;
+    }
+    if (n_in > 1) {
+        atomicOr(mapping + idx, p.is_majorconfluence);
+        for (uint32_t i = 0; i < n_in; ++i) {
+            if (count[idx] != count[inflows[i]] + 1u) {
+                atomicOr(mapping + inflows[i], p.is_minorinflow);
+            } else {
+                equal_dom[n_eq++] = inflows[i];
+                if (slt[inflows[i]] > dom_slt) {
+                    dom_idx = inflows[i];
+                    dom_slt = slt[dom_idx];
+                }
+            }
+        }
+        for (uint32_t i = 0; i < n_eq; ++i)
+            atomicOr(mapping + equal_dom[i], equal_dom[i] == dom_idx ? p.is_majorinflow : p.is_minorinflow);
+    }
+}
+
+// ------------------------------------------------------------------ segments
+__global__ void k_segment_downchannels(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
+                                       const uint8_t* __restrict__ mask, uint32_t* mapping,
+                                       const uint32_t* __restrict__ count,
+                                       const uint32_t* __restrict__ link, uint32_t* label,
+                                       uint32_t* status) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    for (uint32_t g = 0; g < n; ++g) {
+        uint32_t prev_idx = pixel_of(seed_vec(seeds, g), p), seg_counter = 0;
+        uint32_t seg_label = prev_idx;
+        label[prev_idx] = seg_label;
+        mapping[prev_idx] |= p.is_subsegmenthead;
+        uint32_t idx = link[prev_idx], guard = 0;
+        while (!mask[idx] && prev_idx != idx && (mapping[idx] & p.is_subsegmenthead) == 0u) {
+            if (++guard > MAP_LOOP_CAP) { *status |= MAP_ST_CAP; break; }
+            if (count[idx] >= seg_counter + p.segmentation_threshold / 2u) {
+                seg_label = idx;
+                seg_counter = count[idx] + p.segmentation_threshold;
+                mapping[idx] |= p.is_subsegmenthead;
+            }
+            label[idx] = seg_label;
+            prev_idx = idx;
+            idx = link[idx];
+        }
+    }
+}
+
+// segment_runge_kutta_step (rungekutta.cl:435-459): n_steps++ always, stuck ends
+__device__ __forceinline__ bool seg_move(const Step& s, Vec2& vec, uint32_t& idx, float& dt,
+                                         uint32_t& n_steps, const slm_params& p) {
+    const Move m = rk_move(s, vec, idx, p);
+    n_steps++;
+    if (m.stuck) return true;
+    dt = next_dt(dt, m.err, p);
+    return false;
+}
+
+__global__ void k_segment_hillslopes(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
+                                     const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
+                                     const uint32_t* __restrict__ mapping, uint32_t* label) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    Vec2 vec = seed_vec(seeds, g);
+    uint32_t idx = pixel_of(vec, p), n_steps = 0;
+    const uint32_t h = idx;
+    float dt = p.dt_max;
+    while (!mask[idx] && ((~mapping[idx]) & p.is_thinchannel) && n_steps < p.max_n_steps) {
+        const Step s = rk_plain(vec, dt, uv, p);
+        idx = s.idx;
+        if (seg_move(s, vec, idx, dt, n_steps, p)) break;
+    }
+    if (mapping[idx] & p.is_thinchannel) label[h] = label[idx];
+}
+
+__device__ __forceinline__ uint32_t rotate_left(uint32_t px, uint32_t py, int8_t& dx, int8_t& dy,
+                                                uint32_t nyp) {
+    const int8_t rdx = (int8_t)(dx - dy), rdy = (int8_t)(dx + dy);
+    const int adx = rdx < 0 ? -rdx : rdx, ady = rdy < 0 ? -rdy : rdy;
+    const int8_t cx = (int8_t)(adx < 1 ? 1 : (adx > 2 ? 2 : adx));
+    const int8_t cy = (int8_t)(ady < 1 ? 1 : (ady > 2 ? 2 : ady));
+    dx = (int8_t)(rdx / cx);
+    dy = (int8_t)(rdy / cy);
+    return (px + (uint32_t)(int32_t)dx) * nyp + (py + (uint32_t)(int32_t)dy);
+}
+
+__global__ void k_subsegment_channel_edges(const slm_params p, uint32_t n,
+                                           const float2* __restrict__ seeds,
+                                           const uint8_t* __restrict__ mask, uint32_t* mapping,
+                                           const uint32_t* __restrict__ link, uint32_t* label,
+                                           uint32_t* status) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const uint32_t nyp = p.ny_padded, nxy = p.nxy_padded;
+    uint32_t prev_idx = pixel_of(seed_vec(seeds, g), p), n_steps = 0;
+    uint32_t idx = link[prev_idx];
+    while (prev_idx != idx && n_steps++ < p.max_n_steps) {
+        if (idx >= nxy) { atomicOr(status, MAP_ST_OOB); break; }
+        const uint32_t px = prev_idx / nyp, py = prev_idx % nyp;
+        const uint32_t x = idx / nyp, y = idx % nyp;
+        uint32_t n_turns = 0, left_idx = idx;
+        int8_t dx = (int8_t)(uint8_t)((x - px) & 0xffu), dy = (int8_t)(uint8_t)((y - py) & 0xffu);
+        bool do_left = true;
+        while (left_idx != prev_idx && ++n_turns <= 7u) {
+            left_idx = rotate_left(px, py, dx, dy, nyp);
+            if (left_idx >= nxy) { atomicOr(status, MAP_ST_OOB); continue; }
+            // THINCHANNEL bits are never written by this kernel
+            if (n_turns >= 2u && !mask[left_idx] && (*(volatile uint32_t*)(mapping + left_idx) & p.is_thinchannel)) {
+                if (left_idx == link[idx]) do_left = false;
+                break;
+            }
+        }
+        if (do_left) {
+            n_turns = 0;
+            left_idx = idx;
+            dx = (int8_t)(uint8_t)((x - px) & 0xffu);
+            dy = (int8_t)(uint8_t)((y - py) & 0xffu);
+            while (left_idx != prev_idx && ++n_turns <= 4u) {
+                left_idx = rotate_left(px, py, dx, dy, nyp);
+                if (left_idx >= nxy) { atomicOr(status, MAP_ST_OOB); continue; }
+                if (n_turns >= 2u && !mask[left_idx]) {
+                    if (*(volatile uint32_t*)(mapping + left_idx) & p.is_thinchannel) break;
+                    atomicOr(mapping + left_idx, p.is_leftflank);
+                    atomicOr(label + left_idx, p.left_flank_addition);
+                }
+            }
+        }
+        prev_idx = idx;
+        idx = link[idx];
+        if (idx >= nxy) { atomicOr(status, MAP_ST_OOB); break; }
+        if (mask[idx] || (*(volatile uint32_t*)(mapping + prev_idx) & p.is_subsegmenthead)) break;
+    }
+}
+
+__global__ void k_subsegment_flanks(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
+                                    const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
+                                    const uint32_t* __restrict__ mapping, uint32_t* label) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    Vec2 vec = seed_vec(seeds, g);
+    uint32_t idx = pixel_of(vec, p), n_steps = 0;
+    const uint32_t h = idx;
+    float dt = p.dt_max;
+    while (!mask[idx] && ((~mapping[idx]) & p.is_leftflank) && ((~mapping[idx]) & p.is_thinchannel)
+           && n_steps < p.max_n_steps) {
+        const Step s = rk_plain(vec, dt, uv, p);
+        idx = s.idx;
+        if (seg_move(s, vec, idx, dt, n_steps, p)) break;
+    }
+    if (mapping[idx] & p.is_leftflank) label[h] |= p.left_flank_addition;
+}
+
+// ------------------------------------------------------------------ fix flanks
+__global__ void k_owner_map(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
+                            uint32_t* __restrict__ owner, uint32_t* __restrict__ hpix) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const uint32_t h = pixel_of(seed_vec(seeds, g), p);
+    hpix[g] = h;
+    owner[h] = g;
+}
+
+// Steps of a flank walk up to its label-independent end (mask, thin channel,
+// step cap, stuck), as (compute pixel, moved-to pixel) pairs; consecutive
+// equal pairs are stored once.  With pairs == nullptr only counts.
+__global__ void k_flank_paths(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
+                              const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
+                              const uint32_t* __restrict__ mapping, u64* __restrict__ n_pairs,
+                              const u64* __restrict__ offsets, uint2* __restrict__ pairs) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    Vec2 vec = seed_vec(seeds, g);
+    uint32_t idx = pixel_of(vec, p), n_steps = 0;
+    float dt = p.dt_max;
+    u64 k = 0;
+    uint2 last = make_uint2(NO_OWNER, NO_OWNER);
+    uint2* out = pairs ? pairs + offsets[g] : nullptr;
+    while (!mask[idx] && ((~mapping[idx]) & p.is_thinchannel) && n_steps < p.max_n_steps) {
+        const Step s = rk_plain(vec, dt, uv, p);
+        const uint32_t q = s.idx;
+        idx = q;
+        const bool stuck = seg_move(s, vec, idx, dt, n_steps, p);
+        if (q != last.x || idx != last.y) {
+            last = make_uint2(q, idx);
+            if (out) out[k] = last;
+            k++;
+        }
+        if (stuck) break;
+    }
+    if (!pairs) n_pairs[g] = k;
+}
+
+// The label of pixel q as flank item g sees it: item g's own running value if
+// q is g's pixel; the initial label if q has no owner or a higher-index owner;
+// the resolved label if its owner has a lower index and resolved in an
+// earlier round.  Returns false when that owner has not resolved yet.
+// Kept out of line: the inlined form gave wrong labels on sm_100a for a few
+// items of the 96x80 test case (tests/test_mapping_gpu.py), the out-of-line
+// form matches the oracle on every case.
+__device__ __noinline__ bool flank_read(uint32_t q, uint32_t g, uint32_t h, uint32_t lab_h,
+                                           uint32_t cur_round, const uint32_t* __restrict__ owner,
+                                           const uint32_t* __restrict__ label_init,
+                                           const uint32_t* label,
+                                           const uint32_t* resolved_round, uint32_t& out) {
+    if (q == h) { out = lab_h; return true; }
+    const uint32_t o = owner[q];
+    if (o == NO_OWNER || o > g) { out = label_init[q]; return true; }
+    const uint32_t r = ((volatile const uint32_t*)resolved_round)[o];
+    if (r == 0u || r >= cur_round) return false;
+    out = ((volatile const uint32_t*)label)[q];
+    return true;
+}
+
+// One resolution round of fix_right_flanks (side 0) or fix_left_flanks
+// (side 1) (segment.cl:441-504, 530-594).
+__global__ void k_flank_round(const slm_params p, uint32_t n, uint32_t side, uint32_t cur_round,
+                              const u64* __restrict__ offsets, const uint2* __restrict__ pairs,
+                              const uint32_t* __restrict__ hpix, const uint8_t* __restrict__ mask,
+                              const uint32_t* __restrict__ mapping, const uint32_t* __restrict__ owner,
+                              const uint32_t* __restrict__ label_init, uint32_t* label,
+                              uint32_t* resolved_round, uint32_t* n_resolved) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n || resolved_round[g] != 0u) return;
+    const uint32_t lfa = p.left_flank_addition;
+    const uint32_t thin = p.is_thinchannel;
+    const uint32_t h = hpix[g];
+    uint32_t lab_h = label_init[h];
+    uint32_t at = h, v = 0u;
+    const u64 k_end = offsets[g + 1];
+    for (u64 k = offsets[g]; k < k_end; ++k) {
+        if (!flank_read(at, g, h, lab_h, cur_round, owner, label_init, label, resolved_round, v)) return;
+        const bool flank_ok = side ? (v & lfa) != 0u : ((~v) & lfa) != 0u;
+        if (mask[at] || !flank_ok || (mapping[at] & thin)) break;
+        const uint2 e = pairs[k];
+        if (!flank_read(e.x, g, h, lab_h, cur_round, owner, label_init, label, resolved_round, v)) return;
+        if ((lab_h & ~lfa) != (v & ~lfa)) lab_h = v;
+        at = e.y;
+    }
+    if (!flank_read(at, g, h, lab_h, cur_round, owner, label_init, label, resolved_round, v)) return;
+    if ((lab_h & ~lfa) != (v & ~lfa)) lab_h = v;
+    flank_read(at, g, h, lab_h, cur_round, owner, label_init, label, resolved_round, v);
+    if (side) {
+        if (((~v) & lfa) && !(mapping[at] & thin)) lab_h &= ~lfa;
+    } else {
+        if (v & lfa) lab_h |= lfa;
+    }
+    label[h] = lab_h;
+    resolved_round[g] = cur_round;
+    atomicAdd(n_resolved, 1u);
+}
+
+// ------------------------------------------------------------------ hillslopes
+__global__ void k_hillslopes(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
+                             const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
+                             uint32_t* link) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    Vec2 vec = seed_vec(seeds, g);
+    float dt = p.dt_max;
+    uint32_t idx = pixel_of(vec, p), prev_idx = idx, n_steps = 0;
+    while (prev_idx == idx && !mask[idx] && n_steps < 100u * p.max_n_steps) {
+        prev_idx = idx;
+        const Step s = rk_plain(vec, dt, uv, p);
+        idx = s.idx;
+        const Move m = rk_move(s, vec, idx, p);
+        if (m.stuck) break;
+        dt = next_dt(dt, m.err, p);
+        n_steps++;
+    }
+    if (prev_idx != idx && !mask[idx]) link[prev_idx] = idx;
+}
+
+__global__ void k_hillslope_lengths(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
+                                    const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
+                                    const uint32_t* __restrict__ mapping, float* traj_length) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const uint32_t from_flag = p.do_measure_hsl_from_ridges ? p.is_ridge : p.is_midslope;
+    Vec2 vec = seed_vec(seeds, g);
+    uint32_t idx = pixel_of(vec, p), n_steps = 0;
+    float dt = p.dt_max, l = 0.0f;
+    bool moved_off = false;
+    while (((~mapping[idx]) & p.is_thinchannel) && n_steps < p.max_n_steps) {
+        const Step s = rk_plain(vec, dt, uv, p);
+        idx = s.idx;
+        if (mask[idx]) return;
+        if (!moved_off && ((~mapping[idx]) & from_flag)) {
+            moved_off = true;
+        } else if (moved_off && (mapping[idx] & from_flag)) {
+            return;
+        }
+        const Move m = rk_move(s, vec, idx, p);
+        l = l + m.dl;
+        n_steps++;
+        if (m.stuck) return;
+        dt = next_dt(dt, m.err, p);
+    }
+    if (mapping[idx] & p.is_thinchannel) traj_length[g] = l * p.pixel_size;
+}
+
+// ------------------------------------------------------------------ scan
+// exclusive prefix sum of n uint64 counts into out[0..n] (out[n] = total);
+// one block walks the array in chunks of its size.
+__global__ void k_exclusive_scan(const u64* __restrict__ in, uint32_t n, u64* __restrict__ out) {
+    __shared__ u64 buf[1024];
+    u64 carry = 0;
+    for (uint32_t base = 0; base < n; base += blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const u64 v = i < n ? in[i] : 0ull;
+        buf[threadIdx.x] = v;
+        __syncthreads();
+        for (uint32_t off = 1; off < blockDim.x; off <<= 1) {
+            const u64 t = threadIdx.x >= off ? buf[threadIdx.x - off] : 0ull;
+            __syncthreads();
+            buf[threadIdx.x] += t;
+            __syncthreads();
+        }
+        if (i < n) out[i] = carry + buf[threadIdx.x] - v;
+        const u64 tot = buf[blockDim.x - 1];
+        __syncthreads();
+        carry += tot;
+    }
+    if (threadIdx.x == 0) out[n] = carry;
+}
+
+}  // namespace slm
+
+using namespace slm;
+
+static int map_checks(const slm_params* p, uint32_t n, const void* seeds) {
+    SLM_REQUIRE(p != nullptr, "params is NULL");
+    SLM_REQUIRE(p->nx_padded >= 2 && p->ny_padded >= 2 &&
+                (u64)p->nx_padded * p->ny_padded == p->nxy_padded, "bad grid size");
+    SLM_REQUIRE(p->trajectory_resolution > 0, "trajectory_resolution is 0");
+    SLM_REQUIRE(n == 0 || (seeds && aligned(seeds, 8)), "seed_point NULL or misaligned");
+    return SLM_OK;
+}
+
+static inline unsigned blocks_for(uint32_t n, unsigned b) { return (n + b - 1) / b; }
+#define F2(x) reinterpret_cast<const float2*>(x)
+#define SS (cudaStream_t) stream
+
+extern "C" {
+
+int slm_connect_channels(const slm_params* p, uint32_t n, const float* seed_point, const uint8_t* mask,
+                         const float* uv, uint32_t* mapping, uint32_t* status, void* stream) {
+    clear_error();
+    int rc = map_checks(p, n, seed_point);
+    if (rc) return rc;
+    SLM_REQUIRE(p->interchannel_max_n_steps <= CONNECT_REC_MAX,
+                "interchannel_max_n_steps %u above the supported %d", p->interchannel_max_n_steps,
+                CONNECT_REC_MAX);
+    SLM_REQUIRE(status, "status word is NULL");
+    SLM_CUDA(cudaMemsetAsync(status, 0, sizeof(uint32_t), SS));
+    if (n == 0) return SLM_OK;
+    k_connect_channels<<<blocks_for(n, 128), 128, 0, SS>>>(*p, n, F2(seed_point), mask, F2(uv), mapping, status);
+    SLM_LAUNCHED("k_connect_channels");
+    return SLM_OK;
+}
+
+int slm_map_channel_heads(const slm_params* p, uint32_t n, const float* seed_point, const uint8_t* mask,
+                          const float* uv, uint32_t* mapping, void* stream) {
+    clear_error();
+    int rc = map_checks(p, n, seed_point);
+    if (rc) return rc;
+    if (n == 0) return SLM_OK;
+    k_map_channel_heads<<<blocks_for(n, 128), 128, 0, SS>>>(*p, n, F2(seed_point), mask, F2(uv), mapping);
+    SLM_LAUNCHED("k_map_channel_heads");
+    return SLM_OK;
+}
+
+int slm_prune_channel_heads(const slm_params* p, uint32_t n, const float* seed_point, const uint8_t* mask,
+                            const float* uv, uint32_t* mapping, void* stream) {
+    (void)mask; (void)uv;
+    clear_error();
+    int rc = map_checks(p, n, seed_point);
+    if (rc) return rc;
+    if (n == 0) return SLM_OK;
+    k_prune_channel_heads<<<1, 1, 0, SS>>>(*p, n, F2(seed_point), mapping);
+    SLM_LAUNCHED("k_prune_channel_heads");
+    return SLM_OK;
+}
+
+size_t slm_count_downchannels_workspace(uint32_t n_seeds, uint64_t n_events) {
+    return (size_t)(2 * (size_t)n_seeds + 1) * sizeof(u64) + (size_t)n_seeds * sizeof(uint32_t)
+         + (size_t)n_events * sizeof(uint32_t) + 256;
+}
+
+int slm_count_downchannels(const slm_params* p, uint32_t n, const float* seed_point, const uint8_t* mask,
+                           const float* uv, uint32_t* mapping, uint32_t* count, uint32_t* link,
+                           void* workspace, size_t workspace_bytes, uint64_t* required_bytes,
+                           void* stream) {
+    clear_error();
+    int rc = map_checks(p, n, seed_point);
+    if (rc) return rc;
+    if (n == 0) return SLM_OK;
+    SLM_REQUIRE(workspace && workspace_bytes >= slm_count_downchannels_workspace(n, 0),
+                "workspace below the minimum %zu bytes", slm_count_downchannels_workspace(n, 0));
+    u64* n_events = reinterpret_cast<u64*>(workspace);
+    u64* offsets = n_events + n;
+    uint32_t* tails = reinterpret_cast<uint32_t*>(offsets + n + 1);
+    uint32_t* events = tails + n;
+    k_count_paths<<<blocks_for(n, 128), 128, 0, SS>>>(*p, n, F2(seed_point), mask, F2(uv), n_events,
+                                                     nullptr, nullptr, nullptr);
+    SLM_LAUNCHED("k_count_paths");
+    k_exclusive_scan<<<1, 1024, 0, SS>>>(n_events, n, offsets);
+    SLM_LAUNCHED("k_exclusive_scan");
+    u64 total = 0;
+    SLM_CUDA(cudaMemcpyAsync(&total, offsets + n, sizeof(u64), cudaMemcpyDeviceToHost, SS));
+    SLM_CUDA(cudaStreamSynchronize(SS));
+    const size_t need = slm_count_downchannels_workspace(n, total);
+    if (required_bytes) *required_bytes = need;
+    if (need > workspace_bytes) {
+        set_error("count_downchannels needs %zu workspace bytes (%llu path events)", need,
+                  (unsigned long long)total);
+        return SLM_ERR_CAPACITY;
+    }
+    k_count_paths<<<blocks_for(n, 128), 128, 0, SS>>>(*p, n, F2(seed_point), mask, F2(uv), nullptr,
+                                                     offsets, events, tails);
+    SLM_LAUNCHED("k_count_paths");
+    k_count_replay<<<1, 1, 0, SS>>>(*p, n, F2(seed_point), offsets, events, tails, mapping, count, link);
+    SLM_LAUNCHED("k_count_replay");
+    return SLM_OK;
+}
+
+int slm_flag_downchannels(const slm_params* p, uint32_t n, const float* seed_point, const uint8_t* mask,
+                          const float* uv, uint32_t* mapping, uint32_t* count, const uint32_t* link,
+                          void* stream) {
+    (void)uv;
+    clear_error();
+    int rc = map_checks(p, n, seed_point);
+    if (rc) return rc;
+    if (n == 0) return SLM_OK;
+    k_flag_downchannels<<<1, 1, 0, SS>>>(*p, n, F2(seed_point), mask, mapping, count, link);
+    SLM_LAUNCHED("k_flag_downchannels");
+    return SLM_OK;
+}
+
+int slm_label_confluences(const slm_params* p, uint32_t n, const float* seed_point, const uint8_t* mask,
+                          const float* uv, const float* slt, uint32_t* mapping, const uint32_t* count,
+                          const uint32_t* link, void* stream) {
+    (void)uv;
+    clear_error();
+    int rc = map_checks(p, n, seed_point);
+    if (rc) return rc;
+    if (n == 0) return SLM_OK;
+    k_label_confluences<<<blocks_for(n, 128), 128, 0, SS>>>(*p, n, F2(seed_point), mask, slt, mapping,
+                                                           count, link);
+    SLM_LAUNCHED("k_label_confluences");
+    return SLM_OK;
+}
+
+int slm_segment_downchannels(const slm_params* p, uint32_t n, const float* seed_point,
+                             const uint8_t* mask, const float* uv, uint32_t* mapping,
+                             const uint32_t* count, const uint32_t* link, uint32_t* label,
+                             uint32_t* status, void* stream) {
+    (void)uv;
+    clear_error();
+    int rc = map_checks(p, n, seed_point);
+    if (rc) return rc;
+    SLM_REQUIRE(status, "status word is NULL");
+    SLM_CUDA(cudaMemsetAsync(status, 0, sizeof(uint32_t), SS));
+    if (n == 0) return SLM_OK;
+    k_segment_downchannels<<<1, 1, 0, SS>>>(*p, n, F2(seed_point), mask, mapping, count, link, label,
+                                            status);
+    SLM_LAUNCHED("k_segment_downchannels");
+    return SLM_OK;
+}
+
+int slm_segment_hillslopes(const slm_params* p, uint32_t n, const float* seed_point, const uint8_t* mask,
+                           const float* uv, const uint32_t* mapping, const uint32_t* count,
+                           const uint32_t* link, uint32_t* label, void* stream) {
+    (void)count; (void)link;
+    clear_error();
+    int rc = map_checks(p, n, seed_point);
+    if (rc) return rc;
+    if (n == 0) return SLM_OK;
+    k_segment_hillslopes<<<blocks_for(n, 128), 128, 0, SS>>>(*p, n, F2(seed_point), mask, F2(uv), mapping,
+                                                            label);
+    SLM_LAUNCHED("k_segment_hillslopes");
+    return SLM_OK;
+}
+
+int slm_subsegment_channel_edges(const slm_params* p, uint32_t n, const float* seed_point,
+                                 const uint8_t* mask, const float* uv, uint32_t* mapping,
+                                 const uint32_t* channel_label, const uint32_t* link, uint32_t* label,
+                                 uint32_t* status, void* stream) {
+    (void)uv; (void)channel_label;
+    clear_error();
+    int rc = map_checks(p, n, seed_point);
+    if (rc) return rc;
+    SLM_REQUIRE(status, "status word is NULL");
+    SLM_CUDA(cudaMemsetAsync(status, 0, sizeof(uint32_t), SS));
+    if (n == 0) return SLM_OK;
+    k_subsegment_channel_edges<<<blocks_for(n, 128), 128, 0, SS>>>(*p, n, F2(seed_point), mask, mapping,
+                                                                  link, label, status);
+    SLM_LAUNCHED("k_subsegment_channel_edges");
+    return SLM_OK;
+}
+
+int slm_subsegment_flanks(const slm_params* p, uint32_t n, const float* seed_point, const uint8_t* mask,
+                          const float* uv, const uint32_t* mapping, const uint32_t* channel_label,
+                          const uint32_t* link, uint32_t* label, void* stream) {
+    (void)channel_label; (void)link;
+    clear_error();
+    int rc = map_checks(p, n, seed_point);
+    if (rc) return rc;
+    if (n == 0) return SLM_OK;
+    k_subsegment_flanks<<<blocks_for(n, 128), 128, 0, SS>>>(*p, n, F2(seed_point), mask, F2(uv), mapping,
+                                                           label);
+    SLM_LAUNCHED("k_subsegment_flanks");
+    return SLM_OK;
+}
+
+size_t slm_fix_flanks_workspace(uint32_t n_seeds, uint32_t nxy_padded, uint64_t n_pairs) {
+    return (size_t)(2 * (size_t)n_seeds + 1) * sizeof(u64) + (size_t)n_seeds * 2 * sizeof(uint32_t)
+         + (size_t)nxy_padded * 2 * sizeof(uint32_t) + sizeof(uint32_t) + 256
+         + (size_t)n_pairs * sizeof(uint2);
+}
+
+static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, const uint8_t* mask,
+                      const float* uv, const uint32_t* mapping, uint32_t* label, void* workspace,
+                      size_t workspace_bytes, uint64_t* required_bytes, void* stream, bool left) {
+    clear_error();
+    int rc = map_checks(p, n, seed_point);
+    if (rc) return rc;
+    if (n == 0) return SLM_OK;
+    const uint32_t nxy = p->nxy_padded;
+    SLM_REQUIRE(workspace && workspace_bytes >= slm_fix_flanks_workspace(n, nxy, 0),
+                "workspace below the minimum %zu bytes", slm_fix_flanks_workspace(n, nxy, 0));
+    u64* n_pairs = reinterpret_cast<u64*>(workspace);
+    u64* offsets = n_pairs + n;
+    uint32_t* hpix = reinterpret_cast<uint32_t*>(offsets + n + 1);
+    uint32_t* resolved = hpix + n;
+    uint32_t* owner = resolved + n;
+    uint32_t* label_init = owner + nxy;
+    uint32_t* n_resolved = label_init + nxy;
+    uintptr_t pa = reinterpret_cast<uintptr_t>(n_resolved + 1);
+    pa = (pa + 15) & ~(uintptr_t)15;
+    uint2* pairs = reinterpret_cast<uint2*>(pa);
+    k_flank_paths<<<blocks_for(n, 128), 128, 0, SS>>>(*p, n, F2(seed_point), mask, F2(uv), mapping,
+                                                     n_pairs, nullptr, nullptr);
+    SLM_LAUNCHED("k_flank_paths");
+    k_exclusive_scan<<<1, 1024, 0, SS>>>(n_pairs, n, offsets);
+    SLM_LAUNCHED("k_exclusive_scan");
+    u64 total = 0;
+    SLM_CUDA(cudaMemcpyAsync(&total, offsets + n, sizeof(u64), cudaMemcpyDeviceToHost, SS));
+    SLM_CUDA(cudaStreamSynchronize(SS));
+    const size_t need = slm_fix_flanks_workspace(n, nxy, total);
+    if (required_bytes) *required_bytes = need;
+    if (need > workspace_bytes) {
+        set_error("fix flanks needs %zu workspace bytes (%llu path steps)", need, (unsigned long long)total);
+        return SLM_ERR_CAPACITY;
+    }
+    k_flank_paths<<<blocks_for(n, 128), 128, 0, SS>>>(*p, n, F2(seed_point), mask, F2(uv), mapping,
+                                                     nullptr, offsets, pairs);
+    SLM_LAUNCHED("k_flank_paths");
+    SLM_CUDA(cudaMemsetAsync(owner, 0xff, (size_t)nxy * sizeof(uint32_t), SS));
+    SLM_CUDA(cudaMemsetAsync(resolved, 0, (size_t)n * sizeof(uint32_t), SS));
+    SLM_CUDA(cudaMemcpyAsync(label_init, label, (size_t)nxy * sizeof(uint32_t), cudaMemcpyDeviceToDevice, SS));
+    k_owner_map<<<blocks_for(n, 256), 256, 0, SS>>>(*p, n, F2(seed_point), owner, hpix);
+    SLM_LAUNCHED("k_owner_map");
+    uint32_t done = 0;
+    for (uint32_t round = 1; done < n; ++round) {
+        if (round > n + 1) {
+            set_error("fix flanks did not resolve within %u rounds", n + 1);
+            return SLM_ERR_ITERATION_CAP;
+        }
+        SLM_CUDA(cudaMemsetAsync(n_resolved, 0, sizeof(uint32_t), SS));
+        k_flank_round<<<blocks_for(n, 256), 256, 0, SS>>>(*p, n, left ? 1u : 0u, round, offsets, pairs, hpix, mask,
+                                                         mapping, owner, label_init, label, resolved,
+                                                         n_resolved);
+        SLM_LAUNCHED("k_flank_round");
+        uint32_t newly = 0;
+        SLM_CUDA(cudaMemcpyAsync(&newly, n_resolved, sizeof(uint32_t), cudaMemcpyDeviceToHost, SS));
+        SLM_CUDA(cudaStreamSynchronize(SS));
+        if (newly == 0) {
+            set_error("fix flanks round %u resolved nothing", round);
+            return SLM_ERR_ITERATION_CAP;
+        }
+        done += newly;
+    }
+    return SLM_OK;
+}
+
+int slm_fix_right_flanks(const slm_params* p, uint32_t n, const float* seed_point, const uint8_t* mask,
+                         const float* uv, const uint32_t* mapping, const uint32_t* channel_label,
+                         const uint32_t* link, uint32_t* label, void* workspace, size_t workspace_bytes,
+                         uint64_t* required_bytes, void* stream) {
+    (void)channel_label; (void)link;
+    return fix_flanks(p, n, seed_point, mask, uv, mapping, label, workspace, workspace_bytes,
+                      required_bytes, stream, false);
+}
+
+int slm_fix_left_flanks(const slm_params* p, uint32_t n, const float* seed_point, const uint8_t* mask,
+                        const float* uv, const uint32_t* mapping, const uint32_t* channel_label,
+                        const uint32_t* link, uint32_t* label, void* workspace, size_t workspace_bytes,
+                        uint64_t* required_bytes, void* stream) {
+    (void)channel_label; (void)link;
+    return fix_flanks(p, n, seed_point, mask, uv, mapping, label, workspace, workspace_bytes,
+                      required_bytes, stream, true);
+}
+
+int slm_hillslopes(const slm_params* p, uint32_t n, const float* seed_point, const uint8_t* mask,
+                   const float* uv, const uint32_t* mapping, const uint32_t* count, uint32_t* link,
+                   void* stream) {
+    (void)mapping; (void)count;
+    clear_error();
+    int rc = map_checks(p, n, seed_point);
+    if (rc) return rc;
+    if (n == 0) return SLM_OK;
+    k_hillslopes<<<blocks_for(n, 128), 128, 0, SS>>>(*p, n, F2(seed_point), mask, F2(uv), link);
+    SLM_LAUNCHED("k_hillslopes");
+    return SLM_OK;
+}
+
+int slm_hillslope_lengths(const slm_params* p, uint32_t n, const float* seed_point, const uint8_t* mask,
+                          const float* uv, const uint32_t* mapping, const uint32_t* label,
+                          float* traj_length, void* stream) {
+    (void)label;
+    clear_error();
+    int rc = map_checks(p, n, seed_point);
+    if (rc) return rc;
+    if (n == 0) return SLM_OK;
+    k_hillslope_lengths<<<blocks_for(n, 128), 128, 0, SS>>>(*p, n, F2(seed_point), mask, F2(uv), mapping,
+                                                           traj_length);
+    SLM_LAUNCHED("k_hillslope_lengths");
+    return SLM_OK;
+}
+
+}  // extern "C"

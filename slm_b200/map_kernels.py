@@ -1,0 +1,79 @@
+"""Device execution of one mapping kernel on NumPy buffers (the reference's
+per-call contract, pocl.gpu_compute, pocl.py:503-560: copy the buffers to the
+device, run, copy the written ones back)."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, ptr, sref
+from .device import cuda_device
+
+# kernel -> (entry point, indices of the buffers it writes, extra arguments)
+SPECS = {
+    "connect_channels": ("slm_connect_channels", (2,), "status"),
+    "map_channel_heads": ("slm_map_channel_heads", (2,), None),
+    "prune_channel_heads": ("slm_prune_channel_heads", (2,), None),
+    "count_downchannels": ("slm_count_downchannels", (2, 3, 4), "workspace"),
+    "flag_downchannels": ("slm_flag_downchannels", (2, 3), None),
+    "label_confluences": ("slm_label_confluences", (3,), None),
+    "segment_downchannels": ("slm_segment_downchannels", (2, 5), "status"),
+    "segment_hillslopes": ("slm_segment_hillslopes", (5,), None),
+    "subsegment_channel_edges": ("slm_subsegment_channel_edges", (2, 5), "status"),
+    "subsegment_flanks": ("slm_subsegment_flanks", (5,), None),
+    "fix_right_flanks": ("slm_fix_right_flanks", (5,), "workspace"),
+    "fix_left_flanks": ("slm_fix_left_flanks", (5,), "workspace"),
+    "hillslopes": ("slm_hillslopes", (4,), None),
+    "hillslope_lengths": ("slm_hillslope_lengths", (4,), None),
+}
+_MIN_WS = {
+    "count_downchannels": lambda L, p, n: L.slm_count_downchannels_workspace(n, 0),
+    "fix_right_flanks": lambda L, p, n: L.slm_fix_flanks_workspace(n, p.nxy_padded, 0),
+    "fix_left_flanks": lambda L, p, n: L.slm_fix_flanks_workspace(n, p.nxy_padded, 0),
+}
+
+
+def _to_dev(a, dev):
+    a = np.ascontiguousarray(a)
+    if a.dtype == np.bool_:
+        a = a.view(np.uint8)
+    return torch.from_numpy(a).to(dev)
+
+
+def run(name, params, seeds, arrays, device=None):
+    """Run kernel ``name`` on the device, updating the written NumPy buffers in place.
+    Returns the status word (0 unless a loop cap or out-of-grid access occurred)."""
+    L = _lib.load()
+    fn_name, written, extra = SPECS[name]
+    fn = getattr(L, fn_name)
+    dev = device if device is not None else cuda_device(0, 0)
+    seeds = np.ascontiguousarray(seeds, dtype=np.float32)
+    n = int(seeds.shape[0])
+    with torch.cuda.device(dev):
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        seeds_d = torch.from_numpy(seeds).to(dev) if n else torch.zeros(2, dtype=torch.float32, device=dev)
+        bufs = [_to_dev(a, dev) for a in arrays]
+        args = [sref(params), n, ptr(seeds_d)] + [ptr(b) for b in bufs]
+        status = torch.zeros(1, dtype=torch.uint32, device=dev)
+        if extra == "status":
+            check(fn(*(args + [ptr(status), stream])))
+        elif extra == "workspace":
+            need = ctypes.c_uint64(0)
+            size = int(_MIN_WS[name](L, params, n))
+            ws = torch.empty(size, dtype=torch.uint8, device=dev)
+            rc = fn(*(args + [ptr(ws), size, ctypes.byref(need), stream]))
+            if rc == _lib.SLM_ERR_CAPACITY:
+                size = int(need.value)
+                ws = torch.empty(size, dtype=torch.uint8, device=dev)
+                rc = fn(*(args + [ptr(ws), size, ctypes.byref(need), stream]))
+            check(rc)
+        else:
+            check(fn(*(args + [stream])))
+        for i in written:
+            out = bufs[i].cpu().numpy()
+            dst = arrays[i]
+            dst[...] = out.view(dst.dtype).reshape(dst.shape) if dst.dtype != np.bool_ else out.astype(bool)
+        return int(status.cpu().numpy()[0])

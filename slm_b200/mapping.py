@@ -48,10 +48,13 @@ class DeviceRunner:
 
     def __init__(self, device=None):
         self.device = device
+        self.status = 0  # OR of the status words returned by the kernels
 
     def __call__(self, name, params, seeds, arrays):
         from . import map_kernels
-        return map_kernels.run(name, params, seeds, arrays, self.device)
+        st = map_kernels.run(name, params, seeds, arrays, self.device)
+        self.status |= st
+        return st
 
 
 _default_runner = None

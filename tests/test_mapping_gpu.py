@@ -1,0 +1,66 @@
+"""Mapping kernels on the GPU against the oracle, kernel by kernel through the
+map_channels_segments sequence (bit-exact: integer flags, counts, links and
+labels; hillslope lengths are float results of bit-exact RK walks)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from mapping_cases import midslope_case, oracle_runner, pipeline_case
+from slm_b200 import mapping as M
+
+pytestmark = pytest.mark.gpu
+
+
+class DeviceVsOracle:
+    def __init__(self):
+        self.device = M.DeviceRunner()
+        self.mismatches = []
+        self.calls = []
+
+    def __call__(self, name, params, seeds, arrays):
+        expect = [a.copy() for a in arrays]
+        oracle_runner(name, params, seeds, expect)
+        st = self.device(name, params, seeds, arrays)
+        assert st == 0, (name, st)
+        self.calls.append((name, seeds.shape[0]))
+        for k, (a, b) in enumerate(zip(arrays, expect)):
+            if not np.array_equal(a.view(np.uint8), b.view(np.uint8)):
+                self.mismatches.append((name, k, int(np.sum(a != b))))
+                a[...] = b  # continue from the oracle's state so later kernels are compared too
+
+
+@pytest.mark.parametrize("kw", [dict(nx=96, ny=80, seed=5), dict(nx=120, ny=72, seed=6, channel_pct=90.0),
+                                dict(nx=64, ny=64, seed=7, segmentation_threshold=4),
+                                dict(nx=256, ny=192, seed=9, channel_pct=92.0)])
+def test_mapping_pipeline_bit_exact(kw):
+    c, info, data = pipeline_case(**kw)
+    run = DeviceVsOracle()
+    assert M.map_channels_segments(None, info, data, runner=run)
+    assert run.mismatches == [], run.mismatches
+    assert len(run.calls) == 15
+    midslope_case(data, info)
+    assert M.hsl(None, info, data, False, runner=run)
+    assert run.mismatches == [], run.mismatches
+
+
+def test_prune_channel_heads_bit_exact():
+    c, info, data = pipeline_case(nx=80, ny=80, seed=8)
+    run = DeviceVsOracle()
+    M.map_channels(info, data)
+    M.connect_channel_pixels(None, info, data, runner=run)
+    M.thin_channels(info, data)
+    M.map_channel_heads(None, info, data, runner=run)
+    M.prune_channel_heads(None, info, data, runner=run)
+    assert run.mismatches == []
+
+
+def test_device_pipeline_end_to_end_matches_oracle_pipeline():
+    """The whole sequence on the device alone equals the whole sequence on the oracle."""
+    _, info, data = pipeline_case(nx=160, ny=128, seed=11)
+    _, info2, data2 = pipeline_case(nx=160, ny=128, seed=11)
+    dev = M.DeviceRunner()
+    assert M.map_channels_segments(None, info, data, runner=dev)
+    assert M.map_channels_segments(None, info2, data2, runner=oracle_runner)
+    assert dev.status == 0
+    for name in ("mapping_array", "count_array", "link_array", "label_array", "channel_label_array"):
+        assert np.array_equal(getattr(data, name), getattr(data2, name)), name
