@@ -112,6 +112,21 @@ int slm_integrate_fields(const slm_params* p, const slm_launch* launch,
                          uint32_t* mapping, uint64_t* slc, uint64_t* slt,
                          uint64_t* workspace, void* stream);
 
+/* slm_integrate_fields_scheduled: slm_integrate_fields with two options for
+ * the scheduler (no counterpart in the reference; neither changes a result):
+ *   seed_order  [n_seed_points] uint32 or NULL: queue position j traces seed
+ *               seed_order[j] (its RNG stream still follows the seed index),
+ *               so trajectories can be issued e.g. longest first;
+ *   item_steps  [(n_seed_points - seeds_chunk_offset) * d*d] uint16 or NULL:
+ *               RK steps of each trajectory (saturated at 65535), indexed by
+ *               queue position * d*d + sub-pixel index -- the training data of
+ *               the learned length scheduler. */
+int slm_integrate_fields_scheduled(const slm_params* p, const slm_launch* launch,
+                                   const float* seed_point, const uint8_t* mask, const float* uv,
+                                   uint32_t* mapping, uint64_t* slc, uint64_t* slt,
+                                   uint64_t* workspace, const uint32_t* seed_order,
+                                   uint16_t* item_steps, void* stream);
+
 /* slm_integrate_fields_noalloc -- no counterpart in the reference.
  * For callers that cannot call cudaMalloc: a host application that hands a
  * plugin only its own pre-allocated device buffers, or a binding of the
@@ -253,6 +268,58 @@ int slm_hillslopes(const slm_params* p, uint32_t n_seeds, const float* seed_poin
 int slm_hillslope_lengths(const slm_params* p, uint32_t n_seeds, const float* seed_point,
                           const uint8_t* mask, const float* uv, const uint32_t* mapping,
                           const uint32_t* label, float* traj_length, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Learned trajectory-length scheduler -- no counterpart in the reference.
+ * A small BF16 CNN reads the 16x16x2 uv patch around each seed pixel and
+ * predicts log(1 + RK steps) of its downstream and upstream trajectories;
+ * slm_order_by_prediction turns one column of predictions into the
+ * seed_order of slm_integrate_fields_scheduled (longest predicted first).
+ * Ordering never changes the traced fields.
+ *
+ * Weights (fp32 arrays holding bfloat16-rounded values):
+ *   w1 [32][32]  conv1 4x4/4, row f = 2*(4*di+dj)+c     b1 [32]
+ *   w2 [128][64] conv2 2x2/2, row g = 32*(2*ei+ej)+o    b2 [64]
+ *   w3 [256][2]  dense, row h = 64*u+o2                 b3 [2]
+ * ---------------------------------------------------------------------- */
+/* conv1 input rows: x1[(s*16 + t)*32 + f], the uv patch of seed index[s]
+ * (index NULL: s), clamped to the padded grid, rounded to bfloat16 */
+int slm_cnn_gather(const float* uv, uint32_t nx_padded, uint32_t ny_padded, uint32_t pad,
+                   const float* seed_point, const uint32_t* index, uint32_t n, float* x1,
+                   void* stream);
+/* conv1 activations [n*16][32] -> conv2 input rows [n*4][128] (backward = 0),
+ * or the gradient the other way (backward = 1) */
+int slm_cnn_rearrange(const float* src, uint32_t n, float* dst, int backward, void* stream);
+/* C[M][N] = op(A) op(B) (+ bias[N], ReLU, pre-activation into Z, bf16 round
+ * of the output), fp32; op(A) = A [M][K] or, trans_a, A^T with A [K][M];
+ * op(B) = B [K][N] or, trans_b, B^T with B [N][K].  split_k > 0 instead adds
+ * the product into C over split_k K-slices (C zeroed by the caller; bias,
+ * Z, relu and round_out are then ignored). */
+int slm_gemm(int trans_a, int trans_b, int M, int N, int K, const float* A, const float* B,
+             float* C, float* Z, const float* bias, int relu, int round_out, int split_k,
+             void* stream);
+/* dz[i] = z[i] > 0 ? da[i] : 0 */
+int slm_relu_backward(const float* da, const float* z, uint64_t n, float* dz, void* stream);
+/* db[c] += sum_r dz[r][c] */
+int slm_bias_grad(const float* dz, uint64_t rows, int cols, float* db, void* stream);
+/* dy = 2 w (y - t) * inv_n, *loss += sum w (y - t)^2 * inv_n (w NULL: 1) */
+int slm_mse(const float* y, const float* t, const float* w, uint64_t n_el, float inv_n, float* dy,
+            float* loss, void* stream);
+/* one Adam step (bias corrections for step >= 1) on fp32 master weights w;
+ * wq receives the bfloat16-rounded weights (round_w = 1) or a copy */
+int slm_adam(float* w, float* wq, const float* g, float* m, float* v, uint64_t n, float lr,
+             float b1, float b2, float eps, int step, int round_w, void* stream);
+/* fused inference on the tensor cores: out [n][2] predictions for seeds
+ * seed_point [n] (float2 pixel coordinates, unpadded) */
+int slm_cnn_infer(const float* uv, uint32_t nx_padded, uint32_t ny_padded, uint32_t pad,
+                  const float* seed_point, uint32_t n, const float* w1, const float* b1,
+                  const float* w2, const float* b2, const float* w3, const float* b3,
+                  float* out, void* stream);
+/* order [n]: seed indices by column col of pred [n][stride], longest predicted
+ * first, in n_bins equal bins over [lo, hi] (bins: n_bins uint32 scratch) */
+int slm_order_by_prediction(const float* pred, uint32_t stride, uint32_t col, uint32_t n,
+                            float lo, float hi, uint32_t n_bins, uint32_t* bins,
+                            uint32_t* order, void* stream);
 
 #ifdef __cplusplus
 }

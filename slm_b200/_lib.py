@@ -49,6 +49,7 @@ SIGNATURES = {
     "slm_fields_workspace_words": (ctypes.c_size_t, []),
     "slm_integrate_fields": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_integrate_fields_noalloc": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "slm_integrate_fields_scheduled": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_integrate_trajectory": (ctypes.c_int, [_P, _I, _U, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_histogram_univariate": (ctypes.c_int, [_P, _P, _U, _P, _P]),
     "slm_histogram_bivariate": (ctypes.c_int, [_P, _P, _U, _P, _P]),
@@ -71,6 +72,17 @@ SIGNATURES = {
     "slm_fix_left_flanks": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P, _P, ctypes.c_size_t, _P, _P]),
     "slm_hillslopes": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P]),
     "slm_hillslope_lengths": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P]),
+    "slm_cnn_gather": (ctypes.c_int, [_P, _U, _U, _U, _P, _P, _U, _P, _P]),
+    "slm_cnn_rearrange": (ctypes.c_int, [_P, _U, _P, _I, _P]),
+    "slm_gemm": (ctypes.c_int, [_I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _I, _I, _P]),
+    "slm_relu_backward": (ctypes.c_int, [_P, _P, ctypes.c_uint64, _P, _P]),
+    "slm_bias_grad": (ctypes.c_int, [_P, ctypes.c_uint64, _I, _P, _P]),
+    "slm_mse": (ctypes.c_int, [_P, _P, _P, ctypes.c_uint64, ctypes.c_float, _P, _P, _P]),
+    "slm_adam": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_uint64, ctypes.c_float, ctypes.c_float,
+                                ctypes.c_float, ctypes.c_float, _I, _I, _P]),
+    "slm_cnn_infer": (ctypes.c_int, [_P, _U, _U, _U, _P, _U, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "slm_order_by_prediction": (ctypes.c_int, [_P, _U, _U, _U, ctypes.c_float, ctypes.c_float, _U,
+                                               _P, _P, _P]),
 }
 
 _lock = threading.Lock()

@@ -55,13 +55,19 @@ struct FieldLane {
     Vec2 a;
     float l, dt;
     uint32_t n, rng;
+    uint32_t item, k;  // queue position and RK steps so far (kept only when recording)
     bool alive;
 };
 
 // Start trajectory `item` = (seed - seed_begin) * d*d + j*d + i
 // (integratefields.cl:83-113; jittertrajectory.cl:56-62).
+//
+// `order` (optional) maps queue positions to seed indices, so trajectories can
+// be traced in any order; the RNG stream still follows the seed index, so no
+// trajectory changes.
 __device__ __forceinline__ void field_start(FieldLane& s, u64 item, uint32_t seed_begin,
                                             const float2* __restrict__ seeds,
+                                            const uint32_t* __restrict__ order,
                                             const uint8_t* __restrict__ mask, const slm_params& p,
                                             Acc& acc, u64* __restrict__ slc, u64* __restrict__ slt) {
     const uint32_t d = p.subpixel_seed_point_density;
@@ -75,7 +81,7 @@ __device__ __forceinline__ void field_start(FieldLane& s, u64 item, uint32_t see
         seed_off = (uint32_t)(item / dd);
         sub = (uint32_t)(item - (u64)seed_off * dd);
     }
-    const uint32_t seed_idx = seed_begin + seed_off;
+    const uint32_t seed_idx = order ? __ldg(order + seed_begin + seed_off) : seed_begin + seed_off;
     const uint32_t j = sub / d, i = sub % d;
     const float2 c = __ldg(seeds + seed_idx);
     s.a.x = c.x + ((float)i * p.subpixel_seed_step - p.subpixel_seed_halfspan);
@@ -84,6 +90,8 @@ __device__ __forceinline__ void field_start(FieldLane& s, u64 item, uint32_t see
     s.l = 0.0f;
     s.dt = p.dt_max;
     s.n = 0;
+    s.item = (uint32_t)item;
+    s.k = 0;
     const uint32_t idx = pixel_of(s.a, p);
     const bool masked = __ldg(mask + idx) != 0;
     if (!masked) acc_visit(acc, idx, 0.0f, slc, slt);
@@ -120,6 +128,12 @@ __device__ __forceinline__ void field_step(FieldLane& s, const uint8_t* __restri
     s.alive = (s.l < p.max_length) && (s.n < p.max_n_steps);
 }
 
+// per-trajectory RK step count, saturated to 16 bits, indexed by queue position
+template <bool RECORD>
+__device__ __forceinline__ void record_end(const FieldLane& s, uint16_t* __restrict__ item_steps) {
+    if (RECORD) item_steps[s.item] = (uint16_t)(s.k < 65535u ? s.k : 65535u);
+}
+
 __device__ __forceinline__ void warp_add_counters(u64 steps, u64 ntraj, u64* work) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -132,22 +146,25 @@ __device__ __forceinline__ void warp_add_counters(u64 steps, u64 ntraj, u64* wor
     }
 }
 
-template <int ORDER>
+template <int ORDER, bool RECORD>
 __global__ void __launch_bounds__(256)
 k_fields_plain(const slm_params p, const float2* __restrict__ seeds, uint32_t seed_begin,
                u64 n_items, const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
-               u64* __restrict__ slc, u64* __restrict__ slt, u64* __restrict__ work) {
+               u64* __restrict__ slc, u64* __restrict__ slt, u64* __restrict__ work,
+               const uint32_t* __restrict__ order, uint16_t* __restrict__ item_steps) {
     const u64 item = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     u64 steps = 0, ntraj = 0;
     Acc acc{0u, 0u, 0ull};
     if (item < n_items) {
         FieldLane s;
-        field_start(s, item, seed_begin, seeds, mask, p, acc, slc, slt);
+        field_start(s, item, seed_begin, seeds, order, mask, p, acc, slc, slt);
         ntraj = 1;
         while (s.alive) {
             field_step<ORDER>(s, mask, uv, p, acc, slc, slt);
             steps++;
+            if (RECORD) s.k++;
         }
+        record_end<RECORD>(s, item_steps);
         acc_flush(acc, slc, slt);
     }
     warp_add_counters(steps, ntraj, work);
@@ -157,11 +174,12 @@ k_fields_plain(const slm_params p, const float2* __restrict__ seeds, uint32_t se
 // pass either hands queue items to idle lanes or advances every live
 // trajectory by one step, and each trajectory ends within max_n_steps steps,
 // so the loop ends; the exit test is warp-uniform.
-template <int ORDER>
+template <int ORDER, bool RECORD>
 __global__ void __launch_bounds__(256)
 k_fields_persistent(const slm_params p, const float2* __restrict__ seeds, uint32_t seed_begin,
                     u64 n_items, const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
-                    u64* __restrict__ slc, u64* __restrict__ slt, u64* __restrict__ work) {
+                    u64* __restrict__ slc, u64* __restrict__ slt, u64* __restrict__ work,
+                    const uint32_t* __restrict__ order, uint16_t* __restrict__ item_steps) {
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
     FieldLane s;
@@ -182,8 +200,9 @@ k_fields_persistent(const slm_params p, const float2* __restrict__ seeds, uint32
                 if (!s.alive) {
                     const u64 item = base + __popc(idle & ((1u << lane) - 1u));
                     if (item < n_items) {
-                        field_start(s, item, seed_begin, seeds, mask, p, acc, slc, slt);
+                        field_start(s, item, seed_begin, seeds, order, mask, p, acc, slc, slt);
                         ntraj++;
+                        if (!s.alive) record_end<RECORD>(s, item_steps);
                     }
                 }
             }
@@ -195,6 +214,10 @@ k_fields_persistent(const slm_params p, const float2* __restrict__ seeds, uint32
         if (s.alive) {
             field_step<ORDER>(s, mask, uv, p, acc, slc, slt);
             steps++;
+            if (RECORD) {
+                s.k++;
+                if (!s.alive) record_end<RECORD>(s, item_steps);
+            }
         }
     }
     acc_flush(acc, slc, slt);
@@ -300,6 +323,34 @@ static int check_grid(const slm_params* p) {
     return SLM_OK;
 }
 
+template <int ORDER, bool RECORD>
+static int launch_fields(const slm_params* p, const slm_launch& L, int block, const float2* sp,
+                         uint32_t begin, u64 n_items, const uint8_t* mask, const float2* u2, u64* slc,
+                         u64* slt, u64* work, const uint32_t* order, uint16_t* rec, cudaStream_t s) {
+    if (L.schedule == SLM_SCHED_PLAIN) {
+        const u64 grid = (n_items + block - 1) / block;
+        SLM_REQUIRE(grid < (1ull << 31), "too many trajectories for one launch");
+        k_fields_plain<ORDER, RECORD><<<(unsigned)grid, block, 0, s>>>(*p, sp, begin, n_items, mask, u2,
+                                                                      slc, slt, work, order, rec);
+        SLM_LAUNCHED("k_fields_plain");
+    } else if (L.schedule == SLM_SCHED_PERSISTENT) {
+        int per_sm = L.blocks_per_sm;
+        if (per_sm <= 0) {
+            int occ = 0;
+            SLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fields_persistent<ORDER, RECORD>, block, 0));
+            per_sm = occ > 0 ? occ : 1;
+        }
+        const unsigned grid = (unsigned)(num_sms() * per_sm);
+        k_fields_persistent<ORDER, RECORD><<<grid, block, 0, s>>>(*p, sp, begin, n_items, mask, u2, slc, slt,
+                                                                  work, order, rec);
+        SLM_LAUNCHED("k_fields_persistent");
+    } else {
+        set_error("unknown schedule %d", L.schedule);
+        return SLM_ERR_ARGS;
+    }
+    return SLM_OK;
+}
+
 extern "C" {
 
 size_t slm_fields_workspace_words(void) { return 4; }
@@ -307,6 +358,15 @@ size_t slm_fields_workspace_words(void) { return 4; }
 int slm_integrate_fields(const slm_params* p, const slm_launch* launch, const float* seed_point,
                          const uint8_t* mask, const float* uv, uint32_t* mapping, uint64_t* slc,
                          uint64_t* slt, uint64_t* workspace, void* stream) {
+    return slm_integrate_fields_scheduled(p, launch, seed_point, mask, uv, mapping, slc, slt,
+                                          workspace, nullptr, nullptr, stream);
+}
+
+int slm_integrate_fields_scheduled(const slm_params* p, const slm_launch* launch,
+                                   const float* seed_point, const uint8_t* mask, const float* uv,
+                                   uint32_t* mapping, uint64_t* slc, uint64_t* slt,
+                                   uint64_t* workspace, const uint32_t* seed_order,
+                                   uint16_t* item_steps, void* stream) {
     (void)mapping;
     clear_error();
     int rc = check_grid(p);
@@ -327,37 +387,15 @@ int slm_integrate_fields(const slm_params* p, const slm_launch* launch, const fl
     if (begin >= p->n_seed_points) return SLM_OK;
     const u64 dd = (u64)p->subpixel_seed_point_density * p->subpixel_seed_point_density;
     const u64 n_items = (u64)(p->n_seed_points - begin) * dd;
+    SLM_REQUIRE(!item_steps || n_items < (1ull << 32), "step recording needs fewer than 2^32 trajectories");
     const float2* sp = reinterpret_cast<const float2*>(seed_point);
     const float2* u2 = reinterpret_cast<const float2*>(uv);
-    if (L.schedule == SLM_SCHED_PLAIN) {
-        const u64 grid = (n_items + block - 1) / block;
-        SLM_REQUIRE(grid < (1ull << 31), "too many trajectories for one launch");
-        if (L.integrator == SLM_RK4)
-            k_fields_plain<4><<<(unsigned)grid, block, 0, s>>>(*p, sp, begin, n_items, mask, u2, (u64*)slc, (u64*)slt, (u64*)workspace);
-        else
-            k_fields_plain<2><<<(unsigned)grid, block, 0, s>>>(*p, sp, begin, n_items, mask, u2, (u64*)slc, (u64*)slt, (u64*)workspace);
-        SLM_LAUNCHED("k_fields_plain");
-    } else if (L.schedule == SLM_SCHED_PERSISTENT) {
-        int per_sm = L.blocks_per_sm;
-        if (per_sm <= 0) {
-            int occ = 0;
-            if (L.integrator == SLM_RK4)
-                SLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fields_persistent<4>, block, 0));
-            else
-                SLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fields_persistent<2>, block, 0));
-            per_sm = occ > 0 ? occ : 1;
-        }
-        const unsigned grid = (unsigned)(num_sms() * per_sm);
-        if (L.integrator == SLM_RK4)
-            k_fields_persistent<4><<<grid, block, 0, s>>>(*p, sp, begin, n_items, mask, u2, (u64*)slc, (u64*)slt, (u64*)workspace);
-        else
-            k_fields_persistent<2><<<grid, block, 0, s>>>(*p, sp, begin, n_items, mask, u2, (u64*)slc, (u64*)slt, (u64*)workspace);
-        SLM_LAUNCHED("k_fields_persistent");
-    } else {
-        set_error("unknown schedule %d", L.schedule);
-        return SLM_ERR_ARGS;
-    }
-    return SLM_OK;
+    u64* w = (u64*)workspace;
+    if (L.integrator == SLM_RK4)
+        return item_steps ? launch_fields<4, true>(p, L, block, sp, begin, n_items, mask, u2, (u64*)slc, (u64*)slt, w, seed_order, item_steps, s)
+                          : launch_fields<4, false>(p, L, block, sp, begin, n_items, mask, u2, (u64*)slc, (u64*)slt, w, seed_order, nullptr, s);
+    return item_steps ? launch_fields<2, true>(p, L, block, sp, begin, n_items, mask, u2, (u64*)slc, (u64*)slt, w, seed_order, item_steps, s)
+                      : launch_fields<2, false>(p, L, block, sp, begin, n_items, mask, u2, (u64*)slc, (u64*)slt, w, seed_order, nullptr, s);
 }
 
 int slm_integrate_trajectory(const slm_params* p, int32_t integrator, uint32_t n_chunk,

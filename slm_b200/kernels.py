@@ -47,8 +47,13 @@ def launch_config(schedule="persistent", integrator=2, block_threads=0, blocks_p
 
 
 def integrate_fields(params, seeds, mask, uv, slc, slt, work, schedule="persistent",
-                     integrator=2, block_threads=0, blocks_per_sm=0, stream=None):
-    """Trace every seed's d*d jittered trajectories, adding into slc/slt (uint64)."""
+                     integrator=2, block_threads=0, blocks_per_sm=0, stream=None,
+                     order=None, item_steps=None):
+    """Trace every seed's d*d jittered trajectories, adding into slc/slt (uint64).
+
+    ``order`` (uint32 per seed, optional) issues seeds in that order (results
+    unchanged); ``item_steps`` (uint16 per trajectory, optional) receives each
+    trajectory's RK step count."""
     lib = _lib.load()
     nxy = params.nxy_padded
     _need(seeds, torch.float32, 2 * params.n_seed_points, "seeds")
@@ -58,8 +63,15 @@ def integrate_fields(params, seeds, mask, uv, slc, slt, work, schedule="persiste
     _need(slt, torch.uint64, nxy, "slt")
     _need(work, torch.uint64, lib.slm_fields_workspace_words(), "workspace")
     L = launch_config(schedule, integrator, block_threads, blocks_per_sm)
-    check(lib.slm_integrate_fields(sref(params), sref(L), ptr(seeds), ptr(mask), ptr(uv), None,
-                                   ptr(slc), ptr(slt), ptr(work), _stream(stream)))
+    if order is not None:
+        _need(order, torch.uint32, int(params.n_seed_points), "order")
+    if item_steps is not None:
+        d = int(params.subpixel_seed_point_density)
+        n_items = (int(params.n_seed_points) - int(params.seeds_chunk_offset)) * d * d
+        _need(item_steps, torch.uint16, n_items, "item_steps")
+    check(lib.slm_integrate_fields_scheduled(sref(params), sref(L), ptr(seeds), ptr(mask), ptr(uv),
+                                             None, ptr(slc), ptr(slt), ptr(work), ptr(order),
+                                             ptr(item_steps), _stream(stream)))
 
 
 def integrate_trajectory(params, n_chunk, seeds, mask, uv, traj, nsteps, length,

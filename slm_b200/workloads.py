@@ -41,6 +41,8 @@ SPECS = {
                             8192, 1.0, 2, 1.0, 4, 0.1, 20000, "config5"),
     "small": WorkloadSpec("256x256 @1m, d=2, jitter +-0.5, RK2, step 0.1 px, max 2000 steps",
                           256, 1.0, 2, 1.0, 2, 0.1, 2000, "tile"),
+    "incised512": WorkloadSpec("512x512 @2m incised fBm, d=2, jitter +-0.5, RK2, step 0.1 px, "
+                               "max 10000 steps", 512, 2.0, 2, 1.0, 2, 0.1, 10000, "incised"),
 }
 
 
@@ -51,6 +53,8 @@ def make_dtm(spec, seed=None):
         return synth.config2_dtm(spec.n, seed or 2)
     if spec.dtm == "config5":
         return synth.config5_dtm(spec.n, seed or 5)
+    if spec.dtm == "incised":  # the 2048^2 recipe, incision count scaled by area
+        return synth.config2_dtm(spec.n, seed or 2, max(8, round(400 * spec.n * spec.n / 2048 ** 2)))
     return synth.tile_dtm(spec.n, spec.n, seed or 9)
 
 
