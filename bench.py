@@ -15,6 +15,10 @@ d*d jittered sub-pixel trajectories down and up accumulating slc/slt
          139 B) x steps / kernel time, against the measured HBM copy peak
   cpu_baseline  the reference's CPU path timed on this host's cores on a
          bounded stride of the same seeds
+  scheduler  learned length scheduler vs the unsorted order (plain and
+         persistent field kernels, both directions, identical fields checked):
+         a BF16 CNN trained here on step counts recorded on a held-out DTM of
+         the same family; inference + ordering inside the learned arms' time
 
 N>1 (torchrun): the field seeds are split into contiguous ranges per rank,
 each rank accumulates its own uint64 slc/slt, then one NCCL all-reduce (sum)
@@ -320,6 +324,8 @@ def run_b200(args):
     }
     if e2e is not None:
         line["e2e"] = e2e
+    if ws == 1 and not args.no_sched:
+        line["scheduler"] = sched_compare(args, wl, dev, seeds_d, mask_d, uv_d, field_prm, flush)
     if rank == 0 and not args.no_cpu and ws == 1:
         line["cpu_baseline"] = cpu_baseline(wl, args)
     if ws > 1:
@@ -328,6 +334,112 @@ def run_b200(args):
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
+
+
+def sched_compare(args, wl, dev, seeds_d, mask_d, uv_d, field_prm, flush):
+    """Learned length scheduler against the unsorted order, for the plain
+    (one thread per trajectory) and persistent field kernels, on identical
+    trajectories.  The model is trained here, on the GPU, on step counts the
+    tracer records on a held-out DTM of the same family (another seed); the
+    learned arms' timed region includes inference and ordering."""
+    import torch
+
+    from slm_b200 import kernels, scheduler as S
+    from slm_b200.workloads import Workload
+
+    t0 = time.time()
+    train = Workload(args.workload, seed=args.sched_train_seed)
+    spec = wl.spec
+    d = spec.density
+    dd = d * d
+    tr_seeds = torch.from_numpy(train.seeds).to(dev)
+    tr_mask = torch.from_numpy(train.mask.view(np.uint8)).to(dev)
+    tr_uv = torch.from_numpy(train.uv).to(dev)
+    from slm_b200.params import kernel_params
+    n_tr = int(train.info.n_seed_points)
+    cols = []
+    for s in (1.0, -1.0):
+        prm = kernel_params(train.info, "INTEGRATE_FIELDS", s)
+        st = S.record_steps(prm, tr_seeds, tr_mask, tr_uv, integrator=spec.integrator)
+        cols.append(S.step_targets(st, n_tr, d))
+    targets = torch.stack(cols, 1).contiguous()
+    model = S.LengthModel(dev, seed=0)
+    torch.cuda.synchronize()
+    t1 = time.time()
+    hist = model.fit(tr_uv, tr_uv.shape[0], tr_uv.shape[1], 2, tr_seeds, targets,
+                     steps=args.sched_train_steps, batch=4096)
+    torch.cuda.synchronize()
+    t_train = time.time() - t1
+    del tr_seeds, tr_mask, tr_uv, targets
+
+    n = int(wl.info.n_seed_points)
+    nxp, nyp = uv_d.shape[0], uv_d.shape[1]
+    pred = model.predict(uv_d, nxp, nyp, 2, seeds_d, n)
+    # held-out prediction error against the step counts the tracer records
+    err = {}
+    for col in (0, 1):
+        st = S.record_steps(field_prm[col], seeds_d, mask_d, uv_d, integrator=spec.integrator)
+        truth = S.step_targets(st, n, d)
+        p = pred[:, col]
+        rank = lambda x: torch.argsort(torch.argsort(x)).double()
+        rp, rt = rank(p), rank(truth)
+        rho = float(torch.corrcoef(torch.stack([rp, rt]))[0, 1])
+        err["down" if col == 0 else "up"] = {
+            "mae_log_steps": float((p - truth).abs().mean()), "spearman": rho}
+        del st, truth, rp, rt
+    cap = S.log_cap(field_prm[0])
+    orders = [torch.empty(n, dtype=torch.uint32, device=dev) for _ in range(2)]
+    bins = torch.empty(S.N_BINS, dtype=torch.uint32, device=dev)
+    nxy = int(field_prm[0].nxy_padded)
+    acc = torch.zeros((2, 2, nxy), dtype=torch.uint64, device=dev)
+    work = [kernels.workspace(dev) for _ in range(2)]
+    stream = torch.cuda.current_stream()
+
+    def arm(schedule, learned):
+        acc.zero_()
+        if learned:
+            model.predict(uv_d, nxp, nyp, 2, seeds_d, n, out=pred)
+            for col in (0, 1):
+                model.order(pred, col, cap, out=orders[col], bins=bins)
+        for col in (0, 1):
+            work[col].zero_()
+            kernels.integrate_fields(field_prm[col], seeds_d, mask_d, uv_d, acc[col, 0], acc[col, 1],
+                                     work[col], schedule=schedule, integrator=spec.integrator,
+                                     order=orders[col] if learned else None)
+
+    out = {"trained_on": "{} (seed {})".format(spec.name, args.sched_train_seed),
+           "train_pairs": n_tr, "train_steps": args.sched_train_steps, "train_batch": 4096,
+           "train_s": t_train, "prep_s": t1 - t0,
+           "loss_first": float(np.mean(hist[:10])), "loss_last": float(np.mean(hist[-50:])),
+           "held_out_error": err, "ms": {}}
+    ref = None
+    for schedule in ("plain", "persistent"):
+        for learned in (False, True):
+            arm(schedule, learned)
+            torch.cuda.synchronize()
+            res = (acc.clone(), int(work[0][1].item()) + int(work[1][1].item()))
+            if ref is None:
+                ref = res
+            elif not (torch.equal(res[0], ref[0]) and res[1] == ref[1]):
+                raise RuntimeError("scheduled trace differs from the unsorted one")
+            ts = []
+            for _ in range(args.sched_reps):
+                flush.fill_(1)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record(stream)
+                arm(schedule, learned)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            out["ms"][schedule + ("_learned" if learned else "")] = float(np.median(ts))
+    f_steps = ref[1]
+    out["field_steps"] = f_steps
+    out["steps_per_s"] = {k: f_steps / (v / 1e3) for k, v in out["ms"].items()}
+    out["learned_vs_plain"] = out["ms"]["plain"] / out["ms"]["plain_learned"]
+    out["persistent_learned_vs_plain"] = out["ms"]["plain"] / out["ms"]["persistent_learned"]
+    out["identical_fields"] = True
+    return out
 
 
 def run_e2e(args, wl, dev):
@@ -397,6 +509,10 @@ def main():
     ap.add_argument("--schedule", default="persistent", choices=["plain", "persistent"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-sched", action="store_true", help="skip the learned-scheduler comparison")
+    ap.add_argument("--sched-train-seed", type=int, default=12)
+    ap.add_argument("--sched-train-steps", type=int, default=1500)
+    ap.add_argument("--sched-reps", type=int, default=3)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
