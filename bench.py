@@ -442,6 +442,98 @@ def sched_compare(args, wl, dev, seeds_d, mask_d, uv_d, field_prm, flush):
     return out
 
 
+def run_batched(args):
+    """Batched form: ``--tiles`` fBm tiles of uneven sizes (edges log-uniform in
+    256..3072 px), 2x2 jittered seeds, RK2, step 0.1 px, max 2000 steps, both
+    directions.  Times, on identical fields: one plain (thread per trajectory)
+    launch per tile and direction; one persistent launch per tile and
+    direction; one batched persistent launch per direction with the
+    autotuned shape; the same captured in a CUDA graph (the headline)."""
+    import torch
+
+    from slm_b200 import autotune, batch
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    t0 = time.time()
+    tiles = batch.uneven_tiles(args.tiles, 256, 3072, seed=3, density=2, jitter=1.0, step=0.1,
+                               max_steps=2000)
+    t_gen = time.time() - t0
+    b = batch.TileBatch(tiles, dev, integrator=2)
+    n_px = sum(int(t.info.nx) * int(t.info.ny) for t in tiles)
+    sample = batch.TileBatch(tiles[:12], dev, integrator=2)
+    launch, table = autotune.tune(lambda L: sample.trace(L), "k_fields_batched", 2,
+                                  "uneven fBm tiles, d=2, RK2, 12-tile sample",
+                                  force=args.retune)
+    del sample
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, reps):
+        ts = []
+        for _ in range(reps):
+            flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1) / 1e3)
+        return ts
+
+    b.trace(launch)
+    torch.cuda.synchronize()
+    ref = b.acc.clone()
+    steps = b.field_steps()
+    forms = {}
+    for name, fn in (("per_tile_plain", lambda: b.trace_per_tile("plain")),
+                     ("per_tile_persistent", lambda: b.trace_per_tile("persistent")),
+                     ("batched", lambda: b.trace(launch))):
+        fn()
+        torch.cuda.synchronize()
+        if not torch.equal(b.acc, ref):
+            raise RuntimeError(name + " fields differ from the batched launch")
+        forms[name] = float(np.median(timed(fn, max(1, args.steps // 2))))
+    g = b.capture(launch)
+    for _ in range(args.warmup):
+        g.replay()
+    torch.cuda.synchronize()
+    with ClockSampler(0) as clocks:
+        times = timed(g.replay, args.steps)
+    if not torch.equal(b.acc, ref):
+        raise RuntimeError("graph replay differs from the eager trace")
+    step_t = float(np.sum(times))
+    forms["batched_graph"] = step_t / args.steps
+    peak, peak_kind = _peaks()
+    bps = BYTES_PER_STEP[2]
+    line = {
+        "metric": "trajectory steps/s (fields, batched tiles)", "value": steps * args.steps / step_t,
+        "unit": "steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * step_t / args.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded fBm tiles; no dataset)",
+        "config": {"workload": "{} fBm tiles, edges log-uniform 256..3072 px, d=2 jitter +-0.5, RK2, "
+                               "step 0.1 px, max 2000 steps, both directions".format(args.tiles),
+                   "tiles": args.tiles, "pixels": n_px, "trajectories_per_direction": b.n_seeds * 4,
+                   "rk_steps_per_step": steps, "mpx_per_s": n_px / (step_t / args.steps) / 1e6,
+                   "l2": "256 MiB buffer written between steps", "generation_s": t_gen,
+                   "launch": {"block_threads": launch.block_threads,
+                              "blocks_per_sm": launch.blocks_per_sm},
+                   "autotune_ms": table, "parallelism": "1 GPU"},
+        "forms_ms": {k: 1e3 * v for k, v in forms.items()},
+        "forms_steps_per_s": {k: steps / v for k, v in forms.items()},
+        "batched_vs_per_tile_plain": forms["per_tile_plain"] / forms["batched_graph"],
+        "roofline": {"bound": "hbm", "achieved": steps * bps / forms["batched_graph"] / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": steps * bps / forms["batched_graph"] / 1e9 / peak,
+                     "traffic": None, "peak_source": peak_kind, "kernel": "k_fields_batched<2>",
+                     "bytes_per_step": bps},
+        "clocks": clocks.summary(),
+        "gpu_launches": args.steps * 2,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_e2e(args, wl, dev):
     """Public-API step: Trajectories then Fields on pinned host arrays."""
     import torch
@@ -510,12 +602,16 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-sched", action="store_true", help="skip the learned-scheduler comparison")
+    ap.add_argument("--tiles", type=int, default=96, help="config3: number of tiles")
+    ap.add_argument("--retune", action="store_true", help="config3: ignore the autotuner cache")
     ap.add_argument("--sched-train-seed", type=int, default=12)
     ap.add_argument("--sched-train-steps", type=int, default=1500)
     ap.add_argument("--sched-reps", type=int, default=3)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "config3":
+        return run_batched(args)
     return run_b200(args)
 
 

@@ -83,6 +83,22 @@ typedef struct slm_launch {
     int32_t reserved[3];
 } slm_launch;
 
+/* One DTM tile of a batched field trace (no counterpart in the reference: it
+ * traces each grid with its own kernel launch).  A tile's grids are the
+ * reference's padded (nx_padded x ny_padded, x-major) arrays, stored
+ * back to back with the other tiles' in shared uv / mask / slc / slt
+ * buffers; its seeds (tile-local, unpadded coordinates as the reference's
+ * seed_point array) are a contiguous range of the shared seed array.  The
+ * three float fields are the tile's GRID_SCALE, COMBO_FACTOR (signed by the
+ * direction) and DT_MAX as pocl.set_compile_options derives them. */
+typedef struct slm_tile {
+    uint64_t grid_offset;          /* first padded pixel of the tile */
+    uint32_t nx_padded, ny_padded;
+    uint32_t seed_begin, n_seeds;  /* seed_point[seed_begin .. seed_begin + n_seeds) */
+    float grid_scale, combo_factor, dt_max;
+    uint32_t reserved;
+} slm_tile;
+
 const char* slm_version(void);
 const char* slm_last_error(void);
 int slm_device_count(void);
@@ -126,6 +142,28 @@ int slm_integrate_fields_scheduled(const slm_params* p, const slm_launch* launch
                                    uint32_t* mapping, uint64_t* slc, uint64_t* slt,
                                    uint64_t* workspace, const uint32_t* seed_order,
                                    uint16_t* item_steps, void* stream);
+
+/* slm_integrate_fields_batched -- no counterpart in the reference (which
+ * launches integrate_fields once per grid).  Traces every tile of a batch in
+ * one persistent work-queue launch; each tile's slc/slt equal those of
+ * slm_integrate_fields on that tile alone (same trajectories: the RNG stream
+ * of the tile-local seed index).
+ *   p        shared parameters (direction, step factor, errors, MAX_LENGTH,
+ *            MAX_N_STEPS, pad, d, jitter, resolution); its grid fields and
+ *            n_seed_points / seeds_chunk_offset are not used
+ *   tiles    [n_tiles] DEVICE array, sorted by seed_begin, seed ranges
+ *            contiguous from 0 and summing to n_seeds; all tiles share pad
+ *            width and pixel size; total padded pixels < 2^32
+ *   seed_order [n_seeds] or NULL: queue position j traces global seed
+ *            seed_order[j]; item_steps [n_seeds*d*d] or NULL as in
+ *            slm_integrate_fields_scheduled
+ *   workspace  slm_fields_workspace_words() uint64; word 3 becomes 1 if a
+ *            seed fell outside its tile (an inconsistent table). */
+int slm_integrate_fields_batched(const slm_params* p, const slm_launch* launch, const slm_tile* tiles,
+                                 uint32_t n_tiles, uint32_t n_seeds, const float* seed_point,
+                                 const uint8_t* mask, const float* uv, uint64_t* slc, uint64_t* slt,
+                                 uint64_t* workspace, const uint32_t* seed_order, uint16_t* item_steps,
+                                 void* stream);
 
 /* slm_integrate_fields_noalloc -- no counterpart in the reference.
  * For callers that cannot call cudaMalloc: a host application that hands a

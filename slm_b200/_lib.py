@@ -31,6 +31,14 @@ class SlmLaunch(ctypes.Structure):
                 ("chunk", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3)]
 
 
+class SlmTile(ctypes.Structure):
+    _fields_ = [("grid_offset", ctypes.c_uint64), ("nx_padded", ctypes.c_uint32),
+                ("ny_padded", ctypes.c_uint32), ("seed_begin", ctypes.c_uint32),
+                ("n_seeds", ctypes.c_uint32), ("grid_scale", ctypes.c_float),
+                ("combo_factor", ctypes.c_float), ("dt_max", ctypes.c_float),
+                ("reserved", ctypes.c_uint32)]
+
+
 class SlmError(RuntimeError):
     def __init__(self, code, message):
         super().__init__("slm_b200 error {}: {}".format(code, message))
@@ -50,6 +58,7 @@ SIGNATURES = {
     "slm_integrate_fields": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_integrate_fields_noalloc": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_integrate_fields_scheduled": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "slm_integrate_fields_batched": (ctypes.c_int, [_P, _P, _P, _U, _U, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_integrate_trajectory": (ctypes.c_int, [_P, _I, _U, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_histogram_univariate": (ctypes.c_int, [_P, _P, _U, _P, _P]),
     "slm_histogram_bivariate": (ctypes.c_int, [_P, _P, _U, _P, _P]),

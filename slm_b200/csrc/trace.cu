@@ -19,6 +19,8 @@
 
 #define SLM_MAX_DEVICES 64
 
+static_assert(sizeof(slm_tile) == 40, "slm_tile layout is part of the ABI");
+
 namespace slm {
 
 // Run-length merge of pixel visits for one lane.
@@ -59,8 +61,43 @@ struct FieldLane {
     bool alive;
 };
 
-// Start trajectory `item` = (seed - seed_begin) * d*d + j*d + i
-// (integratefields.cl:83-113; jittertrajectory.cl:56-62).
+// Begin the trajectory of sub-pixel `sub` (= j*d + i) of the seed at `c`,
+// whose RNG stream is that of seed index `rng_idx`
+// (integratefields.cl:83-113; jittertrajectory.cl:56-62).  `mask` is the
+// grid's own; pixel indices are offset by `base` into slc/slt.
+__device__ __forceinline__ void field_init(FieldLane& s, float2 c, uint32_t rng_idx, uint32_t sub,
+                                           uint32_t item, const uint8_t* __restrict__ mask,
+                                           const slm_params& p, const Geo& g, uint32_t base,
+                                           Acc& acc, u64* __restrict__ slc, u64* __restrict__ slt) {
+    const uint32_t d = p.subpixel_seed_point_density;
+    const uint32_t j = sub / d, i = sub % d;
+    s.a.x = c.x + ((float)i * p.subpixel_seed_step - p.subpixel_seed_halfspan);
+    s.a.y = c.y + ((float)j * p.subpixel_seed_step - p.subpixel_seed_halfspan);
+    s.rng = seed_rng(rng_idx);
+    s.l = 0.0f;
+    s.dt = g.dt_max;
+    s.n = 0;
+    s.item = item;
+    s.k = 0;
+    const uint32_t idx = pixel_of(s.a, p, g);
+    const bool masked = __ldg(mask + idx) != 0;
+    if (!masked) acc_visit(acc, base + idx, 0.0f, slc, slt);
+    s.alive = !masked && (0.0f < p.max_length) && (0u < p.max_n_steps);
+}
+
+// queue item -> (queue position, sub-pixel index)
+__device__ __forceinline__ void split_item(u64 item, uint32_t dd, uint32_t& pos, uint32_t& sub) {
+    if (item < 0x100000000ull) {  // 32-bit division unless the queue is huge
+        const uint32_t it = (uint32_t)item;
+        pos = it / dd;
+        sub = it - pos * dd;
+    } else {
+        pos = (uint32_t)(item / dd);
+        sub = (uint32_t)(item - (u64)pos * dd);
+    }
+}
+
+// Start trajectory `item` = (seed - seed_begin) * d*d + j*d + i of one grid.
 //
 // `order` (optional) maps queue positions to seed indices, so trajectories can
 // be traced in any order; the RNG stream still follows the seed index, so no
@@ -71,31 +108,11 @@ __device__ __forceinline__ void field_start(FieldLane& s, u64 item, uint32_t see
                                             const uint8_t* __restrict__ mask, const slm_params& p,
                                             Acc& acc, u64* __restrict__ slc, u64* __restrict__ slt) {
     const uint32_t d = p.subpixel_seed_point_density;
-    const uint32_t dd = d * d;
     uint32_t seed_off, sub;
-    if (item < 0x100000000ull) {  // 32-bit division unless the queue is huge
-        const uint32_t it = (uint32_t)item;
-        seed_off = it / dd;
-        sub = it - seed_off * dd;
-    } else {
-        seed_off = (uint32_t)(item / dd);
-        sub = (uint32_t)(item - (u64)seed_off * dd);
-    }
+    split_item(item, d * d, seed_off, sub);
     const uint32_t seed_idx = order ? __ldg(order + seed_begin + seed_off) : seed_begin + seed_off;
-    const uint32_t j = sub / d, i = sub % d;
-    const float2 c = __ldg(seeds + seed_idx);
-    s.a.x = c.x + ((float)i * p.subpixel_seed_step - p.subpixel_seed_halfspan);
-    s.a.y = c.y + ((float)j * p.subpixel_seed_step - p.subpixel_seed_halfspan);
-    s.rng = seed_rng(seed_idx);
-    s.l = 0.0f;
-    s.dt = p.dt_max;
-    s.n = 0;
-    s.item = (uint32_t)item;
-    s.k = 0;
-    const uint32_t idx = pixel_of(s.a, p);
-    const bool masked = __ldg(mask + idx) != 0;
-    if (!masked) acc_visit(acc, idx, 0.0f, slc, slt);
-    s.alive = !masked && (0.0f < p.max_length) && (0u < p.max_n_steps);
+    field_init(s, __ldg(seeds + seed_idx), seed_idx, sub, (uint32_t)item, mask, p, geo_of(p), 0u, acc,
+               slc, slt);
 }
 
 // One pass of the while loop of jittered_trajectory with
@@ -104,28 +121,35 @@ __device__ __forceinline__ void field_start(FieldLane& s, u64 item, uint32_t see
 template <int ORDER>
 __device__ __forceinline__ void field_step(FieldLane& s, const uint8_t* __restrict__ mask,
                                            const float2* __restrict__ uv, const slm_params& p,
-                                           Acc& acc, u64* __restrict__ slc, u64* __restrict__ slt) {
-    const Step st = rk_step<ORDER, true>(s.a, s.dt, s.rng, uv, p);
+                                           const Geo& g, uint32_t base, Acc& acc,
+                                           u64* __restrict__ slc, u64* __restrict__ slt) {
+    const Step st = rk_step<ORDER, true>(s.a, s.dt, s.rng, uv, p, g);
     if (__ldg(mask + st.idx)) {
         s.alive = false;
         return;
     }
-    const float err = vlen(__fdiv_rn(st.d2.x - st.d1.x, p.grid_scale),
-                           __fdiv_rn(st.d2.y - st.d1.y, p.grid_scale));
+    const float err = vlen(__fdiv_rn(st.d2.x - st.d1.x, g.gs), __fdiv_rn(st.d2.y - st.d1.y, g.gs));
     const float dl = vlen(st.d2.x, st.d2.y);
     s.a = st.next;
     if (dl < p.integration_halt_threshold) {
         s.l = s.l + dl;
         s.n += 1;
-        acc_visit(acc, st.idx, s.l, slc, slt);
+        acc_visit(acc, base + st.idx, s.l, slc, slt);
         s.alive = false;
         return;
     }
-    s.dt = next_dt(s.dt, err, p);
+    s.dt = next_dt(s.dt, err, p, g);
     s.l = s.l + dl;
     s.n += 1;
-    acc_visit(acc, st.idx, s.l, slc, slt);
+    acc_visit(acc, base + st.idx, s.l, slc, slt);
     s.alive = (s.l < p.max_length) && (s.n < p.max_n_steps);
+}
+
+template <int ORDER>
+__device__ __forceinline__ void field_step(FieldLane& s, const uint8_t* __restrict__ mask,
+                                           const float2* __restrict__ uv, const slm_params& p,
+                                           Acc& acc, u64* __restrict__ slc, u64* __restrict__ slt) {
+    field_step<ORDER>(s, mask, uv, p, geo_of(p), 0u, acc, slc, slt);
 }
 
 // per-trajectory RK step count, saturated to 16 bits, indexed by queue position
@@ -213,6 +237,98 @@ k_fields_persistent(const slm_params p, const float2* __restrict__ seeds, uint32
         }
         if (s.alive) {
             field_step<ORDER>(s, mask, uv, p, acc, slc, slt);
+            steps++;
+            if (RECORD) {
+                s.k++;
+                if (!s.alive) record_end<RECORD>(s, item_steps);
+            }
+        }
+    }
+    acc_flush(acc, slc, slt);
+    warp_add_counters(steps, ntraj, work);
+}
+
+// ------------------------------------------------------------------ batched tiles
+// Last tile whose first seed is <= x (tiles sorted by seed_begin; the host
+// checks the table), found by binary search over the L1-cached table.
+__device__ __forceinline__ uint32_t find_tile(const slm_tile* __restrict__ tiles, uint32_t n_tiles,
+                                              uint32_t x) {
+    uint32_t lo = 0, hi = n_tiles;
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(&tiles[mid].seed_begin) <= x) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Many grids (DTM tiles of any sizes) in one persistent launch.  The queue
+// runs over every trajectory of every tile; a lane that takes an item looks up
+// its tile and keeps the tile's geometry (Geo) and pixel base with its
+// trajectory, so lanes of one warp may trace different tiles.  Each
+// trajectory is computed exactly as a single-grid launch on its tile computes
+// it (RNG stream of the tile-local seed index).  work[3] receives 1 if a seed
+// falls outside its tile's range (an inconsistent table).
+template <int ORDER, bool RECORD>
+__global__ void __launch_bounds__(256)
+k_fields_batched(const slm_params p, const slm_tile* __restrict__ tiles, uint32_t n_tiles,
+                 const float2* __restrict__ seeds, u64 n_items, const uint8_t* __restrict__ mask,
+                 const float2* __restrict__ uv, u64* __restrict__ slc, u64* __restrict__ slt,
+                 u64* __restrict__ work, const uint32_t* __restrict__ order,
+                 uint16_t* __restrict__ item_steps) {
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    const uint32_t dd = p.subpixel_seed_point_density * p.subpixel_seed_point_density;
+    FieldLane s;
+    s.alive = false;
+    Geo g{2u, 2u, 0.0f, 0.0f, 1.0f};
+    uint32_t base = 0;
+    Acc acc{0u, 0u, 0ull};
+    u64 steps = 0, ntraj = 0;
+    bool drained = false;
+    while (true) {
+        if (!drained) {
+            const unsigned idle = __ballot_sync(FULL, !s.alive);
+            if (idle) {
+                const int leader = __ffs(idle) - 1;
+                const unsigned n_idle = __popc(idle);
+                u64 head = 0;
+                if ((int)lane == leader) head = atomicAdd(work, (u64)n_idle);
+                head = __shfl_sync(FULL, head, leader);
+                if (head + n_idle >= n_items) drained = true;
+                if (!s.alive) {
+                    const u64 item = head + __popc(idle & ((1u << lane) - 1u));
+                    if (item < n_items) {
+                        uint32_t pos, sub;
+                        split_item(item, dd, pos, sub);
+                        const uint32_t seed = order ? __ldg(order + pos) : pos;
+                        const uint32_t t = find_tile(tiles, n_tiles, seed);
+                        const slm_tile& T = tiles[t];
+                        const uint32_t local = seed - __ldg(&T.seed_begin);
+                        ntraj++;
+                        if (local < __ldg(&T.n_seeds)) {
+                            g = Geo{__ldg(&T.nx_padded), __ldg(&T.ny_padded), __ldg(&T.combo_factor),
+                                    __ldg(&T.dt_max), __ldg(&T.grid_scale)};
+                            base = (uint32_t)__ldg(&T.grid_offset);
+                            field_init(s, __ldg(seeds + seed), local, sub, (uint32_t)item, mask + base, p,
+                                       g, base, acc, slc, slt);
+                        } else {
+                            atomicOr(reinterpret_cast<unsigned long long*>(work + 3), 1ull);
+                            s.alive = false;
+                            s.item = (uint32_t)item;
+                            s.k = 0;
+                        }
+                        if (!s.alive) record_end<RECORD>(s, item_steps);
+                    }
+                }
+            }
+        }
+        if (!__any_sync(FULL, s.alive)) {
+            if (drained) break;
+            continue;
+        }
+        if (s.alive) {
+            field_step<ORDER>(s, mask + base, uv + base, p, g, base, acc, slc, slt);
             steps++;
             if (RECORD) {
                 s.k++;
@@ -351,6 +467,24 @@ static int launch_fields(const slm_params* p, const slm_launch& L, int block, co
     return SLM_OK;
 }
 
+template <int ORDER, bool RECORD>
+static int launch_batched(const slm_params* p, const slm_launch& L, int block, const slm_tile* tiles,
+                          uint32_t n_tiles, const float2* sp, u64 n_items, const uint8_t* mask,
+                          const float2* u2, u64* slc, u64* slt, u64* work, const uint32_t* order,
+                          uint16_t* rec, cudaStream_t s) {
+    int per_sm = L.blocks_per_sm;
+    if (per_sm <= 0) {
+        int occ = 0;
+        SLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fields_batched<ORDER, RECORD>, block, 0));
+        per_sm = occ > 0 ? occ : 1;
+    }
+    const unsigned grid = (unsigned)(num_sms() * per_sm);
+    k_fields_batched<ORDER, RECORD><<<grid, block, 0, s>>>(*p, tiles, n_tiles, sp, n_items, mask, u2, slc, slt,
+                                                          work, order, rec);
+    SLM_LAUNCHED("k_fields_batched");
+    return SLM_OK;
+}
+
 extern "C" {
 
 size_t slm_fields_workspace_words(void) { return 4; }
@@ -396,6 +530,43 @@ int slm_integrate_fields_scheduled(const slm_params* p, const slm_launch* launch
                           : launch_fields<4, false>(p, L, block, sp, begin, n_items, mask, u2, (u64*)slc, (u64*)slt, w, seed_order, nullptr, s);
     return item_steps ? launch_fields<2, true>(p, L, block, sp, begin, n_items, mask, u2, (u64*)slc, (u64*)slt, w, seed_order, item_steps, s)
                       : launch_fields<2, false>(p, L, block, sp, begin, n_items, mask, u2, (u64*)slc, (u64*)slt, w, seed_order, nullptr, s);
+}
+
+int slm_integrate_fields_batched(const slm_params* p, const slm_launch* launch, const slm_tile* tiles,
+                                 uint32_t n_tiles, uint32_t n_seeds, const float* seed_point,
+                                 const uint8_t* mask, const float* uv, uint64_t* slc, uint64_t* slt,
+                                 uint64_t* workspace, const uint32_t* seed_order, uint16_t* item_steps,
+                                 void* stream) {
+    clear_error();
+    SLM_REQUIRE(p != nullptr, "params is NULL");
+    SLM_REQUIRE(tiles && n_tiles >= 1, "no tiles");
+    SLM_REQUIRE(seed_point && mask && uv && slc && slt && workspace, "NULL buffer");
+    SLM_REQUIRE(aligned(uv, 8) && aligned(seed_point, 8) && aligned(tiles, 8),
+                "uv/seed_point/tiles must be 8-byte aligned");
+    SLM_REQUIRE(aligned(slc, 8) && aligned(slt, 8) && aligned(workspace, 8),
+                "slc/slt/workspace must be 8-byte aligned");
+    SLM_REQUIRE(p->subpixel_seed_point_density >= 1, "subpixel_seed_point_density is 0");
+    SLM_REQUIRE(p->trajectory_resolution > 0, "trajectory_resolution is 0");
+    slm_launch def{SLM_SCHED_PERSISTENT, SLM_RK2, 256, 0, 1, {0, 0, 0}};
+    const slm_launch& L = launch ? *launch : def;
+    SLM_REQUIRE(L.schedule == SLM_SCHED_PERSISTENT, "batched tracing runs the persistent schedule");
+    SLM_REQUIRE(L.integrator == SLM_RK2 || L.integrator == SLM_RK4, "integrator must be 2 or 4");
+    const int block = L.block_threads > 0 ? L.block_threads : 256;
+    SLM_REQUIRE(block % 32 == 0 && block <= 256, "block_threads must be a multiple of 32, <= 256");
+    cudaStream_t s = (cudaStream_t)stream;
+    SLM_CUDA(cudaMemsetAsync(workspace, 0, slm_fields_workspace_words() * sizeof(uint64_t), s));
+    if (n_seeds == 0) return SLM_OK;
+    const u64 dd = (u64)p->subpixel_seed_point_density * p->subpixel_seed_point_density;
+    const u64 n_items = (u64)n_seeds * dd;
+    SLM_REQUIRE(!item_steps || n_items < (1ull << 32), "step recording needs fewer than 2^32 trajectories");
+    const float2* sp = reinterpret_cast<const float2*>(seed_point);
+    const float2* u2 = reinterpret_cast<const float2*>(uv);
+    u64* w = (u64*)workspace;
+    if (L.integrator == SLM_RK4)
+        return item_steps ? launch_batched<4, true>(p, L, block, tiles, n_tiles, sp, n_items, mask, u2, (u64*)slc, (u64*)slt, w, seed_order, item_steps, s)
+                          : launch_batched<4, false>(p, L, block, tiles, n_tiles, sp, n_items, mask, u2, (u64*)slc, (u64*)slt, w, seed_order, nullptr, s);
+    return item_steps ? launch_batched<2, true>(p, L, block, tiles, n_tiles, sp, n_items, mask, u2, (u64*)slc, (u64*)slt, w, seed_order, item_steps, s)
+                      : launch_batched<2, false>(p, L, block, tiles, n_tiles, sp, n_items, mask, u2, (u64*)slc, (u64*)slt, w, seed_order, nullptr, s);
 }
 
 int slm_integrate_trajectory(const slm_params* p, int32_t integrator, uint32_t n_chunk,

@@ -40,18 +40,36 @@ __device__ __forceinline__ uint32_t axis_index(float c, float pp5, uint32_t n) {
     return (i < n - 1u) ? i : n - 1u;
 }
 
+// The values of the step arithmetic that belong to one grid (one DTM tile):
+// padded size and the macros the reference derives from it (pocl.py:231-277:
+// GRID_SCALE = sqrt(nx*ny), COMBO_FACTOR = GRID_SCALE * step factor * sign,
+// DT_MAX = min(1/nx, 1/ny, 0.1)).  Single-grid kernels take them from the
+// parameter block; the batched kernel holds one per lane.
+struct Geo {
+    uint32_t nxp, nyp;
+    float cf, dt_max, gs;
+};
+
+__device__ __forceinline__ Geo geo_of(const slm_params& p) {
+    return Geo{p.nx_padded, p.ny_padded, p.combo_factor, p.dt_max, p.grid_scale};
+}
+
+__device__ __forceinline__ uint32_t pixel_of(Vec2 a, const slm_params& p, const Geo& g) {
+    return axis_index(a.y, p.pad_width_pp5, g.nyp)
+         + g.nyp * axis_index(a.x, p.pad_width_pp5, g.nxp);
+}
+
 __device__ __forceinline__ uint32_t pixel_of(Vec2 a, const slm_params& p) {
-    return axis_index(a.y, p.pad_width_pp5, p.ny_padded)
-         + p.ny_padded * axis_index(a.x, p.pad_width_pp5, p.nx_padded);
+    return pixel_of(a, p, geo_of(p));
 }
 
 // Bilinear, renormalised flow vector at a (essentials.cl:24-45).
 __device__ __forceinline__ Vec2 sample_uv(Vec2 a, const float2* __restrict__ uv,
-                                          const slm_params& p) {
-    const uint32_t nyp = p.ny_padded;
-    const uint32_t xl = axis_index(a.x, p.pad_width_pp5, p.nx_padded);
-    const uint32_t yd = axis_index(a.y, p.pad_width_pp5, p.ny_padded);
-    const uint32_t xr = (xl + 1u < p.nx_padded - 1u) ? xl + 1u : p.nx_padded - 1u;
+                                          const slm_params& p, const Geo& g) {
+    const uint32_t nyp = g.nyp;
+    const uint32_t xl = axis_index(a.x, p.pad_width_pp5, g.nxp);
+    const uint32_t yd = axis_index(a.y, p.pad_width_pp5, nyp);
+    const uint32_t xr = (xl + 1u < g.nxp - 1u) ? xl + 1u : g.nxp - 1u;
     const uint32_t yu = (yd + 1u < nyp - 1u) ? yd + 1u : nyp - 1u;
     const float wr = a.x - (float)xl + (float)p.pad_width;
     const float wl = 1.0f - wr;
@@ -66,6 +84,11 @@ __device__ __forceinline__ Vec2 sample_uv(Vec2 a, const float2* __restrict__ uv,
     const float vx = bx * wd + tx * wu, vy = by * wd + ty * wu;
     const float len = __fsqrt_rn(vx * vx + vy * vy);
     return Vec2{__fdiv_rn(vx, len), __fdiv_rn(vy, len)};
+}
+
+__device__ __forceinline__ Vec2 sample_uv(Vec2 a, const float2* __restrict__ uv,
+                                          const slm_params& p) {
+    return sample_uv(a, uv, p, geo_of(p));
 }
 
 // Quantisation scale.  When trajectory_resolution is a power of two (128 by
@@ -137,18 +160,19 @@ struct Step {
 // quantisation; d1 = approx(h k1) for the error estimate).
 template <int ORDER, bool JITTER>
 __device__ __forceinline__ Step rk_step(Vec2 a, float dt, uint32_t& rng,
-                                        const float2* __restrict__ uv, const slm_params& p) {
+                                        const float2* __restrict__ uv, const slm_params& p,
+                                        const Geo& g) {
     Step s;
-    const float cf = p.combo_factor;
+    const float cf = g.cf;
     const Quant quant = make_quant(p.trajectory_resolution);
-    Vec2 k1 = sample_uv(a, uv, p);
+    Vec2 k1 = sample_uv(a, uv, p, g);
     if (JITTER) k1 = jitter(k1, rng, p.jitter_magnitude);
     s.u1 = k1;
     if (ORDER == 2) {
         s.d1.x = quant(k1.x * cf * dt);
         s.d1.y = quant(k1.y * cf * dt);
         const Vec2 b{a.x + s.d1.x, a.y + s.d1.y};
-        Vec2 k2 = sample_uv(b, uv, p);
+        Vec2 k2 = sample_uv(b, uv, p, g);
         if (JITTER) k2 = jitter(k2, rng, p.jitter_magnitude);
         s.d2.x = quant(0.5f * (s.d1.x + k2.x * cf * dt));
         s.d2.y = quant(0.5f * (s.d1.y + k2.y * cf * dt));
@@ -157,15 +181,15 @@ __device__ __forceinline__ Step rk_step(Vec2 a, float dt, uint32_t& rng,
         s.d1.x = quant(h1x);
         s.d1.y = quant(h1y);
         const Vec2 b{a.x + 0.5f * h1x, a.y + 0.5f * h1y};
-        Vec2 k2 = sample_uv(b, uv, p);
+        Vec2 k2 = sample_uv(b, uv, p, g);
         if (JITTER) k2 = jitter(k2, rng, p.jitter_magnitude);
         const float h2x = k2.x * cf * dt, h2y = k2.y * cf * dt;
         const Vec2 c{a.x + 0.5f * h2x, a.y + 0.5f * h2y};
-        Vec2 k3 = sample_uv(c, uv, p);
+        Vec2 k3 = sample_uv(c, uv, p, g);
         if (JITTER) k3 = jitter(k3, rng, p.jitter_magnitude);
         const float h3x = k3.x * cf * dt, h3y = k3.y * cf * dt;
         const Vec2 d{a.x + h3x, a.y + h3y};
-        Vec2 k4 = sample_uv(d, uv, p);
+        Vec2 k4 = sample_uv(d, uv, p, g);
         if (JITTER) k4 = jitter(k4, rng, p.jitter_magnitude);
         const float h4x = k4.x * cf * dt, h4y = k4.y * cf * dt;
         s.d2.x = quant(__fdiv_rn(h1x + 2.0f * h2x + 2.0f * h3x + h4x, 6.0f));
@@ -173,17 +197,27 @@ __device__ __forceinline__ Step rk_step(Vec2 a, float dt, uint32_t& rng,
     }
     s.next.x = a.x + s.d2.x;
     s.next.y = a.y + s.d2.y;
-    s.idx = pixel_of(s.next, p);
+    s.idx = pixel_of(s.next, p, g);
     return s;
+}
+
+template <int ORDER, bool JITTER>
+__device__ __forceinline__ Step rk_step(Vec2 a, float dt, uint32_t& rng,
+                                        const float2* __restrict__ uv, const slm_params& p) {
+    return rk_step<ORDER, JITTER>(a, dt, rng, uv, p, geo_of(p));
 }
 
 __device__ __forceinline__ float vlen(float x, float y) { return __fsqrt_rn(x * x + y * y); }
 
 // adaptive dt (rungekutta.cl:70-71): DT_MAX when the error is 0, else
 // fmin(DT_MAX, ADJUSTED_MAX_ERROR*dt/err)
+__device__ __forceinline__ float next_dt(float dt, float err, const slm_params& p, const Geo& g) {
+    const float cand = fminf(g.dt_max, __fdiv_rn(p.adjusted_max_error * dt, err));
+    return (err == 0.0f) ? g.dt_max : cand;
+}
+
 __device__ __forceinline__ float next_dt(float dt, float err, const slm_params& p) {
-    const float cand = fminf(p.dt_max, __fdiv_rn(p.adjusted_max_error * dt, err));
-    return (err == 0.0f) ? p.dt_max : cand;
+    return next_dt(dt, err, p, geo_of(p));
 }
 
 }  // namespace slm

@@ -44,7 +44,9 @@ def fbm(nx, ny, hurst, rms, rng):
     return z
 
 
-def gaussian_hills(nx, ny, n, amp_range, sigma_range, rng):
+def gaussian_hills(nx, ny, n, amp_range, sigma_range, rng, truncate=None):
+    """Sum of n Gaussian hills; with ``truncate`` (in sigmas) each hill is
+    evaluated only within that radius (for large grids; the same draws)."""
     x = np.arange(nx, dtype=np.float64)[:, None]
     y = np.arange(ny, dtype=np.float64)[None, :]
     z = np.zeros((nx, ny))
@@ -52,7 +54,15 @@ def gaussian_hills(nx, ny, n, amp_range, sigma_range, rng):
         a = rng.uniform(*amp_range)
         s = rng.uniform(*sigma_range)
         cx, cy = rng.uniform(0, nx), rng.uniform(0, ny)
-        z += a * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2.0 * s * s))
+        if truncate is None:
+            z += a * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2.0 * s * s))
+        else:
+            r = truncate * s
+            x0, x1 = max(0, int(cx - r)), min(nx, int(cx + r) + 1)
+            y0, y1 = max(0, int(cy - r)), min(ny, int(cy + r) + 1)
+            if x0 < x1 and y0 < y1:
+                xs, ys = x[x0:x1], y[:, y0:y1]
+                z[x0:x1, y0:y1] += a * np.exp(-((xs - cx) ** 2 + (ys - cy) ** 2) / (2.0 * s * s))
     return z
 
 
@@ -97,13 +107,13 @@ def config1_dtm(n=512, seed=1, fill=True):
     return z.astype(np.float32)
 
 
-def tile_dtm(nx, ny, seed):
+def tile_dtm(nx, ny, seed, hill_truncate=None):
     """Config-1-like relief without sink filling (for uneven batched tiles)."""
     rng = np.random.default_rng(seed)
     x = np.arange(nx, dtype=np.float64)[:, None]
     z = 0.05 * x + np.zeros((1, ny))
     n_hills = max(1, int(round(12 * nx * ny / 512.0 ** 2)))
-    z = z + gaussian_hills(nx, ny, n_hills, (5.0, 40.0), (20.0, 80.0), rng)
+    z = z + gaussian_hills(nx, ny, n_hills, (5.0, 40.0), (20.0, 80.0), rng, hill_truncate)
     z = z + fbm(nx, ny, 0.7, 0.5, rng)
     return z.astype(np.float32)
 
