@@ -229,6 +229,11 @@ def run_b200(args):
     stream = torch.cuda.current_stream()
     side = torch.cuda.Stream()
     traj_d2 = torch.zeros_like(traj_d)
+    from slm_b200.scheduler import spatial_order
+    spatial = args.seed_order == "spatial"
+    order_d = torch.empty(max(1, n_seeds), dtype=torch.uint32, device=dev)
+    bins_d = torch.empty(int(kernels._lib.load().slm_order_spatial_bins(
+        int(info.nx), int(info.ny), 64, 0)), dtype=torch.uint32, device=dev)
 
     def device_step(ev=None):
         # the trajectory recorder (1000 seeds, latency-bound) runs on a side
@@ -245,9 +250,12 @@ def run_b200(args):
         join.record(side)
         if ev is not None:
             ev[0].record(stream)
+        if spatial:
+            spatial_order(seeds_d, n_seeds, info.nx, info.ny, out=order_d, bins=bins_d)
         for d in range(2):
             kernels.integrate_fields(field_prm[d], seeds_d, mask_d, uv_d, acc[d, 0], acc[d, 1],
-                                     work[d], schedule=args.schedule, integrator=integrator)
+                                     work[d], schedule=args.schedule, integrator=integrator,
+                                     order=order_d if spatial else None)
         if ev is not None:
             ev[1].record(stream)
         stream.wait_event(join)
@@ -309,6 +317,8 @@ def run_b200(args):
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded DTM; no dataset)",
         "config": {"workload": spec.name, "schedule": args.schedule,
+                   "seed_order": "spatial (64 px blocks, ordered inside the timed step)"
+                   if spatial else "shuffled (the reference's)",
                    "field_trajectories_per_direction": n_seeds * spec.density ** 2,
                    "trajectory_seeds": n_traj, "l2": "256 MiB buffer written between steps",
                    "mpx_per_s": wl.n_pixels / (step_t / args.steps) / 1e6,
@@ -320,7 +330,7 @@ def run_b200(args):
                      "kernel": "k_fields_{}<{}>".format(args.schedule, integrator),
                      "bytes_per_step": bps},
         "clocks": clocks.summary(),
-        "gpu_launches": args.steps * 4,
+        "gpu_launches": args.steps * (7 if spatial else 4),
     }
     if e2e is not None:
         line["e2e"] = e2e
@@ -363,6 +373,12 @@ def sched_compare(args, wl, dev, seeds_d, mask_d, uv_d, field_prm, flush):
         st = S.record_steps(prm, tr_seeds, tr_mask, tr_uv, integrator=spec.integrator)
         cols.append(S.step_targets(st, n_tr, d))
     targets = torch.stack(cols, 1).contiguous()
+    # "predicted long" class of the learned+spatial order: the top 1% of the
+    # training targets
+    g = torch.Generator(device=dev)
+    g.manual_seed(0)
+    sub = targets[torch.randint(0, n_tr, (min(n_tr, 1 << 20),), device=dev, generator=g)]
+    long_thr = [float(torch.quantile(sub[:, c], 0.99)) for c in (0, 1)]
     model = S.LengthModel(dev, seed=0)
     torch.cuda.synchronize()
     t1 = time.time()
@@ -395,17 +411,27 @@ def sched_compare(args, wl, dev, seeds_d, mask_d, uv_d, field_prm, flush):
     work = [kernels.workspace(dev) for _ in range(2)]
     stream = torch.cuda.current_stream()
 
-    def arm(schedule, learned):
+    sbins = torch.empty(int(kernels._lib.load().slm_order_spatial_bins(
+        int(wl.info.nx), int(wl.info.ny), S.SPATIAL_BLOCK, 1)), dtype=torch.uint32, device=dev)
+
+    def arm(schedule, mode):
         acc.zero_()
-        if learned:
+        if mode in ("learned", "learned_spatial"):
             model.predict(uv_d, nxp, nyp, 2, seeds_d, n, out=pred)
-            for col in (0, 1):
+        for col in (0, 1):
+            if mode == "learned":
                 model.order(pred, col, cap, out=orders[col], bins=bins)
+            elif mode == "learned_spatial":
+                S.spatial_order(seeds_d, n, wl.info.nx, wl.info.ny, pred=pred, col=col,
+                                threshold=long_thr[col], out=orders[col], bins=sbins)
+        if mode == "spatial":
+            S.spatial_order(seeds_d, n, wl.info.nx, wl.info.ny, out=orders[0], bins=sbins)
         for col in (0, 1):
             work[col].zero_()
+            o = None if mode == "shuffled" else orders[0 if mode == "spatial" else col]
             kernels.integrate_fields(field_prm[col], seeds_d, mask_d, uv_d, acc[col, 0], acc[col, 1],
                                      work[col], schedule=schedule, integrator=spec.integrator,
-                                     order=orders[col] if learned else None)
+                                     order=o)
 
     out = {"trained_on": "{} (seed {})".format(spec.name, args.sched_train_seed),
            "train_pairs": n_tr, "train_steps": args.sched_train_steps, "train_batch": 4096,
@@ -413,31 +439,35 @@ def sched_compare(args, wl, dev, seeds_d, mask_d, uv_d, field_prm, flush):
            "loss_first": float(np.mean(hist[:10])), "loss_last": float(np.mean(hist[-50:])),
            "held_out_error": err, "ms": {}}
     ref = None
-    for schedule in ("plain", "persistent"):
-        for learned in (False, True):
-            arm(schedule, learned)
+    arms = [("plain", "shuffled"), ("plain", "learned"), ("plain", "spatial"),
+            ("persistent", "shuffled"), ("persistent", "learned"), ("persistent", "spatial"),
+            ("persistent", "learned_spatial")]
+    for schedule, mode in arms:
+        arm(schedule, mode)
+        torch.cuda.synchronize()
+        res = (acc.clone(), int(work[0][1].item()) + int(work[1][1].item()))
+        if ref is None:
+            ref = res
+        elif not (torch.equal(res[0], ref[0]) and res[1] == ref[1]):
+            raise RuntimeError("scheduled trace differs from the unsorted one")
+        ts = []
+        for _ in range(args.sched_reps):
+            flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             torch.cuda.synchronize()
-            res = (acc.clone(), int(work[0][1].item()) + int(work[1][1].item()))
-            if ref is None:
-                ref = res
-            elif not (torch.equal(res[0], ref[0]) and res[1] == ref[1]):
-                raise RuntimeError("scheduled trace differs from the unsorted one")
-            ts = []
-            for _ in range(args.sched_reps):
-                flush.fill_(1)
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                torch.cuda.synchronize()
-                e0.record(stream)
-                arm(schedule, learned)
-                e1.record(stream)
-                torch.cuda.synchronize()
-                ts.append(e0.elapsed_time(e1))
-            out["ms"][schedule + ("_learned" if learned else "")] = float(np.median(ts))
+            e0.record(stream)
+            arm(schedule, mode)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        out["ms"][schedule + ("" if mode == "shuffled" else "_" + mode)] = float(np.median(ts))
     f_steps = ref[1]
     out["field_steps"] = f_steps
     out["steps_per_s"] = {k: f_steps / (v / 1e3) for k, v in out["ms"].items()}
     out["learned_vs_plain"] = out["ms"]["plain"] / out["ms"]["plain_learned"]
     out["persistent_learned_vs_plain"] = out["ms"]["plain"] / out["ms"]["persistent_learned"]
+    out["persistent_learned_spatial_vs_plain"] = out["ms"]["plain"] / out["ms"]["persistent_learned_spatial"]
+    out["long_class_threshold_log_steps"] = long_thr
     out["identical_fields"] = True
     return out
 
@@ -602,6 +632,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-sched", action="store_true", help="skip the learned-scheduler comparison")
+    ap.add_argument("--seed-order", default="spatial", choices=["spatial", "shuffled"])
     ap.add_argument("--tiles", type=int, default=96, help="config3: number of tiles")
     ap.add_argument("--retune", action="store_true", help="config3: ignore the autotuner cache")
     ap.add_argument("--sched-train-seed", type=int, default=12)

@@ -358,6 +358,17 @@ int slm_cnn_infer(const float* uv, uint32_t nx_padded, uint32_t ny_padded, uint3
 int slm_order_by_prediction(const float* pred, uint32_t stride, uint32_t col, uint32_t n,
                             float lo, float hi, uint32_t n_bins, uint32_t* bins,
                             uint32_t* order, void* stream);
+/* Spatial seed order (no counterpart in the reference, which shuffles the
+ * seeds): order [n] lists the seeds by block_px x block_px pixel block of an
+ * nx x ny (unpadded) grid, blocks x-major, so the trajectories traced at the
+ * same time share uv / mask / slc / slt cache lines.  With pred (NULL: none),
+ * the seeds whose pred[i*stride+col] >= threshold come first, each class in
+ * spatial order.  bins: scratch of slm_order_spatial_bins(...) uint32. */
+uint32_t slm_order_spatial_bins(uint32_t nx, uint32_t ny, uint32_t block_px, int with_prediction);
+int slm_order_spatial(const float* seed_point, uint32_t n, uint32_t nx, uint32_t ny,
+                      uint32_t block_px, const float* pred, uint32_t stride, uint32_t col,
+                      float threshold, uint32_t* bins, uint32_t n_bins_capacity, uint32_t* order,
+                      void* stream);
 
 #ifdef __cplusplus
 }

@@ -345,6 +345,10 @@ k_cnn_infer(const float2* __restrict__ uv, uint32_t nxp, uint32_t nyp, uint32_t 
 }
 
 // ------------------------------------------------------------------ ordering
+// Seed orders are counting sorts of the seed indices by a small integer key
+// (a bin); seeds within one bin keep no particular order, which is harmless:
+// the traced fields do not depend on the order.
+
 // bin of a predicted log length: higher prediction -> lower bin (issued first)
 __device__ __forceinline__ uint32_t pred_bin(float v, float lo, float hi, uint32_t nb) {
     const float t = fminf(fmaxf((v - lo) / (hi - lo), 0.0f), 1.0f);  // NaN -> 0
@@ -352,29 +356,135 @@ __device__ __forceinline__ uint32_t pred_bin(float v, float lo, float hi, uint32
     return nb - 1u - b;
 }
 
-__global__ void k_bin_hist(const float* __restrict__ pred, uint32_t stride, uint32_t col, uint32_t n,
-                           float lo, float hi, uint32_t nb, uint32_t* __restrict__ hist) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) atomicAdd(hist + pred_bin(pred[(size_t)i * stride + col], lo, hi, nb), 1u);
-}
+struct PredKey {
+    const float* __restrict__ pred;
+    uint32_t stride, col;
+    float lo, hi;
+    uint32_t nb;
+    __device__ __forceinline__ uint32_t operator()(uint32_t i) const {
+        return pred_bin(pred[(size_t)i * stride + col], lo, hi, nb);
+    }
+};
 
-__global__ void k_bin_scan(uint32_t* __restrict__ hist, uint32_t nb) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    uint32_t run = 0;
-    for (uint32_t b = 0; b < nb; ++b) {
-        const uint32_t c = hist[b];
-        hist[b] = run;
-        run += c;
+// Spatial key: the block_px x block_px block of the seed's pixel, blocks in
+// x-major order (the grids' own layout), so seeds traced together lie close
+// together and their uv / mask / slc / slt lines stay in L2.  With a
+// prediction, seeds predicted at or above `thr` come first (class 0).
+struct SpatialKey {
+    const float2* __restrict__ seeds;
+    uint32_t nx, ny, bs, nby, nblocks;
+    const float* __restrict__ pred;
+    uint32_t stride, col;
+    float thr;
+    __device__ __forceinline__ uint32_t operator()(uint32_t i) const {
+        const float2 c = seeds[i];
+        const float fx = fminf(fmaxf(c.x + 0.5f, 0.0f), (float)(nx - 1u));  // NaN -> 0
+        const float fy = fminf(fmaxf(c.y + 0.5f, 0.0f), (float)(ny - 1u));
+        const uint32_t xi = (uint32_t)fx, yi = (uint32_t)fy;
+        const uint32_t cls = (pred && !(pred[(size_t)i * stride + col] >= thr)) ? 1u : 0u;
+        return cls * nblocks + (xi / bs) * nby + yi / bs;
+    }
+};
+
+constexpr uint32_t SMEM_BINS = 4096;  // bins counted in shared memory per block
+
+template <class K>
+__global__ void k_key_hist(K key, uint32_t n, uint32_t nb, uint32_t* __restrict__ hist) {
+    extern __shared__ uint32_t sh[];
+    const bool local = nb <= SMEM_BINS;
+    if (local) {
+        for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) sh[b] = 0;
+        __syncthreads();
+    }
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t b = key(i);
+        if (local) atomicAdd(sh + b, 1u);
+        else atomicAdd(hist + b, 1u);
+    }
+    if (local) {
+        __syncthreads();
+        for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x)
+            if (sh[b]) atomicAdd(hist + b, sh[b]);
     }
 }
 
-__global__ void k_bin_scatter(const float* __restrict__ pred, uint32_t stride, uint32_t col, uint32_t n,
-                              float lo, float hi, uint32_t nb, uint32_t* __restrict__ cursor,
+// Exclusive prefix sum of a[0..n) in place, one block of 1024 threads.
+__global__ void __launch_bounds__(1024) k_scan_u32(uint32_t* __restrict__ a, uint32_t n) {
+    __shared__ uint32_t wsum[32];
+    __shared__ uint32_t carry;
+    const unsigned FULL = 0xffffffffu;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < n; base += blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = i < n ? a[i] : 0u;
+        uint32_t x = v;
+#pragma unroll
+        for (uint32_t o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULL, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t w = lane < nw ? wsum[lane] : 0u;
+#pragma unroll
+            for (uint32_t o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(FULL, w, o);
+                if (lane >= o) w += y;
+            }
+            wsum[lane] = w;
+        }
+        __syncthreads();
+        const uint32_t excl = carry + (warp ? wsum[warp - 1] : 0u) + x - v;
+        if (i < n) a[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = excl + v;
+        __syncthreads();
+    }
+}
+
+// Each block places a contiguous range of seeds: per-bin counts in shared
+// memory, one global reservation per (block, bin), then local slots.
+template <class K>
+__global__ void k_key_scatter(K key, uint32_t n, uint32_t nb, uint32_t* __restrict__ cursor,
                               uint32_t* __restrict__ order) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t pos = atomicAdd(cursor + pred_bin(pred[(size_t)i * stride + col], lo, hi, nb), 1u);
-    order[pos] = i;
+    extern __shared__ uint32_t sh[];
+    const uint32_t chunk = (n + gridDim.x - 1) / gridDim.x;
+    const uint32_t b0 = blockIdx.x * chunk;
+    const uint32_t b1 = min(n, b0 + chunk);
+    if (nb > SMEM_BINS) {
+        for (uint32_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) order[atomicAdd(cursor + key(i), 1u)] = i;
+        return;
+    }
+    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) sh[b] = 0;
+    __syncthreads();
+    for (uint32_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) atomicAdd(sh + key(i), 1u);
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) {
+        const uint32_t c = sh[b];
+        sh[b] = c ? atomicAdd(cursor + b, c) : 0u;
+    }
+    __syncthreads();
+    for (uint32_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) order[atomicAdd(sh + key(i), 1u)] = i;
+}
+
+template <class K>
+static int counting_order(const K& key, uint32_t n, uint32_t nb, uint32_t* bins, uint32_t* order,
+                          cudaStream_t s) {
+    SLM_CUDA(cudaMemsetAsync(bins, 0, (size_t)nb * sizeof(uint32_t), s));
+    const size_t smem = nb <= SMEM_BINS ? (size_t)nb * sizeof(uint32_t) : 0;
+    unsigned grid = (n + 255) / 256;
+    const unsigned cap = (unsigned)num_sms() * 4u;
+    if (grid > cap) grid = cap;
+    k_key_hist<K><<<grid, 256, smem, s>>>(key, n, nb, bins);
+    SLM_LAUNCHED("k_key_hist");
+    k_scan_u32<<<1, 1024, 0, s>>>(bins, nb);
+    SLM_LAUNCHED("k_scan_u32");
+    k_key_scatter<K><<<grid, 256, smem, s>>>(key, n, nb, bins, order);
+    SLM_LAUNCHED("k_key_scatter");
+    return SLM_OK;
 }
 
 }  // namespace slm
@@ -485,16 +595,31 @@ int slm_order_by_prediction(const float* pred, uint32_t stride, uint32_t col, ui
     clear_error();
     if (n == 0) return SLM_OK;
     SLM_REQUIRE(pred && bins && order && n_bins >= 2 && hi > lo, "bad ordering arguments");
-    cudaStream_t s = (cudaStream_t)stream;
-    SLM_CUDA(cudaMemsetAsync(bins, 0, (size_t)n_bins * sizeof(uint32_t), s));
-    const unsigned grid = (n + 255) / 256;
-    k_bin_hist<<<grid, 256, 0, s>>>(pred, stride, col, n, lo, hi, n_bins, bins);
-    SLM_LAUNCHED("k_bin_hist");
-    k_bin_scan<<<1, 1, 0, s>>>(bins, n_bins);
-    SLM_LAUNCHED("k_bin_scan");
-    k_bin_scatter<<<grid, 256, 0, s>>>(pred, stride, col, n, lo, hi, n_bins, bins, order);
-    SLM_LAUNCHED("k_bin_scatter");
-    return SLM_OK;
+    return counting_order(PredKey{pred, stride, col, lo, hi, n_bins}, n, n_bins, bins, order,
+                          (cudaStream_t)stream);
+}
+
+uint32_t slm_order_spatial_bins(uint32_t nx, uint32_t ny, uint32_t block_px, int with_prediction) {
+    if (nx == 0 || ny == 0 || block_px == 0) return 0;
+    const uint64_t nbl = (uint64_t)((nx + block_px - 1) / block_px) * ((ny + block_px - 1) / block_px);
+    const uint64_t nb = nbl * (with_prediction ? 2u : 1u);
+    return nb < (1ull << 32) ? (uint32_t)nb : 0u;
+}
+
+int slm_order_spatial(const float* seed_point, uint32_t n, uint32_t nx, uint32_t ny, uint32_t block_px,
+                      const float* pred, uint32_t stride, uint32_t col, float threshold, uint32_t* bins,
+                      uint32_t n_bins_capacity, uint32_t* order, void* stream) {
+    clear_error();
+    if (n == 0) return SLM_OK;
+    SLM_REQUIRE(seed_point && bins && order, "NULL buffer");
+    SLM_REQUIRE(nx > 0 && ny > 0 && block_px > 0, "bad grid or block size");
+    const uint32_t nb = slm_order_spatial_bins(nx, ny, block_px, pred != nullptr);
+    SLM_REQUIRE(nb > 0 && nb <= n_bins_capacity, "bins holds %u entries, needs %u", n_bins_capacity, nb);
+    const uint32_t nby = (ny + block_px - 1) / block_px;
+    const uint32_t nblocks = pred ? nb / 2u : nb;
+    SpatialKey key{reinterpret_cast<const float2*>(seed_point), nx, ny, block_px, nby, nblocks, pred,
+                   stride, col, threshold};
+    return counting_order(key, n, nb, bins, order, (cudaStream_t)stream);
 }
 
 }  // extern "C"

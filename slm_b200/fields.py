@@ -33,7 +33,7 @@ from .useful import create_seeds, vprint
 class Fields:
     def __init__(self, cl_platform, cl_device, cl_src_path=None, info=None, data=None,
                  verbose=False, gpu_verbose=False, schedule="persistent", integrator=2,
-                 exact=False, process_group=None):
+                 exact=False, process_group=None, seed_order="spatial"):
         self.device = cuda_device(cl_platform, cl_device)
         self.cl_src_path = cl_src_path  # unused: kernels are prebuilt
         self.info = info
@@ -45,6 +45,12 @@ class Fields:
         self.integrator = integrator
         self.exact = exact
         self.process_group = process_group
+        # "spatial": trace seeds in pixel-block order (slm_order_spatial), which
+        # keeps large grids' working set in L2; "shuffled": the seed array's
+        # own order, as the reference.  The fields are identical either way.
+        if seed_order not in ("spatial", "shuffled"):
+            raise ValueError("seed_order must be 'spatial' or 'shuffled'")
+        self.seed_order = seed_order
         self.n_steps = [0, 0]
         self.n_trajectories = [0, 0]
 
@@ -82,13 +88,18 @@ class Fields:
             uv_d = to_device(self.data.uv_array, dev, torch.float32)
             work = kernels.workspace(dev)
             acc = torch.zeros((2, 2, nxy), dtype=torch.uint64, device=dev)  # [downup, slc/slt]
+            order = None
+            if self.seed_order == "spatial" and int(info.n_seed_points) > 0:
+                from .scheduler import spatial_order
+                order = spatial_order(seeds_d, info.n_seed_points, info.nx, info.ny)
             for downup_idx, downup_sign in ((0, +1.0), (1, -1.0)):
                 info.downup_sign = downup_sign
                 prm = kernel_params(info, "INTEGRATE_FIELDS", downup_sign)
 
                 def trace(p, slc, slt):
                     kernels.integrate_fields(p, seeds_d, mask_d, uv_d, slc, slt, work,
-                                             schedule=self.schedule, integrator=self.integrator)
+                                             schedule=self.schedule, integrator=self.integrator,
+                                             order=order)
                     return int(work[1].view(torch.int64).item())
 
                 if self.process_group is None:

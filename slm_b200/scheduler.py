@@ -235,6 +235,31 @@ class LengthModel:
         return out
 
 
+SPATIAL_BLOCK = 64
+
+
+def spatial_order(seeds, n, nx, ny, block=SPATIAL_BLOCK, pred=None, col=0, threshold=0.0, out=None,
+                  bins=None, stream=None):
+    """Seed order by ``block`` x ``block`` pixel block of the nx x ny grid
+    (uint32 [n]); with ``pred`` [n][2], seeds predicted >= ``threshold`` first.
+
+    Trajectories traced together then share cache lines of uv / mask /
+    slc / slt: on grids larger than L2 this is what keeps the tracer
+    compute-bound (the reference shuffles the seeds instead)."""
+    L = _lib.load()
+    dev = seeds.device
+    n = int(n)
+    nb = int(L.slm_order_spatial_bins(int(nx), int(ny), int(block), 1 if pred is not None else 0))
+    if out is None:
+        out = torch.empty(max(1, n), dtype=torch.uint32, device=dev)
+    if bins is None or bins.numel() < nb:
+        bins = torch.empty(max(1, nb), dtype=torch.uint32, device=dev)
+    check(L.slm_order_spatial(ptr(seeds), n, int(nx), int(ny), int(block), ptr(pred), 2, int(col),
+                              ctypes.c_float(threshold), ptr(bins), int(bins.numel()), ptr(out),
+                              _stream(stream)))
+    return out
+
+
 def log_cap(params):
     """Upper end of the prediction range for a trace: log(1 + max_n_steps)."""
     return float(math.log1p(float(params.max_n_steps)))

@@ -197,3 +197,41 @@ def test_learned_order_beats_shuffled():
         print("warp cost", col, ideal, learned, shuffled, "spearman", rho)
         assert ideal <= learned < 0.92 * shuffled, (col, ideal, learned, shuffled)
         assert rho > 0.3, rho
+
+
+@pytest.mark.parametrize("block", [64, 4])  # 64: bins counted in shared memory; 4: 5625 bins, global
+@pytest.mark.parametrize("with_pred", [False, True])
+def test_spatial_order(block, with_pred):
+    rng = np.random.default_rng(10)
+    nx, ny, n = 300, 300, 70001
+    seeds = np.stack([rng.integers(0, nx, n), rng.integers(0, ny, n)], 1).astype(np.float32)
+    seeds[3] = [np.nan, -5.0]  # clamped into the grid
+    pred = rng.uniform(0, 8, (n, 2)).astype(np.float32)
+    sd, pd = torch.from_numpy(seeds).to(DEV), torch.from_numpy(pred).to(DEV)
+    order = S.spatial_order(sd, n, nx, ny, block=block, pred=pd if with_pred else None, col=1,
+                            threshold=6.0).cpu().numpy().astype(np.int64)
+    assert np.array_equal(np.sort(order), np.arange(n))
+    xs = np.clip(np.nan_to_num(seeds[:, 0] + 0.5, nan=0.0), 0, nx - 1).astype(np.int64)
+    ys = np.clip(np.nan_to_num(seeds[:, 1] + 0.5, nan=0.0), 0, ny - 1).astype(np.int64)
+    nby = -(-ny // block)
+    key = (xs // block) * nby + ys // block
+    if with_pred:
+        key = key + (pred[:, 1] < 6.0) * (-(-nx // block) * nby)
+    assert np.all(np.diff(key[order]) >= 0)
+
+
+def test_fields_spatial_order_identical():
+    """Fields (the public API) traces in spatial order by default; the raw
+    fields equal those of the reference's shuffled order."""
+    from slm_b200.fields import Fields
+    from slm_b200.useful import Data
+    c = Case(nx=90, ny=70, seed=61, density=2, step=0.25, max_length=80.0)
+    out = []
+    for order in ("shuffled", "spatial"):
+        data = Data(mask_array=c.mask, uv_array=c.uv)
+        data.seed_point_array = c.seeds
+        f = Fields(0, 0, info=c.info, data=data, seed_order=order)
+        f.gpu_integrate()
+        out.append((data.slc_array.copy(), data.slt_array.copy(), list(f.n_steps)))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    assert out[0][2] == out[1][2] and out[0][2][0] > 0
