@@ -79,7 +79,9 @@ typedef struct slm_launch {
     int32_t integrator;      /* SLM_RK2 or SLM_RK4 */
     int32_t block_threads;   /* threads per block (multiple of 32); 0 = default */
     int32_t blocks_per_sm;   /* persistent schedule: resident blocks per SM; 0 = default */
-    int32_t chunk;           /* persistent schedule: items taken per queue grab per lane */
+    int32_t chunk;           /* persistent schedule: a warp takes new trajectories from the
+                                queue once at least this many of its lanes are idle (or all
+                                are); 1 = as soon as one lane is idle; 0 = default (4) */
     int32_t reserved[3];
 } slm_launch;
 

@@ -1,7 +1,8 @@
 """Launch-shape autotuner for the persistent field kernels.
 
 Times a caller-supplied run (one trace of a representative sample) for each
-candidate launch shape -- threads per block x resident blocks per SM -- with
+candidate launch shape -- threads per block x resident blocks per SM x refill
+threshold (idle lanes a warp waits for before taking new work) -- with
 CUDA events, keeps the fastest, and caches the choice in a JSON file keyed by
 device name, kernel, integrator and a caller-given workload signature, so
 later runs reuse it without tuning.
@@ -21,13 +22,19 @@ CACHE_PATH = os.environ.get(
     "SLM_AUTOTUNE_CACHE", os.path.join(os.path.dirname(os.path.abspath(__file__)), "_autotune.json"))
 _lock = threading.Lock()
 
-# threads per block -> resident blocks per SM to try (bounded by the
-# register-limited occupancy, which the library clamps to on launch)
-CANDIDATES = {64: (8, 12, 16, 20), 128: (4, 6, 8, 10), 256: (2, 3, 4, 5)}
+# (threads per block, resident blocks per SM, refill threshold): the
+# threshold is slm_launch.chunk, the number of idle lanes a warp waits for
+# before it takes new trajectories from the queue
+CANDIDATES = [(256, 5, c) for c in (1, 2, 4, 8, 16)] + [(256, 4, c) for c in (1, 4)] \
+    + [(128, 10, c) for c in (1, 4)] + [(128, 8, 4), (64, 20, 4), (64, 16, 4)]
 
 
 def candidates():
-    return [(b, k) for b, ks in CANDIDATES.items() for k in ks]
+    return list(CANDIDATES)
+
+
+def _shape(c):
+    return (c[0], c[1], c[2] if len(c) > 2 else 0)
 
 
 def _load(path):
@@ -53,12 +60,14 @@ def tune(run, kernel, integrator, signature, reps=2, path=CACHE_PATH, force=Fals
     with _lock:
         cache = _load(path)
     if not force and key in cache:
-        b, k = cache[key]["block_threads"], cache[key]["blocks_per_sm"]
-        return kernels.launch_config("persistent", integrator, b, k), {}
+        e = cache[key]
+        return kernels.launch_config("persistent", integrator, e["block_threads"], e["blocks_per_sm"],
+                                     e.get("chunk", 1)), {}
     table = {}
     best = None
-    for b, k in (shapes or candidates()):
-        L = kernels.launch_config("persistent", integrator, b, k)
+    for cand in (shapes or candidates()):
+        b, k, c = _shape(cand)
+        L = kernels.launch_config("persistent", integrator, b, k, c)
         run(L)  # warm-up
         ts = []
         for _ in range(reps):
@@ -70,15 +79,15 @@ def tune(run, kernel, integrator, signature, reps=2, path=CACHE_PATH, force=Fals
             torch.cuda.synchronize()
             ts.append(e0.elapsed_time(e1))
         ms = float(np.median(ts))
-        table["{}x{}".format(b, k)] = ms
+        table["{}x{}" .format(b, k) + ("" if len(cand) == 2 else "/{}".format(c))] = ms
         if best is None or ms < best[0]:
-            best = (ms, b, k)
-    _, b, k = best
+            best = (ms, b, k, c)
+    _, b, k, c = best
     with _lock:
         cache = _load(path)
-        cache[key] = {"block_threads": b, "blocks_per_sm": k, "ms": best[0], "table": table}
+        cache[key] = {"block_threads": b, "blocks_per_sm": k, "chunk": c, "ms": best[0], "table": table}
         tmp = path + ".tmp"
         with open(tmp, "w") as f:
             json.dump(cache, f, indent=1, sort_keys=True)
         os.replace(tmp, path)
-    return kernels.launch_config("persistent", integrator, b, k), table
+    return kernels.launch_config("persistent", integrator, b, k, c), table

@@ -106,13 +106,13 @@ __device__ __forceinline__ void field_start(FieldLane& s, u64 item, uint32_t see
                                             const float2* __restrict__ seeds,
                                             const uint32_t* __restrict__ order,
                                             const uint8_t* __restrict__ mask, const slm_params& p,
-                                            Acc& acc, u64* __restrict__ slc, u64* __restrict__ slt) {
+                                            const Geo& g, Acc& acc, u64* __restrict__ slc,
+                                            u64* __restrict__ slt) {
     const uint32_t d = p.subpixel_seed_point_density;
     uint32_t seed_off, sub;
     split_item(item, d * d, seed_off, sub);
     const uint32_t seed_idx = order ? __ldg(order + seed_begin + seed_off) : seed_begin + seed_off;
-    field_init(s, __ldg(seeds + seed_idx), seed_idx, sub, (uint32_t)item, mask, p, geo_of(p), 0u, acc,
-               slc, slt);
+    field_init(s, __ldg(seeds + seed_idx), seed_idx, sub, (uint32_t)item, mask, p, g, 0u, acc, slc, slt);
 }
 
 // One pass of the while loop of jittered_trajectory with
@@ -128,7 +128,7 @@ __device__ __forceinline__ void field_step(FieldLane& s, const uint8_t* __restri
         s.alive = false;
         return;
     }
-    const float err = vlen(__fdiv_rn(st.d2.x - st.d1.x, g.gs), __fdiv_rn(st.d2.y - st.d1.y, g.gs));
+    const float err = vlen(div_gs(st.d2.x - st.d1.x, g), div_gs(st.d2.y - st.d1.y, g));
     const float dl = vlen(st.d2.x, st.d2.y);
     s.a = st.next;
     if (dl < p.integration_halt_threshold) {
@@ -145,12 +145,6 @@ __device__ __forceinline__ void field_step(FieldLane& s, const uint8_t* __restri
     s.alive = (s.l < p.max_length) && (s.n < p.max_n_steps);
 }
 
-template <int ORDER>
-__device__ __forceinline__ void field_step(FieldLane& s, const uint8_t* __restrict__ mask,
-                                           const float2* __restrict__ uv, const slm_params& p,
-                                           Acc& acc, u64* __restrict__ slc, u64* __restrict__ slt) {
-    field_step<ORDER>(s, mask, uv, p, geo_of(p), 0u, acc, slc, slt);
-}
 
 // per-trajectory RK step count, saturated to 16 bits, indexed by queue position
 template <bool RECORD>
@@ -179,12 +173,13 @@ k_fields_plain(const slm_params p, const float2* __restrict__ seeds, uint32_t se
     const u64 item = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     u64 steps = 0, ntraj = 0;
     Acc acc{0u, 0u, 0ull};
+    const Geo g = geo_of(p);
     if (item < n_items) {
         FieldLane s;
-        field_start(s, item, seed_begin, seeds, order, mask, p, acc, slc, slt);
+        field_start(s, item, seed_begin, seeds, order, mask, p, g, acc, slc, slt);
         ntraj = 1;
         while (s.alive) {
-            field_step<ORDER>(s, mask, uv, p, acc, slc, slt);
+            field_step<ORDER>(s, mask, uv, p, g, 0u, acc, slc, slt);
             steps++;
             if (RECORD) s.k++;
         }
@@ -203,9 +198,11 @@ __global__ void __launch_bounds__(256)
 k_fields_persistent(const slm_params p, const float2* __restrict__ seeds, uint32_t seed_begin,
                     u64 n_items, const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
                     u64* __restrict__ slc, u64* __restrict__ slt, u64* __restrict__ work,
-                    const uint32_t* __restrict__ order, uint16_t* __restrict__ item_steps) {
+                    const uint32_t* __restrict__ order, uint16_t* __restrict__ item_steps,
+                    uint32_t refill_min) {
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
+    const Geo g = geo_of(p);
     FieldLane s;
     s.alive = false;
     Acc acc{0u, 0u, 0ull};
@@ -214,7 +211,7 @@ k_fields_persistent(const slm_params p, const float2* __restrict__ seeds, uint32
     while (true) {
         if (!drained) {
             const unsigned idle = __ballot_sync(FULL, !s.alive);
-            if (idle) {
+            if (idle && (idle == FULL || (uint32_t)__popc(idle) >= refill_min)) {
                 const int leader = __ffs(idle) - 1;
                 const unsigned n_idle = __popc(idle);
                 u64 base = 0;
@@ -224,7 +221,7 @@ k_fields_persistent(const slm_params p, const float2* __restrict__ seeds, uint32
                 if (!s.alive) {
                     const u64 item = base + __popc(idle & ((1u << lane) - 1u));
                     if (item < n_items) {
-                        field_start(s, item, seed_begin, seeds, order, mask, p, acc, slc, slt);
+                        field_start(s, item, seed_begin, seeds, order, mask, p, g, acc, slc, slt);
                         ntraj++;
                         if (!s.alive) record_end<RECORD>(s, item_steps);
                     }
@@ -236,7 +233,7 @@ k_fields_persistent(const slm_params p, const float2* __restrict__ seeds, uint32
             continue;
         }
         if (s.alive) {
-            field_step<ORDER>(s, mask, uv, p, acc, slc, slt);
+            field_step<ORDER>(s, mask, uv, p, g, 0u, acc, slc, slt);
             steps++;
             if (RECORD) {
                 s.k++;
@@ -270,18 +267,18 @@ __device__ __forceinline__ uint32_t find_tile(const slm_tile* __restrict__ tiles
 // it (RNG stream of the tile-local seed index).  work[3] receives 1 if a seed
 // falls outside its tile's range (an inconsistent table).
 template <int ORDER, bool RECORD>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 5)
 k_fields_batched(const slm_params p, const slm_tile* __restrict__ tiles, uint32_t n_tiles,
                  const float2* __restrict__ seeds, u64 n_items, const uint8_t* __restrict__ mask,
                  const float2* __restrict__ uv, u64* __restrict__ slc, u64* __restrict__ slt,
                  u64* __restrict__ work, const uint32_t* __restrict__ order,
-                 uint16_t* __restrict__ item_steps) {
+                 uint16_t* __restrict__ item_steps, uint32_t refill_min) {
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
     const uint32_t dd = p.subpixel_seed_point_density * p.subpixel_seed_point_density;
     FieldLane s;
     s.alive = false;
-    Geo g{2u, 2u, 0.0f, 0.0f, 1.0f};
+    Geo g = make_geo(2u, 2u, 0.0f, 0.0f, 1.0f);
     uint32_t base = 0;
     Acc acc{0u, 0u, 0ull};
     u64 steps = 0, ntraj = 0;
@@ -289,7 +286,7 @@ k_fields_batched(const slm_params p, const slm_tile* __restrict__ tiles, uint32_
     while (true) {
         if (!drained) {
             const unsigned idle = __ballot_sync(FULL, !s.alive);
-            if (idle) {
+            if (idle && (idle == FULL || (uint32_t)__popc(idle) >= refill_min)) {
                 const int leader = __ffs(idle) - 1;
                 const unsigned n_idle = __popc(idle);
                 u64 head = 0;
@@ -307,8 +304,8 @@ k_fields_batched(const slm_params p, const slm_tile* __restrict__ tiles, uint32_
                         const uint32_t local = seed - __ldg(&T.seed_begin);
                         ntraj++;
                         if (local < __ldg(&T.n_seeds)) {
-                            g = Geo{__ldg(&T.nx_padded), __ldg(&T.ny_padded), __ldg(&T.combo_factor),
-                                    __ldg(&T.dt_max), __ldg(&T.grid_scale)};
+                            g = make_geo(__ldg(&T.nx_padded), __ldg(&T.ny_padded), __ldg(&T.combo_factor),
+                                         __ldg(&T.dt_max), __ldg(&T.grid_scale));
                             base = (uint32_t)__ldg(&T.grid_offset);
                             field_init(s, __ldg(seeds + seed), local, sub, (uint32_t)item, mask + base, p,
                                        g, base, acc, slc, slt);
@@ -379,13 +376,13 @@ k_trajectory(const slm_params p, uint32_t n_chunk, const float2* __restrict__ se
     Vec2 a{c.x, c.y}, prev = a;
     uint32_t n = 0, rng = 0;
     float l = 0.0f, dt = p.dt_max;
-    uint32_t idx = pixel_of(a, p);
+    const Geo geo = geo_of(p);
+    uint32_t idx = pixel_of(a, p, geo);
     while (!__ldg(mask + idx) && (l < p.max_length && n < p.max_n_steps)) {
-        const Step st = rk_step<ORDER, false>(a, dt, rng, uv, p);
+        const Step st = rk_step<ORDER, false>(a, dt, rng, uv, p, geo);
         idx = st.idx;
         if (!__ldg(mask + idx)) {
-            const float err = vlen(__fdiv_rn(st.d2.x - st.d1.x, p.grid_scale),
-                                   __fdiv_rn(st.d2.y - st.d1.y, p.grid_scale));
+            const float err = vlen(div_gs(st.d2.x - st.d1.x, geo), div_gs(st.d2.y - st.d1.y, geo));
             Vec2 next = st.next;
             float dl = vlen(st.d2.x, st.d2.y);
             if (dl < p.integration_halt_threshold) {
@@ -394,9 +391,9 @@ k_trajectory(const slm_params p, uint32_t n_chunk, const float2* __restrict__ se
                 dl = vlen(st.d1.x, st.d1.y);
             }
             a = next;
-            idx = pixel_of(next, p);
+            idx = pixel_of(next, p, geo);
             const bool stuck = dl < p.integration_halt_threshold;
-            if (!stuck) dt = next_dt(dt, err, p);
+            if (!stuck) dt = next_dt(dt, err, p, geo);
             l = l + dl;
             put_step(rec, n, a.x - prev.x, a.y - prev.y, res);
             n++;
@@ -439,6 +436,14 @@ static int check_grid(const slm_params* p) {
     return SLM_OK;
 }
 
+// slm_launch.chunk: a warp takes queue items once at least this many of its
+// lanes are idle (or all are); 0 selects 4, which measured best on the 2048^2
+// and 8192^2 RK4 workloads (fewer refill passes run by one or two lanes).
+static uint32_t refill_min(const slm_launch& L) {
+    if (L.chunk == 0) return 4u;
+    return L.chunk <= 1 ? 1u : (L.chunk >= 32 ? 32u : (uint32_t)L.chunk);
+}
+
 template <int ORDER, bool RECORD>
 static int launch_fields(const slm_params* p, const slm_launch& L, int block, const float2* sp,
                          uint32_t begin, u64 n_items, const uint8_t* mask, const float2* u2, u64* slc,
@@ -458,7 +463,7 @@ static int launch_fields(const slm_params* p, const slm_launch& L, int block, co
         }
         const unsigned grid = (unsigned)(num_sms() * per_sm);
         k_fields_persistent<ORDER, RECORD><<<grid, block, 0, s>>>(*p, sp, begin, n_items, mask, u2, slc, slt,
-                                                                  work, order, rec);
+                                                                  work, order, rec, refill_min(L));
         SLM_LAUNCHED("k_fields_persistent");
     } else {
         set_error("unknown schedule %d", L.schedule);
@@ -480,7 +485,7 @@ static int launch_batched(const slm_params* p, const slm_launch& L, int block, c
     }
     const unsigned grid = (unsigned)(num_sms() * per_sm);
     k_fields_batched<ORDER, RECORD><<<grid, block, 0, s>>>(*p, tiles, n_tiles, sp, n_items, mask, u2, slc, slt,
-                                                          work, order, rec);
+                                                          work, order, rec, refill_min(L));
     SLM_LAUNCHED("k_fields_batched");
     return SLM_OK;
 }
@@ -510,7 +515,7 @@ int slm_integrate_fields_scheduled(const slm_params* p, const slm_launch* launch
     SLM_REQUIRE(aligned(slc, 8) && aligned(slt, 8) && aligned(workspace, 8),
                 "slc/slt/workspace must be 8-byte aligned");
     SLM_REQUIRE(p->subpixel_seed_point_density >= 1, "subpixel_seed_point_density is 0");
-    slm_launch def{SLM_SCHED_PERSISTENT, SLM_RK2, 256, 0, 1, {0, 0, 0}};
+    slm_launch def{SLM_SCHED_PERSISTENT, SLM_RK2, 256, 0, 0, {0, 0, 0}};
     const slm_launch& L = launch ? *launch : def;
     SLM_REQUIRE(L.integrator == SLM_RK2 || L.integrator == SLM_RK4, "integrator must be 2 or 4");
     const int block = L.block_threads > 0 ? L.block_threads : 256;
@@ -547,7 +552,7 @@ int slm_integrate_fields_batched(const slm_params* p, const slm_launch* launch, 
                 "slc/slt/workspace must be 8-byte aligned");
     SLM_REQUIRE(p->subpixel_seed_point_density >= 1, "subpixel_seed_point_density is 0");
     SLM_REQUIRE(p->trajectory_resolution > 0, "trajectory_resolution is 0");
-    slm_launch def{SLM_SCHED_PERSISTENT, SLM_RK2, 256, 0, 1, {0, 0, 0}};
+    slm_launch def{SLM_SCHED_PERSISTENT, SLM_RK2, 256, 0, 0, {0, 0, 0}};
     const slm_launch& L = launch ? *launch : def;
     SLM_REQUIRE(L.schedule == SLM_SCHED_PERSISTENT, "batched tracing runs the persistent schedule");
     SLM_REQUIRE(L.integrator == SLM_RK2 || L.integrator == SLM_RK4, "integrator must be 2 or 4");

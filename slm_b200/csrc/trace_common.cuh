@@ -48,10 +48,28 @@ __device__ __forceinline__ uint32_t axis_index(float c, float pp5, uint32_t n) {
 struct Geo {
     uint32_t nxp, nyp;
     float cf, dt_max, gs;
+    float gs_inv;  // 1/gs when gs is a power of two (x/gs == x*gs_inv exactly), else 0
 };
 
+__device__ __forceinline__ float pow2_reciprocal(float v) {
+    const uint32_t b = __float_as_uint(v);
+    const uint32_t e = (b >> 23) & 0xffu;
+    const bool pow2 = (b >> 31) == 0u && (b & 0x7fffffu) == 0u && e >= 1u && e <= 253u;
+    return pow2 ? __fdiv_rn(1.0f, v) : 0.0f;
+}
+
+__device__ __forceinline__ Geo make_geo(uint32_t nxp, uint32_t nyp, float cf, float dt_max, float gs) {
+    return Geo{nxp, nyp, cf, dt_max, gs, pow2_reciprocal(gs)};
+}
+
 __device__ __forceinline__ Geo geo_of(const slm_params& p) {
-    return Geo{p.nx_padded, p.ny_padded, p.combo_factor, p.dt_max, p.grid_scale};
+    return make_geo(p.nx_padded, p.ny_padded, p.combo_factor, p.dt_max, p.grid_scale);
+}
+
+// x / GRID_SCALE: a multiplication when GRID_SCALE is a power of two (both
+// are the correctly rounded value of the same quotient)
+__device__ __forceinline__ float div_gs(float x, const Geo& g) {
+    return g.gs_inv != 0.0f ? x * g.gs_inv : __fdiv_rn(x, g.gs);
 }
 
 __device__ __forceinline__ uint32_t pixel_of(Vec2 a, const slm_params& p, const Geo& g) {

@@ -36,7 +36,7 @@ def workspace(device=None):
     return torch.zeros(n, dtype=torch.uint64, device=device or "cuda")
 
 
-def launch_config(schedule="persistent", integrator=2, block_threads=0, blocks_per_sm=0, chunk=1):
+def launch_config(schedule="persistent", integrator=2, block_threads=0, blocks_per_sm=0, chunk=0):
     L = SlmLaunch()
     L.schedule = SCHEDULES[schedule] if isinstance(schedule, str) else int(schedule)
     L.integrator = int(integrator)
@@ -48,7 +48,7 @@ def launch_config(schedule="persistent", integrator=2, block_threads=0, blocks_p
 
 def integrate_fields(params, seeds, mask, uv, slc, slt, work, schedule="persistent",
                      integrator=2, block_threads=0, blocks_per_sm=0, stream=None,
-                     order=None, item_steps=None):
+                     order=None, item_steps=None, chunk=0):
     """Trace every seed's d*d jittered trajectories, adding into slc/slt (uint64).
 
     ``order`` (uint32 per seed, optional) issues seeds in that order (results
@@ -62,7 +62,7 @@ def integrate_fields(params, seeds, mask, uv, slc, slt, work, schedule="persiste
     _need(slc, torch.uint64, nxy, "slc")
     _need(slt, torch.uint64, nxy, "slt")
     _need(work, torch.uint64, lib.slm_fields_workspace_words(), "workspace")
-    L = launch_config(schedule, integrator, block_threads, blocks_per_sm)
+    L = launch_config(schedule, integrator, block_threads, blocks_per_sm, chunk)
     if order is not None:
         _need(order, torch.uint32, int(params.n_seed_points), "order")
     if item_steps is not None:
