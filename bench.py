@@ -604,10 +604,15 @@ def run_e2e(args, wl, dev):
     t = time.perf_counter() - t0
     nxy = wl.mask.size
     h2d = wl.uv.nbytes * 2 + wl.mask.nbytes * 2 + wl.seeds.nbytes + wl.traj_seeds.nbytes
-    d2h = nxy * 4 * 4 + wl.n_traj * 2 * (2 + 4)
+    # finished slc (float64), slt and sla (float32) per direction, the
+    # trajectory step counts and lengths (recorded steps come back as well,
+    # up to each trajectory's length)
+    d2h = nxy * 2 * (8 + 4 + 4) + wl.n_traj * 2 * (2 + 4)
     return {"value": n / t, "unit": "steps/s", "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "steps": k,
-            "note": "Trajectories.integrate + Fields.integrate incl. seed shuffle and host post-processing"}
+            "note": "Trajectories.integrate + Fields.integrate through the public API: seed "
+                    "creation and shuffle, uploads, tracing, the fields' post-processing (on the "
+                    "GPU) and the finished arrays copied back, every step"}
 
 
 def cpu_baseline(wl, args):

@@ -188,6 +188,22 @@ int slm_integrate_fields_noalloc(const slm_params* p, const slm_launch* launch,
                                  const float* seed_point, const uint8_t* mask, const float* uv,
                                  uint32_t* mapping, uint64_t* slc, uint64_t* slt, void* stream);
 
+/* slm_fields_finish: the host arithmetic of Fields.integrate
+ * (fields.py:146-167, 293-310) on the device, so only the finished fields
+ * leave the GPU.  acc [2 directions][slc, slt][nxy_padded] uint64 raw sums
+ * (as accumulated by slm_integrate_fields); ds_scale_* = mean ds / pixel
+ * size per direction (the trajectory statistics).  Outputs [nxy_padded][2]
+ * (direction innermost, the (nxp, nyp, 2) arrays): slc float64, slt and
+ * sla float32.  The same NumPy promotion order as the reference (raw sums
+ * wrapped to uint32 unless exact); slc's pow(x, 2/3) is taken from
+ * slc_table[count] when count < table_len (a table the caller computes with
+ * the reference expression, for bit-identical values), else computed here
+ * (within 2 ulp). */
+int slm_fields_finish(const uint64_t* acc, uint32_t nxy_padded, uint32_t density,
+                      double ds_scale_down, double ds_scale_up, int exact,
+                      const double* slc_table, uint32_t table_len, double* slc_out,
+                      float* slt_out, float* sla_out, void* stream);
+
 /* integrate_trajectory: one un-jittered trajectory per seed of the chunk
  * seeds_chunk_offset .. seeds_chunk_offset+n_chunk-1 (clipped to
  * n_seed_points), recording each step as a char2 at 1/trajectory_resolution

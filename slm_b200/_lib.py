@@ -59,6 +59,8 @@ SIGNATURES = {
     "slm_integrate_fields_noalloc": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_integrate_fields_scheduled": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_integrate_fields_batched": (ctypes.c_int, [_P, _P, _P, _U, _U, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "slm_fields_finish": (ctypes.c_int, [_P, _U, _U, ctypes.c_double, ctypes.c_double, _I, _P, _U, _P, _P,
+                                         _P, _P]),
     "slm_integrate_trajectory": (ctypes.c_int, [_P, _I, _U, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_histogram_univariate": (ctypes.c_int, [_P, _P, _U, _P, _P]),
     "slm_histogram_bivariate": (ctypes.c_int, [_P, _P, _U, _P, _P]),

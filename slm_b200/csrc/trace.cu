@@ -422,6 +422,52 @@ k_trajectory(const slm_params p, uint32_t n_chunk, const float2* __restrict__ se
     length_out[g] = l;
 }
 
+// ------------------------------------------------------------------ finish
+// Fields.integrate's host arithmetic on the raw sums (fields.py:146-167 and
+// :293-310), in NumPy's promotion order: per pixel and direction
+//   slc  (uint32 wrap of the sum, or float64 of it when exact)
+//   slt  float32(slt)                    (exact: float32(float64(sum)))
+//   sla  float32(float64(sqrt 2) * slt / slc)       where slc > 0, else 0
+//   slt  float32(float64(slt) / d^2)                where slc > 0
+//   slt  float32(slt * ds_scale[dir]),  slt = sqrt(slt)
+//   slc  sqrt 2 * pow(slc / d^2, 2/3)   (float64; table[slc] when given)
+// Outputs are [nxy][2] (direction innermost), as the (nxp, nyp, 2) arrays.
+__global__ void k_fields_finish(const u64* __restrict__ acc, uint32_t nxy, uint32_t dd, double ds0,
+                                double ds1, int exact, const double* __restrict__ table,
+                                uint32_t table_len, double* __restrict__ slc_out,
+                                float* __restrict__ slt_out, float* __restrict__ sla_out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nxy) return;
+    const double sqrt2 = 1.4142135623730951;  // np.sqrt(2.0), correctly rounded
+#pragma unroll
+    for (int d = 0; d < 2; ++d) {
+        const u64 c64 = acc[(size_t)(2 * d) * nxy + i];
+        const u64 t64 = acc[(size_t)(2 * d + 1) * nxy + i];
+        double c;
+        float t;
+        if (exact) {
+            c = (double)c64;
+            t = (float)(double)t64;
+        } else {
+            c = (double)(uint32_t)c64;
+            t = (float)(uint32_t)t64;
+        }
+        float a = 0.0f;
+        if (c > 0.0) {
+            a = (float)((sqrt2 * (double)t) / c);
+            t = (float)((double)t / (double)dd);  // d^2 is a uint32 scalar: float64 division
+        }
+        t = (float)((double)t * (d == 0 ? ds0 : ds1));
+        t = sqrtf(t);
+        double f;
+        if (table && c < (double)table_len) f = table[(uint32_t)c];
+        else f = sqrt2 * pow(c / (double)dd, 2.0 / 3.0);
+        slc_out[2 * (size_t)i + d] = f;
+        slt_out[2 * (size_t)i + d] = t;
+        sla_out[2 * (size_t)i + d] = a;
+    }
+}
+
 }  // namespace slm
 
 using namespace slm;
@@ -572,6 +618,22 @@ int slm_integrate_fields_batched(const slm_params* p, const slm_launch* launch, 
                           : launch_batched<4, false>(p, L, block, tiles, n_tiles, sp, n_items, mask, u2, (u64*)slc, (u64*)slt, w, seed_order, nullptr, s);
     return item_steps ? launch_batched<2, true>(p, L, block, tiles, n_tiles, sp, n_items, mask, u2, (u64*)slc, (u64*)slt, w, seed_order, item_steps, s)
                       : launch_batched<2, false>(p, L, block, tiles, n_tiles, sp, n_items, mask, u2, (u64*)slc, (u64*)slt, w, seed_order, nullptr, s);
+}
+
+int slm_fields_finish(const uint64_t* acc, uint32_t nxy_padded, uint32_t density, double ds_scale_down,
+                      double ds_scale_up, int exact, const double* slc_table, uint32_t table_len,
+                      double* slc_out, float* slt_out, float* sla_out, void* stream) {
+    clear_error();
+    if (nxy_padded == 0) return SLM_OK;
+    SLM_REQUIRE(acc && slc_out && slt_out && sla_out, "NULL buffer");
+    SLM_REQUIRE(density >= 1, "density is 0");
+    SLM_REQUIRE(aligned(acc, 8) && aligned(slc_out, 8) && aligned(slt_out, 4) && aligned(sla_out, 4),
+                "misaligned buffer");
+    k_fields_finish<<<(nxy_padded + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+        (const u64*)acc, nxy_padded, density * density, ds_scale_down, ds_scale_up, exact, slc_table,
+        slc_table ? table_len : 0u, slc_out, slt_out, sla_out);
+    SLM_LAUNCHED("k_fields_finish");
+    return SLM_OK;
 }
 
 int slm_integrate_trajectory(const slm_params* p, int32_t integrator, uint32_t n_chunk,

@@ -5,7 +5,11 @@ constructor, same ``integrate()`` contract on ``data`` -- fills
 ``data.seed_point_array`` and ``data.slc_array`` / ``slt_array`` /
 ``sla_array`` of shape ``(nxp, nyp, 2)`` (index 0 downstream, 1 upstream) --
 with the tracing done by the CUDA kernels of ``libslm_b200.so`` instead of
-PyOpenCL.  The host post-processing is the reference's, step for step.
+PyOpenCL.  ``integrate()`` runs the reference's post-processing on the GPU
+(``slm_fields_finish``, NumPy's promotion order, the pow of slc through a
+table computed with the reference expression) and copies back only the
+finished arrays; ``gpu_integrate()`` alone leaves the reference's raw
+intermediate arrays, converted on the host step for step.
 
 Differences from the reference (none changes a result):
 * one parameter block per pass instead of an OpenCL program rebuild per pass;
@@ -28,6 +32,36 @@ from .device import cuda_device, low32, to_device
 from .distributed import sharded_field_pass
 from .params import kernel_params
 from .useful import create_seeds, vprint
+
+
+_SLC_TABLES = {}
+
+
+def _slc_table(dev, dd, n):
+    """Device table of sqrt(2) * (count / d^2) ** (2/3) for counts 0..n-1,
+    computed with the reference's NumPy expression (so looked-up values are
+    the reference's bit for bit); kept per device and d^2, grown on demand."""
+    key = (str(dev), int(dd))
+    t = _SLC_TABLES.get(key)
+    if t is None or t.numel() < n:
+        m = max(n, 2 * t.numel() if t is not None else 0, 1 << 16)
+        table = np.sqrt(2.0) * np.power(np.arange(m) / dd, 2 / 3)
+        t = torch.from_numpy(table).to(dev)
+        _SLC_TABLES[key] = t
+    return t
+
+
+_STAGING = {}
+
+
+def _staging(slot, t):
+    """Pinned host tensor shaped like device tensor ``t`` (kept for reuse, one per slot)."""
+    key = (slot, tuple(t.shape), t.dtype)
+    st = _STAGING.get(key)
+    if st is None:
+        st = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+        _STAGING[key] = st
+    return st
 
 
 class Fields:
@@ -54,6 +88,9 @@ class Fields:
         self.n_steps = [0, 0]
         self.n_trajectories = [0, 0]
 
+    # largest slc count whose pow is looked up in a host-computed table
+    SLC_TABLE_MAX = 1 << 22
+
     def integrate(self):
         """Trace all seeds down and up, then post-process slt/slc/sla (fields.py:69-167)."""
         vprint(self.verbose, "Integrating streamline fields...")
@@ -64,19 +101,48 @@ class Fields:
             = create_seeds(mask_array, info.pad_width, info.n_work_items,
                            do_shuffle=info.do_shuffle, rng_seed=info.shuffle_rng_seed,
                            verbose=self.verbose)
-        self.gpu_integrate()
         pixel_size = info.pixel_size
         dds = traj_stats_df["ds"]["downstream", "mean"]
         uds = traj_stats_df["ds"]["upstream", "mean"]
-        self.data.slt_array[:, :, 0] = self.data.slt_array[:, :, 0] * (dds / pixel_size)
-        self.data.slt_array[:, :, 1] = self.data.slt_array[:, :, 1] * (uds / pixel_size)
-        self.data.slt_array = np.sqrt(self.data.slt_array)
-        self.data.slc_array = np.sqrt(2.0) * np.power(
-            self.data.slc_array / info.subpixel_seed_point_density ** 2, 2 / 3)
+        nxp, nyp = mask_array.shape
+        with torch.cuda.device(self.device):
+            acc = self._trace()
+            self._finish(acc, float(dds / pixel_size), float(uds / pixel_size), nxp, nyp)
         vprint(self.verbose, "...done")
 
-    def gpu_integrate(self):
-        """Both passes on the device; fills raw slc/slt/sla like fields.py:169-310."""
+    def _finish(self, acc, scale_down, scale_up, nxp, nyp):
+        """slm_fields_finish on the device; finished arrays copied to the host."""
+        from . import _lib
+        from ._lib import check, ptr
+        dev = self.device
+        info = self.info
+        nxy = nxp * nyp
+        dd = info.subpixel_seed_point_density ** 2
+        counts = acc[:, 0].reshape(-1).view(torch.int64)
+        if not self.exact:
+            counts = counts & 0xFFFFFFFF  # the uint32 wrap the kernel applies
+        cmax = int(counts.max().item()) if nxy else 0
+        n_tab = min(cmax, self.SLC_TABLE_MAX) + 1
+        table_d = _slc_table(dev, dd, n_tab)
+        slc = torch.empty((nxp, nyp, 2), dtype=torch.float64, device=dev)
+        slt = torch.empty((nxp, nyp, 2), dtype=torch.float32, device=dev)
+        sla = torch.empty((nxp, nyp, 2), dtype=torch.float32, device=dev)
+        check(_lib.load().slm_fields_finish(
+            ptr(acc), nxy, int(info.subpixel_seed_point_density), scale_down, scale_up,
+            1 if self.exact else 0, ptr(table_d), n_tab, ptr(slc), ptr(slt), ptr(sla),
+            kernels._stream(None)))
+        # through pinned staging buffers (reused per shape), then into arrays
+        # the caller owns
+        out = []
+        for slot, t in enumerate((slc, slt, sla)):
+            st = _staging(slot, t)
+            st.copy_(t, non_blocking=True)
+            out.append(st)
+        torch.cuda.current_stream(dev).synchronize()
+        self.data.slc_array, self.data.slt_array, self.data.sla_array = (o.numpy().copy() for o in out)
+
+    def _trace(self):
+        """Both passes on the device; returns the uint64 accumulators [2, 2, nxy]."""
         info = self.info
         dev = self.device
         mask_array = self.data.mask_array
@@ -108,6 +174,16 @@ class Fields:
                     _, self.n_steps[downup_idx] = sharded_field_pass(
                         prm, trace, acc[downup_idx, 0], acc[downup_idx, 1], self.process_group)
                 self.n_trajectories[downup_idx] = int(prm.n_seed_points) * int(prm.subpixel_seed_point_density) ** 2
+        return acc
+
+    def gpu_integrate(self):
+        """Both passes on the device; fills raw slc/slt/sla like fields.py:169-310."""
+        info = self.info
+        dev = self.device
+        nxp, nyp = self.data.mask_array.shape
+        nxy = nxp * nyp
+        with torch.cuda.device(dev):
+            acc = self._trace()
             if self.exact:
                 raw = acc.cpu().numpy()
                 slc_raw = raw[:, 0].astype(np.float64)

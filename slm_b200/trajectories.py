@@ -81,16 +81,38 @@ class Trajectories:
             seeds_d = to_device(self.data.seed_point_array, dev, torch.float32)
             mask_d = to_device(self.data.mask_array, dev)
             uv_d = to_device(self.data.uv_array, dev, torch.float32)
-            traj_d = torch.zeros(self.chunk_size * nl * 2, dtype=torch.int8, device=dev)
-            nsteps_d = torch.zeros(self.chunk_size, dtype=torch.uint16, device=dev)
-            length_d = torch.zeros(self.chunk_size, dtype=torch.float32, device=dev)
-            for (_, downup_idx, downup_sign, _chunk_idx, seeds_chunk_offset, n_chunk_seeds,
-                 n_chunk_ki) in [td[1:] for td in self.trace_do_chunks if td[0]]:
-                info.downup_sign = downup_sign
-                info.seeds_chunk_offset = seeds_chunk_offset
-                prm = kernel_params(info, "INTEGRATE_TRAJECTORY", downup_sign)
-                kernels.integrate_trajectory(prm, n_chunk_ki, seeds_d, mask_d, uv_d, traj_d,
-                                             nsteps_d, length_d, integrator=self.integrator)
+            todo = [td[1:] for td in self.trace_do_chunks if td[0]]
+            # one chunk per direction (the usual case): both directions run
+            # at once on their own streams (each kernel is a few thousand
+            # latency-bound threads); otherwise chunk after chunk
+            concurrent = len(todo) == 2 and todo[0][1] != todo[1][1]
+            n_buf = 2 if concurrent else 1
+            trajs = [torch.zeros(self.chunk_size * nl * 2, dtype=torch.int8, device=dev) for _ in range(n_buf)]
+            nsteps = [torch.zeros(self.chunk_size, dtype=torch.uint16, device=dev) for _ in range(n_buf)]
+            lengths = [torch.zeros(self.chunk_size, dtype=torch.float32, device=dev) for _ in range(n_buf)]
+            cur = torch.cuda.current_stream(dev)
+            if concurrent:
+                streams = [torch.cuda.Stream(dev) for _ in range(2)]
+                for j, (_, downup_idx, downup_sign, _c, seeds_chunk_offset, _n, n_chunk_ki) in enumerate(todo):
+                    info.downup_sign = downup_sign
+                    info.seeds_chunk_offset = seeds_chunk_offset
+                    prm = kernel_params(info, "INTEGRATE_TRAJECTORY", downup_sign)
+                    streams[j].wait_stream(cur)
+                    kernels.integrate_trajectory(prm, n_chunk_ki, seeds_d, mask_d, uv_d, trajs[j],
+                                                 nsteps[j], lengths[j], integrator=self.integrator,
+                                                 stream=streams[j])
+                for st in streams:
+                    cur.wait_stream(st)
+            for j, (_, downup_idx, downup_sign, _chunk_idx, seeds_chunk_offset, n_chunk_seeds,
+                    n_chunk_ki) in enumerate(todo):
+                b = j if concurrent else 0
+                traj_d, nsteps_d, length_d = trajs[b], nsteps[b], lengths[b]
+                if not concurrent:
+                    info.downup_sign = downup_sign
+                    info.seeds_chunk_offset = seeds_chunk_offset
+                    prm = kernel_params(info, "INTEGRATE_TRAJECTORY", downup_sign)
+                    kernels.integrate_trajectory(prm, n_chunk_ki, seeds_d, mask_d, uv_d, traj_d,
+                                                 nsteps_d, length_d, integrator=self.integrator)
                 n = max(n_chunk_seeds, 0)
                 chunk_nsteps = nsteps_d[:n].cpu().numpy()
                 chunk_length = length_d[:n].cpu().numpy()

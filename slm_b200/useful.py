@@ -222,7 +222,7 @@ def _shuffled_seeds(mask, pad, do_shuffle, rng_seed):
         hit = _SEED_CACHE.get(key)
         if hit is not None:
             np.random.set_state(hit[1])
-            return hit[0].copy()
+            return hit[0]  # create_seeds returns a copy
     seed_point_array = (np.argwhere(~m).astype(np.float32) - pad)
     if do_shuffle:
         np.random.seed(rng_seed)
@@ -230,7 +230,7 @@ def _shuffled_seeds(mask, pad, do_shuffle, rng_seed):
         seed_point_array = seed_point_array[perm]
         if len(_SEED_CACHE) >= _SEED_CACHE_MAX:
             _SEED_CACHE.pop(next(iter(_SEED_CACHE)))
-        _SEED_CACHE[key] = (seed_point_array.copy(), np.random.get_state())
+        _SEED_CACHE[key] = (seed_point_array, np.random.get_state())
     return seed_point_array
 
 

@@ -60,3 +60,48 @@ def test_fields_stage_raw_and_postprocessed():
     expect_slc = np.sqrt(2.0) * np.power(raw_slc / 4, 2 / 3)
     assert np.array_equal(f2.data.slc_array, expect_slc)
     assert np.isfinite(f2.data.sla_array).all()
+
+
+def _host_finish(data, info, stats):
+    """The reference's integrate() post-processing (fields.py:146-167) on the
+    raw arrays gpu_integrate() leaves, in NumPy."""
+    dds = stats["ds"]["downstream", "mean"]
+    uds = stats["ds"]["upstream", "mean"]
+    slt = data.slt_array.copy()
+    slt[:, :, 0] = slt[:, :, 0] * (dds / info.pixel_size)
+    slt[:, :, 1] = slt[:, :, 1] * (uds / info.pixel_size)
+    slt = np.sqrt(slt)
+    slc = np.sqrt(2.0) * np.power(data.slc_array / info.subpixel_seed_point_density ** 2, 2 / 3)
+    return slc, slt, data.sla_array.copy()
+
+
+@pytest.mark.parametrize("density,exact", [(2, False), (3, False), (2, True)])
+def test_fields_device_finish_matches_host(density, exact):
+    """integrate() finishes the fields on the GPU; the arrays equal the
+    reference's host post-processing of the same raw sums bit for bit."""
+    kw = dict(nx=70, ny=52, seed=83, density=density, step=0.25, max_length=60.0)
+    ct = Case(n_traj_seeds=200, **kw)
+    tr = Trajectories(0, 0, info=ct.info, data=_data(ct))
+    tr.integrate()
+    stats = tr.data.traj_stats_df
+    a = Case(**kw)
+    fa = Fields(0, 0, info=a.info, data=_data(a, stats), exact=exact)
+    fa.integrate()
+    b = Case(**kw)
+    fb = Fields(0, 0, info=b.info, data=_data(b, stats), exact=exact)
+    seeds, ns, npad = create_seeds(b.mask, 2, b.info.n_work_items)
+    fb.data.seed_point_array = seeds
+    b.info.n_seed_points, b.info.n_padded_seed_points = ns, npad
+    fb.gpu_integrate()
+    slc, slt, sla = _host_finish(fb.data, b.info, stats)
+    assert fa.data.slc_array.dtype == np.float64 and fa.data.slt_array.dtype == np.float32
+    assert np.array_equal(fa.data.slc_array, slc)
+    assert np.array_equal(fa.data.slt_array.view(np.uint32), slt.view(np.uint32))
+    assert np.array_equal(fa.data.sla_array.view(np.uint32), sla.view(np.uint32))
+    # without the table the kernel's own pow stays within 2 ulp
+    c = Case(**kw)
+    fc = Fields(0, 0, info=c.info, data=_data(c, stats), exact=exact)
+    fc.SLC_TABLE_MAX = 0
+    fc.integrate()
+    assert np.allclose(fc.data.slc_array, slc, rtol=4.5e-16, atol=0.0)
+    assert np.array_equal(fc.data.slt_array, slt)
