@@ -47,6 +47,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path[:0] = [ROOT, os.path.join(ROOT, "oracle")]
 
 BYTES_PER_STEP = {2: 75, 4: 139}
+# dram__bytes_read.sum + dram__bytes_write.sum of one field launch, from an
+# ncu capture of this bench's own workload (spatial seed order); null for
+# workloads without a capture
+TRAFFIC_PER_LAUNCH = {"config2": 211.9e6}
 
 
 def _peaks():
@@ -325,7 +329,9 @@ def run_b200(args):
                    "rk_steps_per_step": steps_per_step,
                    "parallelism": "seed shards + NCCL all-reduce" if ws > 1 else "1 GPU"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak,
+                     "traffic": TRAFFIC_PER_LAUNCH.get(args.workload) if spatial else None,
+                     "algorithmic_bytes_per_launch": field_steps_rank * bps / 2,
                      "peak_source": peak_kind,
                      "kernel": "k_fields_{}<{}>".format(args.schedule, integrator),
                      "bytes_per_step": bps},
