@@ -342,6 +342,8 @@ def run_b200(args):
         line["e2e"] = e2e
     if ws == 1 and not args.no_sched:
         line["scheduler"] = sched_compare(args, wl, dev, seeds_d, mask_d, uv_d, field_prm, flush)
+    if ws == 1 and args.stages:
+        line["stages"] = run_stages(args, wl, dev)
     if rank == 0 and not args.no_cpu and ws == 1:
         line["cpu_baseline"] = cpu_baseline(wl, args)
     if ws > 1:
@@ -350,6 +352,11 @@ def run_b200(args):
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
+
+
+def SPECS_NAME(key):
+    from slm_b200.workloads import SPECS
+    return SPECS[key].name
 
 
 def sched_compare(args, wl, dev, seeds_d, mask_d, uv_d, field_prm, flush):
@@ -364,21 +371,46 @@ def sched_compare(args, wl, dev, seeds_d, mask_d, uv_d, field_prm, flush):
     from slm_b200.workloads import Workload
 
     t0 = time.time()
-    train = Workload(args.workload, seed=args.sched_train_seed)
     spec = wl.spec
     d = spec.density
-    dd = d * d
-    tr_seeds = torch.from_numpy(train.seeds).to(dev)
-    tr_mask = torch.from_numpy(train.mask.view(np.uint8)).to(dev)
-    tr_uv = torch.from_numpy(train.uv).to(dev)
     from slm_b200.params import kernel_params
-    n_tr = int(train.info.n_seed_points)
-    cols = []
-    for s in (1.0, -1.0):
-        prm = kernel_params(train.info, "INTEGRATE_FIELDS", s)
-        st = S.record_steps(prm, tr_seeds, tr_mask, tr_uv, integrator=spec.integrator)
-        cols.append(S.step_targets(st, n_tr, d))
-    targets = torch.stack(cols, 1).contiguous()
+
+    def recorded(w):
+        """(uv, seeds, targets [n][2]) of workload w on the device."""
+        sd = torch.from_numpy(w.seeds).to(dev)
+        md = torch.from_numpy(w.mask.view(np.uint8)).to(dev)
+        ud = torch.from_numpy(w.uv).to(dev)
+        n_w = int(w.info.n_seed_points)
+        cols = []
+        for s in (1.0, -1.0):
+            prm = kernel_params(w.info, "INTEGRATE_FIELDS", s)
+            st = S.record_steps(prm, sd, md, ud, integrator=w.spec.integrator)
+            cols.append(S.step_targets(st, n_w, w.spec.density))
+        return w.uv, w.seeds[:n_w], torch.stack(cols, 1).contiguous()
+
+    if args.workload == "config4":
+        # 40 seeded 512^2 DTMs of the same family, 4x4 seeds: 10.5 M pairs.
+        # Their uv grids are stacked along x with an 8 px edge-replicated
+        # margin each, so a patch clamps exactly as on its own grid.
+        train_keys = [("incised512_d4", 100 + i) for i in range(40)]
+        held_keys = [("incised512_d4", 200 + i) for i in range(4)]
+    else:
+        train_keys = [(args.workload, args.sched_train_seed)]
+        held_keys = []
+    grids, seed_sets, tsets = [], [], []
+    xoff = 0
+    for key, seed in train_keys:
+        g_uv, g_seeds, g_t = recorded(Workload(key, seed=seed))
+        m = 8 if len(train_keys) > 1 else 0
+        grids.append(np.pad(g_uv, ((m, m), (m, m), (0, 0)), mode="edge"))
+        seed_sets.append(g_seeds + np.array([xoff + m, m], np.float32))
+        tsets.append(g_t)
+        xoff += grids[-1].shape[0]
+    tr_uv = torch.from_numpy(np.ascontiguousarray(np.concatenate(grids, 0))).to(dev)
+    tr_seeds = torch.from_numpy(np.ascontiguousarray(np.concatenate(seed_sets, 0))).to(dev)
+    targets = torch.cat(tsets, 0).contiguous()
+    del grids, seed_sets, tsets
+    n_tr = int(targets.shape[0])
     # "predicted long" class of the learned+spatial order: the top 1% of the
     # training targets
     g = torch.Generator(device=dev)
@@ -392,12 +424,29 @@ def sched_compare(args, wl, dev, seeds_d, mask_d, uv_d, field_prm, flush):
                      steps=args.sched_train_steps, batch=4096)
     torch.cuda.synchronize()
     t_train = time.time() - t1
-    del tr_seeds, tr_mask, tr_uv, targets
+    del tr_seeds, tr_uv, targets
 
     n = int(wl.info.n_seed_points)
     nxp, nyp = uv_d.shape[0], uv_d.shape[1]
     pred = model.predict(uv_d, nxp, nyp, 2, seeds_d, n)
+
     # held-out prediction error against the step counts the tracer records
+    def error_of(p_all, truth_all):
+        rank = lambda x: torch.argsort(torch.argsort(x)).double()
+        out_e = {}
+        for col in (0, 1):
+            p, truth = p_all[:, col], truth_all[:, col]
+            rho = float(torch.corrcoef(torch.stack([rank(p), rank(truth)]))[0, 1])
+            out_e["down" if col == 0 else "up"] = {
+                "mae_log_steps": float((p - truth).abs().mean()), "spearman": rho}
+        return out_e
+
+    held = {}
+    for key, seed in held_keys:
+        h_uv, h_seeds, h_t = recorded(Workload(key, seed=seed))
+        hu, hs = torch.from_numpy(h_uv).to(dev), torch.from_numpy(np.ascontiguousarray(h_seeds)).to(dev)
+        hp = model.predict(hu, hu.shape[0], hu.shape[1], 2, hs, int(hs.shape[0]))
+        held["{} seed {}".format(key, seed)] = error_of(hp, h_t)
     err = {}
     for col in (0, 1):
         st = S.record_steps(field_prm[col], seeds_d, mask_d, uv_d, integrator=spec.integrator)
@@ -420,10 +469,14 @@ def sched_compare(args, wl, dev, seeds_d, mask_d, uv_d, field_prm, flush):
     sbins = torch.empty(int(kernels._lib.load().slm_order_spatial_bins(
         int(wl.info.nx), int(wl.info.ny), S.SPATIAL_BLOCK, 1)), dtype=torch.uint32, device=dev)
 
+    visit = torch.empty(n, dtype=torch.uint32, device=dev)
+
     def arm(schedule, mode):
         acc.zero_()
         if mode in ("learned", "learned_spatial"):
-            model.predict(uv_d, nxp, nyp, 2, seeds_d, n, out=pred)
+            # inference visits the seeds in spatial order (patch locality)
+            S.spatial_order(seeds_d, n, wl.info.nx, wl.info.ny, out=visit, bins=sbins)
+            model.predict(uv_d, nxp, nyp, 2, seeds_d, n, out=pred, visit=visit)
         for col in (0, 1):
             if mode == "learned":
                 model.order(pred, col, cap, out=orders[col], bins=bins)
@@ -439,7 +492,9 @@ def sched_compare(args, wl, dev, seeds_d, mask_d, uv_d, field_prm, flush):
                                      work[col], schedule=schedule, integrator=spec.integrator,
                                      order=o)
 
-    out = {"trained_on": "{} (seed {})".format(spec.name, args.sched_train_seed),
+    trained_on = ("40 x {} (seeds 100..139)".format(SPECS_NAME("incised512_d4"))
+                  if args.workload == "config4" else "{} (seed {})".format(spec.name, args.sched_train_seed))
+    out = {"trained_on": trained_on, "held_out_dtms": held,
            "train_pairs": n_tr, "train_steps": args.sched_train_steps, "train_batch": 4096,
            "train_s": t_train, "prep_s": t1 - t0,
            "loss_first": float(np.mean(hist[:10])), "loss_last": float(np.mean(hist[-50:])),
@@ -570,6 +625,127 @@ def run_batched(args):
     return 0
 
 
+def run_stages(args, wl, dev):
+    """Every stage of the path on the workload DTM through the public API, each
+    timed (wall clock, synchronised; the mapping wrappers copy their buffers
+    per kernel call as the reference's do), then the same mapping and KDE
+    with the oracle's CPU restatement on identical inputs: the CPU timing, and
+    a full-size parity check (mapping bit-exact, KDE within the tests'
+    tolerance)."""
+    import copy
+
+    import torch
+
+    import oracle as O
+    from slm_b200 import kde as K
+    from slm_b200 import mapping
+    from slm_b200.analysis import Bivariate_distribution, Univariate_distribution
+    from slm_b200.fields import Fields
+    from slm_b200.trajectories import Trajectories
+    from slm_b200.useful import Data
+
+    spec = wl.spec
+    out = {}
+
+    def timed(key, fn):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        out[key] = time.perf_counter() - t
+        return r
+
+    info = wl.fresh_info()
+    data = Data(info=info, mask_array=wl.mask, uv_array=wl.uv,
+                mapping_array=np.zeros(wl.mask.shape, np.uint32))
+    tr = Trajectories(0, dev.index, info=info, data=data, integrator=spec.integrator)
+    timed("trajectories_s", tr.integrate)
+    info2 = wl.fresh_info()
+    data2 = Data(info=info2, mask_array=wl.mask, uv_array=wl.uv,
+                 mapping_array=np.zeros(wl.mask.shape, np.uint32), traj_stats_df=tr.data.traj_stats_df)
+    f = Fields(0, dev.index, info=info2, data=data2, integrator=spec.integrator)
+    timed("fields_s", f.integrate)
+    slt_dn = data2.slt_array[:, :, 0]
+    thr = np.float32(np.percentile(slt_dn[~wl.mask], 94.0))
+    info2.set_thresholds(segmentation_threshold=np.uint32(50), channel_threshold=thr)
+    cpu_data = copy.deepcopy(data2)
+    cpu_info = copy.deepcopy(info2)
+
+    runner = mapping.DeviceRunner(dev)
+    ok = timed("mapping_s", lambda: mapping.map_channels_segments(None, info2, data2, runner=runner))
+
+    cpu_status = [0]
+
+    def oracle_runner(name, params, seeds, arrays):
+        # status bits (1: a loop the reference leaves unbounded hit its cap;
+        # 2: an out-of-grid read skipped) are compared with the GPU's
+        cpu_status[0] |= O.map_kernel(name, params, seeds, arrays)
+
+    cpu = args.stages_cpu
+    if cpu:
+        t = time.perf_counter()
+        ok_cpu = mapping.map_channels_segments(None, cpu_info, cpu_data, runner=oracle_runner)
+        out["mapping_cpu_s"] = time.perf_counter() - t
+        same = bool(ok == ok_cpu)
+        for name in ("mapping_array", "count_array", "link_array", "label_array", "channel_label_array"):
+            a, b = getattr(data2, name, None), getattr(cpu_data, name, None)
+            if a is not None or b is not None:
+                same = same and a is not None and b is not None and np.array_equal(a, b)
+        out["mapping_identical"] = same
+    out["mapping_status"] = {"gpu": int(runner.status), "cpu_oracle": int(cpu_status[0]) if cpu else None}
+    out["mapping_kernels_s"] = {k: round(v, 4) for k, v in runner.seconds.items()}
+    m = data2.mapping_array
+    out["channel_pixels"] = int(np.sum((m & info2.is_thinchannel) > 0))
+    out["segments"] = int(data2.label_array.max()) if ok else 0
+
+    # hillslope lengths from a seeded 2 % of the hillslope pixels
+    rng = np.random.default_rng(3)
+    hill = (~wl.mask) & ((m & info2.is_thinchannel) == 0)
+    pick = hill & (rng.random(hill.shape) < 0.02)
+    for dd_, ii in ((data2, info2), (cpu_data, cpu_info)):
+        dd_.mapping_array[pick] |= ii.is_midslope
+        nmid = int(np.sum(~wl.mask & ((dd_.mapping_array & ii.is_midslope) > 0)))
+        dd_.subsegment_hsl_array = np.zeros(nmid, dtype=np.float32)
+    timed("hillslope_lengths_s", lambda: mapping.hsl(None, info2, data2, False, runner=runner))
+    out["hillslope_lengths"] = int(data2.subsegment_hsl_array.size)
+    if cpu:
+        t = time.perf_counter()
+        mapping.hsl(None, cpu_info, cpu_data, False, runner=oracle_runner)
+        out["hillslope_lengths_cpu_s"] = time.perf_counter() - t
+        out["hillslope_lengths_identical"] = bool(np.array_equal(
+            data2.subsegment_hsl_array.view(np.uint32), cpu_data.subsegment_hsl_array.view(np.uint32)))
+
+    # KDEs: hillslope lengths (univariate, 8192 bins -> 1024 points, gaussian,
+    # bandwidth 2) and downstream vs upstream slt (bivariate)
+    hsl = data2.subsegment_hsl_array
+    logx = np.log(hsl[hsl > 0]).astype(np.float32)
+    ud = Univariate_distribution(logx_array=logx, logy_array=logx, pixel_size=spec.pixel_size,
+                                 n_hist_bins=8192, n_pdf_points=1024)
+    timed("kde_univariate_s", lambda: ud.compute_kde_opencl(kernel="gaussian", bandwidth=2.0))
+    prm = K.kde_params(ud, "pdf_univariate")
+    dat = np.ascontiguousarray(ud.logx_data.reshape(-1), dtype=np.float32)
+    t = time.perf_counter()
+    h_o = O.histogram_univariate(prm, dat)
+    p_o = O.pdf_univariate(prm, h_o)
+    out["kde_univariate_cpu_s"] = time.perf_counter() - t
+    h_o = h_o.reshape(-1, 1)
+    p_o = p_o.reshape(-1, 1)
+    out["kde_univariate_hist_identical"] = bool(np.array_equal(ud.histogram, h_o / (np.sum(h_o) * ud.bin_dx)))
+    p_ref = p_o / (np.sum(p_o) * ud.bin_dx)
+    out["kde_univariate_max_rel_err"] = float(np.max(np.abs(ud.pdf - p_ref)) / np.max(np.abs(p_ref)))
+    sl = data2.slt_array
+    sel = (~wl.mask) & (sl[:, :, 0] > 0) & (sl[:, :, 1] > 0)
+    lx, ly = np.log(sl[:, :, 0]), np.log(sl[:, :, 1])
+    lx[~sel] = np.finfo(np.float32).min
+    ly[~sel] = np.finfo(np.float32).min
+    bd = Bivariate_distribution(logx_array=lx, logy_array=ly, mask_array=wl.mask,
+                                pixel_size=spec.pixel_size, n_hist_bins=1024, n_pdf_points=256)
+    timed("kde_bivariate_s", lambda: bd.compute_kde_opencl(kernel="gaussian", bandwidth=0.1))
+    out["kde_bivariate_points"] = int(bd.n_data)
+    out["ok"] = bool(ok)
+    return out
+
+
 def run_e2e(args, wl, dev):
     """Public-API step: Trajectories then Fields on pinned host arrays."""
     import torch
@@ -644,6 +820,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-sched", action="store_true", help="skip the learned-scheduler comparison")
     ap.add_argument("--seed-order", default="spatial", choices=["spatial", "shuffled"])
+    ap.add_argument("--stages", action="store_true",
+                    help="also time mapping, hillslope lengths and KDE on the GPU")
+    ap.add_argument("--stages-cpu", action="store_true",
+                    help="with --stages: the same stages with the CPU oracle, timed, and compared")
     ap.add_argument("--tiles", type=int, default=96, help="config3: number of tiles")
     ap.add_argument("--retune", action="store_true", help="config3: ignore the autotuner cache")
     ap.add_argument("--sched-train-seed", type=int, default=12)

@@ -366,9 +366,12 @@ int slm_mse(const float* y, const float* t, const float* w, uint64_t n_el, float
 int slm_adam(float* w, float* wq, const float* g, float* m, float* v, uint64_t n, float lr,
              float b1, float b2, float eps, int step, int round_w, void* stream);
 /* fused inference on the tensor cores: out [n][2] predictions for seeds
- * seed_point [n] (float2 pixel coordinates, unpadded) */
+ * seed_point [n] (float2 pixel coordinates, unpadded).  index (NULL: none)
+ * is the order the seeds are visited in (e.g. a spatial order, so that
+ * neighbouring patches share cache lines); out stays indexed by seed. */
 int slm_cnn_infer(const float* uv, uint32_t nx_padded, uint32_t ny_padded, uint32_t pad,
-                  const float* seed_point, uint32_t n, const float* w1, const float* b1,
+                  const float* seed_point, const uint32_t* index, uint32_t n,
+                  const float* w1, const float* b1,
                   const float* w2, const float* b2, const float* w3, const float* b3,
                   float* out, void* stream);
 /* order [n]: seed indices by column col of pred [n][stride], longest predicted

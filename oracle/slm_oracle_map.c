@@ -156,10 +156,15 @@ uint32_t oracle_connect_channels(const slm_params* p, const float* seeds, uint32
                 if (!m.stuck) prev = vec;
             }
         }
-        /* until back on a channel pixel or masked (connect.cl:70-79) */
+        /* until back on a channel pixel or masked (connect.cl:70-79).  Every
+         * pass that does not exit adds a step, so the loop ends at
+         * n_steps == INTERCHANNEL_MAX_N_STEPS; when the first loop already
+         * went past that count, the reference's loop writes nothing and ends
+         * with n_steps >= the count (at a channel, a masked pixel or the
+         * 32-bit wrap), so the flagging below does not run either way. */
         guard = 0;
-        while ((mapping[idx] & p->is_channel) == 0 && !mask[idx]
-               && n_steps != p->interchannel_max_n_steps) {
+        while (n_steps <= p->interchannel_max_n_steps && (mapping[idx] & p->is_channel) == 0
+               && !mask[idx] && n_steps != p->interchannel_max_n_steps) {
             if (++guard > LOOP_CAP) { status |= ST_CAP; break; }
             rk_t s = rk_compute(vec, dt, uv, p, &idx);
             if (!mask[idx]) {

@@ -91,7 +91,7 @@ SIGNATURES = {
     "slm_mse": (ctypes.c_int, [_P, _P, _P, ctypes.c_uint64, ctypes.c_float, _P, _P, _P]),
     "slm_adam": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_uint64, ctypes.c_float, ctypes.c_float,
                                 ctypes.c_float, ctypes.c_float, _I, _I, _P]),
-    "slm_cnn_infer": (ctypes.c_int, [_P, _U, _U, _U, _P, _U, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "slm_cnn_infer": (ctypes.c_int, [_P, _U, _U, _U, _P, _P, _U, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_order_spatial_bins": (ctypes.c_uint32, [_U, _U, _U, _I]),
     "slm_order_spatial": (ctypes.c_int, [_P, _U, _U, _U, _U, _P, _U, _U, ctypes.c_float, _P, _U, _P, _P]),
     "slm_order_by_prediction": (ctypes.c_int, [_P, _U, _U, _U, ctypes.c_float, ctypes.c_float, _U,

@@ -88,7 +88,7 @@ def tile_table(tiles, sign):
 class TileBatch:
     """Device-resident batch of tiles with accumulators for both directions."""
 
-    def __init__(self, tiles, device=None, integrator=2):
+    def __init__(self, tiles, device=None, integrator=2, seed_order="spatial"):
         self.tiles = list(tiles)
         self.device = torch.device(device) if device is not None else torch.device("cuda")
         self.integrator = int(integrator)
@@ -113,9 +113,24 @@ class TileBatch:
         self.work = [kernels.workspace(dev) for _ in range(2)]
         self.launch = kernels.launch_config("persistent", self.integrator)
         self._graph = None
+        # queue order: each tile's seeds in pixel-block order (the tiles in
+        # table order), as global seed indices; None = the seed arrays' order
+        self.order = None
+        if seed_order == "spatial" and self.n_seeds:
+            from .scheduler import spatial_order
+            parts = []
+            for t, b in zip(self.tiles, self.seed_begins):
+                if t.n_seeds:
+                    o = spatial_order(self.seeds[b:b + t.n_seeds], t.n_seeds, t.info.nx, t.info.ny)
+                    parts.append(o.view(torch.int32) + b)
+            self.order = torch.cat(parts).contiguous().view(torch.uint32)
+        elif seed_order not in ("spatial", "shuffled"):
+            raise ValueError("seed_order must be 'spatial' or 'shuffled'")
 
     # ------------------------------------------------------------ tracing
     def trace_direction(self, d, launch=None, order=None, item_steps=None, stream=None):
+        """One direction over all tiles; ``order`` defaults to the batch's queue order."""
+        order = self.order if order is None else order
         L = launch if launch is not None else self.launch
         L.integrator = self.integrator
         lib = _lib.load()
@@ -137,6 +152,14 @@ class TileBatch:
             self.work_tiles = [[kernels.workspace(self.device) for _ in self.tiles] for _ in range(2)]
             self.tile_prm = [[kernel_params(t.info, "INTEGRATE_FIELDS", sign) for t in self.tiles]
                              for sign in (1.0, -1.0)]
+            # each tile's own slice of the queue order, as tile-local indices
+            self._tile_orders = []
+            for t, b in zip(self.tiles, self.seed_begins):
+                if self.order is None or t.n_seeds == 0:
+                    self._tile_orders.append(None)
+                else:
+                    sl = self.order.view(torch.int32)[b:b + t.n_seeds] - b
+                    self._tile_orders.append(sl.contiguous().view(torch.uint32))
         for d in range(2):
             for i, t in enumerate(self.tiles):
                 self.work_tiles[d][i].zero_()
@@ -149,7 +172,7 @@ class TileBatch:
                                          self.uv[o:o + n], self.acc[d, 0, o:o + n],
                                          self.acc[d, 1, o:o + n], self.work_tiles[d][i], schedule=schedule,
                                          integrator=self.integrator, block_threads=block_threads,
-                                         stream=stream)
+                                         stream=stream, order=self._tile_orders[i])
 
     def capture(self, launch=None):
         """CUDA graph of zeroing + both batched directions; returns it (also kept)."""

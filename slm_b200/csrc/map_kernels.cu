@@ -34,7 +34,9 @@
 // Every loop is bounded; a cap that the reference would exceed (it would loop
 // on) or a neighbour index outside the grid sets a bit in the caller's status
 // word instead of trapping.
+#include <algorithm>
 #include <cstring>
+#include <vector>
 #include "capi_util.cuh"
 #include "trace_common.cuh"
 
@@ -105,8 +107,15 @@ __global__ void k_connect_channels(const slm_params p, uint32_t n, const float2*
             if (!m.stuck) prev = vec;
         }
     }
+    // The second loop ends at n_steps == INTERCHANNEL_MAX_N_STEPS (every pass
+    // that does not exit adds a step).  If the first loop already went past
+    // that count, the reference's loop runs until a channel, a masked pixel
+    // or the 32-bit wrap of n_steps, writes nothing, and leaves n_steps >=
+    // INTERCHANNEL_MAX_N_STEPS, so the flagging below does not run: skipping
+    // it gives the same flags, and bounds the kernel.
     guard = 0;
-    while ((mapping[idx] & p.is_channel) == 0 && !mask[idx] && n_steps != p.interchannel_max_n_steps) {
+    while (n_steps <= p.interchannel_max_n_steps && (mapping[idx] & p.is_channel) == 0 && !mask[idx]
+           && n_steps != p.interchannel_max_n_steps) {
         if (++guard > MAP_LOOP_CAP) { atomicOr(status, MAP_ST_CAP); break; }
         const Step s = rk_plain(vec, dt, uv, p);
         idx = s.idx;
@@ -185,6 +194,75 @@ __global__ void k_prune_channel_heads(const slm_params p, uint32_t n, const floa
 // ------------------------------------------------------------------ count / flag
 // Phase A of count_downchannels: the pixels each head's walk enters, in order,
 // up to the walk's state-independent end; with events == nullptr only counts.
+// Event stream of one count_downchannels walk: the pixels it enters, in
+// order.  Walks that oscillate (e.g. across a valley floor) run to the
+// 1000*MAX_N_STEPS bound and enter millions of pixels in a short repeating
+// pattern, so the stream is compressed losslessly: literal events are pixel
+// indices (< 2^31); a repeat record (two words: 0x80000000|P, n) stands for
+// the next n events continuing the pattern of the last P decoded events.
+constexpr uint32_t CNT_PMAX = 8;
+constexpr uint32_t CNT_REPEAT = 0x80000000u;
+// A period record (words 0xC0000000|E, the E pattern pixels, n) stands for the
+// walk's remaining n events: the E-event pattern repeated (last lap partial).
+constexpr uint32_t CNT_PERIOD = 0xC0000000u;
+constexpr uint32_t CNT_KIND = 0xC0000000u;
+
+struct EventWriter {
+    uint32_t* out;  // null: count words only
+    u64 k;          // words written
+    uint32_t ring[2 * CNT_PMAX];
+    uint32_t nlit;  // literals in the ring (capped at 2*CNT_PMAX)
+    uint32_t P, pos;
+    uint32_t pat[CNT_PMAX];
+    uint32_t reps;  // events matched by the open repeat record
+    __device__ void put(uint32_t w) {
+        if (out) out[k] = w;
+        k++;
+    }
+    __device__ void close_repeat() {
+        if (P && reps) {
+            put(CNT_REPEAT | P);
+            put(reps);
+        }
+        P = 0;
+        reps = 0;
+        nlit = 0;
+    }
+    __device__ void literal(uint32_t e) {
+        put(e);
+        if (nlit == 2 * CNT_PMAX) {
+#pragma unroll
+            for (uint32_t q = 0; q + 1 < 2 * CNT_PMAX; ++q) ring[q] = ring[q + 1];
+            ring[2 * CNT_PMAX - 1] = e;
+        } else {
+            ring[nlit++] = e;
+        }
+        // the literal tail periodic over two periods -> open a repeat record
+        for (uint32_t q = 1; q <= CNT_PMAX && 2 * q <= nlit; ++q) {
+            bool same = true;
+            for (uint32_t t = 0; t < q && same; ++t) same = ring[nlit - 1 - t] == ring[nlit - 1 - q - t];
+            if (same) {
+                P = q;
+                pos = 0;
+                reps = 0;
+                for (uint32_t t = 0; t < q; ++t) pat[t] = ring[nlit - q + t];
+                return;
+            }
+        }
+    }
+    __device__ void event(uint32_t e) {
+        if (P) {
+            if (e == pat[pos]) {
+                reps++;
+                pos = pos + 1 == P ? 0 : pos + 1;
+                return;
+            }
+            close_repeat();
+        }
+        literal(e);
+    }
+};
+
 __global__ void k_count_paths(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
                               const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
                               u64* __restrict__ n_events, const u64* __restrict__ offsets,
@@ -195,8 +273,21 @@ __global__ void k_count_paths(const slm_params p, uint32_t n, const float2* __re
     float dt = p.dt_max;
     uint32_t idx = pixel_of(vec, p), prev_idx = idx, n_steps = 0;
     const uint32_t lim = 1000u * p.max_n_steps;
-    u64 k = 0;
-    uint32_t* out = events ? events + offsets[g] : nullptr;
+    EventWriter w;
+    w.out = events ? events + offsets[g] : nullptr;
+    w.k = 0;
+    w.nlit = 0;
+    w.P = 0;
+    w.reps = 0;
+    // The walk's dynamics depend only on (vec, dt): once that state repeats
+    // bit for bit (Brent's cycle detection), every later step repeats the
+    // period, up to the 1000*MAX_N_STEPS bound.  The period is then walked
+    // again from the repeated state -- once to count its events and find the
+    // pixel the walk ends on, once to write them -- and the remaining events
+    // go out as one period record instead of being traced.
+    Vec2 tv = vec;
+    float tdt = dt;
+    uint32_t power = 1, lam = 0;
     while (!mask[idx] && n_steps < lim) {
         const Step s = rk_plain(vec, dt, uv, p);
         idx = s.idx;
@@ -205,33 +296,138 @@ __global__ void k_count_paths(const slm_params p, uint32_t n, const float2* __re
         dt = next_dt(dt, m.err, p);
         n_steps++;
         if (prev_idx != idx) {
-            if (out) out[k] = idx;
-            k++;
+            w.event(idx);
             prev_idx = idx;
         }
+        lam++;
+        if (__float_as_uint(vec.x) == __float_as_uint(tv.x) && __float_as_uint(vec.y) == __float_as_uint(tv.y)
+            && __float_as_uint(dt) == __float_as_uint(tdt)) {
+            const uint32_t L = lam, R = lim - n_steps, Rm = R % L;
+            uint32_t E = 0, partial = 0, end_idx = idx;
+            for (int pass = 0; pass < 2; ++pass) {
+                Vec2 v2 = vec;
+                float d2 = dt;
+                uint32_t i2 = idx, prev2 = idx;
+                if (pass == 1) {
+                    const uint32_t nfut = (R / L) * E + partial;
+                    if (nfut == 0) break;
+                    w.close_repeat();
+                    w.put(CNT_PERIOD | E);
+                    E = nfut;  // written after the pattern
+                }
+                for (uint32_t t = 1; t <= L; ++t) {
+                    const Step s2 = rk_plain(v2, d2, uv, p);
+                    i2 = s2.idx;
+                    const Move m2 = rk_move(s2, v2, i2, p);
+                    d2 = next_dt(d2, m2.err, p);
+                    if (prev2 != i2) {
+                        if (pass == 0) {
+                            E++;
+                            if (t <= Rm) partial++;
+                        } else {
+                            w.put(i2);
+                        }
+                        prev2 = i2;
+                    }
+                    if (pass == 0 && t == Rm) end_idx = i2;
+                }
+                if (pass == 1) w.put(E);
+            }
+            idx = end_idx;  // the pixel after the walk's last step
+            break;
+        }
+        if (lam == power) {
+            tv = vec;
+            tdt = dt;
+            power <<= 1;
+            lam = 0;
+        }
     }
+    w.close_repeat();
     if (events) tail_idx[g] = idx;
-    else n_events[g] = k;
+    else n_events[g] = w.k;
 }
 
-// Phase B: the integer updates in seed order (countlink.cl:56-112).
+// The reference's per-event update of count_downchannels (countlink.cl:
+// 104-118); false = the walk stops (it joined a longer path)
+__device__ __forceinline__ bool count_event(const slm_params& p, uint32_t e, uint32_t& counter,
+                                            uint32_t& prev, uint32_t* mapping, uint32_t* count,
+                                            uint32_t* link) {
+    mapping[e] &= ~p.is_channelhead;
+    mapping[e] |= p.is_thinchannel;
+    link[prev] = e;
+    if (++counter < count[e]) return false;
+    count[e] = counter;
+    prev = e;
+    return true;
+}
+
+// One thread replays the walks head by head (the pinned sequential order).
+// A repeat record is replayed event by event for its first lap; after a lap
+// every pattern pixel holds a count this walk wrote at most one lap ago,
+// below the running counter, so no later event can stop the walk.  The laps
+// in between only rewrite the same links, flags and growing counts, so they
+// are skipped and the final lap is replayed with its own counter values.
 __global__ void k_count_replay(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
                                const u64* __restrict__ offsets, const uint32_t* __restrict__ events,
                                const uint32_t* __restrict__ tail_idx, uint32_t* mapping,
                                uint32_t* count, uint32_t* link) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    uint32_t last8[CNT_PMAX];
     for (uint32_t g = 0; g < n; ++g) {
         const uint32_t head = pixel_of(seed_vec(seeds, g), p);
         uint32_t counter = 1, prev = head, last = tail_idx[g];
+        uint32_t nd = 0;  // decoded events (for the pattern ring)
         count[head] = counter++;
-        for (u64 k = offsets[g]; k < offsets[g + 1]; ++k) {
-            const uint32_t e = events[k];
-            mapping[e] &= ~p.is_channelhead;
-            mapping[e] |= p.is_thinchannel;
-            link[prev] = e;
-            if (++counter < count[e]) { last = e; break; }
-            count[e] = counter;
-            prev = e;
+        bool stopped = false;
+        for (u64 k = offsets[g]; k < offsets[g + 1] && !stopped; ++k) {
+            const uint32_t wd = events[k];
+            if ((wd & CNT_REPEAT) == 0u) {
+                if (!count_event(p, wd, counter, prev, mapping, count, link)) { last = wd; stopped = true; break; }
+                last8[nd % CNT_PMAX] = wd;
+                nd++;
+                continue;
+            }
+            uint32_t pat_ring[CNT_PMAX];
+            const uint32_t* pat;
+            uint32_t P, reps;
+            if ((wd & CNT_KIND) == CNT_PERIOD) {
+                P = wd & ~CNT_KIND;
+                pat = events + k + 1;
+                k += P;
+                reps = events[++k];
+            } else {
+                P = wd & ~CNT_REPEAT;
+                reps = events[++k];
+                for (uint32_t t = 0; t < P; ++t) pat_ring[t] = last8[(nd - P + t) % CNT_PMAX];
+                pat = pat_ring;
+            }
+            const uint32_t lap = reps < P ? reps : P;
+            for (uint32_t t = 0; t < lap; ++t) {
+                const uint32_t e = pat[t];
+                if (!count_event(p, e, counter, prev, mapping, count, link)) { last = e; stopped = true; break; }
+                last8[nd % CNT_PMAX] = e;
+                nd++;
+            }
+            if (stopped) break;
+            const uint32_t r = reps - lap;  // events after the first lap, from pattern position 0
+            if (r > 0) {
+                // skip to the final lap (events start..r-1) and replay it in order:
+                // every pattern pixel's last link and count assignments fall in
+                // it; flags were set by the first lap
+                const uint32_t c0 = counter;
+                const uint32_t start = r > P ? r - P : 0u;
+                prev = pat[(start + P - 1) % P];
+                for (uint32_t i = start; i < r; ++i) {
+                    const uint32_t e = pat[i % P];
+                    link[prev] = e;
+                    count[e] = c0 + 1 + i;
+                    prev = e;
+                    last8[nd % CNT_PMAX] = e;
+                    nd++;
+                }
+                counter = c0 + r;
+            }
         }
         link[prev] = last;
     }
@@ -247,6 +443,13 @@ __global__ void k_flag_downchannels(const slm_params p, uint32_t n, const float2
         uint32_t idx = head, prev_idx = idx + 1u, counter = 1;
         count[idx] = counter;
         mapping[idx] |= p.is_thinchannel;
+        // Brent's cycle detection on the walk: link is not written by this
+        // kernel, so a walk that meets its own earlier pixel circles until
+        // counter reaches the bound.  Once a full lap has been walked (and the
+        // counter < 20 window has passed), the remaining laps are applied as
+        // their final effect: each cycle pixel's count becomes the counter of
+        // its last visit (when larger), and no tail is flagged.
+        uint32_t tort = idx, power = 1, lam = 0;
         while (!mask[idx] && prev_idx != idx && counter < lim) {
             prev_idx = idx;
             idx = link[idx];
@@ -259,6 +462,26 @@ __global__ void k_flag_downchannels(const slm_params p, uint32_t n, const float2
                 if (counter >= count[idx]) count[idx] = counter;
             } else {
                 break;
+            }
+            lam++;
+            if (idx == tort && counter >= 20u && prev_idx != idx && counter < lim) {
+                // cycle of length lam through idx, walked once since tort
+                const uint32_t r = lim - counter;  // iterations left
+                uint32_t q = idx;
+                for (uint32_t o = 1; o <= lam && o <= r; ++o) {
+                    q = link[q];
+                    const uint32_t v = counter + o + lam * ((r - o) / lam);
+                    if (v >= count[q]) count[q] = v;
+                }
+                // the walk ends after r more steps at counter == lim; the tail
+                // flag needs counter < lim, so nothing else changes
+                counter = lim;
+                break;
+            }
+            if (lam == power) {
+                tort = idx;
+                power <<= 1;
+                lam = 0;
             }
         }
         if (!mask[prev_idx] && counter < lim) mapping[prev_idx] |= p.is_channeltail;
@@ -444,18 +667,21 @@ __global__ void k_owner_map(const slm_params p, uint32_t n, const float2* __rest
 // Steps of a flank walk up to its label-independent end (mask, thin channel,
 // step cap, stuck), as (compute pixel, moved-to pixel) pairs; consecutive
 // equal pairs are stored once.  With pairs == nullptr only counts.
-__global__ void k_flank_paths(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
+// Items g0 .. g0+n-1; paths are stored at pairs[offsets[g] - base] (a chunk
+// of the item range at a time, so the stored paths fit the workspace).
+__global__ void k_flank_paths(const slm_params p, uint32_t g0, uint32_t n, const float2* __restrict__ seeds,
                               const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
                               const uint32_t* __restrict__ mapping, u64* __restrict__ n_pairs,
-                              const u64* __restrict__ offsets, uint2* __restrict__ pairs) {
-    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= n) return;
+                              const u64* __restrict__ offsets, u64 base, uint2* __restrict__ pairs) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint32_t g = g0 + t;
     Vec2 vec = seed_vec(seeds, g);
     uint32_t idx = pixel_of(vec, p), n_steps = 0;
     float dt = p.dt_max;
     u64 k = 0;
     uint2 last = make_uint2(NO_OWNER, NO_OWNER);
-    uint2* out = pairs ? pairs + offsets[g] : nullptr;
+    uint2* out = pairs ? pairs + (offsets[g] - base) : nullptr;
     while (!mask[idx] && ((~mapping[idx]) & p.is_thinchannel) && n_steps < p.max_n_steps) {
         const Step s = rk_plain(vec, dt, uv, p);
         const uint32_t q = s.idx;
@@ -494,14 +720,16 @@ __device__ __noinline__ bool flank_read(uint32_t q, uint32_t g, uint32_t h, uint
 
 // One resolution round of fix_right_flanks (side 0) or fix_left_flanks
 // (side 1) (segment.cl:441-504, 530-594).
-__global__ void k_flank_round(const slm_params p, uint32_t n, uint32_t side, uint32_t cur_round,
-                              const u64* __restrict__ offsets, const uint2* __restrict__ pairs,
+__global__ void k_flank_round(const slm_params p, uint32_t g0, uint32_t n, uint32_t side, uint32_t cur_round,
+                              const u64* __restrict__ offsets, u64 base, const uint2* __restrict__ pairs,
                               const uint32_t* __restrict__ hpix, const uint8_t* __restrict__ mask,
                               const uint32_t* __restrict__ mapping, const uint32_t* __restrict__ owner,
                               const uint32_t* __restrict__ label_init, uint32_t* label,
                               uint32_t* resolved_round, uint32_t* n_resolved) {
-    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= n || resolved_round[g] != 0u) return;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint32_t g = g0 + t;
+    if (resolved_round[g] != 0u) return;
     const uint32_t lfa = p.left_flank_addition;
     const uint32_t thin = p.is_thinchannel;
     const uint32_t h = hpix[g];
@@ -512,7 +740,7 @@ __global__ void k_flank_round(const slm_params p, uint32_t n, uint32_t side, uin
         if (!flank_read(at, g, h, lab_h, cur_round, owner, label_init, label, resolved_round, v)) return;
         const bool flank_ok = side ? (v & lfa) != 0u : ((~v) & lfa) != 0u;
         if (mask[at] || !flank_ok || (mapping[at] & thin)) break;
-        const uint2 e = pairs[k];
+        const uint2 e = pairs[k - base];
         if (!flank_read(e.x, g, h, lab_h, cur_round, owner, label_init, label, resolved_round, v)) return;
         if ((lab_h & ~lfa) != (v & ~lfa)) lab_h = v;
         at = e.y;
@@ -807,8 +1035,8 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
     if (rc) return rc;
     if (n == 0) return SLM_OK;
     const uint32_t nxy = p->nxy_padded;
-    SLM_REQUIRE(workspace && workspace_bytes >= slm_fix_flanks_workspace(n, nxy, 0),
-                "workspace below the minimum %zu bytes", slm_fix_flanks_workspace(n, nxy, 0));
+    const size_t fixed = slm_fix_flanks_workspace(n, nxy, 0);
+    SLM_REQUIRE(workspace && workspace_bytes >= fixed, "workspace below the minimum %zu bytes", fixed);
     u64* n_pairs = reinterpret_cast<u64*>(workspace);
     u64* offsets = n_pairs + n;
     uint32_t* hpix = reinterpret_cast<uint32_t*>(offsets + n + 1);
@@ -819,47 +1047,77 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
     uintptr_t pa = reinterpret_cast<uintptr_t>(n_resolved + 1);
     pa = (pa + 15) & ~(uintptr_t)15;
     uint2* pairs = reinterpret_cast<uint2*>(pa);
-    k_flank_paths<<<blocks_for(n, 128), 128, 0, SS>>>(*p, n, F2(seed_point), mask, F2(uv), mapping,
-                                                     n_pairs, nullptr, nullptr);
+    const u64 cap_pairs = (workspace_bytes - fixed) / sizeof(uint2);
+    k_flank_paths<<<blocks_for(n, 128), 128, 0, SS>>>(*p, 0u, n, F2(seed_point), mask, F2(uv), mapping,
+                                                     n_pairs, nullptr, 0ull, nullptr);
     SLM_LAUNCHED("k_flank_paths");
     k_exclusive_scan<<<1, 1024, 0, SS>>>(n_pairs, n, offsets);
     SLM_LAUNCHED("k_exclusive_scan");
     u64 total = 0;
     SLM_CUDA(cudaMemcpyAsync(&total, offsets + n, sizeof(u64), cudaMemcpyDeviceToHost, SS));
     SLM_CUDA(cudaStreamSynchronize(SS));
-    const size_t need = slm_fix_flanks_workspace(n, nxy, total);
-    if (required_bytes) *required_bytes = need;
-    if (need > workspace_bytes) {
-        set_error("fix flanks needs %zu workspace bytes (%llu path steps)", need, (unsigned long long)total);
-        return SLM_ERR_CAPACITY;
+    if (required_bytes) *required_bytes = slm_fix_flanks_workspace(n, nxy, total);
+    // Items run in index order, chunk after chunk, each chunk's paths stored
+    // at once: an item reads only initial labels and the final labels of
+    // lower-index owners, which earlier chunks have resolved; rounds keep
+    // counting across chunks, so those owners count as resolved before.
+    std::vector<std::pair<uint32_t, uint32_t>> chunks;
+    if (total <= cap_pairs) {
+        chunks.emplace_back(0u, n);
+    } else {
+        std::vector<u64> off((size_t)n + 1);
+        SLM_CUDA(cudaMemcpyAsync(off.data(), offsets, ((size_t)n + 1) * sizeof(u64), cudaMemcpyDeviceToHost, SS));
+        SLM_CUDA(cudaStreamSynchronize(SS));
+        u64 biggest = 0;
+        for (uint32_t g = 0; g < n; ++g) biggest = std::max<u64>(biggest, off[g + 1] - off[g]);
+        if (biggest > cap_pairs) {
+            if (required_bytes) *required_bytes = slm_fix_flanks_workspace(n, nxy, biggest);
+            set_error("fix flanks: one path has %llu steps; the workspace holds %llu",
+                      (unsigned long long)biggest, (unsigned long long)cap_pairs);
+            return SLM_ERR_CAPACITY;
+        }
+        uint32_t a = 0;
+        while (a < n) {
+            uint32_t b = a + 1;
+            while (b < n && off[b + 1] - off[a] <= cap_pairs) ++b;
+            chunks.emplace_back(a, b);
+            a = b;
+        }
     }
-    k_flank_paths<<<blocks_for(n, 128), 128, 0, SS>>>(*p, n, F2(seed_point), mask, F2(uv), mapping,
-                                                     nullptr, offsets, pairs);
-    SLM_LAUNCHED("k_flank_paths");
     SLM_CUDA(cudaMemsetAsync(owner, 0xff, (size_t)nxy * sizeof(uint32_t), SS));
     SLM_CUDA(cudaMemsetAsync(resolved, 0, (size_t)n * sizeof(uint32_t), SS));
     SLM_CUDA(cudaMemcpyAsync(label_init, label, (size_t)nxy * sizeof(uint32_t), cudaMemcpyDeviceToDevice, SS));
     k_owner_map<<<blocks_for(n, 256), 256, 0, SS>>>(*p, n, F2(seed_point), owner, hpix);
     SLM_LAUNCHED("k_owner_map");
-    uint32_t done = 0;
-    for (uint32_t round = 1; done < n; ++round) {
-        if (round > n + 1) {
-            set_error("fix flanks did not resolve within %u rounds", n + 1);
-            return SLM_ERR_ITERATION_CAP;
-        }
-        SLM_CUDA(cudaMemsetAsync(n_resolved, 0, sizeof(uint32_t), SS));
-        k_flank_round<<<blocks_for(n, 256), 256, 0, SS>>>(*p, n, left ? 1u : 0u, round, offsets, pairs, hpix, mask,
-                                                         mapping, owner, label_init, label, resolved,
-                                                         n_resolved);
-        SLM_LAUNCHED("k_flank_round");
-        uint32_t newly = 0;
-        SLM_CUDA(cudaMemcpyAsync(&newly, n_resolved, sizeof(uint32_t), cudaMemcpyDeviceToHost, SS));
+    uint32_t round = 1;
+    for (const auto& c : chunks) {
+        const uint32_t a = c.first, m = c.second - c.first;
+        u64 base = 0;
+        SLM_CUDA(cudaMemcpyAsync(&base, offsets + a, sizeof(u64), cudaMemcpyDeviceToHost, SS));
         SLM_CUDA(cudaStreamSynchronize(SS));
-        if (newly == 0) {
-            set_error("fix flanks round %u resolved nothing", round);
-            return SLM_ERR_ITERATION_CAP;
+        k_flank_paths<<<blocks_for(m, 128), 128, 0, SS>>>(*p, a, m, F2(seed_point), mask, F2(uv), mapping,
+                                                         nullptr, offsets, base, pairs);
+        SLM_LAUNCHED("k_flank_paths");
+        uint32_t done = 0;
+        for (uint32_t r0 = round; done < m; ++round) {
+            if (round - r0 > m + 1) {
+                set_error("fix flanks did not resolve within %u rounds", m + 1);
+                return SLM_ERR_ITERATION_CAP;
+            }
+            SLM_CUDA(cudaMemsetAsync(n_resolved, 0, sizeof(uint32_t), SS));
+            k_flank_round<<<blocks_for(m, 256), 256, 0, SS>>>(*p, a, m, left ? 1u : 0u, round, offsets, base,
+                                                             pairs, hpix, mask, mapping, owner, label_init,
+                                                             label, resolved, n_resolved);
+            SLM_LAUNCHED("k_flank_round");
+            uint32_t newly = 0;
+            SLM_CUDA(cudaMemcpyAsync(&newly, n_resolved, sizeof(uint32_t), cudaMemcpyDeviceToHost, SS));
+            SLM_CUDA(cudaStreamSynchronize(SS));
+            if (newly == 0) {
+                set_error("fix flanks round %u resolved nothing", round);
+                return SLM_ERR_ITERATION_CAP;
+            }
+            done += newly;
         }
-        done += newly;
     }
     return SLM_OK;
 }

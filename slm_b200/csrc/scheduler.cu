@@ -224,7 +224,8 @@ struct InferSmem {
 
 __global__ void __launch_bounds__(INF_WARPS * 32)
 k_cnn_infer(const float2* __restrict__ uv, uint32_t nxp, uint32_t nyp, uint32_t pad,
-            const float2* __restrict__ seeds, uint32_t n, const float* __restrict__ w1,
+            const float2* __restrict__ seeds, const uint32_t* __restrict__ index, uint32_t n,
+            const float* __restrict__ w1,
             const float* __restrict__ b1, const float* __restrict__ w2, const float* __restrict__ b2,
             const float* __restrict__ w3, const float* __restrict__ b3, float* __restrict__ out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -255,7 +256,7 @@ k_cnn_infer(const float2* __restrict__ uv, uint32_t nxp, uint32_t nyp, uint32_t 
             for (int sl = 0; sl < 4; ++sl) {
                 const uint32_t s = grp * 16 + q * 4 + sl;
                 const uint32_t sc = s < n ? s : n - 1;
-                const float2 sp = seeds[sc];
+                const float2 sp = seeds[index ? __ldg(index + sc) : sc];
                 const int cx = (int)sp.x + (int)pad, cy = (int)sp.y + (int)pad;
                 // conv1: M = 16 tiles, K = 32, N = 32
                 float c[4][4] = {};
@@ -337,8 +338,16 @@ k_cnn_infer(const float2* __restrict__ uv, uint32_t nxp, uint32_t nyp, uint32_t 
         }
         if (tig == 0) {
             const uint32_t s0 = grp * 16 + gid, s1 = s0 + 8;
-            if (s0 < n) { out[2 * (size_t)s0] = c3[0] + S.b3[0]; out[2 * (size_t)s0 + 1] = c3[1] + S.b3[1]; }
-            if (s1 < n) { out[2 * (size_t)s1] = c3[2] + S.b3[0]; out[2 * (size_t)s1 + 1] = c3[3] + S.b3[1]; }
+            if (s0 < n) {
+                const size_t o = index ? __ldg(index + s0) : s0;
+                out[2 * o] = c3[0] + S.b3[0];
+                out[2 * o + 1] = c3[1] + S.b3[1];
+            }
+            if (s1 < n) {
+                const size_t o = index ? __ldg(index + s1) : s1;
+                out[2 * o] = c3[2] + S.b3[0];
+                out[2 * o + 1] = c3[3] + S.b3[1];
+            }
         }
         __syncwarp();
     }
@@ -571,7 +580,8 @@ int slm_adam(float* w, float* wq, const float* g, float* m, float* v, uint64_t n
 }
 
 int slm_cnn_infer(const float* uv, uint32_t nx_padded, uint32_t ny_padded, uint32_t pad,
-                  const float* seed_point, uint32_t n, const float* w1, const float* b1,
+                  const float* seed_point, const uint32_t* index, uint32_t n, const float* w1,
+                  const float* b1,
                   const float* w2, const float* b2, const float* w3, const float* b3, float* out,
                   void* stream) {
     clear_error();
@@ -585,7 +595,7 @@ int slm_cnn_infer(const float* uv, uint32_t nx_padded, uint32_t ny_padded, uint3
     if (grid > cap) grid = cap;
     k_cnn_infer<<<grid, INF_WARPS * 32, smem, (cudaStream_t)stream>>>(
         reinterpret_cast<const float2*>(uv), nx_padded, ny_padded, pad,
-        reinterpret_cast<const float2*>(seed_point), n, w1, b1, w2, b2, w3, b3, out);
+        reinterpret_cast<const float2*>(seed_point), index, n, w1, b1, w2, b2, w3, b3, out);
     SLM_LAUNCHED("k_cnn_infer");
     return SLM_OK;
 }

@@ -29,6 +29,7 @@ SPECS = {
     "hillslopes": ("slm_hillslopes", (4,), None),
     "hillslope_lengths": ("slm_hillslope_lengths", (4,), None),
 }
+FLANK_PATH_BUDGET = 4 << 30  # bytes of stored flank paths per chunk
 _MIN_WS = {
     "count_downchannels": lambda L, p, n: L.slm_count_downchannels_workspace(n, 0),
     "fix_right_flanks": lambda L, p, n: L.slm_fix_flanks_workspace(n, p.nxy_padded, 0),
@@ -63,6 +64,9 @@ def run(name, params, seeds, arrays, device=None):
         elif extra == "workspace":
             need = ctypes.c_uint64(0)
             size = int(_MIN_WS[name](L, params, n))
+            if name.startswith("fix_"):
+                # the flank fix stores paths chunk by chunk within this budget
+                size += FLANK_PATH_BUDGET
             ws = torch.empty(size, dtype=torch.uint8, device=dev)
             rc = fn(*(args + [ptr(ws), size, ctypes.byref(need), stream]))
             if rc == _lib.SLM_ERR_CAPACITY:

@@ -49,10 +49,14 @@ class DeviceRunner:
     def __init__(self, device=None):
         self.device = device
         self.status = 0  # OR of the status words returned by the kernels
+        self.seconds = {}  # wall time per kernel name (each call copies in and out)
 
     def __call__(self, name, params, seeds, arrays):
+        import time
         from . import map_kernels
+        t = time.perf_counter()
         st = map_kernels.run(name, params, seeds, arrays, self.device)
+        self.seconds[name] = self.seconds.get(name, 0.0) + time.perf_counter() - t
         self.status |= st
         return st
 

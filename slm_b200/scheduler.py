@@ -212,12 +212,14 @@ class LengthModel:
         return torch.cat(hist).cpu().numpy()
 
     # ------------------------------------------------------------ inference
-    def predict(self, uv, nxp, nyp, pad, seeds, n, out=None, stream=None):
-        """Fused tensor-core inference: predictions [n][2] (down, up)."""
+    def predict(self, uv, nxp, nyp, pad, seeds, n, out=None, visit=None, stream=None):
+        """Fused tensor-core inference: predictions [n][2] (down, up).
+        ``visit`` (uint32 [n], optional): the order the seeds are processed
+        in, e.g. ``spatial_order(...)``, for cache locality of the patches."""
         W = self.W
         if out is None:
             out = torch.empty((n, 2), dtype=torch.float32, device=self.device)
-        check(self.L.slm_cnn_infer(ptr(uv), int(nxp), int(nyp), int(pad), ptr(seeds), int(n),
+        check(self.L.slm_cnn_infer(ptr(uv), int(nxp), int(nyp), int(pad), ptr(seeds), ptr(visit), int(n),
                                    ptr(W["w1"]), ptr(W["b1"]), ptr(W["w2"]), ptr(W["b2"]), ptr(W["w3"]),
                                    ptr(W["b3"]), ptr(out), _stream(stream)))
         return out

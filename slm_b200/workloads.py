@@ -41,6 +41,10 @@ SPECS = {
                             8192, 1.0, 2, 1.0, 4, 0.1, 20000, "config5"),
     "small": WorkloadSpec("256x256 @1m, d=2, jitter +-0.5, RK2, step 0.1 px, max 2000 steps",
                           256, 1.0, 2, 1.0, 2, 0.1, 2000, "tile"),
+    "config4": WorkloadSpec("4096x4096 @2m incised fBm, d=4, jitter +-0.5, RK4, step 0.1 px, "
+                            "max 10000 steps", 4096, 2.0, 4, 1.0, 4, 0.1, 10000, "incised"),
+    "incised512_d4": WorkloadSpec("512x512 @2m incised fBm, d=4, jitter +-0.5, RK4, step 0.1 px, "
+                                  "max 10000 steps", 512, 2.0, 4, 1.0, 4, 0.1, 10000, "incised"),
     "incised512": WorkloadSpec("512x512 @2m incised fBm, d=2, jitter +-0.5, RK2, step 0.1 px, "
                                "max 10000 steps", 512, 2.0, 2, 1.0, 2, 0.1, 10000, "incised"),
 }

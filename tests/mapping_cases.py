@@ -68,3 +68,39 @@ def midslope_case(data, info, seed=3, frac=0.05):
 
 def clone(data):
     return copy.deepcopy(data)
+
+
+def incised_pipeline_case(n=128, seed=3, n_incisions=12, max_steps=300, channel_pct=94.0,
+                          segmentation_threshold=10):
+    """Mapping inputs on the incised relief of the 2048^2 workload at a small
+    size.  Its V-shaped valley floors make count_downchannels walks oscillate
+    to the 1000*MAX_N_STEPS bound and leave link cycles for
+    flag_downchannels; max_steps keeps that bound small for the oracle."""
+    from slm_b200 import synth
+    from slm_b200.useful import Info, create_seeds, default_parameters
+    d = default_parameters()
+    d.trace.subpixel_seed_point_density = 1
+    d.trace.jitter_magnitude = 0.0
+    d.trace.integrator_step_factor = 0.1
+    d.trace.max_length = max_steps * 0.1
+    dtm = synth.config2_dtm(n, seed, n_incisions)
+    uv, mask = synth.uv_from_dtm(dtm, 2.0, 2)
+    info = Info(d.state, d.trace, 2.0)
+    info.set_xy(n, n, 2)
+    seeds, ns, npad = create_seeds(mask, 2, info.n_work_items, do_shuffle=True, rng_seed=1)
+    info.n_seed_points, info.n_padded_seed_points = ns, npad
+    nxp, nyp = mask.shape
+    slc = np.zeros((nxp, nyp, 2), np.float64)
+    slt = np.zeros((nxp, nyp, 2), np.float32)
+    from slm_b200.params import kernel_params
+    for k, sign in ((0, 1.0), (1, -1.0)):
+        prm = kernel_params(info, "INTEGRATE_FIELDS", sign)
+        a, b, _, _ = O.integrate_fields(prm, seeds, mask, uv)
+        slc[:, :, k] = a.reshape(nxp, nyp)
+        slt[:, :, k] = np.sqrt(b.reshape(nxp, nyp).astype(np.float32) * np.float32(1.0))
+    slc = np.sqrt(2.0) * np.power(slc, 2 / 3)
+    thr = np.float32(np.percentile(slt[:, :, 0][~mask], channel_pct))
+    info.set_thresholds(segmentation_threshold=np.uint32(segmentation_threshold), channel_threshold=thr)
+    data = Data(info=info, mask_array=mask, uv_array=uv, mapping_array=np.zeros(mask.shape, np.uint32),
+                slt_array=slt, slc_array=slc)
+    return info, data

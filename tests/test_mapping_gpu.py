@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from mapping_cases import midslope_case, oracle_runner, pipeline_case
+from mapping_cases import incised_pipeline_case, midslope_case, oracle_runner, pipeline_case
 from slm_b200 import mapping as M
 
 pytestmark = pytest.mark.gpu
@@ -64,3 +64,28 @@ def test_device_pipeline_end_to_end_matches_oracle_pipeline():
     assert dev.status == 0
     for name in ("mapping_array", "count_array", "link_array", "label_array", "channel_label_array"):
         assert np.array_equal(getattr(data, name), getattr(data2, name)), name
+
+
+@pytest.mark.parametrize("seed", [3, 4])
+def test_mapping_pipeline_incised_bit_exact(seed):
+    """Valley floors one pixel wide: count_downchannels walks oscillate to the
+    1000*MAX_N_STEPS bound, exercising the compressed event replay."""
+    info, data = incised_pipeline_case(seed=seed)
+    run = DeviceVsOracle()
+    assert M.map_channels_segments(None, info, data, runner=run)
+    assert run.mismatches == [], run.mismatches
+    midslope_case(data, info)
+    assert M.hsl(None, info, data, False, runner=run)
+    assert run.mismatches == [], run.mismatches
+
+
+def test_flank_fix_in_chunks_bit_exact(monkeypatch):
+    """A path budget far below the total makes fix_right/left_flanks run their
+    items in many index-ordered chunks; labels equal the oracle's."""
+    from slm_b200 import map_kernels
+    monkeypatch.setattr(map_kernels, "FLANK_PATH_BUDGET", 2048)
+    c, info, data = pipeline_case(nx=120, ny=96, seed=12)
+    run = DeviceVsOracle()
+    assert M.map_channels_segments(None, info, data, runner=run)
+    assert run.mismatches == [], run.mismatches
+    assert ("fix_right_flanks", ) == tuple(n for n, _ in run.calls if n == "fix_right_flanks")

@@ -101,6 +101,10 @@ def test_inference_matches_oracle_forward():
     scale = np.abs(ref).max()
     assert np.abs(pred.cpu().numpy() - ref).max() <= 2e-3 * scale
     assert np.abs(y.cpu().numpy() - ref).max() <= 2e-3 * scale
+    # visiting the seeds in another order changes no prediction
+    perm = torch.from_numpy(np.random.default_rng(11).permutation(seeds.shape[0]).astype(np.int32)).to(DEV)
+    pred2 = m.predict(uv_d, uv.shape[0], uv.shape[1], 2, seeds_d, seeds.shape[0], visit=perm.view(torch.uint32))
+    assert torch.equal(pred, pred2)
 
 
 def test_order_by_prediction():
