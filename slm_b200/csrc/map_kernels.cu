@@ -45,6 +45,7 @@
 #define MAP_LOOP_CAP (1u << 26)
 #define CONNECT_REC_MAX 256
 #define NO_OWNER 0xffffffffu
+#define FLANK_PERIOD 0x80000000u
 
 namespace slm {
 
@@ -682,6 +683,13 @@ __global__ void k_flank_paths(const slm_params p, uint32_t g0, uint32_t n, const
     u64 k = 0;
     uint2 last = make_uint2(NO_OWNER, NO_OWNER);
     uint2* out = pairs ? pairs + (offsets[g] - base) : nullptr;
+    // As in count_downchannels: once (vec, dt) repeats bit for bit the
+    // per-step pairs repeat with the period, so the rest of the walk is
+    // stored as one period record {0x80000000|E, n} + the E pairs of a lap
+    // (after every step `last` is that step's pair, so each lap merges alike).
+    Vec2 tv = vec;
+    float tdt = dt;
+    uint32_t power = 1, lam = 0;
     while (!mask[idx] && ((~mapping[idx]) & p.is_thinchannel) && n_steps < p.max_n_steps) {
         const Step s = rk_plain(vec, dt, uv, p);
         const uint32_t q = s.idx;
@@ -693,6 +701,47 @@ __global__ void k_flank_paths(const slm_params p, uint32_t g0, uint32_t n, const
             k++;
         }
         if (stuck) break;
+        lam++;
+        if (__float_as_uint(vec.x) == __float_as_uint(tv.x) && __float_as_uint(vec.y) == __float_as_uint(tv.y)
+            && __float_as_uint(dt) == __float_as_uint(tdt) && n_steps < p.max_n_steps) {
+            const uint32_t L = lam, R = p.max_n_steps - n_steps, Rm = R % L;
+            uint32_t E = 0, partial = 0;
+            for (int pass = 0; pass < 2; ++pass) {
+                Vec2 v2 = vec;
+                float d2 = dt;
+                uint32_t i2 = idx, ns2 = 0;
+                uint2 l2 = last;
+                if (pass == 1) {
+                    const uint32_t nfut = (R / L) * E + partial;
+                    if (nfut == 0) break;
+                    if (out) out[k] = make_uint2(FLANK_PERIOD | E, nfut);
+                    k++;
+                }
+                for (uint32_t t2 = 1; t2 <= L; ++t2) {
+                    const Step s2 = rk_plain(v2, d2, uv, p);
+                    const uint32_t q2 = s2.idx;
+                    i2 = q2;
+                    seg_move(s2, v2, i2, d2, ns2, p);
+                    if (q2 != l2.x || i2 != l2.y) {
+                        l2 = make_uint2(q2, i2);
+                        if (pass == 0) {
+                            E++;
+                            if (t2 <= Rm) partial++;
+                        } else {
+                            if (out) out[k] = l2;
+                            k++;
+                        }
+                    }
+                }
+            }
+            break;
+        }
+        if (lam == power) {
+            tv = vec;
+            tdt = dt;
+            power <<= 1;
+            lam = 0;
+        }
     }
     if (!pairs) n_pairs[g] = k;
 }
@@ -736,15 +785,53 @@ __global__ void k_flank_round(const slm_params p, uint32_t g0, uint32_t n, uint3
     uint32_t lab_h = label_init[h];
     uint32_t at = h, v = 0u;
     const u64 k_end = offsets[g + 1];
-    for (u64 k = offsets[g]; k < k_end; ++k) {
-        if (!flank_read(at, g, h, lab_h, cur_round, owner, label_init, label, resolved_round, v)) return;
+    // one step of the walk's label scan: 0 go on, 1 the walk stops, 2 wait
+    // (a lower-index owner on the path is not resolved yet)
+    auto scan = [&](uint2 e) -> int {
+        if (!flank_read(at, g, h, lab_h, cur_round, owner, label_init, label, resolved_round, v)) return 2;
         const bool flank_ok = side ? (v & lfa) != 0u : ((~v) & lfa) != 0u;
-        if (mask[at] || !flank_ok || (mapping[at] & thin)) break;
-        const uint2 e = pairs[k - base];
-        if (!flank_read(e.x, g, h, lab_h, cur_round, owner, label_init, label, resolved_round, v)) return;
+        if (mask[at] || !flank_ok || (mapping[at] & thin)) return 1;
+        if (!flank_read(e.x, g, h, lab_h, cur_round, owner, label_init, label, resolved_round, v)) return 2;
         if ((lab_h & ~lfa) != (v & ~lfa)) lab_h = v;
         at = e.y;
+        return 0;
+    };
+    int st = 0;
+    for (u64 k = offsets[g]; k < k_end && st == 0; ++k) {
+        const uint2 e = pairs[k - base];
+        if ((e.x & FLANK_PERIOD) == 0u) {
+            st = scan(e);
+            continue;
+        }
+        // period record: n pairs cycling through the next E.  Every read but
+        // that of the item's own pixel gives the same value each lap and `at`
+        // starts each lap at the lap's last pair, so a lap is a function of
+        // lab_h at its start: once a lap-start lab_h repeats, whole multiples
+        // of that lap period change nothing and are skipped.
+        const uint32_t E = e.x & ~FLANK_PERIOD;
+        const uint32_t nfut = e.y;
+        const uint2* pat = pairs + (k + 1 - base);
+        k += E;
+        const uint32_t full = nfut / E, rem = nfut % E;
+        uint32_t seen[8];
+        bool skipped = false;
+        for (uint32_t lap = 0; lap < full && st == 0; ++lap) {
+            if (!skipped && lap < 8) {
+                for (uint32_t j = 0; j < lap; ++j)
+                    if (seen[j] == lab_h) {
+                        const uint32_t per = lap - j;
+                        lap += ((full - lap) / per) * per;
+                        skipped = true;
+                        break;
+                    }
+                if (!skipped) seen[lap] = lab_h;
+                if (lap >= full) break;
+            }
+            for (uint32_t i = 0; i < E && st == 0; ++i) st = scan(pat[i]);
+        }
+        for (uint32_t i = 0; i < rem && st == 0; ++i) st = scan(pat[i]);
     }
+    if (st == 2) return;
     if (!flank_read(at, g, h, lab_h, cur_round, owner, label_init, label, resolved_round, v)) return;
     if ((lab_h & ~lfa) != (v & ~lfa)) lab_h = v;
     flank_read(at, g, h, lab_h, cur_round, owner, label_init, label, resolved_round, v);
@@ -767,6 +854,11 @@ __global__ void k_hillslopes(const slm_params p, uint32_t n, const float2* __res
     Vec2 vec = seed_vec(seeds, g);
     float dt = p.dt_max;
     uint32_t idx = pixel_of(vec, p), prev_idx = idx, n_steps = 0;
+    // a (vec, dt) state repeating inside the start pixel (Brent) means the
+    // walk circles there until the step bound and writes no link
+    Vec2 tv = vec;
+    float tdt = dt;
+    uint32_t power = 1, lam = 0;
     while (prev_idx == idx && !mask[idx] && n_steps < 100u * p.max_n_steps) {
         prev_idx = idx;
         const Step s = rk_plain(vec, dt, uv, p);
@@ -775,6 +867,15 @@ __global__ void k_hillslopes(const slm_params p, uint32_t n, const float2* __res
         if (m.stuck) break;
         dt = next_dt(dt, m.err, p);
         n_steps++;
+        if (idx == prev_idx && __float_as_uint(vec.x) == __float_as_uint(tv.x)
+            && __float_as_uint(vec.y) == __float_as_uint(tv.y) && __float_as_uint(dt) == __float_as_uint(tdt))
+            return;
+        if (++lam == power) {
+            tv = vec;
+            tdt = dt;
+            power <<= 1;
+            lam = 0;
+        }
     }
     if (prev_idx != idx && !mask[idx]) link[prev_idx] = idx;
 }
