@@ -544,14 +544,22 @@ def run_batched(args):
 
     from slm_b200 import autotune, batch
 
-    dev = torch.device("cuda", 0)
+    import torch.distributed as dist
+    ws, rank, local = _dist()
+    dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    if ws > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     t0 = time.time()
-    tiles = batch.uneven_tiles(args.tiles, 256, 3072, seed=3, density=2, jitter=1.0, step=0.1,
-                               max_steps=2000)
+    all_tiles = batch.uneven_tiles(args.tiles, 256, 3072, seed=3, density=2, jitter=1.0, step=0.1,
+                                   max_steps=2000)
     t_gen = time.time() - t0
+    # whole tiles per rank (no collective on the data path)
+    sizes = [int(t.info.nx) * int(t.info.ny) for t in all_tiles]
+    tiles = [all_tiles[i] for i in batch.shard_tiles(sizes, rank, ws)]
     b = batch.TileBatch(tiles, dev, integrator=2)
-    n_px = sum(int(t.info.nx) * int(t.info.ny) for t in tiles)
+    n_px = sum(sizes)
     sample = batch.TileBatch(tiles[:12], dev, integrator=2)
     launch, table = autotune.tune(lambda L: sample.trace(L), "k_fields_batched", 2,
                                   "uneven fBm tiles, d=2, RK2, 12-tile sample",
@@ -590,17 +598,31 @@ def run_batched(args):
     for _ in range(args.warmup):
         g.replay()
     torch.cuda.synchronize()
-    with ClockSampler(0) as clocks:
+    if ws > 1:
+        dist.barrier()
+    with ClockSampler(local) as clocks:
         times = timed(g.replay, args.steps)
     if not torch.equal(b.acc, ref):
         raise RuntimeError("graph replay differs from the eager trace")
     step_t = float(np.sum(times))
+    if ws > 1:
+        t = torch.tensor([step_t], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_t = float(t[0])
+        st = torch.tensor([steps], dtype=torch.int64, device=dev)
+        dist.all_reduce(st, op=dist.ReduceOp.SUM)
+        steps = int(st.item())
+        del g
+        dist.barrier()
+        dist.destroy_process_group()
+        if rank != 0:
+            return 0
     forms["batched_graph"] = step_t / args.steps
     peak, peak_kind = _peaks()
     bps = BYTES_PER_STEP[2]
     line = {
         "metric": "trajectory steps/s (fields, batched tiles)", "value": steps * args.steps / step_t,
-        "unit": "steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "unit": "steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * step_t / args.steps, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded fBm tiles; no dataset)",
         "config": {"workload": "{} fBm tiles, edges log-uniform 256..3072 px, d=2 jitter +-0.5, RK2, "
@@ -610,7 +632,8 @@ def run_batched(args):
                    "l2": "256 MiB buffer written between steps", "generation_s": t_gen,
                    "launch": {"block_threads": launch.block_threads,
                               "blocks_per_sm": launch.blocks_per_sm},
-                   "autotune_ms": table, "parallelism": "1 GPU"},
+                   "autotune_ms": table,
+                   "parallelism": "whole tiles per rank ({} ranks)".format(ws) if ws > 1 else "1 GPU"},
         "forms_ms": {k: 1e3 * v for k, v in forms.items()},
         "forms_steps_per_s": {k: steps / v for k, v in forms.items()},
         "batched_vs_per_tile_plain": forms["per_tile_plain"] / forms["batched_graph"],
@@ -792,6 +815,7 @@ def run_e2e(args, wl, dev):
     d2h = nxy * 2 * (8 + 4 + 4) + wl.n_traj * 2 * (2 + 4)
     return {"value": n / t, "unit": "steps/s", "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "steps": k,
+            "mpx_per_s": wl.n_pixels * k / t / 1e6,
             "note": "Trajectories.integrate + Fields.integrate through the public API: seed "
                     "creation and shuffle, uploads, tracing, the fields' post-processing (on the "
                     "GPU) and the finished arrays copied back, every step"}

@@ -205,6 +205,24 @@ class TileBatch:
         return self.acc[:, 0, o:o + n].reshape(shape), self.acc[:, 1, o:o + n].reshape(shape)
 
 
+def shard_tiles(sizes, rank, world_size):
+    """Indices of the tiles rank ``rank`` of ``world_size`` traces: whole tiles,
+    largest first onto the least-loaded rank (ties to the lower rank), so the
+    ranks' pixel counts balance and every tile is traced exactly once.  Tiles
+    are independent (own grids, own fields), so sharding needs no collective
+    beyond gathering the ranks' counters."""
+    if not 0 <= rank < world_size:
+        raise ValueError("rank {} outside world size {}".format(rank, world_size))
+    load = [0] * world_size
+    mine = []
+    for i in sorted(range(len(sizes)), key=lambda i: (-int(sizes[i]), i)):
+        r = min(range(world_size), key=lambda k: (load[k], k))
+        load[r] += int(sizes[i])
+        if r == rank:
+            mine.append(i)
+    return sorted(mine)
+
+
 def uneven_tiles(n_tiles=96, lo=256, hi=3072, seed=3, **kw):
     """``n_tiles`` fBm tiles (tilt + hills + fBm, each its own seed, hills cut
     at 5 sigma) with edge lengths log-uniform in [lo, hi] px, each edge drawn

@@ -62,3 +62,51 @@ def test_uneven_tile_sizes():
     edges = [int(round(np.exp(rng.uniform(np.log(256), np.log(3072))))) for _ in range(2 * 96)]
     assert 256 <= min(edges) and max(edges) <= 3072
     assert B.uneven_tiles.__defaults__[:3] == (96, 256, 3072)
+
+
+def test_shard_tiles_whole_tiles_balanced():
+    rng = np.random.default_rng(7)
+    sizes = [int(np.exp(rng.uniform(np.log(256), np.log(3072)))) ** 2 for _ in range(96)]
+    for ws in (1, 2, 3, 8):
+        parts = [batch.shard_tiles(sizes, r, ws) for r in range(ws)]
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(96))
+        loads = [sum(sizes[i] for i in p) for p in parts]
+        # LPT: every rank within the largest tile of the mean
+        assert max(loads) - min(loads) <= max(sizes)
+    with pytest.raises(ValueError):
+        batch.shard_tiles(sizes, 2, 2)
+
+
+def _gather_rank(rank, ws, port, sizes, q):
+    import os
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"], os.environ["MASTER_PORT"] = "127.0.0.1", str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=ws)
+    mine = batch.shard_tiles(sizes, rank, ws)
+    t = torch.tensor([sum(sizes[i] for i in mine), len(mine)], dtype=torch.int64)
+    dist.all_reduce(t)
+    q.put((rank, int(t[0]), int(t[1])))
+    dist.destroy_process_group()
+
+
+def test_shard_tiles_gloo_gather():
+    """Two gloo ranks shard the tiles and gather their counters: totals are
+    the whole batch's (the only exchange the batched form needs)."""
+    import multiprocessing as mp
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    sizes = [(50 + 7 * i) ** 2 for i in range(20)]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_gather_rank, args=(r, 2, port, sizes, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=120) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+    assert all(o[1] == sum(sizes) and o[2] == len(sizes) for o in out)
