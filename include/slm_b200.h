@@ -319,6 +319,15 @@ int slm_fix_left_flanks(const slm_params* p, uint32_t n_seeds, const float* seed
 int slm_hillslopes(const slm_params* p, uint32_t n_seeds, const float* seed_point,
                    const uint8_t* mask, const float* uv, const uint32_t* mapping,
                    const uint32_t* count, uint32_t* link, void* stream);
+/* slm_thin: Zhang-Suen thinning of a 0/1 image [nx][ny] (x-major; outside
+ * the image counts as 0) in place on the device, the host step that thins
+ * the channel mask between the mapping kernels (the reference does it with
+ * scikit-image's skeletonize(medial_axis(...)), mapping.py:707-719).  Each
+ * iteration is two sub-iterations; stops after an iteration that removes
+ * nothing, or after max_iter.  scratch: nx*ny bytes; flag: 1 uint32 of
+ * device scratch; *iterations (may be NULL) receives the iterations run. */
+int slm_thin(uint8_t* image, uint8_t* scratch, uint32_t nx, uint32_t ny, uint32_t max_iter,
+             uint32_t* flag, uint32_t* iterations, void* stream);
 /* hillslope_lengths (opencl/lengths.cl:37-116; lengths.py:33-92);
  * traj_length [n_seeds] float, written only where a channel is reached */
 int slm_hillslope_lengths(const slm_params* p, uint32_t n_seeds, const float* seed_point,

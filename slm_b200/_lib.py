@@ -83,6 +83,7 @@ SIGNATURES = {
     "slm_fix_left_flanks": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P, _P, ctypes.c_size_t, _P, _P]),
     "slm_hillslopes": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P]),
     "slm_hillslope_lengths": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P]),
+    "slm_thin": (ctypes.c_int, [_P, _P, _U, _U, _U, _P, _P, _P]),
     "slm_cnn_gather": (ctypes.c_int, [_P, _U, _U, _U, _P, _P, _U, _P, _P]),
     "slm_cnn_rearrange": (ctypes.c_int, [_P, _U, _P, _I, _P]),
     "slm_gemm": (ctypes.c_int, [_I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _I, _I, _P]),

@@ -933,6 +933,43 @@ __global__ void k_exclusive_scan(const u64* __restrict__ in, uint32_t n, u64* __
     if (threadIdx.x == 0) out[n] = carry;
 }
 
+// ------------------------------------------------------------------ thinning
+// One sub-iteration of Zhang-Suen thinning (T. Y. Zhang, C. Y. Suen, CACM
+// 27(3), 1984) on a 0/1 image [nx][ny] (x-major, outside = 0): dst = src with
+// every removable pixel cleared; *changed set when one was.  Neighbours P2..P9
+// run clockwise from (x-1, y): (x-1,y) (x-1,y+1) (x,y+1) (x+1,y+1) (x+1,y)
+// (x+1,y-1) (x,y-1) (x-1,y-1).
+__global__ void k_zhang_suen(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, uint32_t nx,
+                             uint32_t ny, int step, uint32_t* changed) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nx * ny) return;
+    const uint32_t x = i / ny, y = i % ny;
+    const uint8_t c = src[i];
+    uint8_t out = c;
+    if (c) {
+        auto at = [&](int dx, int dy) -> uint32_t {
+            const int xx = (int)x + dx, yy = (int)y + dy;
+            if (xx < 0 || yy < 0 || xx >= (int)nx || yy >= (int)ny) return 0u;
+            return src[(size_t)xx * ny + yy] ? 1u : 0u;
+        };
+        const uint32_t n[8] = {at(-1, 0), at(-1, 1), at(0, 1), at(1, 1), at(1, 0), at(1, -1), at(0, -1), at(-1, -1)};
+        uint32_t b = 0, a = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            b += n[k];
+            a += (n[k] == 0u && n[(k + 1) & 7] == 1u) ? 1u : 0u;
+        }
+        const uint32_t p2 = n[0], p4 = n[2], p6 = n[4], p8 = n[6];
+        const bool c1 = step == 0 ? (p2 * p4 * p6) == 0u : (p2 * p4 * p8) == 0u;
+        const bool c2 = step == 0 ? (p4 * p6 * p8) == 0u : (p2 * p6 * p8) == 0u;
+        if (b >= 2u && b <= 6u && a == 1u && c1 && c2) {
+            out = 0;
+            *changed = 1u;
+        }
+    }
+    dst[i] = out;
+}
+
 }  // namespace slm
 
 using namespace slm;
@@ -1251,6 +1288,30 @@ int slm_hillslopes(const slm_params* p, uint32_t n, const float* seed_point, con
     if (n == 0) return SLM_OK;
     k_hillslopes<<<blocks_for(n, 128), 128, 0, SS>>>(*p, n, F2(seed_point), mask, F2(uv), link);
     SLM_LAUNCHED("k_hillslopes");
+    return SLM_OK;
+}
+
+int slm_thin(uint8_t* image, uint8_t* scratch, uint32_t nx, uint32_t ny, uint32_t max_iter,
+             uint32_t* flag, uint32_t* iterations, void* stream) {
+    clear_error();
+    SLM_REQUIRE(image && scratch && flag, "NULL buffer");
+    SLM_REQUIRE((uint64_t)nx * ny < (1ull << 32), "image too large");
+    if (iterations) *iterations = 0;
+    const uint32_t np_ = nx * ny;
+    if (np_ == 0) return SLM_OK;
+    uint32_t it = 0;
+    for (; it < max_iter; ++it) {
+        SLM_CUDA(cudaMemsetAsync(flag, 0, sizeof(uint32_t), SS));
+        k_zhang_suen<<<blocks_for(np_, 256), 256, 0, SS>>>(image, scratch, nx, ny, 0, flag);
+        SLM_LAUNCHED("k_zhang_suen");
+        k_zhang_suen<<<blocks_for(np_, 256), 256, 0, SS>>>(scratch, image, nx, ny, 1, flag);
+        SLM_LAUNCHED("k_zhang_suen");
+        uint32_t changed = 0;
+        SLM_CUDA(cudaMemcpyAsync(&changed, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, SS));
+        SLM_CUDA(cudaStreamSynchronize(SS));
+        if (!changed) { ++it; break; }
+    }
+    if (iterations) *iterations = it;
     return SLM_OK;
 }
 

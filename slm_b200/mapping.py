@@ -233,12 +233,18 @@ def map_channels(info, data):
     data.mapping_array[(slt >= info.channel_threshold) & (slt * 2 >= slc)] = info.is_channel
 
 
-def thin_channels(info, data):
-    """Thin channel + inter-channel pixels to a skeleton (mapping.py:707-719)."""
+def thin_channels(info, data, device=None):
+    """Thin channel + inter-channel pixels to a skeleton (mapping.py:707-719);
+    on the GPU (``slm_thin``) when ``device`` is given, with the same result."""
     m = data.mapping_array
     channel = (((m & info.is_channel) == info.is_channel)
                | ((m & info.is_interchannel) == info.is_interchannel))
-    m[zhang_suen(channel)] |= info.is_thinchannel
+    if device is not None:
+        from .skeleton import zhang_suen_device
+        thin = zhang_suen_device(channel, device=None if device is True else device)
+    else:
+        thin = zhang_suen(channel)
+    m[thin] |= info.is_thinchannel
 
 
 def map_channels_segments(cl_state, info, data, do_map_channels_from_scratch=True,
@@ -249,7 +255,8 @@ def map_channels_segments(cl_state, info, data, do_map_channels_from_scratch=Tru
         map_channels(info, data)
     if not connect_channel_pixels(cl_state, info, data, verbose, runner):
         return False
-    thin_channels(info, data)
+    r = _runner(runner)
+    thin_channels(info, data, device=(r.device or True) if isinstance(r, DeviceRunner) else None)
     if not map_channel_heads(cl_state, info, data, verbose, runner):
         return False
     data.count_array = np.zeros((nxp, nyp), dtype=np.uint32)

@@ -46,3 +46,25 @@ def zhang_suen(mask, max_iter=10000):
         if not changed:
             break
     return img.astype(bool)
+
+
+def zhang_suen_device(mask, max_iter=10000, device=None):
+    """The same thinning on the GPU (``slm_thin``): identical output."""
+    import ctypes
+
+    import torch
+
+    from . import _lib
+    from .device import cuda_device
+    dev = device if device is not None else cuda_device(0, 0)
+    img = np.ascontiguousarray(mask, dtype=np.uint8)
+    nx, ny = img.shape
+    with torch.cuda.device(dev):
+        d = torch.from_numpy(img).to(dev)
+        scratch = torch.empty_like(d)
+        flag = torch.zeros(1, dtype=torch.int32, device=dev)
+        it = ctypes.c_uint32(0)
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        _lib.check(_lib.load().slm_thin(_lib.ptr(d), _lib.ptr(scratch), nx, ny, int(max_iter), _lib.ptr(flag),
+                                        ctypes.byref(it), stream))
+        return d.cpu().numpy().astype(bool)

@@ -89,3 +89,16 @@ def test_flank_fix_in_chunks_bit_exact(monkeypatch):
     assert M.map_channels_segments(None, info, data, runner=run)
     assert run.mismatches == [], run.mismatches
     assert ("fix_right_flanks", ) == tuple(n for n, _ in run.calls if n == "fix_right_flanks")
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_device_thinning_matches_host(seed):
+    from slm_b200.skeleton import zhang_suen, zhang_suen_device
+    rng = np.random.default_rng(seed)
+    img = np.zeros((97, 131), bool)
+    for _ in range(40):
+        x, y = rng.integers(0, 97), rng.integers(0, 131)
+        w, h = rng.integers(1, 9), rng.integers(1, 30)
+        img[max(0, x - w):x + w, max(0, y - h):y + h] = True
+    img[0, :] = True  # touching the border (outside counts as 0)
+    assert np.array_equal(zhang_suen_device(img), zhang_suen(img))
