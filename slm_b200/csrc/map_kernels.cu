@@ -80,6 +80,24 @@ __device__ __forceinline__ Step rk_plain(Vec2 a, float dt, const float2* __restr
     return rk_step<2, false>(a, dt, rng, uv, p);
 }
 
+// Brent's cycle detection on a walk's (vec, dt) state, which determines the
+// rest of the walk: true once the state equals the one at the last
+// power-of-two checkpoint.  A walk whose loop test held at every state of the
+// cycle repeats it until its step bound.
+struct StateCycle {
+    Vec2 tv;
+    float tdt;
+    uint32_t power, lam;
+    __device__ void init(Vec2 v, float dt) { tv = v; tdt = dt; power = 1; lam = 0; }
+    __device__ bool repeated(Vec2 v, float dt) {
+        if (__float_as_uint(v.x) == __float_as_uint(tv.x) && __float_as_uint(v.y) == __float_as_uint(tv.y)
+            && __float_as_uint(dt) == __float_as_uint(tdt))
+            return true;
+        if (++lam == power) { tv = v; tdt = dt; power <<= 1; lam = 0; }
+        return false;
+    }
+};
+
 // ------------------------------------------------------------------ connect
 __global__ void k_connect_channels(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
                                    const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
@@ -570,10 +588,15 @@ __global__ void k_segment_hillslopes(const slm_params p, uint32_t n, const float
     uint32_t idx = pixel_of(vec, p), n_steps = 0;
     const uint32_t h = idx;
     float dt = p.dt_max;
+    StateCycle cyc;
+    cyc.init(vec, dt);
     while (!mask[idx] && ((~mapping[idx]) & p.is_thinchannel) && n_steps < p.max_n_steps) {
         const Step s = rk_plain(vec, dt, uv, p);
         idx = s.idx;
         if (seg_move(s, vec, idx, dt, n_steps, p)) break;
+        // a cycle of states that all continue the loop ends at the bound on a
+        // pixel that is not a thin channel: no label
+        if (cyc.repeated(vec, dt)) return;
     }
     if (mapping[idx] & p.is_thinchannel) label[h] = label[idx];
 }
@@ -646,11 +669,16 @@ __global__ void k_subsegment_flanks(const slm_params p, uint32_t n, const float2
     uint32_t idx = pixel_of(vec, p), n_steps = 0;
     const uint32_t h = idx;
     float dt = p.dt_max;
+    StateCycle cyc;
+    cyc.init(vec, dt);
     while (!mask[idx] && ((~mapping[idx]) & p.is_leftflank) && ((~mapping[idx]) & p.is_thinchannel)
            && n_steps < p.max_n_steps) {
         const Step s = rk_plain(vec, dt, uv, p);
         idx = s.idx;
         if (seg_move(s, vec, idx, dt, n_steps, p)) break;
+        // a cycle of states that all continue the loop ends at the bound on a
+        // pixel that is not left flank: no flank bit
+        if (cyc.repeated(vec, dt)) return;
     }
     if (mapping[idx] & p.is_leftflank) label[h] |= p.left_flank_addition;
 }
