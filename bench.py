@@ -694,8 +694,17 @@ def run_stages(args, wl, dev):
     cpu_data = copy.deepcopy(data2)
     cpu_info = copy.deepcopy(info2)
 
+    from slm_b200.mapping_device import map_channels_segments_device
+    resident = copy.deepcopy(data2)
+    res_info = copy.deepcopy(info2)
+    ok_res, _ = timed("mapping_device_resident_s",
+                      lambda: map_channels_segments_device(res_info, resident, device=dev))
     runner = mapping.DeviceRunner(dev)
     ok = timed("mapping_s", lambda: mapping.map_channels_segments(None, info2, data2, runner=runner))
+    out["mapping_device_resident_identical"] = bool(ok_res == ok) and all(
+        np.array_equal(getattr(resident, k), getattr(data2, k))
+        for k in ("mapping_array", "count_array", "link_array", "label_array", "channel_label_array"))
+    del resident
 
     cpu_status = [0]
 

@@ -328,6 +328,32 @@ int slm_hillslopes(const slm_params* p, uint32_t n_seeds, const float* seed_poin
  * device scratch; *iterations (may be NULL) receives the iterations run. */
 int slm_thin(uint8_t* image, uint8_t* scratch, uint32_t nx, uint32_t ny, uint32_t max_iter,
              uint32_t* flag, uint32_t* iterations, void* stream);
+/* ---- host steps between the mapping kernels, on the device (map_device.cu);
+ * each restates the host wrappers' NumPy expression element for element ---- */
+/* pick_seeds (useful.py:519-538): seed_point [capacity] float2 receives, in
+ * argwhere (index) order, (x - pad, y - pad) of the pixels that are unmasked
+ * (mask non-NULL) and have (map & flag) > 0 (map non-NULL; ~map when
+ * invert_map); *n_picked = their number (SLM_ERR_CAPACITY if > capacity) */
+size_t slm_pick_seeds_workspace(uint32_t n_pixels);
+int slm_pick_seeds(const uint8_t* mask, const uint32_t* map, uint32_t flag, int invert_map,
+                   uint32_t nx_padded, uint32_t ny_padded, uint32_t pad, float* seed_point,
+                   uint32_t capacity, uint32_t* n_picked, void* workspace, size_t workspace_bytes,
+                   void* stream);
+/* map_channels (mapping.py:695-702): mapping = IS_CHANNEL where
+ * slt >= thr and slt*2 >= slc (slt float32, slc float64, downstream) */
+int slm_map_channels(const float* slt_down, const double* slc_down, float channel_threshold,
+                     uint32_t n_pixels, uint32_t is_channel, uint32_t* mapping, void* stream);
+/* flag updates: op 0 m[(m&a)==a] |= b; op 1 m[(m&a)!=0] ^= a;
+ * op 2 m[select!=0] |= b; op 3 select = ((m&a)==a) | ((m&b)==b) */
+int slm_flag_op(uint32_t* mapping, uint8_t* select, uint32_t n_pixels, int op, uint32_t a, uint32_t b,
+                void* stream);
+/* segment relabelling (segment.py:83-88): positive labels -> 1 + their rank
+ * among the distinct positive labels; *n_labels = number of distinct ones */
+size_t slm_relabel_workspace(uint32_t n_pixels);
+int slm_relabel(uint32_t* label, uint32_t n_pixels, void* workspace, size_t workspace_bytes,
+                uint32_t* n_labels, void* stream);
+/* label[label < 0] = -(int64(label) + left_flank_addition) (mapping.py:772-773) */
+int slm_signed_labels(uint32_t* label, uint32_t n_pixels, uint32_t left_flank_addition, void* stream);
 /* hillslope_lengths (opencl/lengths.cl:37-116; lengths.py:33-92);
  * traj_length [n_seeds] float, written only where a channel is reached */
 int slm_hillslope_lengths(const slm_params* p, uint32_t n_seeds, const float* seed_point,

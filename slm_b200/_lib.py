@@ -84,6 +84,13 @@ SIGNATURES = {
     "slm_hillslopes": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P]),
     "slm_hillslope_lengths": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P]),
     "slm_thin": (ctypes.c_int, [_P, _P, _U, _U, _U, _P, _P, _P]),
+    "slm_pick_seeds_workspace": (ctypes.c_size_t, [_U]),
+    "slm_pick_seeds": (ctypes.c_int, [_P, _P, _U, _I, _U, _U, _U, _P, _U, _P, _P, ctypes.c_size_t, _P]),
+    "slm_map_channels": (ctypes.c_int, [_P, _P, ctypes.c_float, _U, _U, _P, _P]),
+    "slm_flag_op": (ctypes.c_int, [_P, _P, _U, _I, _U, _U, _P]),
+    "slm_relabel_workspace": (ctypes.c_size_t, [_U]),
+    "slm_relabel": (ctypes.c_int, [_P, _U, _P, ctypes.c_size_t, _P, _P]),
+    "slm_signed_labels": (ctypes.c_int, [_P, _U, _U, _P]),
     "slm_cnn_gather": (ctypes.c_int, [_P, _U, _U, _U, _P, _P, _U, _P, _P]),
     "slm_cnn_rearrange": (ctypes.c_int, [_P, _U, _P, _I, _P]),
     "slm_gemm": (ctypes.c_int, [_I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _I, _I, _P]),

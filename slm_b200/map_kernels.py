@@ -44,40 +44,49 @@ def _to_dev(a, dev):
     return torch.from_numpy(a).to(dev)
 
 
-def run(name, params, seeds, arrays, device=None):
-    """Run kernel ``name`` on the device, updating the written NumPy buffers in place.
-    Returns the status word (0 unless a loop cap or out-of-grid access occurred)."""
+def run_device(name, params, seeds_d, n, bufs, device=None, stream=None):
+    """Run kernel ``name`` on device tensors (the kernel's buffers after
+    ``seed_point``, in its order); returns the status word."""
     L = _lib.load()
     fn_name, written, extra = SPECS[name]
     fn = getattr(L, fn_name)
     dev = device if device is not None else cuda_device(0, 0)
+    st = stream if stream is not None else ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    args = [sref(params), int(n), ptr(seeds_d)] + [ptr(b) for b in bufs]
+    status = torch.zeros(1, dtype=torch.uint32, device=dev)
+    if extra == "status":
+        check(fn(*(args + [ptr(status), st])))
+    elif extra == "workspace":
+        need = ctypes.c_uint64(0)
+        size = int(_MIN_WS[name](L, params, n))
+        if name.startswith("fix_"):
+            # the flank fix stores paths chunk by chunk within this budget
+            size += FLANK_PATH_BUDGET
+        ws = torch.empty(size, dtype=torch.uint8, device=dev)
+        rc = fn(*(args + [ptr(ws), size, ctypes.byref(need), st]))
+        if rc == _lib.SLM_ERR_CAPACITY:
+            size = int(need.value)
+            ws = torch.empty(size, dtype=torch.uint8, device=dev)
+            rc = fn(*(args + [ptr(ws), size, ctypes.byref(need), st]))
+        check(rc)
+    else:
+        check(fn(*(args + [st])))
+    return int(status.cpu().numpy()[0])
+
+
+def run(name, params, seeds, arrays, device=None):
+    """Run kernel ``name`` on the device, updating the written NumPy buffers in place.
+    Returns the status word (0 unless a loop cap or out-of-grid access occurred)."""
+    written = SPECS[name][1]
+    dev = device if device is not None else cuda_device(0, 0)
     seeds = np.ascontiguousarray(seeds, dtype=np.float32)
     n = int(seeds.shape[0])
     with torch.cuda.device(dev):
-        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         seeds_d = torch.from_numpy(seeds).to(dev) if n else torch.zeros(2, dtype=torch.float32, device=dev)
         bufs = [_to_dev(a, dev) for a in arrays]
-        args = [sref(params), n, ptr(seeds_d)] + [ptr(b) for b in bufs]
-        status = torch.zeros(1, dtype=torch.uint32, device=dev)
-        if extra == "status":
-            check(fn(*(args + [ptr(status), stream])))
-        elif extra == "workspace":
-            need = ctypes.c_uint64(0)
-            size = int(_MIN_WS[name](L, params, n))
-            if name.startswith("fix_"):
-                # the flank fix stores paths chunk by chunk within this budget
-                size += FLANK_PATH_BUDGET
-            ws = torch.empty(size, dtype=torch.uint8, device=dev)
-            rc = fn(*(args + [ptr(ws), size, ctypes.byref(need), stream]))
-            if rc == _lib.SLM_ERR_CAPACITY:
-                size = int(need.value)
-                ws = torch.empty(size, dtype=torch.uint8, device=dev)
-                rc = fn(*(args + [ptr(ws), size, ctypes.byref(need), stream]))
-            check(rc)
-        else:
-            check(fn(*(args + [stream])))
+        st = run_device(name, params, seeds_d, n, bufs, dev)
         for i in written:
             out = bufs[i].cpu().numpy()
             dst = arrays[i]
             dst[...] = out.view(dst.dtype).reshape(dst.shape) if dst.dtype != np.bool_ else out.astype(bool)
-        return int(status.cpu().numpy()[0])
+        return st

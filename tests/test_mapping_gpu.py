@@ -102,3 +102,30 @@ def test_device_thinning_matches_host(seed):
         img[max(0, x - w):x + w, max(0, y - h):y + h] = True
     img[0, :] = True  # touching the border (outside counts as 0)
     assert np.array_equal(zhang_suen_device(img), zhang_suen(img))
+
+
+@pytest.mark.parametrize("case", ["plain96", "plain256", "incised3", "incised4"])
+def test_device_resident_mapping_matches(case):
+    """The whole sequence with the grids on the GPU (seed picking, flag
+    updates, thinning and relabelling as device kernels) equals the
+    reference-shaped wrappers' sequence, array for array, and so do the
+    hillslope lengths."""
+    import copy
+    from slm_b200.mapping_device import map_channels_segments_device
+    if case.startswith("plain"):
+        nx = 96 if case == "plain96" else 256
+        _, info, data = pipeline_case(nx=nx, ny=80 if nx == 96 else 192, seed=9)
+    else:
+        info, data = incised_pipeline_case(seed=int(case[-1]))
+    info2, data2 = copy.deepcopy(info), copy.deepcopy(data)
+    assert M.map_channels_segments(None, info, data)
+    ok, dm = map_channels_segments_device(info2, data2)
+    assert ok and dm.status == 0
+    for name in ("mapping_array", "count_array", "link_array", "label_array", "channel_label_array"):
+        a, b = getattr(data, name), getattr(data2, name)
+        assert a.dtype == b.dtype and np.array_equal(a, b), name
+    midslope_case(data, info)
+    assert M.hsl(None, info, data, False)
+    dm.upload_mapping(data.mapping_array)
+    got = dm.hsl(False)
+    assert np.array_equal(got.view(np.uint32), data.subsegment_hsl_array.view(np.uint32))
