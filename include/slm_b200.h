@@ -275,10 +275,15 @@ int slm_count_downchannels(const slm_params* p, uint32_t n_seeds, const float* s
                            const uint8_t* mask, const float* uv, uint32_t* mapping, uint32_t* count,
                            uint32_t* link, void* workspace, size_t workspace_bytes,
                            uint64_t* required_bytes, void* stream);
-/* flag_downchannels (opencl/countlink.cl:134-210; countlink.py:83-130) */
+/* flag_downchannels (opencl/countlink.cl:134-210; countlink.py:83-130), the
+ * heads' walks all at once with the result of the sequential order; the
+ * workspace (slm_flag_downchannels_workspace bytes; SLM_ERR_CAPACITY with
+ * *required_bytes otherwise) holds four per-pixel and three per-seed arrays */
+size_t slm_flag_downchannels_workspace(uint32_t n_seeds, uint32_t nxy_padded);
 int slm_flag_downchannels(const slm_params* p, uint32_t n_seeds, const float* seed_point,
                           const uint8_t* mask, const float* uv, uint32_t* mapping, uint32_t* count,
-                          const uint32_t* link, void* stream);
+                          const uint32_t* link, void* workspace, size_t workspace_bytes,
+                          uint64_t* required_bytes, void* stream);
 /* label_confluences (opencl/label.cl:49-134; label.py:33-78); slt = downstream slt, float */
 int slm_label_confluences(const slm_params* p, uint32_t n_seeds, const float* seed_point,
                           const uint8_t* mask, const float* uv, const float* slt, uint32_t* mapping,

@@ -72,7 +72,8 @@ SIGNATURES = {
     "slm_prune_channel_heads": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P]),
     "slm_count_downchannels_workspace": (ctypes.c_size_t, [_U, ctypes.c_uint64]),
     "slm_count_downchannels": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P, ctypes.c_size_t, _P, _P]),
-    "slm_flag_downchannels": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P]),
+    "slm_flag_downchannels_workspace": (ctypes.c_size_t, [_U, _U]),
+    "slm_flag_downchannels": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P, ctypes.c_size_t, _P, _P]),
     "slm_label_confluences": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_segment_downchannels": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_segment_hillslopes": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P, _P]),

@@ -452,60 +452,6 @@ __global__ void k_count_replay(const slm_params p, uint32_t n, const float2* __r
     }
 }
 
-__global__ void k_flag_downchannels(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
-                                    const uint8_t* __restrict__ mask, uint32_t* mapping,
-                                    uint32_t* count, const uint32_t* __restrict__ link) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    const uint32_t lim = 1000u * p.max_n_steps;
-    for (uint32_t g = 0; g < n; ++g) {
-        const uint32_t head = pixel_of(seed_vec(seeds, g), p);
-        uint32_t idx = head, prev_idx = idx + 1u, counter = 1;
-        count[idx] = counter;
-        mapping[idx] |= p.is_thinchannel;
-        // Brent's cycle detection on the walk: link is not written by this
-        // kernel, so a walk that meets its own earlier pixel circles until
-        // counter reaches the bound.  Once a full lap has been walked (and the
-        // counter < 20 window has passed), the remaining laps are applied as
-        // their final effect: each cycle pixel's count becomes the counter of
-        // its last visit (when larger), and no tail is flagged.
-        uint32_t tort = idx, power = 1, lam = 0;
-        while (!mask[idx] && prev_idx != idx && counter < lim) {
-            prev_idx = idx;
-            idx = link[idx];
-            counter++;
-            if (!mask[idx]) {
-                if (((mapping[idx] & p.is_minorinflow) > 0u || (counter == 2u && count[idx] > 2u))
-                    && counter < 20u)
-                    mapping[head] &= ~p.is_channelhead;
-                mapping[idx] |= p.is_thinchannel;
-                if (counter >= count[idx]) count[idx] = counter;
-            } else {
-                break;
-            }
-            lam++;
-            if (idx == tort && counter >= 20u && prev_idx != idx && counter < lim) {
-                // cycle of length lam through idx, walked once since tort
-                const uint32_t r = lim - counter;  // iterations left
-                uint32_t q = idx;
-                for (uint32_t o = 1; o <= lam && o <= r; ++o) {
-                    q = link[q];
-                    const uint32_t v = counter + o + lam * ((r - o) / lam);
-                    if (v >= count[q]) count[q] = v;
-                }
-                // the walk ends after r more steps at counter == lim; the tail
-                // flag needs counter < lim, so nothing else changes
-                counter = lim;
-                break;
-            }
-            if (lam == power) {
-                tort = idx;
-                power <<= 1;
-                lam = 0;
-            }
-        }
-        if (!mask[prev_idx] && counter < lim) mapping[prev_idx] |= p.is_channeltail;
-    }
-}
 
 // ------------------------------------------------------------------ label
 __global__ void k_label_confluences(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
@@ -961,6 +907,114 @@ __global__ void k_exclusive_scan(const u64* __restrict__ in, uint32_t n, u64* __
     if (threadIdx.x == 0) out[n] = carry;
 }
 
+// ------------------------------------------------------------------ parallel flag_downchannels
+// The pinned sequential flag_downchannels (countlink.cl:124-210, heads in
+// index order) computed by all heads at once.  link is not written, so each
+// head's walk is fixed; its effects are flag ORs (order-free), the head-flag
+// clear, the tail flag, and count writes, which are "count = counter if
+// counter >= count" (a max) after the unconditional count[head] = 1 of each
+// head.  Per pixel x (g_x = the head whose head pixel is x, if any):
+//   final count[x] = g_x ? max(1, visits by heads g >= g_x)
+//                        : max(initial count[x], all visits)
+// The only order-dependent read is count[x2] > 2 at a head's second pixel
+// (counter 2), i.e. whether an earlier head visited x2 with a counter > 2
+// since x2's reset: F1[x] = first head >= g_x, F0[x] = first head at all,
+// visiting x with a counter > 2.
+constexpr uint32_t NO_HEAD = 0xffffffffu;
+
+__global__ void k_flag_head_index(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
+                                  uint32_t* __restrict__ head_of, uint32_t* __restrict__ head_pix) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const uint32_t hp = pixel_of(seed_vec(seeds, g), p);
+    head_pix[g] = hp;
+    atomicMin(head_of + hp, g);  // seeds are distinct pixels; min keeps it exact regardless
+}
+
+__device__ __forceinline__ void flag_visit(uint32_t x, uint32_t g, uint32_t c, const uint32_t* __restrict__ head_of,
+                                           uint32_t* cmax, uint32_t* f0, uint32_t* f1) {
+    const uint32_t gx = head_of[x];
+    if (gx == NO_HEAD || g >= gx) atomicMax(cmax + x, c);
+    if (c > 2u) {
+        atomicMin(f0 + x, g);
+        if (gx != NO_HEAD && g >= gx) atomicMin(f1 + x, g);
+    }
+}
+
+__global__ void k_flag_walks(const slm_params p, uint32_t n, const uint8_t* __restrict__ mask,
+                             uint32_t* mapping, const uint32_t* __restrict__ link,
+                             const uint32_t* __restrict__ head_pix, const uint32_t* __restrict__ head_of,
+                             uint32_t* cmax, uint32_t* f0, uint32_t* f1, uint8_t* __restrict__ clear_head,
+                             uint32_t* __restrict__ second) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const uint32_t lim = 1000u * p.max_n_steps;
+    const uint32_t head = head_pix[g];
+    uint32_t idx = head, prev_idx = idx + 1u, counter = 1;
+    atomicOr(mapping + idx, p.is_thinchannel);
+    uint8_t clr = 0;
+    uint32_t x2 = NO_HEAD;
+    uint32_t tort = idx, power = 1, lam = 0;
+    while (!mask[idx] && prev_idx != idx && counter < lim) {
+        prev_idx = idx;
+        idx = link[idx];
+        counter++;
+        if (mask[idx]) break;
+        if (counter == 2u) x2 = idx;
+        if (counter < 20u && (mapping[idx] & p.is_minorinflow)) clr = 1;
+        atomicOr(mapping + idx, p.is_thinchannel);
+        flag_visit(idx, g, counter, head_of, cmax, f0, f1);
+        lam++;
+        if (idx == tort && counter >= 20u && prev_idx != idx && counter < lim) {
+            // a cycle of lam pixels walked once since tort (and the counter <
+            // 20 window of the minor-inflow test already walked): the walk
+            // circles until counter == lim; each pixel's last visit counts
+            const uint32_t r = lim - counter;
+            uint32_t q = idx;
+            for (uint32_t o = 1; o <= lam && o <= r; ++o) {
+                q = link[q];
+                flag_visit(q, g, counter + o + lam * ((r - o) / lam), head_of, cmax, f0, f1);
+            }
+            counter = lim;
+            break;
+        }
+        if (lam == power) {
+            tort = idx;
+            power <<= 1;
+            lam = 0;
+        }
+    }
+    if (!mask[prev_idx] && counter < lim) atomicOr(mapping + prev_idx, p.is_channeltail);
+    clear_head[g] = clr;
+    second[g] = x2;
+}
+
+__global__ void k_flag_heads(uint32_t n, uint32_t is_channelhead, const uint32_t* __restrict__ head_pix,
+                             const uint32_t* __restrict__ head_of, const uint32_t* __restrict__ count_init,
+                             const uint32_t* __restrict__ f0, const uint32_t* __restrict__ f1,
+                             const uint8_t* __restrict__ clear_head, const uint32_t* __restrict__ second,
+                             uint32_t* mapping) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    bool clr = clear_head[g] != 0;
+    const uint32_t x2 = second[g], hp = head_pix[g];
+    if (!clr && x2 != NO_HEAD && x2 != hp) {
+        const uint32_t gx = head_of[x2];
+        if (gx != NO_HEAD && gx < g) clr = f1[x2] < g;  // x2 was reset by an earlier head
+        else clr = count_init[x2] > 2u || f0[x2] < g;
+    }
+    if (clr) atomicAnd(mapping + hp, ~is_channelhead);
+}
+
+__global__ void k_flag_counts(uint32_t nxy, const uint32_t* __restrict__ head_of,
+                              const uint32_t* __restrict__ cmax, uint32_t* count) {
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= nxy) return;
+    const uint32_t c = cmax[x];
+    if (head_of[x] != NO_HEAD) count[x] = c > 1u ? c : 1u;
+    else if (c > count[x]) count[x] = c;
+}
+
 // ------------------------------------------------------------------ thinning
 // One sub-iteration of Zhang-Suen thinning (T. Y. Zhang, C. Y. Suen, CACM
 // 27(3), 1984) on a 0/1 image [nx][ny] (x-major, outside = 0): dst = src with
@@ -1098,16 +1152,45 @@ int slm_count_downchannels(const slm_params* p, uint32_t n, const float* seed_po
     return SLM_OK;
 }
 
+size_t slm_flag_downchannels_workspace(uint32_t n_seeds, uint32_t nxy_padded) {
+    return (size_t)nxy_padded * 4 * sizeof(uint32_t) + (size_t)n_seeds * (2 * sizeof(uint32_t) + 1) + 256;
+}
+
 int slm_flag_downchannels(const slm_params* p, uint32_t n, const float* seed_point, const uint8_t* mask,
                           const float* uv, uint32_t* mapping, uint32_t* count, const uint32_t* link,
-                          void* stream) {
+                          void* workspace, size_t workspace_bytes, uint64_t* required_bytes, void* stream) {
     (void)uv;
     clear_error();
     int rc = map_checks(p, n, seed_point);
     if (rc) return rc;
+    const uint32_t nxy = p->nxy_padded;
+    const size_t need = slm_flag_downchannels_workspace(n, nxy);
+    if (required_bytes) *required_bytes = need;
     if (n == 0) return SLM_OK;
-    k_flag_downchannels<<<1, 1, 0, SS>>>(*p, n, F2(seed_point), mask, mapping, count, link);
-    SLM_LAUNCHED("k_flag_downchannels");
+    if (!workspace || workspace_bytes < need) {
+        set_error("flag_downchannels needs %zu workspace bytes", need);
+        return SLM_ERR_CAPACITY;
+    }
+    uint32_t* head_of = reinterpret_cast<uint32_t*>(workspace);
+    uint32_t* cmax = head_of + nxy;
+    uint32_t* f0 = cmax + nxy;
+    uint32_t* f1 = f0 + nxy;
+    uint32_t* head_pix = f1 + nxy;
+    uint32_t* second = head_pix + n;
+    uint8_t* clear_head = reinterpret_cast<uint8_t*>(second + n);
+    SLM_CUDA(cudaMemsetAsync(head_of, 0xff, (size_t)nxy * sizeof(uint32_t), SS));
+    SLM_CUDA(cudaMemsetAsync(cmax, 0, (size_t)nxy * sizeof(uint32_t), SS));
+    SLM_CUDA(cudaMemsetAsync(f0, 0xff, (size_t)2 * nxy * sizeof(uint32_t), SS));
+    k_flag_head_index<<<blocks_for(n, 256), 256, 0, SS>>>(*p, n, F2(seed_point), head_of, head_pix);
+    SLM_LAUNCHED("k_flag_head_index");
+    k_flag_walks<<<blocks_for(n, 128), 128, 0, SS>>>(*p, n, mask, mapping, link, head_pix, head_of, cmax, f0, f1,
+                                                     clear_head, second);
+    SLM_LAUNCHED("k_flag_walks");
+    k_flag_heads<<<blocks_for(n, 256), 256, 0, SS>>>(n, p->is_channelhead, head_pix, head_of, count, f0, f1,
+                                                     clear_head, second, mapping);
+    SLM_LAUNCHED("k_flag_heads");
+    k_flag_counts<<<blocks_for(nxy, 256), 256, 0, SS>>>(nxy, head_of, cmax, count);
+    SLM_LAUNCHED("k_flag_counts");
     return SLM_OK;
 }
 

@@ -18,7 +18,7 @@ SPECS = {
     "map_channel_heads": ("slm_map_channel_heads", (2,), None),
     "prune_channel_heads": ("slm_prune_channel_heads", (2,), None),
     "count_downchannels": ("slm_count_downchannels", (2, 3, 4), "workspace"),
-    "flag_downchannels": ("slm_flag_downchannels", (2, 3), None),
+    "flag_downchannels": ("slm_flag_downchannels", (2, 3), "workspace"),
     "label_confluences": ("slm_label_confluences", (3,), None),
     "segment_downchannels": ("slm_segment_downchannels", (2, 5), "status"),
     "segment_hillslopes": ("slm_segment_hillslopes", (5,), None),
@@ -32,6 +32,7 @@ SPECS = {
 FLANK_PATH_BUDGET = 4 << 30  # bytes of stored flank paths per chunk
 _MIN_WS = {
     "count_downchannels": lambda L, p, n: L.slm_count_downchannels_workspace(n, 0),
+    "flag_downchannels": lambda L, p, n: L.slm_flag_downchannels_workspace(n, p.nxy_padded),
     "fix_right_flanks": lambda L, p, n: L.slm_fix_flanks_workspace(n, p.nxy_padded, 0),
     "fix_left_flanks": lambda L, p, n: L.slm_fix_flanks_workspace(n, p.nxy_padded, 0),
 }

@@ -129,3 +129,42 @@ def test_device_resident_mapping_matches(case):
     dm.upload_mapping(data.mapping_array)
     got = dm.hsl(False)
     assert np.array_equal(got.view(np.uint32), data.subsegment_hsl_array.view(np.uint32))
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_flag_downchannels_random_graphs(seed):
+    """flag_downchannels runs all heads' walks at once; on random link graphs
+    (cycles, self-loops, masked pixels, minor-inflow flags, prior counts,
+    heads walked over by other heads) it equals the oracle's sequential run."""
+    from cases import Case
+    from slm_b200 import map_kernels
+    from slm_b200.params import kernel_params
+    rng = np.random.default_rng(seed)
+    c = Case(nx=36, ny=28, seed=seed + 40, step=0.5, max_length=1.5)  # max_n_steps 3: lim 3000
+    info = c.info
+    nxp, nyp = c.mask.shape
+    n = nxp * nyp
+    mask = rng.random((nxp, nyp)) < 0.08
+    link = rng.integers(0, n, size=n).astype(np.uint32)
+    near = rng.random(n) < 0.7  # mostly a neighbour, as channel links are
+    xs, ys = np.divmod(np.arange(n), nyp)
+    nx2 = np.clip(xs + rng.integers(-1, 2, n), 0, nxp - 1)
+    ny2 = np.clip(ys + rng.integers(-1, 2, n), 0, nyp - 1)
+    link[near] = (nx2 * nyp + ny2)[near].astype(np.uint32)
+    link = link.reshape(nxp, nyp)
+    mapping = np.zeros((nxp, nyp), np.uint32)
+    mapping[rng.random((nxp, nyp)) < 0.05] |= np.uint32(info.is_minorinflow)
+    mapping[rng.random((nxp, nyp)) < 0.3] |= np.uint32(info.is_channelhead)
+    count = rng.integers(0, 6, size=(nxp, nyp)).astype(np.uint32)
+    cand = np.argwhere(~mask)
+    heads = cand[rng.choice(len(cand), size=min(150, len(cand)), replace=False)]
+    seeds = (heads.astype(np.float32) - info.pad_width).astype(np.float32)
+    info.n_seed_points = np.uint32(len(seeds))
+    prm = kernel_params(info, "FLAG_DOWNCHANNELS")
+    uv = np.zeros((nxp, nyp, 2), np.float32)
+    a = [mask, uv, mapping.copy(), count.copy(), link]
+    b = [mask, uv, mapping.copy(), count.copy(), link]
+    O.map_kernel("flag_downchannels", prm, seeds, a)
+    map_kernels.run("flag_downchannels", prm, seeds, b)
+    assert np.array_equal(b[2], a[2]), "mapping"
+    assert np.array_equal(b[3], a[3]), "count"
