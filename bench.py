@@ -50,7 +50,7 @@ BYTES_PER_STEP = {2: 75, 4: 139}
 # dram__bytes_read.sum + dram__bytes_write.sum of one field launch, from an
 # ncu capture of this bench's own workload (spatial seed order); null for
 # workloads without a capture
-TRAFFIC_PER_LAUNCH = {"config2": 211.9e6}
+TRAFFIC_PER_LAUNCH = {"incised2048": 211.9e6}
 
 
 def _peaks():
@@ -388,7 +388,7 @@ def sched_compare(args, wl, dev, seeds_d, mask_d, uv_d, field_prm, flush):
             cols.append(S.step_targets(st, n_w, w.spec.density))
         return w.uv, w.seeds[:n_w], torch.stack(cols, 1).contiguous()
 
-    if args.workload == "config4":
+    if args.workload == "incised4096_d4":
         # 40 seeded 512^2 DTMs of the same family, 4x4 seeds: 10.5 M pairs.
         # Their uv grids are stacked along x with an 8 px edge-replicated
         # margin each, so a patch clamps exactly as on its own grid.
@@ -493,7 +493,7 @@ def sched_compare(args, wl, dev, seeds_d, mask_d, uv_d, field_prm, flush):
                                      order=o)
 
     trained_on = ("40 x {} (seeds 100..139)".format(SPECS_NAME("incised512_d4"))
-                  if args.workload == "config4" else "{} (seed {})".format(spec.name, args.sched_train_seed))
+                  if args.workload == "incised4096_d4" else "{} (seed {})".format(spec.name, args.sched_train_seed))
     out = {"trained_on": trained_on, "held_out_dtms": held,
            "train_pairs": n_tr, "train_steps": args.sched_train_steps, "train_batch": 4096,
            "train_s": t_train, "prep_s": t1 - t0,
@@ -847,7 +847,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="config2")
+    ap.add_argument("--workload", default="incised2048")
     ap.add_argument("--schedule", default="persistent", choices=["plain", "persistent"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -857,15 +857,15 @@ def main():
                     help="also time mapping, hillslope lengths and KDE on the GPU")
     ap.add_argument("--stages-cpu", action="store_true",
                     help="with --stages: the same stages with the CPU oracle, timed, and compared")
-    ap.add_argument("--tiles", type=int, default=96, help="config3: number of tiles")
-    ap.add_argument("--retune", action="store_true", help="config3: ignore the autotuner cache")
+    ap.add_argument("--tiles", type=int, default=96, help="tiles96: number of tiles")
+    ap.add_argument("--retune", action="store_true", help="tiles96: ignore the autotuner cache")
     ap.add_argument("--sched-train-seed", type=int, default=12)
     ap.add_argument("--sched-train-steps", type=int, default=1500)
     ap.add_argument("--sched-reps", type=int, default=3)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
-    if args.workload == "config3":
+    if args.workload == "tiles96":
         return run_batched(args)
     return run_b200(args)
 

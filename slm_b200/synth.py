@@ -11,13 +11,13 @@ with masked pixels (geodata.py:252-273); NaN flow pixels are masked and zeroed
 
 Terrain recipes (all arrays are indexed [x, y], x-major like the reference):
 
-* ``config1_dtm``  512^2 @ 1 m: planar tilt 0.05 + 12 Gaussian hills
+* ``hills_dtm``  512^2 @ 1 m: planar tilt 0.05 + 12 Gaussian hills
   (5-40 m, sigma 20-80 px) + fBm (Hurst 0.7, rms 0.5 m), sinks filled.
-* ``config2_dtm``  2048^2 @ 2 m: fBm (Hurst 0.75, rms 30 m) + 400 random-walk
+* ``incised_dtm``  2048^2 @ 2 m: fBm (Hurst 0.75, rms 30 m) + 400 random-walk
   incisions 1-8 m deep.
-* ``config5_dtm``  8192^2 @ 1 m: fBm mountains + planar alluvial cone (slope
+* ``fan_dtm``  8192^2 @ 1 m: fBm mountains + planar alluvial cone (slope
   0.03, radial ridges +-0.3 m) + 5000 unfilled pits 0.05-0.5 m deep.
-* ``tile_dtm``     config-1-like relief for the batched tiles.
+* ``tile_dtm``  the hills relief without sink filling, any size (batched tiles).
 """
 from __future__ import annotations
 
@@ -96,7 +96,7 @@ def fill_sinks(dtm, eps=1e-3):
     return z
 
 
-def config1_dtm(n=512, seed=1, fill=True):
+def hills_dtm(n=512, seed=1, fill=True):
     rng = np.random.default_rng(seed)
     x = np.arange(n, dtype=np.float64)[:, None]
     z = 0.05 * x + np.zeros((1, n))
@@ -108,7 +108,7 @@ def config1_dtm(n=512, seed=1, fill=True):
 
 
 def tile_dtm(nx, ny, seed, hill_truncate=None):
-    """Config-1-like relief without sink filling (for uneven batched tiles)."""
+    """The hills relief (tilt + hills + fBm) without sink filling, any size (batched tiles)."""
     rng = np.random.default_rng(seed)
     x = np.arange(nx, dtype=np.float64)[:, None]
     z = 0.05 * x + np.zeros((1, ny))
@@ -118,7 +118,7 @@ def tile_dtm(nx, ny, seed, hill_truncate=None):
     return z.astype(np.float32)
 
 
-def config2_dtm(n=2048, seed=2, n_incisions=400):
+def incised_dtm(n=2048, seed=2, n_incisions=400):
     rng = np.random.default_rng(seed)
     z = fbm(n, n, 0.75, 30.0, rng)
     depth_map = np.zeros_like(z)
@@ -145,7 +145,7 @@ def config2_dtm(n=2048, seed=2, n_incisions=400):
     return (z - depth_map).astype(np.float32)
 
 
-def config5_dtm(n=8192, seed=5, n_pits=5000):
+def fan_dtm(n=8192, seed=5, n_pits=5000):
     rng = np.random.default_rng(seed)
     z = fbm(n, n, 0.8, 40.0, rng).astype(np.float32)
     x = np.arange(n, dtype=np.float32)[:, None]

@@ -31,17 +31,17 @@ class WorkloadSpec:
 
 
 SPECS = {
-    "config1": WorkloadSpec("512x512 @1m, d=1, no jitter, RK2, step 0.1 px, max 2000 steps",
-                            512, 1.0, 1, 0.0, 2, 0.1, 2000, "config1"),
-    "config2": WorkloadSpec("2048x2048 @2m, d=2, jitter +-0.5, RK4, step 0.1 px, max 10000 steps",
-                            2048, 2.0, 2, 1.0, 4, 0.1, 10000, "config2"),
-    "config2_rk2": WorkloadSpec("2048x2048 @2m, d=2, jitter +-0.5, RK2, step 0.1 px, max 10000 steps",
-                                2048, 2.0, 2, 1.0, 2, 0.1, 10000, "config2"),
-    "config5": WorkloadSpec("8192x8192 @1m, d=2, jitter +-0.5, RK4, step 0.1 px, max 20000 steps",
-                            8192, 1.0, 2, 1.0, 4, 0.1, 20000, "config5"),
-    "small": WorkloadSpec("256x256 @1m, d=2, jitter +-0.5, RK2, step 0.1 px, max 2000 steps",
+    "hills512": WorkloadSpec("512x512 @1m, d=1, no jitter, RK2, step 0.1 px, max 2000 steps",
+                            512, 1.0, 1, 0.0, 2, 0.1, 2000, "hills"),
+    "incised2048": WorkloadSpec("2048x2048 @2m, d=2, jitter +-0.5, RK4, step 0.1 px, max 10000 steps",
+                            2048, 2.0, 2, 1.0, 4, 0.1, 10000, "incised"),
+    "incised2048_rk2": WorkloadSpec("2048x2048 @2m, d=2, jitter +-0.5, RK2, step 0.1 px, max 10000 steps",
+                                2048, 2.0, 2, 1.0, 2, 0.1, 10000, "incised"),
+    "fan8192": WorkloadSpec("8192x8192 @1m, d=2, jitter +-0.5, RK4, step 0.1 px, max 20000 steps",
+                            8192, 1.0, 2, 1.0, 4, 0.1, 20000, "fan"),
+    "tile256": WorkloadSpec("256x256 @1m, d=2, jitter +-0.5, RK2, step 0.1 px, max 2000 steps",
                           256, 1.0, 2, 1.0, 2, 0.1, 2000, "tile"),
-    "config4": WorkloadSpec("4096x4096 @2m incised fBm, d=4, jitter +-0.5, RK4, step 0.1 px, "
+    "incised4096_d4": WorkloadSpec("4096x4096 @2m incised fBm, d=4, jitter +-0.5, RK4, step 0.1 px, "
                             "max 10000 steps", 4096, 2.0, 4, 1.0, 4, 0.1, 10000, "incised"),
     "incised512_d4": WorkloadSpec("512x512 @2m incised fBm, d=4, jitter +-0.5, RK4, step 0.1 px, "
                                   "max 10000 steps", 512, 2.0, 4, 1.0, 4, 0.1, 10000, "incised"),
@@ -51,14 +51,12 @@ SPECS = {
 
 
 def make_dtm(spec, seed=None):
-    if spec.dtm == "config1":
-        return synth.config1_dtm(spec.n, seed or 1)
-    if spec.dtm == "config2":
-        return synth.config2_dtm(spec.n, seed or 2)
-    if spec.dtm == "config5":
-        return synth.config5_dtm(spec.n, seed or 5)
-    if spec.dtm == "incised":  # the 2048^2 recipe, incision count scaled by area
-        return synth.config2_dtm(spec.n, seed or 2, max(8, round(400 * spec.n * spec.n / 2048 ** 2)))
+    if spec.dtm == "hills":
+        return synth.hills_dtm(spec.n, seed or 1)
+    if spec.dtm == "fan":
+        return synth.fan_dtm(spec.n, seed or 5)
+    if spec.dtm == "incised":  # 400 incisions per 2048^2, scaled by area
+        return synth.incised_dtm(spec.n, seed or 2, max(8, round(400 * spec.n * spec.n / 2048 ** 2)))
     return synth.tile_dtm(spec.n, spec.n, seed or 9)
 
 

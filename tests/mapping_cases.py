@@ -83,7 +83,7 @@ def incised_pipeline_case(n=128, seed=3, n_incisions=12, max_steps=300, channel_
     d.trace.jitter_magnitude = 0.0
     d.trace.integrator_step_factor = 0.1
     d.trace.max_length = max_steps * 0.1
-    dtm = synth.config2_dtm(n, seed, n_incisions)
+    dtm = synth.incised_dtm(n, seed, n_incisions)
     uv, mask = synth.uv_from_dtm(dtm, 2.0, 2)
     info = Info(d.state, d.trace, 2.0)
     info.set_xy(n, n, 2)
