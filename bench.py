@@ -50,7 +50,7 @@ BYTES_PER_STEP = {2: 75, 4: 139}
 # dram__bytes_read.sum + dram__bytes_write.sum of one field launch, from an
 # ncu capture of this bench's own workload (spatial seed order); null for
 # workloads without a capture
-TRAFFIC_PER_LAUNCH = {"incised2048": 211.9e6}
+TRAFFIC_PER_LAUNCH = {("incised2048", False): 211.9e6}
 
 
 def _peaks():
@@ -231,38 +231,47 @@ def run_b200(args):
     tinfo.n_seed_points = n_traj
     traj_prm = [kernel_params(tinfo, "INTEGRATE_TRAJECTORY", np.float32(s)) for s in (1.0, -1.0)]
     stream = torch.cuda.current_stream()
-    side = torch.cuda.Stream()
+    sides = [torch.cuda.Stream(), torch.cuda.Stream()]
     traj_d2 = torch.zeros_like(traj_d)
     from slm_b200.scheduler import spatial_order
     spatial = args.seed_order == "spatial"
+    pair = args.schedule == "persistent" and not args.no_pair
     order_d = torch.empty(max(1, n_seeds), dtype=torch.uint32, device=dev)
     bins_d = torch.empty(int(kernels._lib.load().slm_order_spatial_bins(
         int(info.nx), int(info.ny), 64, 0)), dtype=torch.uint32, device=dev)
 
     def device_step(ev=None):
-        # the trajectory recorder (1000 seeds, latency-bound) runs on a side
-        # stream concurrently with the field passes
+        # the trajectory recorder (1000 seeds, latency-bound) runs on two side
+        # streams, one per direction, concurrently with the field passes
         acc.zero_()
         fork = torch.cuda.Event()
         fork.record(stream)
-        side.wait_event(fork)
-        for d in range(2):
+        joins = []
+        for d, side in enumerate(sides):
+            side.wait_event(fork)
             kernels.integrate_trajectory(traj_prm[d], n_traj, seeds_d, mask_d, uv_d,
                                          traj_d if d == 0 else traj_d2, nsteps_d[d],
                                          length_d[d], integrator, stream=side)
-        join = torch.cuda.Event()
-        join.record(side)
+            joins.append(torch.cuda.Event())
+            joins[-1].record(side)
         if ev is not None:
             ev[0].record(stream)
         if spatial:
             spatial_order(seeds_d, n_seeds, info.nx, info.ny, out=order_d, bins=bins_d)
-        for d in range(2):
-            kernels.integrate_fields(field_prm[d], seeds_d, mask_d, uv_d, acc[d, 0], acc[d, 1],
-                                     work[d], schedule=args.schedule, integrator=integrator,
-                                     order=order_d if spatial else None)
+        if pair:
+            # acc[d, k]: rows of the [slc|slt] arrays; upstream 2*nxy further
+            kernels.integrate_fields_pair(field_prm[0], field_prm[1], seeds_d, mask_d, uv_d, acc[:, 0],
+                                          acc[:, 1], work[0], integrator=integrator,
+                                          order=order_d if spatial else None)
+        else:
+            for d in range(2):
+                kernels.integrate_fields(field_prm[d], seeds_d, mask_d, uv_d, acc[d, 0], acc[d, 1],
+                                         work[d], schedule=args.schedule, integrator=integrator,
+                                         order=order_d if spatial else None)
         if ev is not None:
             ev[1].record(stream)
-        stream.wait_event(join)
+        for join in joins:
+            stream.wait_event(join)
         if ws > 1:
             allreduce_counts(acc)
 
@@ -323,6 +332,7 @@ def run_b200(args):
         "config": {"workload": spec.name, "schedule": args.schedule,
                    "seed_order": "spatial (64 px blocks, ordered inside the timed step)"
                    if spatial else "shuffled (the reference's)",
+                   "directions": "one launch for both" if pair else "one launch each",
                    "field_trajectories_per_direction": n_seeds * spec.density ** 2,
                    "trajectory_seeds": n_traj, "l2": "256 MiB buffer written between steps",
                    "mpx_per_s": wl.n_pixels / (step_t / args.steps) / 1e6,
@@ -330,13 +340,14 @@ def run_b200(args):
                    "parallelism": "seed shards + NCCL all-reduce" if ws > 1 else "1 GPU"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
-                     "traffic": TRAFFIC_PER_LAUNCH.get(args.workload) if spatial else None,
-                     "algorithmic_bytes_per_launch": field_steps_rank * bps / 2,
+                     "traffic": TRAFFIC_PER_LAUNCH.get((args.workload, pair)) if spatial else None,
+                     "algorithmic_bytes_per_launch": field_steps_rank * bps / (1 if pair else 2),
                      "peak_source": peak_kind,
-                     "kernel": "k_fields_{}<{}>".format(args.schedule, integrator),
+                     "kernel": "k_fields_pair<{}>".format(integrator) if pair
+                     else "k_fields_{}<{}>".format(args.schedule, integrator),
                      "bytes_per_step": bps},
         "clocks": clocks.summary(),
-        "gpu_launches": args.steps * (7 if spatial else 4),
+        "gpu_launches": args.steps * ((3 if spatial else 0) + 2 + (1 if pair else 2)),
     }
     if e2e is not None:
         line["e2e"] = e2e
@@ -778,6 +789,106 @@ def run_stages(args, wl, dev):
     return out
 
 
+PREPROCESS_BYTES_PER_PX = 4 + 8 + 4 + 1 + 1 + 1 + 1 + 1 + 4 + 4  # roi in; uv, slope, 2 masks, 3 codes, 2 gradients
+
+
+def run_preprocess(args):
+    """DTM -> conditioned uv (slm_preprocess) on the workload's DTM: kernel time
+    with the ROI resident (CUDA events, L2 flushed between launches), the public
+    API from a host ROI to host arrays, and the oracle's NumPy restatement on
+    the host (full grid up to 2048^2, else a band of rows), checked identical."""
+    import ctypes
+
+    import torch
+
+    import dtm_preprocess as DP
+    from slm_b200 import _lib
+    from slm_b200.preprocess import conditioned_gradient_vector_field as cgvf
+    from slm_b200.workloads import SPECS, make_dtm
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    spec = SPECS[args.workload]
+    roi = np.ascontiguousarray(make_dtm(spec), np.float32)
+    nx, ny = roi.shape
+    pad = 2
+    L = _lib.load()
+    roi_d = torch.from_numpy(roi).to(dev)
+    f32, u8 = torch.float32, torch.uint8
+    uv = torch.empty((nx + 2 * pad, ny + 2 * pad, 2), dtype=f32, device=dev)
+    slope = torch.empty(uv.shape[:2], dtype=f32, device=dev)
+    uvm, mask = (torch.empty(uv.shape[:2], dtype=u8, device=dev) for _ in range(2))
+    blk, nbr, cells = (torch.empty((nx, ny), dtype=u8, device=dev) for _ in range(3))
+    gx, gy = (torch.empty((nx, ny), dtype=f32, device=dev) for _ in range(2))
+    ncell = torch.zeros(1, dtype=torch.int32, device=dev)
+    prm = _lib.SlmPreprocessParams(spec.pixel_size, 0.95, -0.5, 0.0, pad, 1)
+    stream = torch.cuda.current_stream(dev)
+    P = _lib.ptr
+
+    def launch():
+        _lib.check(L.slm_preprocess(P(roi_d), 0, nx, ny, ctypes.byref(prm), P(uv), P(slope), P(uvm), P(mask),
+                                    P(blk), P(nbr), P(cells), P(gx), P(gy), P(ncell),
+                                    ctypes.c_void_p(stream.cuda_stream)))
+
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    for _ in range(max(3, args.warmup)):
+        launch()
+    torch.cuda.synchronize()
+    times = []
+    with ClockSampler(0) as clocks:
+        for _ in range(max(args.steps, 20)):
+            flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            launch()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+    kt = float(np.median(times))
+    n_loops = 4 * int(ncell.item())
+    # public API: host ROI in, host arrays out
+    cgvf(roi, spec.pixel_size, pad, device=dev)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        r = cgvf(roi, spec.pixel_size, pad, device=dev)
+    e2e_s = (time.perf_counter() - t0) / 3
+    # the oracle on the host, and the identity check
+    rows = nx if nx * ny <= 2048 * 2048 else 1024
+    band = roi[:rows]
+    t0 = time.perf_counter()
+    o = DP.conditioned_uv(band, spec.pixel_size, pad)
+    cpu_s = time.perf_counter() - t0
+    keep = rows + pad - 2 if rows < nx else rows + 2 * pad  # band rows unaffected by its lower edge
+    same = all(np.array_equal(np.asarray(a)[:keep].view(np.uint8), np.asarray(b)[:keep].view(np.uint8))
+               for a, b in ((r.uv_array, o["uv_array"]), (r.uv_mask_array, o["uv_mask_array"])))
+    same &= all(np.array_equal(getattr(r, k)[:rows - 2], o[k][:rows - 2])
+                for k in ("blockages_array", "blocked_neighbors_array", "loop_cells"))
+    peak, peak_kind = _peaks()
+    bytes_launch = nx * ny * PREPROCESS_BYTES_PER_PX
+    line = {
+        "metric": "DTM preprocess (conditioned uv) Mpx/s", "value": nx * ny / kt / 1e6, "unit": "Mpx/s",
+        "n_gpus": 1, "steps": len(times), "warmup": max(3, args.warmup), "ms_per_step": 1e3 * kt,
+        "higher_is_better": True, "scaling": "none", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded DTM; no dataset)",
+        "config": {"workload": spec.name, "roi": [nx, ny], "pad_width": pad, "n_loops": n_loops,
+                   "l2": "256 MiB buffer written between launches"},
+        "roofline": {"bound": "hbm", "achieved": bytes_launch / kt / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": bytes_launch / kt / 1e9 / peak, "traffic": None,
+                     "algorithmic_bytes_per_launch": bytes_launch, "peak_source": peak_kind,
+                     "kernel": "k_preprocess<float>"},
+        "e2e": {"value": nx * ny / e2e_s / 1e6, "unit": "Mpx/s", "h2d_bytes_per_step": roi.nbytes,
+                "d2h_bytes_per_step": int(r.uv_array.nbytes + r.slope_array.nbytes + 2 * r.mask_array.size
+                                          + 3 * nx * ny + 2 * 4 * nx * ny)},
+        "cpu_baseline": {"value": band.size / cpu_s / 1e6, "unit": "Mpx/s", "cores": 1, "kind": "port",
+                         "sample": "{} of {} rows, the oracle's NumPy restatement".format(rows, nx)},
+        "identical_to_oracle": bool(same),
+        "gpu_launches": len(times),
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def run_e2e(args, wl, dev):
     """Public-API step: Trajectories then Fields on pinned host arrays."""
     import torch
@@ -853,6 +964,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-sched", action="store_true", help="skip the learned-scheduler comparison")
     ap.add_argument("--seed-order", default="spatial", choices=["spatial", "shuffled"])
+    ap.add_argument("--no-pair", action="store_true", help="one field launch per direction")
+    ap.add_argument("--preprocess", action="store_true",
+                    help="time the DTM preprocessing (slm_preprocess) on the workload's DTM instead")
     ap.add_argument("--stages", action="store_true",
                     help="also time mapping, hillslope lengths and KDE on the GPU")
     ap.add_argument("--stages-cpu", action="store_true",
@@ -865,6 +979,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.preprocess:
+        return run_preprocess(args)
     if args.workload == "tiles96":
         return run_batched(args)
     return run_b200(args)

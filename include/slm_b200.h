@@ -145,6 +145,21 @@ int slm_integrate_fields_scheduled(const slm_params* p, const slm_launch* launch
                                    uint64_t* workspace, const uint32_t* seed_order,
                                    uint16_t* item_steps, void* stream);
 
+/* slm_integrate_fields_pair -- no counterpart in the reference (which runs
+ * one integrate_fields launch per direction): both directions of one grid in
+ * one persistent launch, so one direction's long last trajectories overlap
+ * the other's bulk.  p_down / p_up: the two directions' parameter blocks
+ * (they may differ only in COMBO_FACTOR's sign and DOWNUP_SIGN); slc, slt:
+ * the downstream uint64 arrays, the upstream ones up_stride elements further
+ * (>= nxy_padded), each direction's equal to slm_integrate_fields of that
+ * direction; workspace words 1, 2 count both directions' steps and
+ * trajectories, word 3 the upstream direction's steps; seed_order as in
+ * slm_integrate_fields_scheduled (shared by both directions). */
+int slm_integrate_fields_pair(const slm_params* p_down, const slm_params* p_up, const slm_launch* launch,
+                              const float* seed_point, const uint8_t* mask, const float* uv, uint64_t* slc,
+                              uint64_t* slt, uint64_t up_stride, uint64_t* workspace,
+                              const uint32_t* seed_order, void* stream);
+
 /* slm_integrate_fields_batched -- no counterpart in the reference (which
  * launches integrate_fields once per grid).  Traces every tile of a batch in
  * one persistent work-queue launch; each tile's slc/slt equal those of
@@ -430,6 +445,42 @@ int slm_order_spatial(const float* seed_point, uint32_t n, uint32_t nx, uint32_t
                       uint32_t block_px, const float* pred, uint32_t stride, uint32_t col,
                       float threshold, uint32_t* bins, uint32_t n_bins_capacity, uint32_t* order,
                       void* stream);
+
+/* ---------------------------------------------------------------- preprocess
+ * The conditioned gradient vector field of a DTM region of interest
+ * (Preprocess.conditioned_gradient_vector_field + mask_nan_uv,
+ * python/streamlines/preprocess.py:531-621; find_blockages :647-699,
+ * find_and_fix_loops :302-349, fix_blockages :351-387), replacing the
+ * reference's NumPy / scipy generic_filter / numba host code. */
+#define SLM_F32 0
+#define SLM_F64 1
+typedef struct slm_preprocess_params {
+    double pixel_size;           /* geodata.pixel_size (the gradient divides by its float32 value) */
+    double vecsum_threshold;     /* preprocess parameters (json/defaults.json: 0.95, -0.5, 0.0) */
+    double divergence_threshold;
+    double curl_threshold;
+    uint32_t pad_width;          /* geodata.pad_width */
+    uint32_t do_normalize_speed; /* nonzero: renormalise after the fixes, else scale by the raw speed */
+} slm_preprocess_params;
+/* roi [nx][ny] (x-major, as geodata.roi_array; float32 or float64 by
+ * roi_dtype; NaN = no data), nx, ny >= 2.  Outputs (device; every one but
+ * uv may be NULL), padded = [nx + 2 pad][ny + 2 pad]:
+ *   uv                padded float2, edge-padded, NaN vectors zeroed (uv_array)
+ *   slope             padded float32 degrees (slope_array)
+ *   uv_mask           padded uint8, 1 where uv was NaN (the 'uv' active mask)
+ *   mask              padded uint8: the pad frame, NaN ROI pixels and uv_mask
+ *                     (the 'dtm' mask with h_min 'none', or'd with 'uv')
+ *   blockages, blocked_neighbors  [nx][ny] uint8 flow codes (find_blockages)
+ *   loop_cells        [nx][ny] uint8, 1 at cell (x, y) (pixels x..x+1,
+ *                     y..y+1) detected as a loop; the last row and column
+ *                     are 0 (the reference's cells there read beyond the
+ *                     grid and cannot change the field)
+ *   gradx, grady      [nx][ny] float32 topographic gradient (roi_grad*_array)
+ *   n_loop_cells      1 uint32: looped cells (the reference's n_loops is 4x) */
+int slm_preprocess(const void* roi, int roi_dtype, uint32_t nx, uint32_t ny, const slm_preprocess_params* prm,
+                   float* uv, float* slope, uint8_t* uv_mask, uint8_t* mask, uint8_t* blockages,
+                   uint8_t* blocked_neighbors, uint8_t* loop_cells, float* gradx, float* grady,
+                   uint32_t* n_loop_cells, void* stream);
 
 #ifdef __cplusplus
 }

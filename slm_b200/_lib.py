@@ -39,6 +39,12 @@ class SlmTile(ctypes.Structure):
                 ("reserved", ctypes.c_uint32)]
 
 
+class SlmPreprocessParams(ctypes.Structure):
+    _fields_ = [("pixel_size", ctypes.c_double), ("vecsum_threshold", ctypes.c_double),
+                ("divergence_threshold", ctypes.c_double), ("curl_threshold", ctypes.c_double),
+                ("pad_width", ctypes.c_uint32), ("do_normalize_speed", ctypes.c_uint32)]
+
+
 class SlmError(RuntimeError):
     def __init__(self, code, message):
         super().__init__("slm_b200 error {}: {}".format(code, message))
@@ -58,6 +64,7 @@ SIGNATURES = {
     "slm_integrate_fields": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_integrate_fields_noalloc": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_integrate_fields_scheduled": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "slm_integrate_fields_pair": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, ctypes.c_uint64, _P, _P, _P]),
     "slm_integrate_fields_batched": (ctypes.c_int, [_P, _P, _P, _U, _U, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_fields_finish": (ctypes.c_int, [_P, _U, _U, ctypes.c_double, ctypes.c_double, _I, _P, _U, _P, _P,
                                          _P, _P]),
@@ -85,6 +92,7 @@ SIGNATURES = {
     "slm_hillslopes": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P]),
     "slm_hillslope_lengths": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P]),
     "slm_thin": (ctypes.c_int, [_P, _P, _U, _U, _U, _P, _P, _P]),
+    "slm_preprocess": (ctypes.c_int, [_P, ctypes.c_int, _U, _U, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_pick_seeds_workspace": (ctypes.c_size_t, [_U]),
     "slm_pick_seeds": (ctypes.c_int, [_P, _P, _U, _I, _U, _U, _U, _P, _U, _P, _P, ctypes.c_size_t, _P]),
     "slm_map_channels": (ctypes.c_int, [_P, _P, ctypes.c_float, _U, _U, _P, _P]),

@@ -18,7 +18,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libslm_b200.so")
-SOURCES = ["capi.cu", "trace.cu", "kde.cu", "map_kernels.cu", "scheduler.cu", "map_device.cu"]
+SOURCES = ["capi.cu", "trace.cu", "kde.cu", "map_kernels.cu", "scheduler.cu", "map_device.cu", "preprocess.cu"]
 HEADERS = ["trace_common.cuh", "capi_util.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "nvcc")

@@ -245,6 +245,77 @@ k_fields_persistent(const slm_params p, const float2* __restrict__ seeds, uint32
     warp_add_counters(steps, ntraj, work);
 }
 
+// ------------------------------------------------------------------ both directions
+// Both directions of one grid in one persistent launch: queue items
+// [0, n) trace downstream, [n, 2n) upstream, so the long trajectories that end
+// one direction run alongside the other direction's bulk instead of as its
+// own tail.  A lane keeps its trajectory's COMBO_FACTOR (the only per-
+// direction value of the step) and its accumulator offset (0, or up_stride
+// for the upstream slc/slt); every trajectory is the single-direction
+// kernels'.
+template <int ORDER>
+__global__ void __launch_bounds__(256)
+k_fields_pair(const slm_params p, float cf_up, const float2* __restrict__ seeds, uint32_t seed_begin,
+              u64 n_items, const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
+              u64* __restrict__ slc, u64* __restrict__ slt, uint32_t up_stride, u64* __restrict__ work,
+              const uint32_t* __restrict__ order, uint32_t refill_min) {
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    const uint32_t dd = p.subpixel_seed_point_density * p.subpixel_seed_point_density;
+    const Geo g_down = geo_of(p);
+    Geo g_up = g_down;
+    g_up.cf = cf_up;
+    const u64 n_total = 2 * n_items;
+    FieldLane s;
+    s.alive = false;
+    bool up = false;
+    uint32_t base = 0;
+    Acc acc{0u, 0u, 0ull};
+    u64 steps = 0, ntraj = 0, steps_up = 0;
+    bool drained = false;
+    while (true) {
+        if (!drained) {
+            const unsigned idle = __ballot_sync(FULL, !s.alive);
+            if (idle && (idle == FULL || (uint32_t)__popc(idle) >= refill_min)) {
+                const int leader = __ffs(idle) - 1;
+                const unsigned n_idle = __popc(idle);
+                u64 head = 0;
+                if ((int)lane == leader) head = atomicAdd(work, (u64)n_idle);
+                head = __shfl_sync(FULL, head, leader);
+                if (head + n_idle >= n_total) drained = true;
+                if (!s.alive) {
+                    u64 item = head + __popc(idle & ((1u << lane) - 1u));
+                    if (item < n_total) {
+                        up = item >= n_items;
+                        if (up) item -= n_items;
+                        base = up ? up_stride : 0u;
+                        uint32_t pos, sub;
+                        split_item(item, dd, pos, sub);
+                        const uint32_t seed_idx = order ? __ldg(order + seed_begin + pos) : seed_begin + pos;
+                        field_init(s, __ldg(seeds + seed_idx), seed_idx, sub, (uint32_t)item, mask, p,
+                                   up ? g_up : g_down, base, acc, slc, slt);
+                        ntraj++;
+                    }
+                }
+            }
+        }
+        if (!__any_sync(FULL, s.alive)) {
+            if (drained) break;
+            continue;
+        }
+        if (s.alive) {
+            field_step<ORDER>(s, mask, uv, p, up ? g_up : g_down, base, acc, slc, slt);
+            steps++;
+            steps_up += up;
+        }
+    }
+    acc_flush(acc, slc, slt);
+    warp_add_counters(steps, ntraj, work);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) steps_up += __shfl_xor_sync(FULL, steps_up, o);
+    if (lane == 0) atomicAdd(work + 3, steps_up);
+}
+
 // ------------------------------------------------------------------ batched tiles
 // Last tile whose first seed is <= x (tiles sorted by seed_begin; the host
 // checks the table), found by binary search over the L1-cached table.
@@ -581,6 +652,66 @@ int slm_integrate_fields_scheduled(const slm_params* p, const slm_launch* launch
                           : launch_fields<4, false>(p, L, block, sp, begin, n_items, mask, u2, (u64*)slc, (u64*)slt, w, seed_order, nullptr, s);
     return item_steps ? launch_fields<2, true>(p, L, block, sp, begin, n_items, mask, u2, (u64*)slc, (u64*)slt, w, seed_order, item_steps, s)
                       : launch_fields<2, false>(p, L, block, sp, begin, n_items, mask, u2, (u64*)slc, (u64*)slt, w, seed_order, nullptr, s);
+}
+
+int slm_integrate_fields_pair(const slm_params* p_down, const slm_params* p_up, const slm_launch* launch,
+                              const float* seed_point, const uint8_t* mask, const float* uv, uint64_t* slc,
+                              uint64_t* slt, uint64_t up_stride, uint64_t* workspace, const uint32_t* seed_order,
+                              void* stream) {
+    clear_error();
+    int rc = check_grid(p_down);
+    if (rc) return rc;
+    SLM_REQUIRE(p_up != nullptr, "params is NULL");
+    // the two parameter blocks may differ only in the direction
+    SLM_REQUIRE(p_up->nxy_padded == p_down->nxy_padded && p_up->nx_padded == p_down->nx_padded &&
+                p_up->n_seed_points == p_down->n_seed_points &&
+                p_up->seeds_chunk_offset == p_down->seeds_chunk_offset &&
+                p_up->subpixel_seed_point_density == p_down->subpixel_seed_point_density &&
+                p_up->max_n_steps == p_down->max_n_steps && p_up->max_length == p_down->max_length &&
+                p_up->dt_max == p_down->dt_max && p_up->grid_scale == p_down->grid_scale &&
+                p_up->combo_factor == -p_down->combo_factor,
+                "downstream and upstream parameters differ in more than the direction");
+    SLM_REQUIRE(seed_point && mask && uv && slc && slt && workspace, "NULL buffer");
+    SLM_REQUIRE(aligned(uv, 8) && aligned(seed_point, 8), "uv/seed_point must be 8-byte aligned");
+    SLM_REQUIRE(aligned(slc, 8) && aligned(slt, 8) && aligned(workspace, 8),
+                "slc/slt/workspace must be 8-byte aligned");
+    SLM_REQUIRE(up_stride >= p_down->nxy_padded && up_stride + p_down->nxy_padded < (1ull << 32),
+                "up_stride must be >= nxy_padded and leave the upstream arrays below 2^32 elements");
+    SLM_REQUIRE(p_down->subpixel_seed_point_density >= 1, "subpixel_seed_point_density is 0");
+    slm_launch def{SLM_SCHED_PERSISTENT, SLM_RK2, 256, 0, 0, {0, 0, 0}};
+    const slm_launch& L = launch ? *launch : def;
+    SLM_REQUIRE(L.schedule == SLM_SCHED_PERSISTENT, "the pair form runs the persistent schedule");
+    SLM_REQUIRE(L.integrator == SLM_RK2 || L.integrator == SLM_RK4, "integrator must be 2 or 4");
+    const int block = L.block_threads > 0 ? L.block_threads : 256;
+    SLM_REQUIRE(block % 32 == 0 && block <= 256, "block_threads must be a multiple of 32, <= 256");
+    cudaStream_t s = (cudaStream_t)stream;
+    SLM_CUDA(cudaMemsetAsync(workspace, 0, slm_fields_workspace_words() * sizeof(uint64_t), s));
+    const uint32_t begin = p_down->seeds_chunk_offset;
+    if (begin >= p_down->n_seed_points) return SLM_OK;
+    const u64 dd = (u64)p_down->subpixel_seed_point_density * p_down->subpixel_seed_point_density;
+    const u64 n_items = (u64)(p_down->n_seed_points - begin) * dd;
+    const float2* sp = reinterpret_cast<const float2*>(seed_point);
+    const float2* u2 = reinterpret_cast<const float2*>(uv);
+    int per_sm = L.blocks_per_sm;
+    if (per_sm <= 0) {
+        int occ = 0;
+        if (L.integrator == SLM_RK4)
+            SLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fields_pair<4>, block, 0));
+        else
+            SLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fields_pair<2>, block, 0));
+        per_sm = occ > 0 ? occ : 1;
+    }
+    const unsigned grid = (unsigned)(num_sms() * per_sm);
+    if (L.integrator == SLM_RK4)
+        k_fields_pair<4><<<grid, block, 0, s>>>(*p_down, p_up->combo_factor, sp, begin, n_items, mask, u2,
+                                                (u64*)slc, (u64*)slt, (uint32_t)up_stride, (u64*)workspace,
+                                                seed_order, refill_min(L));
+    else
+        k_fields_pair<2><<<grid, block, 0, s>>>(*p_down, p_up->combo_factor, sp, begin, n_items, mask, u2,
+                                                (u64*)slc, (u64*)slt, (uint32_t)up_stride, (u64*)workspace,
+                                                seed_order, refill_min(L));
+    SLM_LAUNCHED("k_fields_pair");
+    return SLM_OK;
 }
 
 int slm_integrate_fields_batched(const slm_params* p, const slm_launch* launch, const slm_tile* tiles,

@@ -158,6 +158,18 @@ class Fields:
             if self.seed_order == "spatial" and int(info.n_seed_points) > 0:
                 from .scheduler import spatial_order
                 order = spatial_order(seeds_d, info.n_seed_points, info.nx, info.ny)
+            if self.process_group is None and self.schedule == "persistent":
+                # both directions in one persistent launch: each one's tail
+                # fills with the other's trajectories
+                prm = [kernel_params(info, "INTEGRATE_FIELDS", sign) for sign in (+1.0, -1.0)]
+                info.downup_sign = -1.0
+                kernels.integrate_fields_pair(prm[0], prm[1], seeds_d, mask_d, uv_d, acc[:, 0], acc[:, 1], work,
+                                              integrator=self.integrator, order=order)
+                counts = work[1:4].view(torch.int64).cpu().tolist()
+                self.n_steps[0], self.n_steps[1] = counts[0] - counts[2], counts[2]
+                for d in (0, 1):
+                    self.n_trajectories[d] = int(prm[d].n_seed_points) * int(prm[d].subpixel_seed_point_density) ** 2
+                return acc
             for downup_idx, downup_sign in ((0, +1.0), (1, -1.0)):
                 info.downup_sign = downup_sign
                 prm = kernel_params(info, "INTEGRATE_FIELDS", downup_sign)

@@ -74,6 +74,31 @@ def integrate_fields(params, seeds, mask, uv, slc, slt, work, schedule="persiste
                                              ptr(item_steps), _stream(stream)))
 
 
+def integrate_fields_pair(params_down, params_up, seeds, mask, uv, slc, slt, work, integrator=2,
+                          block_threads=0, blocks_per_sm=0, chunk=0, order=None, stream=None):
+    """Both directions in one persistent launch.  ``slc``/``slt``: uint64
+    tensors of shape [2, nxy] (downstream, upstream; any stride between the
+    two rows), each row as ``integrate_fields`` of that direction."""
+    lib = _lib.load()
+    nxy = params_down.nxy_padded
+    _need(seeds, torch.float32, 2 * params_down.n_seed_points, "seeds")
+    _need(mask, torch.uint8, nxy, "mask")
+    _need(uv, torch.float32, 2 * nxy, "uv")
+    for name, t in (("slc", slc), ("slt", slt)):
+        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.uint64 and t.dim() == 2
+                and t.shape[0] == 2 and t.shape[1] >= nxy and t.stride(1) == 1):
+            raise ValueError("{} must be a CUDA uint64 [2, nxy] tensor with contiguous rows".format(name))
+    if slc.stride(0) != slt.stride(0):
+        raise ValueError("slc and slt must have the same row stride")
+    _need(work, torch.uint64, lib.slm_fields_workspace_words(), "workspace")
+    if order is not None:
+        _need(order, torch.uint32, int(params_down.n_seed_points), "order")
+    L = launch_config("persistent", integrator, block_threads, blocks_per_sm, chunk)
+    check(lib.slm_integrate_fields_pair(sref(params_down), sref(params_up), sref(L), ptr(seeds), ptr(mask),
+                                        ptr(uv), ptr(slc), ptr(slt), int(slc.stride(0)), ptr(work), ptr(order),
+                                        _stream(stream)))
+
+
 def integrate_trajectory(params, n_chunk, seeds, mask, uv, traj, nsteps, length,
                          integrator=2, stream=None):
     """Record one trajectory per seed of the chunk starting at params.seeds_chunk_offset."""

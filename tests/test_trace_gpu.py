@@ -153,3 +153,42 @@ def test_golden_on_gpu():
             slc, slt, _, _ = _gpu_fields(c, prm, "persistent")
             assert np.array_equal(slc.astype(np.uint32), g["slc_" + tag])
             assert np.array_equal((slt & 0xFFFFFFFF).astype(np.uint32), g["slt_" + tag])
+
+
+@pytest.mark.parametrize("integrator,ordered,interleaved", [(2, False, False), (4, False, False),
+                                                            (2, True, False), (4, True, True)])
+def test_fields_pair_equals_two_directions(integrator, ordered, interleaved):
+    """One launch over both directions gives each direction's fields and the
+    summed step and trajectory counts of two single-direction launches; the
+    upstream rows may sit at any stride (interleaved: [direction][slc|slt])."""
+    c = Case(nx=70, ny=58, seed=91, density=2, step=0.25, max_length=120.0)
+    seeds, mask, uv = _dev(c)
+    pd, pu = c.params("INTEGRATE_FIELDS", 1.0), c.params("INTEGRATE_FIELDS", -1.0)
+    nxy = pd.nxy_padded
+    order = None
+    if ordered:
+        order = torch.from_numpy(np.random.default_rng(5).permutation(int(pd.n_seed_points)).astype(np.int32)).to(DEV)
+        order = order.view(torch.uint32)
+    ref = []
+    for prm in (pd, pu):
+        slc = torch.zeros(nxy, dtype=torch.uint64, device=DEV)
+        slt = torch.zeros(nxy, dtype=torch.uint64, device=DEV)
+        work = kernels.workspace(DEV)
+        kernels.integrate_fields(prm, seeds, mask, uv, slc, slt, work, integrator=integrator)
+        torch.cuda.synchronize()
+        ref.append((slc.cpu().numpy(), slt.cpu().numpy(), int(work[1].item()), int(work[2].item())))
+    if interleaved:
+        acc = torch.zeros((2, 2, nxy), dtype=torch.uint64, device=DEV)
+        slc2, slt2 = acc[:, 0], acc[:, 1]
+    else:
+        slc2 = torch.zeros((2, nxy), dtype=torch.uint64, device=DEV)
+        slt2 = torch.zeros((2, nxy), dtype=torch.uint64, device=DEV)
+    work = kernels.workspace(DEV)
+    kernels.integrate_fields_pair(pd, pu, seeds, mask, uv, slc2, slt2, work, integrator=integrator, order=order)
+    torch.cuda.synchronize()
+    for d in range(2):
+        assert np.array_equal(slc2[d].cpu().numpy(), ref[d][0])
+        assert np.array_equal(slt2[d].cpu().numpy(), ref[d][1])
+    assert int(work[1].item()) == ref[0][2] + ref[1][2]
+    assert int(work[2].item()) == ref[0][3] + ref[1][3]
+    assert int(work[3].item()) == ref[1][2]
