@@ -1,16 +1,23 @@
-"""Distribution objects that drive the KDE stage.
+"""Distribution objects that drive the KDE stage, and their consumers.
 
 ``Univariate_distribution`` and ``Bivariate_distribution`` restate the
 constructors and ``compute_kde_opencl`` methods of the reference's
 ``python/streamlines/analysis.py`` (:659-786 and :859-969): the data
 selection, log-space ranges, bin and pdf spacings the KDE kernels read, the
-gaussian bandwidth halving (:766-768) and the cdf normalisation.  The scipy
-and sklearn alternatives, mode/threshold searches and plotting helpers of
-those classes are not on the traced path and are not restated.
+gaussian bandwidth halving (:766-768) and the cdf normalisation.  The
+consumers of the device pdfs follow: the univariate ``statistics``,
+``find_modes`` and ``locate_threshold`` (:788-853), the bivariate
+``find_mode`` (:971-984), and ``compute_marginal_distribn`` /
+``estimate_channel_threshold`` (Analysis, :120-188, :236-256), which give
+the mapping stage its channel threshold from the pdf of the downstream slt.
+The scipy and sklearn KDE alternatives and the plotting helpers are not
+restated.
 """
 from __future__ import annotations
 
 import numpy as np
+from scipy.signal import argrelextrema
+from scipy.stats import norm
 
 from . import kde
 
@@ -79,6 +86,58 @@ class Univariate_distribution:
         self.pdf /= cdf_max
         self.cdf /= cdf_max
 
+    def statistics(self):
+        """pdf-weighted mean and spread in log space, and of the raw data
+        (analysis.py:788-798); stored exponentiated."""
+        w = self.pdf
+        total = np.sum(w)
+        mu = np.sum(self.logx_vec * w) / total
+        var = np.sum((self.logx_vec - mu) ** 2 * w) / total
+        self.mean, self.stddev, self.var = np.exp(mu), np.exp(np.sqrt(var)), np.exp(var)
+        self.raw_mean = np.exp(self.logx_data.mean())
+        self.raw_stddev = np.exp(self.logx_data.std())
+        self.raw_var = np.exp(self.logx_data.var())
+
+    def find_modes(self):
+        """The first local maximum (3 points either side) at or above half the
+        global maximum's x (analysis.py:800-812); the middle point and 100 m
+        when there is none."""
+        flat = np.reshape(self.pdf, self.pdf.shape[0])
+        approx_mode = np.round(self.x_vec[self.pdf == self.pdf.max()][0], 2)
+        peaks = [i for i in argrelextrema(flat, np.greater, order=3)[0]
+                 if self.x_vec[i] >= approx_mode * 0.5]
+        if peaks:
+            self.mode_i = peaks[0]
+            self.mode_x = self.x_vec[peaks[0]][0]
+        else:
+            self.mode_i = self.pdf.shape[0] // 2
+            self.mode_x = 100.0
+
+    def locate_threshold(self):
+        """Channel threshold: the first local minimum (3 points either side,
+        plus the last point) of the pdf divided by the log-normal of its own
+        statistics, at or beyond the mode, whose cdf lies in
+        [search_cdf_min, search_cdf_max]; search_cdf_min is lowered by 0.01
+        down to 0.70 until one qualifies (analysis.py:814-853).  Needs
+        find_modes and statistics first."""
+        n = self.pdf.shape[0]
+        log_normal = norm.pdf(np.log(self.x_vec), np.log(self.mean), np.log(self.stddev))
+        ratio = np.reshape(self.pdf / log_normal, n)
+        minima = np.concatenate((argrelextrema(ratio, np.less, order=3)[0], np.array([n - 1])))
+        lo = self.search_cdf_min
+        if lo < 0.70:  # the reference's loop never binds its result list
+            raise NameError("name 'extrema_i' is not defined")
+        chosen = []
+        while lo >= 0.70:
+            chosen = [i for i in minima if self.x_vec[i] >= self.mode_x
+                      and self.cdf[i] >= lo and self.cdf[i] <= self.search_cdf_max]
+            if chosen:
+                break
+            lo -= 0.01
+        if chosen:
+            self.channel_threshold_i = chosen[0]
+            self.channel_threshold_x = self.x_vec[chosen[0]][0]
+
 
 class Bivariate_distribution:
     def __init__(self, logx_array=None, logy_array=None, mask_array=None, pixel_size=None,
@@ -137,3 +196,69 @@ class Bivariate_distribution:
                              .format(self.kernel, AVAILABLE_KERNELS))
         self.pdf, self.histogram = kde.estimate_bivariate_pdf(self)
         self.cdf = np.cumsum(self.pdf) * self.bin_dx
+
+    def find_mode(self):
+        """(x, y) of the pdf maximum, ignoring x or y <= 3 (analysis.py:971-984)."""
+        f = self.pdf.copy()
+        f[(self.x_mesh <= 3.0) | (self.y_mesh <= 3.0)] = 0.0
+        ij = np.unravel_index(np.argmax(f, axis=None), f.shape)
+        self.mode_max = f[ij[0], ij[1]]
+        self.mode_ij = ij
+        self.mode_xy = np.array([self.x_mesh[ij[0], 0], self.y_mesh[0, ij[1]]])
+
+
+ANALYSIS_DEFAULTS = {"n_hist_bins": 2048, "n_pdf_points": 256, "search_cdf_min": 0.8, "search_cdf_max": 0.999,
+                     "marginal_distbn_kde_kernel": "epanechnikov", "marginal_distbn_kde_bandwidth": 10.0,
+                     "pdf_slt_min": 1, "pdf_sla_min": 1}
+
+
+def compute_marginal_distribn(x_array, y_array, mask_array=None, up_down_idx_x=0, up_down_idx_y=0,
+                              n_hist_bins=2048, n_pdf_points=256, kernel="epanechnikov", bandwidth=10.0,
+                              logx_min=None, logy_min=None, logx_max=None, logy_max=None,
+                              search_cdf_min=0.8, search_cdf_max=0.999, pixel_size=None, cl_platform=0,
+                              cl_device=0, verbose=False):
+    """Analysis.compute_marginal_distribn with the device KDE (analysis.py:136-188):
+    the positive (x, y) pairs of the unmasked pixels in log space, the pdf,
+    then find_modes, statistics and locate_threshold."""
+    if mask_array is not None:
+        tx = x_array[~mask_array, up_down_idx_x].astype(np.float32)
+        ty = y_array[~mask_array, up_down_idx_y].astype(np.float32)
+    else:
+        tx = x_array[:, :, up_down_idx_x].astype(np.float32).ravel()
+        ty = y_array[:, :, up_down_idx_y].astype(np.float32).ravel()
+    keep = (tx > 0.0) & (ty > 0.0)
+    d = Univariate_distribution(logx_array=np.log(tx[keep]), logy_array=np.log(ty[keep]), pixel_size=pixel_size,
+                                n_hist_bins=n_hist_bins, n_pdf_points=n_pdf_points, logx_min=logx_min,
+                                logy_min=logy_min, logx_max=logx_max, logy_max=logy_max,
+                                search_cdf_min=search_cdf_min, search_cdf_max=search_cdf_max,
+                                cl_platform=cl_platform, cl_device=cl_device, verbose=verbose)
+    d.compute_kde_opencl(kernel=kernel, bandwidth=bandwidth)
+    d.find_modes()
+    d.statistics()
+    d.locate_threshold()
+    return d
+
+
+def estimate_channel_threshold(data, params=None, pixel_size=None):
+    """Analysis.estimate_channel_threshold (analysis.py:120-134): the
+    threshold located on the marginal pdf of the downstream slt, or None when
+    none qualifies.  ``params``: the 'analysis' section of the job's
+    parameters (defaults: json/defaults.json)."""
+    return getattr(compute_marginal_distribn_dslt(data, params, pixel_size), "channel_threshold_x", None)
+
+
+def compute_marginal_distribn_dslt(data, params=None, pixel_size=None):
+    """Analysis.compute_marginal_distribn_dslt (analysis.py:236-256): the
+    downstream slt limited by sla, pdf_slt_min / pdf_sla_min as log limits."""
+    p = dict(ANALYSIS_DEFAULTS)
+    p.update(params or {})
+    lim = lambda k: np.log(p[k]) if k in p and p[k] is not None else None  # noqa: E731
+    d = compute_marginal_distribn(data.slt_array, data.sla_array, data.mask_array, 0, 0,
+                                  n_hist_bins=p["n_hist_bins"], n_pdf_points=p["n_pdf_points"],
+                                  kernel=p["marginal_distbn_kde_kernel"],
+                                  bandwidth=p["marginal_distbn_kde_bandwidth"],
+                                  logx_min=lim("pdf_slt_min"), logx_max=lim("pdf_slt_max"),
+                                  logy_min=lim("pdf_sla_min"), logy_max=lim("pdf_sla_max"),
+                                  search_cdf_min=p["search_cdf_min"], search_cdf_max=p["search_cdf_max"],
+                                  pixel_size=pixel_size)
+    return d

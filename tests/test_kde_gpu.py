@@ -84,3 +84,41 @@ def test_estimate_bivariate_pdf_end_to_end():
     assert pdf.shape == (64, 64) and hist.shape == (256, 256)
     assert abs(float(np.sum(hist) * d.bin_dx * d.bin_dy) - 1.0) < 1e-6
     assert abs(float(np.sum(pdf) * d.bin_dx * d.bin_dy) - 1.0) < 1e-4
+
+
+def test_channel_threshold_from_device_pdf():
+    """estimate_channel_threshold (device KDE + host consumers) equals the
+    consumers run on the oracle's pdf of the same data."""
+    from types import SimpleNamespace
+
+    from slm_b200 import analysis as A
+    rng = np.random.default_rng(21)
+    nx, ny = 300, 280
+    hill = rng.lognormal(2.5, 0.5, (nx, ny))
+    chan = rng.lognormal(6.0, 0.8, (nx, ny))
+    slt = np.where(rng.random((nx, ny)) < 0.08, chan, hill).astype(np.float32)
+    sla = (slt * rng.uniform(0.5, 1.5, (nx, ny))).astype(np.float32)
+    mask = rng.random((nx, ny)) < 0.05
+    data = SimpleNamespace(slt_array=np.stack([slt, slt], 2), sla_array=np.stack([sla, sla], 2), mask_array=mask)
+    d = A.compute_marginal_distribn_dslt(data)
+    thr = A.estimate_channel_threshold(data)
+    assert thr is not None and thr == d.channel_threshold_x
+    # the same consumers on the oracle's pdf of the same selection
+    prm = kde.kde_params(d, "pdf_univariate")
+    x = np.ascontiguousarray(d.logx_data.reshape(-1), dtype=np.float32)
+    hist_o = O.histogram_univariate(prm, x).reshape(-1, 1)
+    pdf_o = O.pdf_univariate(prm, hist_o).reshape(-1, 1)
+    pdf_o = pdf_o / (sum(pdf_o) * d.bin_dx)
+    o = A.compute_marginal_distribn_dslt(data)  # fresh object, same data selection
+    o.pdf = pdf_o.astype(np.float32)
+    o.cdf = np.cumsum(o.pdf) * o.bin_dx
+    o.pdf /= o.cdf[-1]
+    o.cdf /= o.cdf[-1]
+    for attr in ("mode_x", "channel_threshold_x"):
+        if hasattr(o, attr):
+            delattr(o, attr)
+    o.find_modes()
+    o.statistics()
+    o.locate_threshold()
+    assert o.mode_i == d.mode_i
+    assert o.channel_threshold_i == d.channel_threshold_i
