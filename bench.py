@@ -48,9 +48,9 @@ sys.path[:0] = [ROOT, os.path.join(ROOT, "oracle")]
 
 BYTES_PER_STEP = {2: 75, 4: 139}
 # dram__bytes_read.sum + dram__bytes_write.sum of one field launch, from an
-# ncu capture of this bench's own workload (spatial seed order); null for
-# workloads without a capture
-TRAFFIC_PER_LAUNCH = {("incised2048", False): 211.9e6}
+# ncu capture of this bench's own workload (spatial seed order), keyed by
+# (workload, both directions in one launch); null for workloads without one
+TRAFFIC_PER_LAUNCH = {("incised2048", False): 211.9e6, ("incised2048", True): 418.0e6}
 
 
 def _peaks():
