@@ -689,6 +689,13 @@ def run_stages(args, wl, dev):
         out[key] = time.perf_counter() - t
         return r
 
+    # preprocess: the workload's DTM -> conditioned uv through the public API
+    from slm_b200.preprocess import conditioned_gradient_vector_field
+    conditioned_gradient_vector_field(wl.dtm.astype(np.float32), spec.pixel_size, 2, device=dev)
+    pre = timed("preprocess_s", lambda: conditioned_gradient_vector_field(wl.dtm.astype(np.float32),
+                                                                           spec.pixel_size, 2, device=dev))
+    out["preprocess_loop_pixels"] = int(pre.n_loops)
+
     info = wl.fresh_info()
     data = Data(info=info, mask_array=wl.mask, uv_array=wl.uv,
                 mapping_array=np.zeros(wl.mask.shape, np.uint32))
@@ -699,8 +706,14 @@ def run_stages(args, wl, dev):
                  mapping_array=np.zeros(wl.mask.shape, np.uint32), traj_stats_df=tr.data.traj_stats_df)
     f = Fields(0, dev.index, info=info2, data=data2, integrator=spec.integrator)
     timed("fields_s", f.integrate)
+    # the reference's channel-threshold search on the dslt pdf (reported; the
+    # mapping below keeps the 94th percentile so its timings stay comparable)
+    from slm_b200.analysis import estimate_channel_threshold
+    thr_kde = timed("channel_threshold_s", lambda: estimate_channel_threshold(data2, pixel_size=spec.pixel_size))
+    out["channel_threshold_kde"] = None if thr_kde is None else float(thr_kde)
     slt_dn = data2.slt_array[:, :, 0]
     thr = np.float32(np.percentile(slt_dn[~wl.mask], 94.0))
+    out["channel_threshold_p94"] = float(thr)
     info2.set_thresholds(segmentation_threshold=np.uint32(50), channel_threshold=thr)
     cpu_data = copy.deepcopy(data2)
     cpu_info = copy.deepcopy(info2)

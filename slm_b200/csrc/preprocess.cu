@@ -6,7 +6,7 @@
 // over every cell (find_and_fix_loops, :302-349) and over the blockages
 // (fix_blockages, :351-387), normalisation, edge padding and the NaN mask.
 // Every value of a pixel depends only on the ROI within two pixels of it, so
-// one kernel does it all: a CTA stages an 8 x 32 tile of the ROI with a
+// one kernel does it all: a CTA stages a 16 x 32 tile of the ROI with a
 // two-pixel halo in shared memory, derives velocities, blockage codes and
 // looped cells for the tile plus a one-pixel halo, and writes each pixel's
 // final uv (with its edge-padding replicas), slope, masks and codes.
@@ -27,8 +27,9 @@
 
 namespace slm {
 
-constexpr int PP_TX = 8;    // tile rows (x)
+constexpr int PP_TX = 16;   // tile rows (x)
 constexpr int PP_TY = 32;   // tile columns (y, the contiguous axis)
+constexpr int PP_THREADS = 256;  // each thread finishes PP_TX * PP_TY / PP_THREADS pixels
 constexpr int PP_HX = PP_TX + 4, PP_HY = PP_TY + 4;  // ROI tile with a 2-pixel halo
 constexpr int PP_VX = PP_TX + 2, PP_VY = PP_TY + 2;  // velocities / codes, 1-pixel halo
 constexpr int PP_CX = PP_TX + 1, PP_CY = PP_TY + 1;  // cells x0-1 .. x0+TX-1
@@ -77,11 +78,11 @@ struct PreOut {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(PP_TX * PP_TY)
+__global__ void __launch_bounds__(PP_THREADS)
 k_preprocess(const T* __restrict__ roi, int nx, int ny, float pixel_size, int pad, double vecsum_threshold,
              double divergence_threshold, double curl_threshold, int normalize, PreOut out) {
     __shared__ T h[PP_HX][PP_HY];
-    __shared__ float su[PP_VX][PP_VY], sv[PP_VX][PP_VY];
+    __shared__ float su[PP_VX][PP_VY], sv[PP_VX][PP_VY], sr[PP_VX][PP_VY];  // unit velocity, raw speed
     __shared__ uint8_t code[PP_VX][PP_VY];
     __shared__ uint8_t cell[PP_CX][PP_CY];
     __shared__ uint32_t n_tile_cells;
@@ -92,7 +93,7 @@ k_preprocess(const T* __restrict__ roi, int nx, int ny, float pixel_size, int pa
     // A: the ROI tile, clamped (scipy's 'reflect' of a 3-wide window repeats
     // the edge pixel; the gradient and the loop fixes never read the halo
     // outside the grid)
-    for (int i = tid; i < PP_HX * PP_HY; i += PP_TX * PP_TY) {
+    for (int i = tid; i < PP_HX * PP_HY; i += PP_THREADS) {
         const int a = i / PP_HY, b = i % PP_HY;
         const int gx = clampi(x0 - 2 + a, nx), gy = clampi(y0 - 2 + b, ny);
         h[a][b] = roi[(size_t)gx * ny + gy];
@@ -102,7 +103,7 @@ k_preprocess(const T* __restrict__ roi, int nx, int ny, float pixel_size, int pa
     // B: velocities and blockage codes on the tile plus a 1-pixel halo.
     // Halo positions outside the grid take the code of their clamped pixel
     // (the second generic_filter's 'reflect'); their velocities are unused.
-    for (int i = tid; i < PP_VX * PP_VY; i += PP_TX * PP_TY) {
+    for (int i = tid; i < PP_VX * PP_VY; i += PP_THREADS) {
         const int a = i / PP_VY, b = i % PP_VY;
         const int px = x0 - 1 + a, py = y0 - 1 + b;
         // code of the clamped pixel: its 3x3 window in h (clamped loads)
@@ -120,7 +121,7 @@ k_preprocess(const T* __restrict__ roi, int nx, int ny, float pixel_size, int pa
             if (h[qa + 1][qb + 1] < c) nn |= FV_NE;
             code[a][b] = (uint8_t)(((nn & 0xF0u) == nn) ? nn : 0u);
         }
-        float u = 0.0f, v = 0.0f;
+        float u = 0.0f, v = 0.0f, raw = 1.0f;
         if (px >= 0 && px < nx && py >= 0 && py < ny) {
             const int ha = a + 1, hb = b + 1;  // position in h
             float gxv, gyv;
@@ -140,18 +141,19 @@ k_preprocess(const T* __restrict__ roi, int nx, int ny, float pixel_size, int pa
             }
             u = -gxv;
             v = -gyv;
-            const float s = speed_of(u, v);
-            u = u / s;
-            v = v / s;
+            raw = speed_of(u, v);
+            u = u / raw;
+            v = v / raw;
         }
         su[a][b] = u;
         sv[a][b] = v;
+        sr[a][b] = raw;
     }
     __syncthreads();
 
     // C: looped cells x0-1 .. x0+TX-1 (check_has_loop on the normalised
     // velocities; cells need pixels cx+1, cy+1 inside the grid)
-    for (int i = tid; i < PP_CX * PP_CY; i += PP_TX * PP_TY) {
+    for (int i = tid; i < PP_CX * PP_CY; i += PP_THREADS) {
         const int a = i / PP_CY, b = i % PP_CY;
         const int cx = x0 - 1 + a, cy = y0 - 1 + b;
         uint8_t hit = 0;
@@ -179,99 +181,90 @@ k_preprocess(const T* __restrict__ roi, int nx, int ny, float pixel_size, int pa
     __syncthreads();
     if (tid == 0 && n_tile_cells && out.n_cells) atomicAdd(out.n_cells, n_tile_cells);
 
-    // D: one pixel per thread
-    const int a = tid / PP_TY + 1, b = tid % PP_TY + 1;  // position in the 1-halo arrays
-    const int x = x0 + a - 1, y = y0 + b - 1;
-    if (x >= nx || y >= ny) return;
-    float u = su[a][b], v = sv[a][b];
-    const int ha = a + 1, hb = b + 1;
-    // break_out_of_loop for a pixel marked by any of its four cells
-    const bool marked = cell[a][b] | cell[a - 1][b] | cell[a][b - 1] | cell[a - 1][b - 1];
-    if (marked && x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2) {
-        // break_out_of_loop's vectors: W, E, S, N, SW, SE, NW, NE
-        T h_min = (T)3.402823466e38f;
-        int bdx = -1, bdy = 0;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const int dx = k < 2 ? (k == 0 ? -1 : 1) : (k < 4 ? 0 : ((k & 1) ? 1 : -1));
-            const int dy = k < 2 ? 0 : (k < 4 ? (k == 2 ? -1 : 1) : (k < 6 ? -1 : 1));
-            const T hv = h[ha + dx][hb + dy];
-            if (h_min > hv) { h_min = hv; bdx = dx; bdy = dy; }
-        }
-        const float len = hypot_f32((float)bdx, (float)bdy);
-        u = (float)bdx / len;
-        v = (float)bdy / len;
-    }
-    // fix_blockages: blockages, then blocked neighbours
-    const uint32_t c0 = code[a][b];
-    uint32_t c1 = 0;
-    {
-        const uint8_t sw = code[a - 1][b - 1], s = code[a][b - 1], se = code[a + 1][b - 1];
-        const uint8_t w = code[a - 1][b], e = code[a + 1][b];
-        const uint8_t nw = code[a - 1][b + 1], n = code[a][b + 1], ne = code[a + 1][b + 1];
-        if (sw == FV_SW) c1 |= FV_SW;
-        if (s == FV_SW || s == FV_SE) c1 |= FV_S;
-        if (se == FV_SE) c1 |= FV_SE;
-        if (w == FV_SW || w == FV_NW) c1 |= FV_W;
-        if (e == FV_NE || e == FV_SE) c1 |= FV_E;
-        if (nw == FV_NW) c1 |= FV_NW;
-        if (n == FV_NW || n == FV_NE) c1 |= FV_N;
-        if (ne == FV_NE) c1 |= FV_NE;
-    }
+    // D: PP_TX * PP_TY / PP_THREADS pixels per thread, rows PP_THREADS / PP_TY apart
     const float inv_sqrt2 = __double2float_rn(__ddiv_rn(1.0, __dsqrt_rn(2.0)));
-    if (c0) {
-        int dx, dy;
-        flow_vector(c0, dx, dy);
-        u = dx ? (float)dx * inv_sqrt2 : 0.0f;
-        v = dy ? (float)dy * inv_sqrt2 : 0.0f;
-    }
-    if (c1) {
-        int dx, dy;
-        flow_vector(c1, dx, dy);
-        u = dx ? (float)dx * inv_sqrt2 : 0.0f;
-        v = dy ? (float)dy * inv_sqrt2 : 0.0f;
-    }
-    // raw speed of the unfixed gradient (recomputed: the tile keeps only the
-    // normalised velocity)
-    float raw;
-    {
-        float gxv, gyv;
-        if (x == 0) gxv = (float)h[ha + 1][hb] - (float)h[ha][hb];
-        else if (x == nx - 1) gxv = (float)h[ha][hb] - (float)h[ha - 1][hb];
-        else gxv = ((float)h[ha + 1][hb] - (float)h[ha - 1][hb]) / 2.0f;
-        if (y == 0) gyv = (float)h[ha][hb + 1] - (float)h[ha][hb];
-        else if (y == ny - 1) gyv = (float)h[ha][hb] - (float)h[ha][hb - 1];
-        else gyv = ((float)h[ha][hb + 1] - (float)h[ha][hb - 1]) / 2.0f;
-        raw = speed_of(-(gxv / pixel_size), -(gyv / pixel_size));
-    }
-    if (normalize) {
-        const float s = speed_of(u, v);
-        u = u / s;
-        v = v / s;
-    } else {
-        u = u * raw;
-        v = v * raw;
-    }
-    const bool bad = isnan(u) || isnan(v);
-    if (bad) { u = 0.0f; v = 0.0f; }
-    const float slope = atanf(raw) * (180.0f / 3.14159265358979323846f);
-    const bool roi_nan = isnan((float)h[ha][hb]);
-    const size_t gi = (size_t)x * ny + y;
-    if (out.blockages) out.blockages[gi] = (uint8_t)c0;
-    if (out.blocked) out.blocked[gi] = (uint8_t)c1;
-    // the pixel and its edge-padding replicas
     const int nyp = ny + 2 * pad;
-    const int xa = (x == 0) ? 0 : x + pad, xb = (x == nx - 1) ? nx + 2 * pad - 1 : x + pad;
-    const int ya = (y == 0) ? 0 : y + pad, yb = (y == ny - 1) ? nyp - 1 : y + pad;
-    for (int qx = xa; qx <= xb; ++qx) {
-        for (int qy = ya; qy <= yb; ++qy) {
-            const size_t pi = (size_t)qx * nyp + qy;
-            out.uv[pi] = make_float2(u, v);
-            if (out.slope) out.slope[pi] = slope;
-            if (out.uv_mask) out.uv_mask[pi] = bad ? 1 : 0;
-            if (out.mask) {
-                const bool frame = qx < pad || qx >= nx + pad || qy < pad || qy >= ny + pad;
-                out.mask[pi] = (frame || roi_nan || bad) ? 1 : 0;
+#pragma unroll 1
+    for (int k = tid; k < PP_TX * PP_TY; k += PP_THREADS) {
+        const int a = k / PP_TY + 1, b = k % PP_TY + 1;  // position in the 1-halo arrays
+        const int x = x0 + a - 1, y = y0 + b - 1;
+        if (x >= nx || y >= ny) continue;
+        float u = su[a][b], v = sv[a][b];
+        const float raw = sr[a][b];  // speed of the unfixed gradient
+        const int ha = a + 1, hb = b + 1;
+        // break_out_of_loop for a pixel marked by any of its four cells
+        const bool marked = cell[a][b] | cell[a - 1][b] | cell[a][b - 1] | cell[a - 1][b - 1];
+        if (marked && x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2) {
+            // break_out_of_loop's vectors: W, E, S, N, SW, SE, NW, NE
+            T h_min = (T)3.402823466e38f;
+            int bdx = -1, bdy = 0;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int dx = q < 2 ? (q == 0 ? -1 : 1) : (q < 4 ? 0 : ((q & 1) ? 1 : -1));
+                const int dy = q < 2 ? 0 : (q < 4 ? (q == 2 ? -1 : 1) : (q < 6 ? -1 : 1));
+                const T hv = h[ha + dx][hb + dy];
+                if (h_min > hv) { h_min = hv; bdx = dx; bdy = dy; }
+            }
+            const float len = hypot_f32((float)bdx, (float)bdy);
+            u = (float)bdx / len;
+            v = (float)bdy / len;
+        }
+        // fix_blockages: blockages, then blocked neighbours
+        const uint32_t c0 = code[a][b];
+        uint32_t c1 = 0;
+        {
+            const uint8_t sw = code[a - 1][b - 1], s = code[a][b - 1], se = code[a + 1][b - 1];
+            const uint8_t w = code[a - 1][b], e = code[a + 1][b];
+            const uint8_t nw = code[a - 1][b + 1], n = code[a][b + 1], ne = code[a + 1][b + 1];
+            if (sw == FV_SW) c1 |= FV_SW;
+            if (s == FV_SW || s == FV_SE) c1 |= FV_S;
+            if (se == FV_SE) c1 |= FV_SE;
+            if (w == FV_SW || w == FV_NW) c1 |= FV_W;
+            if (e == FV_NE || e == FV_SE) c1 |= FV_E;
+            if (nw == FV_NW) c1 |= FV_NW;
+            if (n == FV_NW || n == FV_NE) c1 |= FV_N;
+            if (ne == FV_NE) c1 |= FV_NE;
+        }
+        if (c0) {
+            int dx, dy;
+            flow_vector(c0, dx, dy);
+            u = dx ? (float)dx * inv_sqrt2 : 0.0f;
+            v = dy ? (float)dy * inv_sqrt2 : 0.0f;
+        }
+        if (c1) {
+            int dx, dy;
+            flow_vector(c1, dx, dy);
+            u = dx ? (float)dx * inv_sqrt2 : 0.0f;
+            v = dy ? (float)dy * inv_sqrt2 : 0.0f;
+        }
+        if (normalize) {
+            const float sp = speed_of(u, v);
+            u = u / sp;
+            v = v / sp;
+        } else {
+            u = u * raw;
+            v = v * raw;
+        }
+        const bool bad = isnan(u) || isnan(v);
+        if (bad) { u = 0.0f; v = 0.0f; }
+        const float slope = atanf(raw) * (180.0f / 3.14159265358979323846f);
+        const bool roi_nan = isnan((float)h[ha][hb]);
+        const size_t gi = (size_t)x * ny + y;
+        if (out.blockages) out.blockages[gi] = (uint8_t)c0;
+        if (out.blocked) out.blocked[gi] = (uint8_t)c1;
+        // the pixel and its edge-padding replicas
+        const int xa = (x == 0) ? 0 : x + pad, xb = (x == nx - 1) ? nx + 2 * pad - 1 : x + pad;
+        const int ya = (y == 0) ? 0 : y + pad, yb = (y == ny - 1) ? nyp - 1 : y + pad;
+        for (int qx = xa; qx <= xb; ++qx) {
+            for (int qy = ya; qy <= yb; ++qy) {
+                const size_t pi = (size_t)qx * nyp + qy;
+                out.uv[pi] = make_float2(u, v);
+                if (out.slope) out.slope[pi] = slope;
+                if (out.uv_mask) out.uv_mask[pi] = bad ? 1 : 0;
+                if (out.mask) {
+                    const bool frame = qx < pad || qx >= nx + pad || qy < pad || qy >= ny + pad;
+                    out.mask[pi] = (frame || roi_nan || bad) ? 1 : 0;
+                }
             }
         }
     }
@@ -301,15 +294,16 @@ int slm_preprocess(const void* roi, int roi_dtype, uint32_t nx, uint32_t ny, con
              n_loop_cells};
     if (n_loop_cells) SLM_CUDA(cudaMemsetAsync(n_loop_cells, 0, sizeof(uint32_t), s));
     const dim3 grid((ny + PP_TY - 1) / PP_TY, (nx + PP_TX - 1) / PP_TX);
+    static_assert(PP_THREADS % PP_TY == 0 && (PP_TX * PP_TY) % PP_THREADS == 0, "tile / block shape");
     SLM_REQUIRE(grid.y < 65536, "nx too large for the tile grid");
     const float ps = (float)prm->pixel_size;
     if (roi_dtype == SLM_F64)
-        k_preprocess<double><<<grid, PP_TX * PP_TY, 0, s>>>((const double*)roi, (int)nx, (int)ny, ps,
+        k_preprocess<double><<<grid, PP_THREADS, 0, s>>>((const double*)roi, (int)nx, (int)ny, ps,
                                                              (int)prm->pad_width, prm->vecsum_threshold,
                                                              prm->divergence_threshold, prm->curl_threshold,
                                                              prm->do_normalize_speed ? 1 : 0, o);
     else
-        k_preprocess<float><<<grid, PP_TX * PP_TY, 0, s>>>((const float*)roi, (int)nx, (int)ny, ps,
+        k_preprocess<float><<<grid, PP_THREADS, 0, s>>>((const float*)roi, (int)nx, (int)ny, ps,
                                                            (int)prm->pad_width, prm->vecsum_threshold,
                                                            prm->divergence_threshold, prm->curl_threshold,
                                                            prm->do_normalize_speed ? 1 : 0, o);
