@@ -262,7 +262,8 @@ def run_b200(args):
             # acc[d, k]: rows of the [slc|slt] arrays; upstream 2*nxy further
             kernels.integrate_fields_pair(field_prm[0], field_prm[1], seeds_d, mask_d, uv_d, acc[:, 0],
                                           acc[:, 1], work[0], integrator=integrator,
-                                          order=order_d if spatial else None)
+                                          block_threads=args.block_threads, blocks_per_sm=args.blocks_per_sm,
+                                          chunk=args.chunk, order=order_d if spatial else None)
         else:
             for d in range(2):
                 kernels.integrate_fields(field_prm[d], seeds_d, mask_d, uv_d, acc[d, 0], acc[d, 1],
@@ -333,6 +334,8 @@ def run_b200(args):
                    "seed_order": "spatial (64 px blocks, ordered inside the timed step)"
                    if spatial else "shuffled (the reference's)",
                    "directions": "one launch for both" if pair else "one launch each",
+                   "launch": {"block_threads": args.block_threads, "blocks_per_sm": args.blocks_per_sm,
+                              "chunk": args.chunk},
                    "field_trajectories_per_direction": n_seeds * spec.density ** 2,
                    "trajectory_seeds": n_traj, "l2": "256 MiB buffer written between steps",
                    "mpx_per_s": wl.n_pixels / (step_t / args.steps) / 1e6,
@@ -978,6 +981,9 @@ def main():
     ap.add_argument("--no-sched", action="store_true", help="skip the learned-scheduler comparison")
     ap.add_argument("--seed-order", default="spatial", choices=["spatial", "shuffled"])
     ap.add_argument("--no-pair", action="store_true", help="one field launch per direction")
+    ap.add_argument("--block-threads", type=int, default=0, help="pair launch: threads per block (0: default)")
+    ap.add_argument("--blocks-per-sm", type=int, default=0, help="pair launch: resident blocks per SM (0: default)")
+    ap.add_argument("--chunk", type=int, default=0, help="pair launch: refill threshold in idle lanes (0: default)")
     ap.add_argument("--preprocess", action="store_true",
                     help="time the DTM preprocessing (slm_preprocess) on the workload's DTM instead")
     ap.add_argument("--stages", action="store_true",

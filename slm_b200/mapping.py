@@ -287,3 +287,25 @@ def map_channels_segments(cl_state, info, data, do_map_channels_from_scratch=Tru
     lab[neg] = (-(lab[neg].astype(np.int64) + int(info.left_flank_addition))).astype(np.int32)
     vprint(verbose, "mapped channels and segments")
     return True
+
+
+MAPPING_THRESHOLD_DEFAULTS = {"min_channel_threshold": 10, "guess_channel_threshold": 150,
+                              "max_channel_threshold": 1000, "fine_segmentation_threshold": 10}
+
+
+def subsegment_channel_threshold(data, mapping_params=None, analysis_params=None, pixel_size=None):
+    """The channel threshold the reference's per-subsegment pass maps with
+    (mapping.py:460-477): the KDE estimate on the dslt pdf
+    (``analysis.estimate_channel_threshold``), replaced by the guess when
+    there is none or it lies above the maximum, and by half the guess below
+    the minimum.  Sets ``data.channel_threshold`` and returns it."""
+    from .analysis import estimate_channel_threshold
+    p = dict(MAPPING_THRESHOLD_DEFAULTS)
+    p.update(mapping_params or {})
+    t = estimate_channel_threshold(data, analysis_params, pixel_size)
+    if t is None or t > p["max_channel_threshold"]:
+        t = p["guess_channel_threshold"]
+    elif t < p["min_channel_threshold"]:
+        t = p["guess_channel_threshold"] / 2
+    data.channel_threshold = t
+    return t

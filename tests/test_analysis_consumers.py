@@ -104,3 +104,16 @@ def test_threshold_search_floor_raises_like_reference():
     d.statistics()
     with pytest.raises(NameError):
         d.locate_threshold()
+
+
+@pytest.mark.parametrize("estimate,expected", [(None, 150), (5000.0, 150), (4.0, 75.0), (220.0, 220.0)])
+def test_subsegment_channel_threshold_clamps(monkeypatch, estimate, expected):
+    """mapping.py:460-477: the guess when there is no estimate or it is above
+    the maximum, half the guess below the minimum, else the estimate."""
+    from types import SimpleNamespace
+
+    from slm_b200 import mapping
+    monkeypatch.setattr(A, "estimate_channel_threshold", lambda *a, **k: estimate)
+    data = SimpleNamespace()
+    assert mapping.subsegment_channel_threshold(data) == expected
+    assert data.channel_threshold == expected
