@@ -446,6 +446,20 @@ int slm_order_spatial(const float* seed_point, uint32_t n, uint32_t nx, uint32_t
                       float threshold, uint32_t* bins, uint32_t n_bins_capacity, uint32_t* order,
                       void* stream);
 
+/* slm_create_seeds -- HOST code (all pointers are host memory): the field
+ * seed list of create_seeds (python/streamlines/useful.py:470-517):
+ * argwhere(~mask) - pad as float32 (x, y) rows, in the row order NumPy's
+ * global legacy generator gives them after np.random.seed(rng_seed);
+ * np.random.shuffle(...) when do_shuffle.  mask: [nx_padded][ny_padded]
+ * uint8 (nonzero = masked).  *n_seeds receives the number of unmasked
+ * pixels; with seed_point NULL nothing else happens (size query), else
+ * seed_point [capacity][2] receives the rows (SLM_ERR_CAPACITY when too
+ * small).  generator_state (NULL: not wanted) [625]: the MT19937 key and
+ * position after the shuffle, for numpy.random.set_state. */
+int slm_create_seeds(const uint8_t* mask, uint32_t nx_padded, uint32_t ny_padded, uint32_t pad, int do_shuffle,
+                     uint32_t rng_seed, float* seed_point, uint64_t capacity, uint64_t* n_seeds,
+                     uint32_t* generator_state);
+
 /* ---------------------------------------------------------------- preprocess
  * The conditioned gradient vector field of a DTM region of interest
  * (Preprocess.conditioned_gradient_vector_field + mask_nan_uv,

@@ -92,6 +92,7 @@ SIGNATURES = {
     "slm_hillslopes": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P]),
     "slm_hillslope_lengths": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P]),
     "slm_thin": (ctypes.c_int, [_P, _P, _U, _U, _U, _P, _P, _P]),
+    "slm_create_seeds": (ctypes.c_int, [_P, _U, _U, _U, ctypes.c_int, _U, _P, ctypes.c_uint64, _P, _P]),
     "slm_preprocess": (ctypes.c_int, [_P, ctypes.c_int, _U, _U, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_pick_seeds_workspace": (ctypes.c_size_t, [_U]),
     "slm_pick_seeds": (ctypes.c_int, [_P, _P, _U, _I, _U, _U, _U, _P, _U, _P, _P, ctypes.c_size_t, _P]),

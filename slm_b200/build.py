@@ -18,7 +18,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libslm_b200.so")
-SOURCES = ["capi.cu", "trace.cu", "kde.cu", "map_kernels.cu", "scheduler.cu", "map_device.cu", "preprocess.cu"]
+SOURCES = ["capi.cu", "trace.cu", "kde.cu", "map_kernels.cu", "scheduler.cu", "map_device.cu", "preprocess.cu",
+           "seeds.cpp"]
 HEADERS = ["trace_common.cuh", "capi_util.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "nvcc")
@@ -44,7 +45,7 @@ def build(force=False, verbose=False, ptxas_info=False):
     jobs = []
     for src in SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(OBJ, src.replace(".cu", ".o"))
+        o = os.path.join(OBJ, os.path.splitext(src)[0] + ".o")
         objs.append(o)
         if force or _stale(o, [s] + hdrs):
             cmd = [NVCC] + _flags() + ["-c", s, "-o", o]
@@ -63,7 +64,7 @@ def build(force=False, verbose=False, ptxas_info=False):
             if verbose and out:
                 print(out)
     if force or jobs or _stale(LIB, objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lpthread"]
         run(cmd)
     return LIB
 

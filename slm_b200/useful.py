@@ -196,42 +196,51 @@ def vprint(verbose, *args, **kwargs):
         sys.stdout.flush()
 
 
-_SEED_CACHE = {}
-_SEED_CACHE_MAX = 4
 
 
-def _shuffled_seeds(mask, pad, do_shuffle, rng_seed):
-    """argwhere(~mask) - pad, shuffled as the reference shuffles it.
-
-    The reference seeds NumPy's global legacy generator and shuffles the
-    (N, 2) array in place (useful.py:496-501).  Shuffling the rows of an
-    array and ``permutation(N)`` draw the same Fisher-Yates indices from the
-    same stream, so ``rows[permutation(N)]`` is the same array and leaves the
-    global generator in the same state -- ten times faster.  Results are
-    cached by mask content; a cache hit restores the global generator to the
-    state the shuffle leaves, so the side effect is the reference's too.
-    """
-    import hashlib
-    m = np.ascontiguousarray(mask)
-    if m.dtype != np.bool_:
-        m = m.astype(np.bool_)
-    key = None
-    if do_shuffle:
-        key = (m.shape, int(pad), int(rng_seed),
-               hashlib.blake2b(m.view(np.uint8).data, digest_size=16).hexdigest())
-        hit = _SEED_CACHE.get(key)
-        if hit is not None:
-            np.random.set_state(hit[1])
-            return hit[0]  # create_seeds returns a copy
+def _shuffled_seeds_numpy(mask, pad, do_shuffle, rng_seed):
+    """argwhere(~mask) - pad, shuffled as the reference shuffles it, in NumPy
+    (useful.py:496-501): the restatement ``_shuffled_seeds`` is tested
+    against.  Shuffling the rows of an array and ``permutation(N)`` draw the
+    same Fisher-Yates indices from the same stream, so ``rows[permutation(N)]``
+    is the same array and leaves the global generator in the same state."""
+    m = np.ascontiguousarray(mask, dtype=np.bool_)
     seed_point_array = (np.argwhere(~m).astype(np.float32) - pad)
     if do_shuffle:
         np.random.seed(rng_seed)
-        perm = np.random.permutation(seed_point_array.shape[0])
-        seed_point_array = seed_point_array[perm]
-        if len(_SEED_CACHE) >= _SEED_CACHE_MAX:
-            _SEED_CACHE.pop(next(iter(_SEED_CACHE)))
-        _SEED_CACHE[key] = (seed_point_array, np.random.get_state())
+        seed_point_array = seed_point_array[np.random.permutation(seed_point_array.shape[0])]
     return seed_point_array
+
+
+def _shuffled_seeds(mask, pad, do_shuffle, rng_seed):
+    """argwhere(~mask) - pad, shuffled as the reference shuffles it
+    (useful.py:496-501), by ``slm_create_seeds`` (native host code: NumPy's
+    legacy MT19937 Fisher-Yates shuffle with the swap partners drawn ahead).
+    NumPy's global generator is left in the state the reference's shuffle
+    leaves it in."""
+    import ctypes
+
+    from . import _lib
+    m = np.ascontiguousarray(mask)
+    if m.ndim != 2:
+        raise ValueError("mask must be 2-D")
+    m8 = m.view(np.uint8) if m.dtype == np.bool_ else (m != 0).view(np.uint8)
+    L = _lib.load()
+    n = ctypes.c_uint64(0)
+    _lib.check(L.slm_create_seeds(m8.ctypes.data, m.shape[0], m.shape[1], int(pad), 0, 0, None, 0,
+                                  ctypes.byref(n), None))
+    if n.value == 0:
+        if do_shuffle:
+            np.random.seed(rng_seed)  # the shuffle of an empty list draws nothing
+        return np.empty((0, 2), np.float32)
+    out = np.empty((int(n.value), 2), np.float32)
+    state = np.empty(625, np.uint32)
+    _lib.check(L.slm_create_seeds(m8.ctypes.data, m.shape[0], m.shape[1], int(pad), 1 if do_shuffle else 0,
+                                  int(rng_seed) & 0xFFFFFFFF, out.ctypes.data, out.shape[0],
+                                  ctypes.byref(n), state.ctypes.data))
+    if do_shuffle:
+        np.random.set_state(("MT19937", state[:624].copy(), int(state[624]), 0, 0.0))
+    return out
 
 
 def create_seeds(mask, pad, n_work_items, n_seed_points=None, do_shuffle=True,
@@ -253,7 +262,7 @@ def create_seeds(mask, pad, n_work_items, n_seed_points=None, do_shuffle=True,
                   - n_seed_points)
     n_padded_seed_points = n_seed_points + pad_length
     vprint(verbose, "done")
-    return seed_point_array.copy(), n_seed_points, n_padded_seed_points
+    return seed_point_array, n_seed_points, n_padded_seed_points  # a fresh array either way
 
 
 def pick_seeds(mask=None, map=None, flag=None, pad=None):

@@ -1,0 +1,35 @@
+"""create_seeds' native shuffle (slm_create_seeds, host code) against NumPy's
+legacy generator, which the reference uses (useful.py:470-517): the same
+rows in the same order, and the global generator left in the same state."""
+import numpy as np
+import pytest
+
+from slm_b200 import useful as U
+
+
+@pytest.mark.parametrize("shape,pad,seed,frac", [((7, 9), 2, 1, 0.2), ((130, 77), 2, 0, 0.1),
+                                                 ((300, 257), 3, 12345, 0.5), ((1, 1), 0, 5, 0.0),
+                                                 ((64, 64), 2, 2 ** 32 - 1, 0.97), ((40, 33), 0, 7, 1.0)])
+@pytest.mark.parametrize("do_shuffle", [True, False])
+def test_native_seeds_match_numpy(shape, pad, seed, frac, do_shuffle):
+    rng = np.random.default_rng(sum(shape) + seed % 1000)
+    mask = rng.random(shape) < frac
+    a = U._shuffled_seeds_numpy(mask, pad, do_shuffle, seed)
+    sa = np.random.get_state()
+    np.random.seed(99)  # disturb the global generator between the two
+    b = U._shuffled_seeds(mask, pad, do_shuffle, seed)
+    sb = np.random.get_state()
+    assert a.dtype == b.dtype == np.float32 and a.shape == b.shape
+    assert np.array_equal(a, b)
+    if do_shuffle:
+        assert np.array_equal(sa[1], sb[1]) and sa[2] == sb[2]
+        assert np.random.random() == (np.random.set_state(sa), np.random.random())[1]
+
+
+def test_create_seeds_subset_and_padding():
+    mask = np.zeros((20, 30), bool)
+    mask[:2] = mask[-2:] = True
+    mask[:, :2] = mask[:, -2:] = True
+    s, n, npad = U.create_seeds(mask, 2, 32, n_seed_points=10, do_shuffle=True, rng_seed=3)
+    full = U._shuffled_seeds_numpy(mask, 2, True, 3)
+    assert n == 10 and np.array_equal(s, full[:10]) and npad % 32 == 0
