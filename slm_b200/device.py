@@ -1,6 +1,8 @@
 """Device selection and host<->device staging for the stage wrappers."""
 from __future__ import annotations
 
+import os
+
 import numpy as np
 import torch
 
@@ -30,6 +32,28 @@ def to_device(array, device, dtype=None):
     if dtype is not None and t.dtype != dtype:
         t = t.to(dtype)
     return t.to(device, non_blocking=t.is_pinned())
+
+
+_COPY_POOL = None
+
+
+def host_copy(src, min_bytes=8 << 20):
+    """A fresh NumPy copy of a host array, split over up to 8 threads when
+    large (np.copyto releases the GIL; the page faults of the new array are
+    taken in parallel too)."""
+    global _COPY_POOL
+    src = np.ascontiguousarray(src)
+    if src.nbytes < min_bytes:
+        return src.copy()
+    if _COPY_POOL is None:
+        from concurrent.futures import ThreadPoolExecutor
+        _COPY_POOL = ThreadPoolExecutor(max(1, min(8, os.cpu_count() or 1)))
+    dst = np.empty_like(src)
+    f, g = src.reshape(-1), dst.reshape(-1)
+    n, k = f.size, _COPY_POOL._max_workers
+    list(_COPY_POOL.map(lambda i: np.copyto(g[i * n // k:(i + 1) * n // k], f[i * n // k:(i + 1) * n // k]),
+                        range(k)))
+    return dst
 
 
 def pinned_empty(shape, dtype):

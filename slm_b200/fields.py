@@ -28,7 +28,7 @@ import numpy as np
 import torch
 
 from . import kernels
-from .device import cuda_device, low32, to_device
+from .device import cuda_device, host_copy, low32, to_device
 from .distributed import sharded_field_pass
 from .params import kernel_params
 from .useful import create_seeds, vprint
@@ -139,7 +139,7 @@ class Fields:
             st.copy_(t, non_blocking=True)
             out.append(st)
         torch.cuda.current_stream(dev).synchronize()
-        self.data.slc_array, self.data.slt_array, self.data.sla_array = (o.numpy().copy() for o in out)
+        self.data.slc_array, self.data.slt_array, self.data.sla_array = (host_copy(o.numpy()) for o in out)
 
     def _trace(self):
         """Both passes on the device; returns the uint64 accumulators [2, 2, nxy]."""
