@@ -198,20 +198,6 @@ def vprint(verbose, *args, **kwargs):
 
 
 
-def _shuffled_seeds_numpy(mask, pad, do_shuffle, rng_seed):
-    """argwhere(~mask) - pad, shuffled as the reference shuffles it, in NumPy
-    (useful.py:496-501): the restatement ``_shuffled_seeds`` is tested
-    against.  Shuffling the rows of an array and ``permutation(N)`` draw the
-    same Fisher-Yates indices from the same stream, so ``rows[permutation(N)]``
-    is the same array and leaves the global generator in the same state."""
-    m = np.ascontiguousarray(mask, dtype=np.bool_)
-    seed_point_array = (np.argwhere(~m).astype(np.float32) - pad)
-    if do_shuffle:
-        np.random.seed(rng_seed)
-        seed_point_array = seed_point_array[np.random.permutation(seed_point_array.shape[0])]
-    return seed_point_array
-
-
 def _shuffled_seeds(mask, pad, do_shuffle, rng_seed):
     """argwhere(~mask) - pad, shuffled as the reference shuffles it
     (useful.py:496-501), by ``slm_create_seeds`` (native host code: NumPy's

@@ -7,6 +7,20 @@ import pytest
 from slm_b200 import useful as U
 
 
+def numpy_seeds(mask, pad, do_shuffle, rng_seed):
+    """The reference's create_seeds core in NumPy (useful.py:496-501):
+    argwhere(~mask) - pad, rows shuffled by the global legacy generator.
+    Shuffling rows and permutation(N) draw the same Fisher-Yates partners
+    from the same stream, so rows[permutation(N)] is the same array and
+    leaves the generator in the same state."""
+    m = np.ascontiguousarray(mask, dtype=np.bool_)
+    rows = np.argwhere(~m).astype(np.float32) - pad
+    if do_shuffle:
+        np.random.seed(rng_seed)
+        rows = rows[np.random.permutation(rows.shape[0])]
+    return rows
+
+
 @pytest.mark.parametrize("shape,pad,seed,frac", [((7, 9), 2, 1, 0.2), ((130, 77), 2, 0, 0.1),
                                                  ((300, 257), 3, 12345, 0.5), ((1, 1), 0, 5, 0.0),
                                                  ((64, 64), 2, 2 ** 32 - 1, 0.97), ((40, 33), 0, 7, 1.0)])
@@ -14,7 +28,7 @@ from slm_b200 import useful as U
 def test_native_seeds_match_numpy(shape, pad, seed, frac, do_shuffle):
     rng = np.random.default_rng(sum(shape) + seed % 1000)
     mask = rng.random(shape) < frac
-    a = U._shuffled_seeds_numpy(mask, pad, do_shuffle, seed)
+    a = numpy_seeds(mask, pad, do_shuffle, seed)
     sa = np.random.get_state()
     np.random.seed(99)  # disturb the global generator between the two
     b = U._shuffled_seeds(mask, pad, do_shuffle, seed)
@@ -31,5 +45,5 @@ def test_create_seeds_subset_and_padding():
     mask[:2] = mask[-2:] = True
     mask[:, :2] = mask[:, -2:] = True
     s, n, npad = U.create_seeds(mask, 2, 32, n_seed_points=10, do_shuffle=True, rng_seed=3)
-    full = U._shuffled_seeds_numpy(mask, 2, True, 3)
+    full = numpy_seeds(mask, 2, True, 3)
     assert n == 10 and np.array_equal(s, full[:10]) and npad % 32 == 0
