@@ -309,3 +309,42 @@ def subsegment_channel_threshold(data, mapping_params=None, analysis_params=None
         t = p["guess_channel_threshold"] / 2
     data.channel_threshold = t
     return t
+
+
+def _thin_default(image):
+    from .skeleton import zhang_suen_device
+    return zhang_suen_device(image)
+
+
+def map_midslopes(info, data, midslope_filter_sigma=5.0, midslope_threshold=0.03, thin=None):
+    """Mapping.map_midslopes (mapping.py:778-791): unmasked pixels where the
+    Gaussian-smoothed angle between the downstream and upstream sla departs
+    from pi/4 by at most ``midslope_threshold``, thinned to one pixel, get
+    IS_MIDSLOPE.  The reference thins with scikit-image's skeletonize; here
+    ``thin`` (default: this package's Zhang-Suen thinning on the GPU) stands
+    in, so which pixels the thinning keeps is not pinned to the reference."""
+    from scipy.ndimage import gaussian_filter
+    thin = thin or _thin_default
+    dsla, usla = data.sla_array[:, :, 0], data.sla_array[:, :, 1]
+    mid = np.zeros((info.nx_padded, info.ny_padded), dtype=bool)
+    mid[(~data.mask_array) & (np.fabs(gaussian_filter((np.arctan2(dsla, usla) - np.pi / 4),
+                                                      midslope_filter_sigma)) <= midslope_threshold)] = True
+    data.mapping_array[thin(mid)] |= info.is_midslope
+
+
+def map_ridges(info, data, ridge_filter_sigma=2.0, ridge_threshold=0.8, thin=None):
+    """Mapping.map_ridges (mapping.py:793-816): unmasked pixels whose smoothed
+    sla angle lies at least (pi/4) * ridge_threshold below pi/4, dilated twice
+    with the 8-neighbour structure, holes filled, thinned to one pixel (the
+    stand-in for skeletonize as in ``map_midslopes``), get IS_RIDGE."""
+    from scipy.ndimage import binary_dilation, binary_fill_holes, gaussian_filter, generate_binary_structure
+    thin = thin or _thin_default
+    dsla, usla = data.sla_array[:, :, 0], data.sla_array[:, :, 1]
+    nxp, nyp = info.nx_padded, info.ny_padded
+    ridge = np.zeros((nxp, nyp), dtype=bool)
+    fat = np.zeros((nxp, nyp), dtype=bool)
+    ridge[(~data.mask_array) & ((gaussian_filter((np.arctan2(dsla, usla) - np.pi / 4), ridge_filter_sigma))
+                                <= -(np.pi / 4) * ridge_threshold)] = True
+    binary_dilation(ridge, structure=generate_binary_structure(2, 2), iterations=2, output=fat)
+    binary_fill_holes(fat, output=fat)
+    data.mapping_array[thin(fat)] |= info.is_ridge

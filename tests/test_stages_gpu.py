@@ -105,3 +105,42 @@ def test_fields_device_finish_matches_host(density, exact):
     fc.integrate()
     assert np.allclose(fc.data.slc_array, slc, rtol=4.5e-16, atol=0.0)
     assert np.array_equal(fc.data.slt_array, slt)
+
+
+def test_trace_stage_on_a_cropped_region():
+    """Trace.do() with real kernels: the fields of the unmasked bounding box
+    (Fields run directly on the same crop), zero outside it, slc truncated to
+    uint32; trajectory seeds inside the box."""
+    import types
+
+    from slm_b200.trace import Trace
+    from slm_b200.useful import Info, default_parameters, get_bbox
+    c = Case(nx=60, ny=52, seed=83, density=2, step=0.25, max_length=50.0, n_traj_seeds=100)
+    pad = 2
+    mask = c.mask.copy()
+    mask[:pad + 9, :] = True  # a masked band: the crop is smaller than the ROI
+    mask[:, -(pad + 6):] = True
+    d = default_parameters()
+    state = types.SimpleNamespace(**vars(d.state))
+    state.merge_active_masks = lambda: mask.copy()
+    params = {"trace": dict(vars(d.trace), subpixel_seed_point_density=2, integrator_step_factor=0.25,
+                            max_length=50.0, n_trajectory_seed_points=100)}
+    geodata = types.SimpleNamespace(roi_nx=60, roi_ny=52, pad_width=pad, roi_pixel_size=1.0)
+    t = Trace(state, params, geodata, types.SimpleNamespace(uv_array=c.uv))
+    t.do()
+    bbox, bnx, bny = get_bbox(~mask)
+    b = Data(info=None, bbox=bbox, pad=pad, mask_array=mask, uv_array=c.uv).bounds_slx
+    tr = types.SimpleNamespace(**params["trace"])
+    info = Info(state, tr, 1.0)
+    info.set_xy(bnx, bny, pad)
+    data = Data(info=info, bbox=bbox, pad=pad, mask_array=mask, uv_array=c.uv,
+                mapping_array=np.zeros(mask.shape, np.uint32), traj_stats_df=t.traj_stats_df)
+    f = Fields(0, 0, info=info, data=data)
+    f.integrate()
+    assert np.array_equal(t.slc_array[b], f.data.slc_array.astype(np.uint32))
+    assert np.array_equal(t.slt_array[b], f.data.slt_array)
+    outside = np.ones(mask.shape, bool)
+    outside[b[:2]] = False
+    assert not t.slc_array[outside].any() and t.slc_array[b].any()
+    x, y = t.seed_point_array[:, 0] + pad, t.seed_point_array[:, 1] + pad
+    assert (x >= bbox[0]).all() and (x <= bbox[1]).all() and (y >= bbox[2]).all() and (y <= bbox[3]).all()
