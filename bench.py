@@ -794,7 +794,8 @@ def run_stages(args, wl, dev):
     out["kde_univariate_max_rel_err"] = float(np.max(np.abs(ud.pdf - p_ref)) / np.max(np.abs(p_ref)))
     sl = data2.slt_array
     sel = (~wl.mask) & (sl[:, :, 0] > 0) & (sl[:, :, 1] > 0)
-    lx, ly = np.log(sl[:, :, 0]), np.log(sl[:, :, 1])
+    with np.errstate(divide="ignore"):  # log(0) outside the selection, replaced below
+        lx, ly = np.log(sl[:, :, 0]), np.log(sl[:, :, 1])
     lx[~sel] = np.finfo(np.float32).min
     ly[~sel] = np.finfo(np.float32).min
     bd = Bivariate_distribution(logx_array=lx, logy_array=ly, mask_array=wl.mask,
