@@ -42,6 +42,10 @@ CASES = {
     "preprocess_d": dict(nx=30, ny=45, seed=24, pixel_size=1.5, pad=1, noise=0.1, dtype="float64",
                          plateaus=True),
     "preprocess_e": dict(nx=64, ny=64, seed=25, pixel_size=1.0, pad=2, noise=0.05, pits=True),
+    # edge cases: the smallest grid, and a flat plateau (exact ties everywhere)
+    # with one pit and a hole
+    "preprocess_f": dict(nx=2, ny=2, seed=26, pixel_size=1.0, pad=1, noise=1.0),
+    "preprocess_g": dict(nx=23, ny=19, seed=27, pixel_size=1.0, pad=2, noise=0.0, flat=True),
 }
 # The reference stores four pixels per looped cell in an nx*ny array, so at
 # most a quarter of the cells may loop; the noise levels stay well below.
@@ -96,8 +100,13 @@ def load_reference_preprocess(ref=DEFAULT_REF):
     return mod
 
 
-def make_roi(nx, ny, seed, noise, holes=False, dtype="float32", plateaus=False, pits=False, **_):
+def make_roi(nx, ny, seed, noise, holes=False, dtype="float32", plateaus=False, pits=False, flat=False, **_):
     rng = np.random.default_rng(seed)
+    if flat:
+        roi = np.full((nx, ny), 50.0, dtype)
+        roi[nx // 2, ny // 3] = 49.0
+        roi[3, ny - 4] = np.nan
+        return roi
     x = np.arange(nx)[:, None]
     y = np.arange(ny)[None, :]
     roi = 40.0 + 0.35 * x + 0.2 * y + 3.0 * np.sin(x / 5.0) * np.cos(y / 7.0)
