@@ -134,3 +134,22 @@ class Trajectories:
         self.data.streamline_arrays_list = streamline_arrays_list
         self.data.traj_nsteps_array = traj_nsteps_array[0:ns].copy()
         self.data.traj_length_array = traj_length_array[0:ns].copy()
+
+
+def decode_streamlines(seed_point_array, streamline_arrays_list, trajectory_resolution, origin=(0.0, 0.0),
+                       indexes=None):
+    """Positions of recorded trajectories from their wire format: each is a
+    char2 list of steps in units of 1/trajectory_resolution pixel from its
+    seed.  The decoding is the reference's plotting code's (plot.py:1414-1423):
+    a (0, 0) start, the steps as float32 over the resolution, a running
+    float32 sum per axis, plus the ROI origin, plus the seed.  Returns a list
+    of (x, y) float32 arrays, one per trajectory (all, or ``indexes``)."""
+    res = np.float32(trajectory_resolution)
+    ox, oy = np.float32(origin[0]), np.float32(origin[1])
+    out = []
+    for k in (range(len(streamline_arrays_list)) if indexes is None else indexes):
+        steps = np.asarray(streamline_arrays_list[k]).reshape(-1, 2)
+        t = np.concatenate((np.zeros((1, 2), np.float32), steps.astype(np.float32) / res))
+        seed = seed_point_array[k, :]
+        out.append((ox + np.cumsum(t.T[0]) + seed[0], oy + np.cumsum(t.T[1]) + seed[1]))
+    return out

@@ -47,3 +47,20 @@ def test_create_seeds_subset_and_padding():
     s, n, npad = U.create_seeds(mask, 2, 32, n_seed_points=10, do_shuffle=True, rng_seed=3)
     full = numpy_seeds(mask, 2, True, 3)
     assert n == 10 and np.array_equal(s, full[:10]) and npad % 32 == 0
+
+
+def test_decode_streamlines_matches_the_reference_expression():
+    """plot.py:1414-1423 restated inline: (0,0) start, float32 steps over the
+    resolution, cumulative sums plus origin plus seed."""
+    from slm_b200.trajectories import decode_streamlines
+    rng = np.random.default_rng(4)
+    seeds = rng.uniform(0, 50, (5, 2)).astype(np.float32)
+    lists = [rng.integers(-60, 60, (int(n), 2)).astype(np.int8) for n in (0, 1, 7, 300, 33)]
+    origin = (np.float32(0.5), np.float32(0.5))
+    got = decode_streamlines(seeds, lists, 128, origin)
+    for k in range(5):
+        traj = np.concatenate((np.array([[0, 0]], dtype=np.float32), lists[k].astype(np.float32) / np.float32(128)))
+        x = origin[0] + np.cumsum(traj.T[0]) + seeds[k, 0]
+        y = origin[1] + np.cumsum(traj.T[1]) + seeds[k, 1]
+        assert np.array_equal(got[k][0], x) and np.array_equal(got[k][1], y)
+        assert got[k][0].dtype == np.float32 and got[k][0].size == lists[k].shape[0] + 1
