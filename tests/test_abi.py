@@ -55,3 +55,37 @@ def test_bad_arguments_rejected_without_device():
     rc = L.slm_integrate_fields(_lib.sref(p), None, None, None, None, None, None, None, None, None)
     assert rc == _lib.SLM_ERR_ARGS
     assert b"grid too small" in L.slm_last_error()
+
+
+def test_pair_and_preprocess_arguments_rejected_without_device():
+    """Host-side checks of the pair launch, preprocess and seed entry points
+    (nothing reaches the device): mismatched direction blocks, a bad upstream
+    stride, a bad ROI type, a too-small seed buffer."""
+    import numpy as np
+
+    from cases import Case
+    L = _lib.load()
+    c = Case(nx=20, ny=16, seed=3)
+    pd, pu = c.params("INTEGRATE_FIELDS", 1.0), c.params("INTEGRATE_FIELDS", -1.0)
+    fake = ctypes.c_void_p(4096)  # never dereferenced: the checks fail first
+    bad = c.params("INTEGRATE_FIELDS", -1.0)
+    bad.max_n_steps += 1
+    rc = L.slm_integrate_fields_pair(_lib.sref(pd), _lib.sref(bad), None, fake, fake, fake, fake, fake,
+                                     pd.nxy_padded, fake, None, None)
+    assert rc == _lib.SLM_ERR_ARGS and b"differ in more than the direction" in L.slm_last_error()
+    same = c.params("INTEGRATE_FIELDS", 1.0)
+    rc = L.slm_integrate_fields_pair(_lib.sref(pd), _lib.sref(same), None, fake, fake, fake, fake, fake,
+                                     pd.nxy_padded, fake, None, None)
+    assert rc == _lib.SLM_ERR_ARGS  # same sign twice
+    rc = L.slm_integrate_fields_pair(_lib.sref(pd), _lib.sref(pu), None, fake, fake, fake, fake, fake,
+                                     pd.nxy_padded - 1, fake, None, None)
+    assert rc == _lib.SLM_ERR_ARGS and b"up_stride" in L.slm_last_error()
+    prm = _lib.SlmPreprocessParams(1.0, 0.95, -0.5, 0.0, 2, 1)
+    rc = L.slm_preprocess(fake, 7, 10, 10, ctypes.byref(prm), fake, None, None, None, None, None, None, None,
+                          None, None, None)
+    assert rc == _lib.SLM_ERR_ARGS and b"roi_dtype" in L.slm_last_error()
+    mask = np.zeros((6, 5), np.uint8)
+    out = np.empty((3, 2), np.float32)
+    n = ctypes.c_uint64(0)
+    rc = L.slm_create_seeds(mask.ctypes.data, 6, 5, 1, 1, 1, out.ctypes.data, 3, ctypes.byref(n), None)
+    assert rc == _lib.SLM_ERR_CAPACITY and n.value == 30

@@ -80,3 +80,56 @@ def test_sharded_fields_equal_single_rank(world, tmp_path):
         assert np.array_equal(np.load(tmp_path / "slt_{}.npy".format(r)), ref_slt)
         mine, total = np.load(tmp_path / "steps_{}.npy".format(r))
         assert total == ref_steps
+
+
+def _failing_worker(rank, world, port, out_dir):
+    """Rank 1's trace raises before the all-reduce; rank 0 records what its
+    all-reduce does (it must fail within the group's short timeout, not hang)."""
+    import sys
+    import time
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path[:0] = [root, os.path.join(root, "oracle"), os.path.join(root, "tests")]
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=10))
+    c = _case()
+    prm = c.params("INTEGRATE_FIELDS", 1.0)
+    nxy = prm.nxy_padded
+    slc = torch.zeros(nxy, dtype=torch.uint64)
+    slt = torch.zeros(nxy, dtype=torch.uint64)
+
+    def trace(p, a, b):
+        if rank == 1:
+            raise RuntimeError("injected failure on rank 1")
+        return _oracle_trace(c)(p, a, b)
+    t0 = time.time()
+    try:
+        D.sharded_field_pass(prm, trace, slc, slt)
+        outcome = "completed"
+    except Exception as e:  # noqa: BLE001 - the outcome is what the test checks
+        outcome = "{}: {}".format(type(e).__name__, str(e).splitlines()[0] if str(e) else "")
+    with open(os.path.join(out_dir, "outcome_{}.txt".format(rank)), "w") as f:
+        f.write("{}\n{:.1f}\n".format(outcome, time.time() - t0))
+    if rank == 1:
+        os._exit(3)  # the failed rank leaves without joining the collective
+    try:
+        dist.destroy_process_group()
+    except Exception:  # noqa: BLE001
+        pass
+
+
+def test_failing_rank_ends_the_others_with_an_error(tmp_path):
+    world = 2
+    port = 29700 + (os.getpid() % 1000)
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_failing_worker, args=(r, world, port, str(tmp_path))) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+    assert all(p.exitcode is not None for p in procs), "a rank hung"
+    assert procs[1].exitcode == 3
+    r0 = (tmp_path / "outcome_0.txt").read_text().splitlines()
+    r1 = (tmp_path / "outcome_1.txt").read_text().splitlines()
+    assert r1[0].startswith("RuntimeError: injected failure")
+    assert r0[0] != "completed" and float(r0[1]) < 60.0, r0
