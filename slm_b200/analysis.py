@@ -20,6 +20,7 @@ from scipy.signal import argrelextrema
 from scipy.stats import norm
 
 from . import kde
+from .useful import vprint
 
 AVAILABLE_KERNELS = ["tophat", "triangle", "epanechnikov", "cosine", "gaussian"]
 
@@ -262,3 +263,190 @@ def compute_marginal_distribn_dslt(data, params=None, pixel_size=None):
                                   search_cdf_min=p["search_cdf_min"], search_cdf_max=p["search_cdf_max"],
                                   pixel_size=pixel_size)
     return d
+
+
+def compute_joint_distribn(x_array, y_array, mask_array=None, up_down_idx_x=0, up_down_idx_y=0, n_hist_bins=2048,
+                           n_pdf_points=256, kernel="gaussian", bandwidth=5.0, logx_min=None, logy_min=None,
+                           logx_max=None, logy_max=None, pixel_size=None, cl_platform=0, cl_device=0,
+                           verbose=False):
+    """Analysis.compute_joint_distribn with the device KDE (analysis.py:326-381):
+    the positive (x, y) pairs of the unmasked pixels in log space, the
+    bivariate pdf, then find_mode."""
+    if mask_array is not None:
+        tx = x_array[~mask_array, up_down_idx_x].copy().astype(np.float32)
+        ty = y_array[~mask_array, up_down_idx_y].copy().astype(np.float32)
+    else:
+        tx = x_array[:, :, up_down_idx_x].copy().ravel().astype(np.float32)
+        ty = y_array[:, :, up_down_idx_y].copy().ravel().astype(np.float32)
+    keep = (tx > 0.0) & (ty > 0.0)
+    d = Bivariate_distribution(logx_array=np.log(tx[keep]), logy_array=np.log(ty[keep]), pixel_size=pixel_size,
+                               n_hist_bins=n_hist_bins, n_pdf_points=n_pdf_points, logx_min=logx_min,
+                               logy_min=logy_min, logx_max=logx_max, logy_max=logy_max,
+                               cl_platform=cl_platform, cl_device=cl_device, verbose=verbose)
+    d.compute_kde_opencl(kernel=kernel, bandwidth=bandwidth)
+    d.find_mode()
+    return d
+
+
+ANALYSIS_PARAMETERS = {
+    "search_cdf_min": 0.8, "search_cdf_max": 0.999, "marginal_distbn_kde_bandwidth": 10.0,
+    "joint_distbn_kde_bandwidth": 5.0, "n_hist_bins": 2048, "n_pdf_points": 256,
+    "pdf_sla_min": 1, "pdf_slc_min": 1, "pdf_slt_min": 1,
+    "marginal_distbn_kde_method": "opencl", "marginal_distbn_kde_kernel": "epanechnikov",
+    "joint_distbn_kde_method": "opencl", "joint_distbn_kde_kernel": "gaussian",
+    "do_marginal_distbn_dsla": True, "do_marginal_distbn_usla": False, "do_marginal_distbn_dslt": True,
+    "do_marginal_distbn_uslt": False, "do_marginal_distbn_dslc": True, "do_marginal_distbn_uslc": False,
+    "do_joint_distribn_dsla_dslt": True, "do_joint_distribn_usla_uslt": False,
+    "do_joint_distribn_uslt_dslt": False, "do_joint_distribn_dsla_usla": False,
+    "do_joint_distribn_dsla_dslc": True, "do_joint_distribn_dslt_dslc": True,
+    "do_joint_distribn_usla_uslc": False, "do_joint_distribn_uslc_dslc": False,
+}
+
+# name: (x field, y field, x direction, y direction, log-limit parameters), as
+# the reference's compute_marginal_distribn_* / compute_joint_distribn_*
+# methods choose them (analysis.py:191-573), in the order do() runs them
+_SLA_SLC = ("pdf_sla_min", "pdf_sla_max", "pdf_slc_min", "pdf_slc_max")
+_SLT_SLA = ("pdf_slt_min", "pdf_slt_max", "pdf_sla_min", "pdf_sla_max")
+_SLC_SLA = ("pdf_slc_min", "pdf_slc_max", "pdf_sla_min", "pdf_sla_max")
+MARGINALS = [("dsla", "sla", "slc", 0, 0, _SLA_SLC), ("usla", "sla", "slc", 1, 1, _SLA_SLC),
+             ("dslt", "slt", "sla", 0, 0, _SLT_SLA), ("uslt", "slt", "sla", 1, 1, _SLT_SLA),
+             ("dslc", "slc", "sla", 0, 0, _SLC_SLA), ("uslc", "slc", "sla", 1, 1, _SLC_SLA)]
+JOINTS = [("dsla_usla", "sla", "sla", 0, 1, ("pdf_sla_min", "pdf_sla_max", "pdf_sla_min", "pdf_sla_max")),
+          ("usla_uslt", "sla", "slt", 1, 1, ("pdf_sla_min", "pdf_sla_max", "pdf_slt_min", "pdf_slt_max")),
+          # the reference pairs slt (x) with sla (y) here, under sla-then-slt limits
+          ("dsla_dslt", "slt", "sla", 0, 0, ("pdf_sla_min", "pdf_sla_max", "pdf_slt_min", "pdf_slt_max")),
+          ("dslt_dslc", "slt", "slc", 0, 0, ("pdf_slt_min", "pdf_slt_max", "pdf_slc_min", "pdf_slc_max")),
+          ("uslt_dslt", "slt", "slt", 1, 0, ("pdf_slt_min", "pdf_slt_max", "pdf_slt_min", "pdf_slt_max")),
+          ("usla_uslc", "sla", "slc", 1, 1, _SLA_SLC),
+          ("dsla_dslc", "sla", "slc", 0, 0, _SLA_SLC),
+          ("uslc_dslc", "slc", "slc", 1, 0, ("pdf_slc_min", "pdf_slc_max", "pdf_slc_min", "pdf_slc_max"))]
+
+
+class Analysis:
+    """``streamlines.analysis.Analysis`` (analysis.py:40-577) over the device
+    KDE: ``do()`` computes the marginal pdfs (``mpdf_<name>``: modes,
+    statistics, channel threshold) and the joint pdfs (``jpdf_<name>``: mode)
+    that the job's ``do_*`` flags select, from ``trace``'s slc/slt/sla, or
+    from ``data`` when a method is given one.  Only the 'opencl' KDE method
+    exists here (on the GPU); the reference's scipy/sklearn alternatives and
+    the elevation/slope pdfs are not restated."""
+
+    def __init__(self, state, imported_parameters, geodata, preprocess, trace):
+        params = dict(ANALYSIS_PARAMETERS)
+        if imported_parameters:
+            params.update(imported_parameters.get("analysis", imported_parameters))
+        for k, v in params.items():
+            setattr(self, k, v)
+        self.state, self.geodata, self.preprocess, self.trace = state, geodata, preprocess, trace
+        self.mapping = None
+        self.area_correction_factor = 1.0
+        self.length_correction_factor = 1.0
+
+    def _augment(self, mapping):
+        self.mapping = mapping
+
+    def print(self, *args, **kwargs):
+        vprint(getattr(self.state, "verbose", False), *args, **kwargs)
+
+    def do(self):
+        self.print("\n**Analysis begin**")
+        for name, *_ in MARGINALS:
+            if getattr(self, "do_marginal_distbn_" + name, False):
+                getattr(self, "compute_marginal_distribn_" + name)()
+        for name, *_ in JOINTS:
+            if getattr(self, "do_joint_distribn_" + name, False):
+                getattr(self, "compute_joint_distribn_" + name)()
+        self.print("**Analysis end**\n")
+
+    def estimate_channel_threshold(self, data, verbose=None):
+        """analysis.py:120-134: the dslt threshold, None when none qualifies."""
+        try:
+            self.compute_marginal_distribn_dslt(data)
+            return self.mpdf_dslt.channel_threshold_x
+        except AttributeError as error:
+            self.print("Failed to estimate channel threshold:", error)
+            return None
+
+    def _get_limits(self, attr_list):
+        return [np.log(getattr(self, a)) if hasattr(self, a) and getattr(self, a) is not None else None
+                for a in attr_list]
+
+    def _method(self, key):
+        method = getattr(self, key)
+        if method != "opencl":
+            raise NotImplementedError('KDE method "{}": only "opencl" (the device KDE) is built'.format(method))
+
+    def _arrays(self, data, fx, fy):
+        src = data if data is not None else self.trace
+        return getattr(src, fx + "_array"), getattr(src, fy + "_array"), (data.mask_array if data is not None
+                                                                           else None)
+
+    def compute_marginal_distribn(self, x_array, y_array, mask_array=None, up_down_idx_x=0, up_down_idx_y=0,
+                                  n_hist_bins=None, n_pdf_points=None, kernel=None, bandwidth=None, method=None,
+                                  logx_min=None, logy_min=None, logx_max=None, logy_max=None):
+        if method is None:
+            self._method("marginal_distbn_kde_method")
+        elif method != "opencl":
+            raise NotImplementedError('KDE method "{}": only "opencl" (the device KDE) is built'.format(method))
+        return compute_marginal_distribn(
+            x_array, y_array, mask_array, up_down_idx_x, up_down_idx_y,
+            n_hist_bins=n_hist_bins or self.n_hist_bins, n_pdf_points=n_pdf_points or self.n_pdf_points,
+            kernel=kernel or self.marginal_distbn_kde_kernel,
+            bandwidth=bandwidth if bandwidth is not None else self.marginal_distbn_kde_bandwidth,
+            logx_min=logx_min, logy_min=logy_min, logx_max=logx_max, logy_max=logy_max,
+            search_cdf_min=self.search_cdf_min, search_cdf_max=self.search_cdf_max,
+            pixel_size=getattr(self.geodata, "roi_pixel_size", None),
+            cl_platform=getattr(self.state, "cl_platform", 0), cl_device=getattr(self.state, "cl_device", 0),
+            verbose=getattr(self.state, "verbose", False))
+
+    def compute_joint_distribn(self, x_array, y_array, mask_array=None, up_down_idx_x=0, up_down_idx_y=0,
+                               n_hist_bins=None, n_pdf_points=None, thresholding_marginal_distbn=None,
+                               kernel=None, bandwidth=None, method=None, logx_min=None, logy_min=None,
+                               logx_max=None, logy_max=None, upstream_modal_length=None):
+        if method is None:
+            self._method("joint_distbn_kde_method")
+        elif method != "opencl":
+            raise NotImplementedError('KDE method "{}": only "opencl" (the device KDE) is built'.format(method))
+        return compute_joint_distribn(
+            x_array, y_array, mask_array, up_down_idx_x, up_down_idx_y,
+            n_hist_bins=n_hist_bins or self.n_hist_bins, n_pdf_points=n_pdf_points or self.n_pdf_points,
+            kernel=kernel or self.joint_distbn_kde_kernel,
+            bandwidth=bandwidth if bandwidth is not None else self.joint_distbn_kde_bandwidth,
+            logx_min=logx_min, logy_min=logy_min, logx_max=logx_max, logy_max=logy_max,
+            pixel_size=getattr(self.geodata, "roi_pixel_size", None),
+            cl_platform=getattr(self.state, "cl_platform", 0), cl_device=getattr(self.state, "cl_device", 0),
+            verbose=getattr(self.state, "verbose", False))
+
+
+def _marginal_method(name, fx, fy, ix, iy, limits):
+    def method(self, data=None):
+        x_array, y_array, mask_array = self._arrays(data, fx, fy)
+        if name == "usla":
+            mask_array = data.mask_array  # the reference reads it whether or not data is given
+        lx0, lx1, ly0, ly1 = self._get_limits(limits)
+        setattr(self, "mpdf_" + name, self.compute_marginal_distribn(
+            x_array, y_array, mask_array, up_down_idx_x=ix, up_down_idx_y=iy,
+            logx_min=lx0, logy_min=ly0, logx_max=lx1, logy_max=ly1))
+    method.__name__ = "compute_marginal_distribn_" + name
+    method.__doc__ = "The marginal pdf '{}' (analysis.py:191-323).".format(name)
+    return method
+
+
+def _joint_method(name, fx, fy, ix, iy, limits):
+    def method(self, data=None):
+        x_array, y_array, mask_array = self._arrays(data, fx, fy)
+        lx0, lx1, ly0, ly1 = self._get_limits(limits)
+        setattr(self, "jpdf_" + name, self.compute_joint_distribn(
+            x_array, y_array, mask_array, up_down_idx_x=ix, up_down_idx_y=iy,
+            thresholding_marginal_distbn=getattr(self, "mpdf_dsla", None),
+            logx_min=lx0, logy_min=ly0, logx_max=lx1, logy_max=ly1))
+    method.__name__ = "compute_joint_distribn_" + name
+    method.__doc__ = "The joint pdf '{}' (analysis.py:383-573).".format(name)
+    return method
+
+
+for _row in MARGINALS:
+    setattr(Analysis, "compute_marginal_distribn_" + _row[0], _marginal_method(*_row))
+for _row in JOINTS:
+    setattr(Analysis, "compute_joint_distribn_" + _row[0], _joint_method(*_row))
+del _row
