@@ -300,6 +300,9 @@ ANALYSIS_PARAMETERS = {
     "do_joint_distribn_uslt_dslt": False, "do_joint_distribn_dsla_usla": False,
     "do_joint_distribn_dsla_dslc": True, "do_joint_distribn_dslt_dslc": True,
     "do_joint_distribn_usla_uslc": False, "do_joint_distribn_uslc_dslc": False,
+    "pdf_bw_method": "scott", "pdf_bw_factor_h_midline": 0.6, "pdf_bw_factor_h_all": 0.6,
+    "pdf_bw_factor_slope": 0.2, "pdf_h_min": 0, "pdf_h_max": 4000, "pdf_h_steps": 200,
+    "pdf_h_midline_max_bound": 1000, "pdf_slope_min": 0, "pdf_slope_max": 80, "pdf_slope_steps": 10,
 }
 
 # name: (x field, y field, x direction, y direction, log-limit parameters), as
@@ -328,8 +331,9 @@ class Analysis:
     statistics, channel threshold) and the joint pdfs (``jpdf_<name>``: mode)
     that the job's ``do_*`` flags select, from ``trace``'s slc/slt/sla, or
     from ``data`` when a method is given one.  Only the 'opencl' KDE method
-    exists here (on the GPU); the reference's scipy/sklearn alternatives and
-    the elevation/slope pdfs are not restated."""
+    exists here (on the GPU); the reference's scipy/sklearn alternatives are
+    not restated.  ``compute_elevation_slope_pdfs`` is the reference's SciPy
+    code, on the host as there."""
 
     def __init__(self, state, imported_parameters, geodata, preprocess, trace):
         params = dict(ANALYSIS_PARAMETERS)
@@ -366,6 +370,53 @@ class Analysis:
         except AttributeError as error:
             self.print("Failed to estimate channel threshold:", error)
             return None
+
+    def compute_elevation_slope_pdfs(self, bw_method=None, h_min=None, h_max=None, h_steps=None,
+                                     bw_factor_h_midline=None, bw_factor_h_all=None, h_midline_max_bound=None,
+                                     slope_min=None, slope_max=None, slope_steps=None, bw_factor_slope=None):
+        """analysis.py:580-657: Gaussian KDEs (SciPy, host, as the reference) of
+        the elevations of the midslope pixels and of the whole basin, and of
+        the midslope slopes (mirrored about zero), each with its bandwidth
+        scaled by a factor, evaluated on fixed grids; their maxima above the
+        given bounds.  Needs ``_augment(mapping)`` first (the mapping's
+        IS_MIDSLOPE flags), ``geodata.roi_array`` / ``basin_mask_array`` and
+        ``preprocess.slope_array``."""
+        from scipy.stats import gaussian_kde
+        pick = lambda v, k: getattr(self, k) if v is None else v  # noqa: E731
+        bw_method = pick(bw_method, "pdf_bw_method")
+        h_min, h_max, h_steps = pick(h_min, "pdf_h_min"), pick(h_max, "pdf_h_max"), pick(h_steps, "pdf_h_steps")
+        bw_factor_h_midline = pick(bw_factor_h_midline, "pdf_bw_factor_h_midline")
+        bw_factor_h_all = pick(bw_factor_h_all, "pdf_bw_factor_h_all")
+        h_midline_max_bound = pick(h_midline_max_bound, "pdf_h_midline_max_bound")
+        slope_min, slope_max = pick(slope_min, "pdf_slope_min"), pick(slope_max, "pdf_slope_max")
+        slope_steps = pick(slope_steps, "pdf_slope_steps")
+        bw_factor_slope = pick(bw_factor_slope, "pdf_bw_factor_slope")
+        m = self.mapping
+        m.midslope_array = (m.mapping_array & m.info.is_midslope).copy().astype(bool)
+        h_mid = self.geodata.roi_array[m.midslope_array[2:-2, 2:-2]].ravel()
+        h_all = self.geodata.roi_array[~self.geodata.basin_mask_array[2:-2, 2:-2]].ravel()
+        s_mid = np.abs(self.preprocess.slope_array[m.midslope_array].ravel())
+        s_mid = np.concatenate([s_mid, -s_mid])
+        h_grid = np.linspace(h_min, h_max, h_steps)
+        s_grid = np.linspace(slope_min, slope_max, (slope_max - slope_min) * slope_steps + 1)
+        kdes = []
+        for pts, factor in ((h_mid, bw_factor_h_midline), (h_all, bw_factor_h_all), (s_mid, bw_factor_slope)):
+            k = gaussian_kde(pts, bw_method=bw_method)
+            k.set_bandwidth(k.factor * factor)
+            kdes.append(k)
+        h_mid_pdf = kdes[0].evaluate(points=h_grid)
+        h_all_pdf = kdes[1].evaluate(points=h_grid)
+        s_mid_pdf = kdes[2].evaluate(points=s_grid)
+        self.h_midline_pdf_array = h_mid_pdf
+        self.h_midline_pdf_max1 = np.max(h_mid_pdf[h_grid > h_midline_max_bound])
+        self.h_midline_pdf_max1_h = h_grid[h_mid_pdf == self.h_midline_pdf_max1]
+        self.h_all_pdf_array = h_all_pdf
+        self.h_array = h_grid
+        self.h_pdf_sf = np.max(h_mid_pdf)
+        self.slope_midline_pdf_array = s_mid_pdf
+        self.slope_midline_pdf_max = np.max(s_mid_pdf[s_grid >= 10])
+        self.slope_midline_pdf_max_slope = s_grid[s_mid_pdf == self.slope_midline_pdf_max]
+        self.slope_array = s_grid
 
     def _get_limits(self, attr_list):
         return [np.log(getattr(self, a)) if hasattr(self, a) and getattr(self, a) is not None else None
