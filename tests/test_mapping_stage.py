@@ -1,0 +1,119 @@
+"""Mapping.pass1 against the reference's own Mapping.pass1 (CPU only).
+
+Both sides run every mapping kernel through the oracle (the reference's
+wrapper modules are stood in by this package's wrappers with the oracle
+runner), and both thin with this package's host thinning (scikit-image is
+absent).  So what is compared is pass 1 itself: the crop, the midslope and
+ridge flags, the reference's map_channels_segments sequence, the coarse
+subsegments and their mask, and the flag merge."""
+import importlib.util
+import os
+import sys
+import types
+
+import numpy as np
+import pytest
+
+from mapping_cases import incised_pipeline_case, oracle_runner
+from slm_b200 import mapping as M
+from slm_b200.mapping_stage import Mapping
+from slm_b200.skeleton import zhang_suen
+from slm_b200.useful import default_parameters
+from test_params import _load_reference_modules
+
+
+def _reference_mapping_module(reference_dir):
+    mods = _load_reference_modules(reference_dir)
+    names = ["skimage", "skimage.morphology", "skimage.filters", "skimage.filters.rank", "skfmm", "streamlines",
+             "streamlines.core", "streamlines.useful", "streamlines.pocl"] + \
+        ["streamlines." + n for n in ("connect", "channelheads", "countlink", "label", "segment", "hillslopes",
+                                      "lengths")]
+    saved = {k: sys.modules.get(k) for k in names}
+    st = {k: types.ModuleType(k) for k in names}
+    st["skimage.morphology"].skeletonize = zhang_suen
+    st["skimage.morphology"].medial_axis = lambda a: a  # both sides thin once, with the same thinning
+    st["skimage.morphology"].thin = st["skimage.morphology"].disk = None
+    st["skimage.filters"].gaussian = None
+    st["skimage.filters.rank"].mean = st["skimage.filters.rank"].median = None
+    st["streamlines.core"].Core = type("Core", (), {})
+    st["streamlines.pocl"].Initialize_cl = None
+
+    def bind(fn):
+        return lambda cl_state, info, data, verbose=False, **kw: fn(cl_state, info, data, verbose, runner=oracle_runner,
+                                                                   **kw)
+    st["streamlines.connect"].connect_channel_pixels = bind(M.connect_channel_pixels)
+    st["streamlines.channelheads"].map_channel_heads = bind(M.map_channel_heads)
+    st["streamlines.channelheads"].prune_channel_heads = bind(M.prune_channel_heads)
+    st["streamlines.countlink"].count_downchannels = bind(M.count_downchannels)
+    st["streamlines.countlink"].flag_downchannels = bind(M.flag_downchannels)
+    st["streamlines.label"].label_confluences = bind(M.label_confluences)
+    st["streamlines.segment"].segment_channels = bind(M.segment_channels)
+    st["streamlines.segment"].segment_hillslopes = bind(M.segment_hillslopes)
+    st["streamlines.segment"].subsegment_flanks = bind(M.subsegment_flanks)
+    st["streamlines.hillslopes"].link_hillslopes = bind(M.link_hillslopes)
+    for n in ("connect", "channelheads", "countlink", "label", "segment", "hillslopes", "lengths"):
+        setattr(st["streamlines"], n, st["streamlines." + n])
+    sys.modules.update(st)
+    sys.modules["streamlines.useful"] = mods["useful"]
+    if not hasattr(np, "bool"):
+        np.bool = np.bool_
+    try:
+        spec = importlib.util.spec_from_file_location(
+            "reference_mapping_stage", os.path.join(reference_dir, "python", "streamlines", "mapping.py"))
+        mod = importlib.util.module_from_spec(spec)
+        import warnings
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore")
+            spec.loader.exec_module(mod)
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                sys.modules.pop(k, None)
+            else:
+                sys.modules[k] = v
+    return mod
+
+
+@pytest.mark.parametrize("seed,do_map_hsl", [(3, True), (5, False)])
+def test_pass1_matches_reference(reference_dir, seed, do_map_hsl):
+    R = _reference_mapping_module(reference_dir)
+    n = 64
+    info0, data0 = incised_pipeline_case(n=n, seed=seed, n_incisions=6, max_steps=200)
+    slt, slc = data0.slt_array, data0.slc_array
+    with np.errstate(divide="ignore", invalid="ignore"):
+        sla = np.where(slc > 0, np.sqrt(2.0) * slt / slc, 0.0).astype(np.float32)
+    d = default_parameters()
+    trace = types.SimpleNamespace(**vars(d.trace))
+    trace.subpixel_seed_point_density, trace.jitter_magnitude = 1, 0.0
+    trace.integrator_step_factor, trace.max_length = 0.1, 20.0
+    trace.slc_array, trace.slt_array, trace.sla_array = slc, slt, sla
+    mask = data0.mask_array.copy()
+    state = types.SimpleNamespace(**vars(d.state))
+    state.reset_active_masks = lambda: None
+    state.merge_active_masks = lambda: mask.copy()
+    geodata = types.SimpleNamespace(roi_nx=n, roi_ny=n, pad_width=2, roi_pixel_size=2.0)
+    preprocess = types.SimpleNamespace(uv_array=data0.uv_array)
+    params = dict(vars(d.mapping))
+    params.update(coarse_channel_threshold=float(info0.channel_threshold), coarse_segmentation_threshold=10,
+                  fine_segmentation_threshold=10, do_map_channels_segments=True, do_map_hsl=do_map_hsl,
+                  midslope_filter_sigma=2.0, midslope_threshold=0.2, ridge_filter_sigma=2.0, ridge_threshold=0.3,
+                  do_measure_hsl_from_ridges=False)
+    class Info(R.Info):  # NumPy 1.x widened int32 + 2**31 to int64; NumPy 2 raises instead
+        def __init__(self, *a, **k):
+            super().__init__(*a, **k)
+            self.left_flank_addition = np.int64(self.left_flank_addition)
+    R.Info = Info
+    ref = R.Mapping.__new__(R.Mapping)
+    ref.__dict__.update(params)
+    ref.__dict__.update(state=state, geodata=geodata, preprocess=preprocess, trace=trace, cl_state=None,
+                        verbose=False, vprogress=False, vbackup=False, print=lambda *a, **k: None)
+    ref.pass1()
+    mine = Mapping(state, {"mapping": params}, geodata, preprocess, trace, runner=oracle_runner, thin=zhang_suen)
+    mine.pass1()
+    assert np.array_equal(mine.mapping_array, ref.mapping_array)
+    assert np.array_equal(mine.coarse_subsegment_array, ref.coarse_subsegment_array)
+    assert np.array_equal(mine.coarse_subsegments_list_array, ref.coarse_subsegments_list_array)
+    assert np.array_equal(mine.merged_coarse_mask_array, ref.merged_coarse_mask_array)
+    info = mine.info
+    assert mine.n_coarse_subsegments > 0
+    assert ((mine.mapping_array & info.is_midslope) > 0).any() and ((mine.mapping_array & info.is_ridge) > 0).any()
