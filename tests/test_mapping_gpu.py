@@ -168,3 +168,39 @@ def test_flag_downchannels_random_graphs(seed):
     map_kernels.run("flag_downchannels", prm, seeds, b)
     assert np.array_equal(b[2], a[2]), "mapping"
     assert np.array_equal(b[3], a[3]), "count"
+
+
+@pytest.mark.gpu
+def test_mapping_stage_pass1_on_the_gpu():
+    """Mapping.pass1 with its defaults (kernels and thinning on the GPU) equals
+    the same pass on the oracle with the host thinning."""
+    import types
+
+    from mapping_cases import incised_pipeline_case
+    from slm_b200.mapping_stage import Mapping
+    from slm_b200.skeleton import zhang_suen
+    from slm_b200.useful import default_parameters
+    info0, data0 = incised_pipeline_case(n=64, seed=3, n_incisions=6, max_steps=200)
+    slt, slc = data0.slt_array, data0.slc_array
+    with np.errstate(divide="ignore", invalid="ignore"):
+        sla = np.where(slc > 0, np.sqrt(2.0) * slt / slc, 0.0).astype(np.float32)
+    d = default_parameters()
+    trace = types.SimpleNamespace(**vars(d.trace))
+    trace.subpixel_seed_point_density, trace.jitter_magnitude = 1, 0.0
+    trace.integrator_step_factor, trace.max_length = 0.1, 20.0
+    trace.slc_array, trace.slt_array, trace.sla_array = slc, slt, sla
+    mask = data0.mask_array.copy()
+    state = types.SimpleNamespace(**vars(d.state))
+    state.reset_active_masks = lambda: None
+    state.merge_active_masks = lambda: mask.copy()
+    geodata = types.SimpleNamespace(roi_nx=64, roi_ny=64, pad_width=2, roi_pixel_size=2.0)
+    preprocess = types.SimpleNamespace(uv_array=data0.uv_array)
+    params = {"mapping": dict(coarse_channel_threshold=float(info0.channel_threshold), coarse_segmentation_threshold=10,
+                              midslope_filter_sigma=2.0, midslope_threshold=0.2, ridge_threshold=0.3)}
+    gpu = Mapping(state, params, geodata, preprocess, trace)
+    gpu.pass1()
+    cpu = Mapping(state, params, geodata, preprocess, trace, runner=oracle_runner, thin=zhang_suen)
+    cpu.pass1()
+    assert np.array_equal(gpu.mapping_array, cpu.mapping_array)
+    assert np.array_equal(gpu.coarse_subsegment_array, cpu.coarse_subsegment_array)
+    assert gpu.n_coarse_subsegments == cpu.n_coarse_subsegments > 0
