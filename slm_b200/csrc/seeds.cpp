@@ -148,9 +148,21 @@ int slm_create_seeds(const uint8_t* mask, uint32_t nx_padded, uint32_t ny_padded
         // the swap partners j(i), i = n-1 .. 1, in draw order
         // one thread draws the swap partners j(i), i = n-1 .. 1; this one
         // swaps row i with row j(i) as soon as j(i) is final
-        std::vector<uint32_t> js(n);
+        std::vector<uint32_t> js;
+        try {
+            js.resize(n);
+        } catch (...) {
+            return SLM_ERR_CAPACITY;  // no exception crosses the C ABI
+        }
         std::atomic<uint64_t> final_above{n};  // js[i] is final for every i >= final_above
-        std::thread drawer([&] { mt.intervals_down(n - 1, js.data(), &final_above); });
+        std::thread drawer;
+        bool threaded = true;
+        try {
+            drawer = std::thread([&] { mt.intervals_down(n - 1, js.data(), &final_above); });
+        } catch (...) {  // no thread to be had: draw everything first, then swap
+            threaded = false;
+            mt.intervals_down(n - 1, js.data(), &final_above);
+        }
         char* rows = reinterpret_cast<char*>(seed_point);  // 8-byte (x, y) rows
         const uint64_t ahead = 32;
         uint64_t ready = n;  // js[i] final for i >= ready
@@ -168,7 +180,7 @@ int slm_create_seeds(const uint8_t* mask, uint32_t nx_padded, uint32_t ny_padded
             std::memcpy(a, &tb, 8);
             std::memcpy(b, &ta, 8);
         }
-        drawer.join();
+        if (threaded) drawer.join();
     }
     if (generator_state) {
         std::memcpy(generator_state, mt.key, sizeof(mt.key));
