@@ -13,6 +13,10 @@ Mirrors ``streamlines.mapping.Mapping.pass1`` (python/streamlines/mapping.py:
 5. merge the flags back into the full ROI grid, then erase this pass's
    channel-head and thin-channel bits.
 
+The per-subsegment hillslope-length helpers follow: ``select_subsegments``,
+``measure_hsl_traced`` (the lengths kernel), ``parse_hsl`` (per-subsegment
+statistics) and ``remap_hsl`` (mapping.py:819-976).
+
 Kernels run through ``runner`` (default: the GPU, ``mapping.DeviceRunner``;
 tests pass the oracle).  The reference's second pass measures hillslope
 lengths by fast marching (skfmm), which is not available here.  That pass
@@ -27,7 +31,8 @@ from .useful import Data, Info, default_parameters, get_bbox, vprint
 
 MAPPING_PARAMETERS = dict(vars(default_parameters().mapping))
 MAPPING_PARAMETERS.update(do_map_channels_segments=True, do_map_hsl=True, midslope_filter_sigma=5.0,
-                          midslope_threshold=0.03, ridge_filter_sigma=2.0, ridge_threshold=0.8)
+                          midslope_threshold=0.03, ridge_filter_sigma=2.0, ridge_threshold=0.8,
+                          n_hsl_averaging_threshold=1, hsl_averaging_threshold=5.0)
 
 
 class Mapping:
@@ -108,6 +113,78 @@ class Mapping:
         self.mapping_array[(self.mapping_array & info.is_channelhead) != 0] ^= info.is_channelhead
         self.mapping_array[(self.mapping_array & info.is_thinchannel) != 0] ^= info.is_thinchannel
         vprint(self.vprogress, "**Pass#1 end**")
+
+    # ---------------------------------------------- hillslope lengths of subsegments
+    def select_subsegments(self, info, data, do_restrict=True):
+        """mapping.py:819-839: the (fine) subsegment label of every unmasked
+        midslope pixel (every unmasked pixel when not restricted), and the
+        nonzero labels among them."""
+        if do_restrict:
+            if self.do_measure_hsl_from_ridges:
+                pass  # the reference selects nothing new for ridges here
+            else:
+                sel = ((data.mapping_array & info.is_midslope) > 0) & (~data.mask_array)
+                data.subsegment_label_array = data.label_array[sel].astype(np.int32)
+        else:
+            data.subsegment_label_array = data.label_array[~data.mask_array].astype(np.int32)
+        unique = np.unique(data.subsegment_label_array)
+        data.selected_subsegments_array = unique[unique != 0].astype(np.int32)
+        self.n_subsegments = unique.size
+
+    def measure_hsl_traced(self, info, data):
+        """mapping.py:910-918: the hillslope length of every selected pixel,
+        traced on the GPU (``slm_hillslope_lengths``)."""
+        data.subsegment_hsl_array = np.zeros_like(data.subsegment_label_array, dtype=np.float32)
+        return M.hsl(self.cl_state, info, data, self.do_measure_hsl_from_ridges, self.verbose,
+                     runner=self._runner())
+
+    def parse_hsl(self, info, data):
+        """mapping.py:920-944: count, mean and standard deviation of the
+        lengths per selected subsegment, as a DataFrame indexed by
+        (fine, coarse) label."""
+        import pandas as pd
+        n = data.subsegment_hsl_array.shape[0]
+        df = pd.DataFrame(np.zeros((n,), dtype=[("fine", np.int32), ("length", np.float32)]))
+        df["fine"] = data.subsegment_label_array
+        df["length"] = data.subsegment_hsl_array
+        df = df[df.fine != 0]
+        try:
+            stats_df = pd.DataFrame(data.selected_subsegments_array, columns=["fine"])
+            for stat, column in (("count", "count"), ("mean", "mean [m]"), ("std", "stddev [m]")):
+                stats_df = stats_df.join(getattr(df.groupby("fine"), stat)(), on="fine")
+                stats_df.rename(index=str, columns={"length": column}, inplace=True)
+        except Exception:  # noqa: BLE001 - the reference reports failure, not the error
+            self.print("Problem constructing HSL stats dataframe")
+            return False
+        stats_df["coarse"] = getattr(info, "coarse_label", None)
+        stats_df.set_index(["fine", "coarse"], inplace=True)
+        data.hsl_stats_df = stats_df
+        return True
+
+    def remap_hsl(self, info, data, n_hsl_averaging_threshold=None):
+        """mapping.py:946-976: each subsegment's mean length painted on its
+        pixels (0 where it has fewer than ``n_hsl_averaging_threshold``
+        lengths); the mean of the painted values of at least
+        ``hsl_averaging_threshold`` metres."""
+        if n_hsl_averaging_threshold is None:
+            n_hsl_averaging_threshold = self.n_hsl_averaging_threshold
+        stats_df = data.hsl_stats_df
+        try:
+            data.hsl_array = np.zeros((info.nx_padded, info.ny_padded), dtype=np.float32)
+            for idx, row in stats_df.iterrows():
+                data.hsl_array[data.label_array == idx[0]] = (row["mean [m]"] if row["count"] >= n_hsl_averaging_threshold
+                                                              else 0)
+        except Exception:  # noqa: BLE001
+            self.print("Problem with HSL stats dataframe")
+            return False
+        if stats_df.empty:
+            return False
+        hsl = data.hsl_array[~np.isnan(data.hsl_array)]
+        hsl = hsl[hsl >= self.hsl_averaging_threshold]
+        if hsl.shape[0] == 0:
+            return False
+        data.trace_mean_hsl = np.mean(hsl)
+        return True
 
     def pass2(self):
         raise NotImplementedError("pass 2 measures hillslope lengths by fast marching (skfmm, mapping.py:388-560), "

@@ -117,3 +117,37 @@ def test_pass1_matches_reference(reference_dir, seed, do_map_hsl):
     info = mine.info
     assert mine.n_coarse_subsegments > 0
     assert ((mine.mapping_array & info.is_midslope) > 0).any() and ((mine.mapping_array & info.is_ridge) > 0).any()
+
+
+@pytest.mark.parametrize("seed", [3, 4])
+def test_traced_hillslope_length_helpers_match_reference(reference_dir, seed):
+    """select_subsegments, measure_hsl_traced (the lengths kernel on the
+    oracle), parse_hsl and remap_hsl against the reference's methods on the
+    same mapped grids."""
+    import copy
+
+    from mapping_cases import midslope_case
+    R = _reference_mapping_module(reference_dir)
+    R.lengths.hsl = lambda cl_state, info, data, do_use_ridges, verbose=False: M.hsl(
+        cl_state, info, data, do_use_ridges, verbose, runner=oracle_runner)
+    info, data = incised_pipeline_case(n=64, seed=seed, n_incisions=6, max_steps=200)
+    assert M.map_channels_segments(None, info, data, runner=oracle_runner)
+    midslope_case(data, info, seed=seed, frac=0.08)
+    info.coarse_label = 7
+    params = dict(do_measure_hsl_from_ridges=False, n_hsl_averaging_threshold=2, hsl_averaging_threshold=5.0)
+    ref = R.Mapping.__new__(R.Mapping)
+    ref.__dict__.update(params, cl_state=None, verbose=False, print=lambda *a, **k: None)
+    mine = Mapping(types.SimpleNamespace(verbose=False), {"mapping": params}, None, None, None,
+                   runner=oracle_runner)
+    rd, md = copy.deepcopy(data), copy.deepcopy(data)
+    for obj, d in ((ref, rd), (mine, md)):
+        obj.select_subsegments(info, d)
+        assert obj.measure_hsl_traced(info, d)
+        assert obj.parse_hsl(info, d)
+        assert obj.remap_hsl(info, d)
+    assert np.array_equal(md.subsegment_label_array, rd.subsegment_label_array)
+    assert np.array_equal(md.selected_subsegments_array, rd.selected_subsegments_array)
+    assert np.array_equal(md.subsegment_hsl_array.view(np.uint32), rd.subsegment_hsl_array.view(np.uint32))
+    assert md.hsl_stats_df.equals(rd.hsl_stats_df)
+    assert np.array_equal(md.hsl_array, rd.hsl_array) and md.trace_mean_hsl == rd.trace_mean_hsl
+    assert len(md.hsl_stats_df) > 3 and md.hsl_array.any()
