@@ -18,16 +18,17 @@ The per-subsegment hillslope-length helpers follow: ``select_subsegments``,
 statistics) and ``remap_hsl`` (mapping.py:819-976).
 
 Kernels run through ``runner`` (default: the GPU, ``mapping.DeviceRunner``;
-tests pass the oracle).  The reference's second pass measures hillslope
-lengths by fast marching (skfmm), which is not available here.  That pass
-and the third are not restated.
+tests pass the oracle).  ``pass2`` runs the reference's second pass with the
+hillslope lengths traced along streamlines, the alternative the reference
+keeps beside its fast-marching measurement (skfmm, absent here).  The third
+pass is not restated.
 """
 from __future__ import annotations
 
 import numpy as np
 
 from . import mapping as M
-from .useful import Data, Info, default_parameters, get_bbox, vprint
+from .useful import Data, Info, default_parameters, dilate, get_bbox, vprint
 
 MAPPING_PARAMETERS = dict(vars(default_parameters().mapping))
 MAPPING_PARAMETERS.update(do_map_channels_segments=True, do_map_hsl=True, midslope_filter_sigma=5.0,
@@ -186,9 +187,99 @@ class Mapping:
         data.trace_mean_hsl = np.mean(hsl)
         return True
 
-    def pass2(self):
-        raise NotImplementedError("pass 2 measures hillslope lengths by fast marching (skfmm, mapping.py:388-560), "
-                                  "which is not available here")
+    def make_coarse_subsegment_masks(self, coarse_subsegment, is_left_or_right, raw_mask, dilated_mask):
+        """mapping.py:348-386: the mask of one coarse subsegment (raw), and
+        that dilated by 2 pixels for a left flank or 1 for a right flank,
+        never into the pad; returns the dilated mask's bounding box."""
+        raw_mask.fill(True)
+        raw_mask[self.coarse_subsegment_array == coarse_subsegment] = False
+        dilate(~raw_mask, n_iterations=(2 if is_left_or_right == "left" else 1), out=dilated_mask)
+        np.invert(dilated_mask, out=dilated_mask)
+        pad = self.geodata.pad_width
+        dilated_mask[:pad, :] = True
+        dilated_mask[:, :pad] = True
+        dilated_mask[-pad:, :] = True
+        dilated_mask[:, -pad:] = True
+        return get_bbox(~dilated_mask)
+
+    def pass2(self, hsl_method="traced"):
+        """mapping.py:388-560, per coarse subsegment: its dilated mask and
+        crop, the channel threshold from the crop's dslt pdf (clamped as
+        ``mapping.subsegment_channel_threshold`` does), fine channels and
+        segments, the hillslope lengths and their statistics, then the merge
+        of the subsegment's lengths and flags into the ROI grids.
+
+        The reference measures the lengths by fast marching (skfmm, absent
+        here).  Its own alternative, kept in the same method but switched
+        off, measures them along streamlines from the midslopes
+        (``select_subsegments``, ``measure_hsl_traced``, ``parse_hsl``,
+        ``remap_hsl``); that is the ``"traced"`` method, the only one here.
+        Needs ``pass1`` and an ``analysis`` (``estimate_channel_threshold``)."""
+        import pandas as pd
+        if hsl_method != "traced":
+            raise NotImplementedError("hsl_method {!r}: fast marching needs skfmm, which is not available "
+                                      "here; use 'traced'".format(hsl_method))
+        vprint(self.vprogress, "\n**Pass#2 begin**")
+        self.vbackup = getattr(self.state, "verbose", False)
+        pad = self.geodata.pad_width
+        nxp = self.geodata.roi_nx + pad * 2
+        nyp = self.geodata.roi_ny + pad * 2
+        pixel_size = self.geodata.roi_pixel_size
+        self.state.add_active_mask({"merged_coarse": self.merged_coarse_mask_array})
+        raw_mask_array = np.zeros((nxp, nyp), dtype=bool)
+        dilated_mask_array = np.zeros((nxp, nyp), dtype=bool)
+        merged_mask_array = np.zeros((nxp, nyp), dtype=bool)
+        self.hsl_array = np.zeros((nxp, nyp), dtype=np.float32)
+        self.hsl_mean_array = np.array([], dtype=np.float32)
+        self.hsl_stats_df = None
+        for idx, coarse_subsegment in enumerate(self.coarse_subsegments_list_array):
+            if idx > 0:
+                merged_mask_array.fill(False)
+            self.state.reset_active_masks()
+            is_left_or_right = "left" if coarse_subsegment < 0 else "right"
+            bbox, nxb, nyb = self.make_coarse_subsegment_masks(coarse_subsegment, is_left_or_right,
+                                                               raw_mask_array, dilated_mask_array)
+            info = Info(self.state, self.trace, pixel_size, mapping=self, coarse_label=coarse_subsegment)
+            info.set_xy(nxb, nyb, pad)
+            self.state.add_active_mask({"dilated_segment": dilated_mask_array})
+            self.state.merge_active_masks(out=merged_mask_array)
+            data = Data(info=info, bbox=bbox, pad=pad, mapping_array=self.mapping_array,
+                        mask_array=merged_mask_array, uv_array=self.preprocess.uv_array,
+                        slc_array=self.trace.slc_array, slt_array=self.trace.slt_array,
+                        sla_array=self.trace.sla_array)
+            t = self.analysis.estimate_channel_threshold(data, verbose=self.vbackup)
+            if t is None or t > self.max_channel_threshold:
+                t = self.guess_channel_threshold
+            elif t < self.min_channel_threshold:
+                t = self.guess_channel_threshold / 2
+            data.channel_threshold = t
+            info.set_thresholds(channel_threshold=data.channel_threshold,
+                                segmentation_threshold=self.fine_segmentation_threshold)
+            if not M.map_channels_segments(self.cl_state, info, data, verbose=self.verbose, runner=self._runner()):
+                del data
+                continue
+            # this pass's channel heads are remembered as WAS_CHANNELHEAD
+            data.mapping_array[(data.mapping_array & info.is_channelhead) == info.is_channelhead] \
+                |= info.was_channelhead
+            self.select_subsegments(info, data)
+            if not self.measure_hsl_traced(info, data) or not self.parse_hsl(info, data) \
+                    or not self.remap_hsl(info, data):
+                del data
+                continue
+            self.hsl_mean_array = np.append(self.hsl_mean_array, data.trace_mean_hsl)
+            keep = data.hsl_stats_df[(data.hsl_stats_df["count"] > 1) & (data.hsl_stats_df["mean [m]"] > 5.0)]
+            self.hsl_stats_df = keep.copy() if self.hsl_stats_df is None else pd.concat([self.hsl_stats_df, keep])
+            self.state.remove_active_mask("dilated_segment")
+            self.state.add_active_mask({"raw_segment": raw_mask_array})
+            self.state.merge_active_masks(out=merged_mask_array)
+            bounds = data.bounds_grid
+            data.hsl_array[np.isnan(data.hsl_array)] = 0.0
+            self.hsl_array[bounds][~merged_mask_array[bounds]] = data.hsl_array[~merged_mask_array[bounds]]
+            self.mapping_array[bounds][~merged_mask_array[bounds]] |= data.mapping_array[~merged_mask_array[bounds]]
+            self.state.remove_active_mask("raw_segment")
+            del data
+        self.hsl_array[np.isnan(self.hsl_array)] = 0.0
+        vprint(self.vprogress, "\n**Pass#2 end**")
 
     def pass3(self):
         raise NotImplementedError("pass 3 filters pass 2's hillslope lengths (mapping.py:562-625)")

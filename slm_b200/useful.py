@@ -190,6 +190,12 @@ def get_bbox(array):
     return (x_min, x_max, y_min, y_max), (x_max + 1 - x_min), (y_max + 1 - y_min)
 
 
+def dilate(array, n_iterations=1, out=None):
+    """Binary dilation with the 8-neighbour structure (useful.py:573-591)."""
+    from scipy.ndimage import binary_dilation, generate_binary_structure
+    return binary_dilation(array, structure=generate_binary_structure(2, 2), iterations=n_iterations, output=out)
+
+
 def vprint(verbose, *args, **kwargs):
     if verbose:
         print(*args, **kwargs, flush=True)

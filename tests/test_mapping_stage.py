@@ -151,3 +151,107 @@ def test_traced_hillslope_length_helpers_match_reference(reference_dir, seed):
     assert md.hsl_stats_df.equals(rd.hsl_stats_df)
     assert np.array_equal(md.hsl_array, rd.hsl_array) and md.trace_mean_hsl == rd.trace_mean_hsl
     assert len(md.hsl_stats_df) > 3 and md.hsl_array.any()
+
+
+class ActiveMasks:
+    """The reference State's active-mask bookkeeping (state.py:374-459)."""
+
+    def __init__(self, dtm_mask, **params):
+        self.__dict__.update(params)
+        self.verbose = False
+        self.active_masks_dict = {"dtm": dtm_mask.copy()}
+
+    def add_active_mask(self, item):
+        if list(item.keys())[0] not in self.active_masks_dict:
+            self.active_masks_dict.update(item)
+
+    def remove_active_mask(self, name):
+        self.active_masks_dict.pop(name, None)
+
+    def reset_active_masks(self):
+        self.active_masks_dict = {k: v for k, v in self.active_masks_dict.items() if k in ("dtm", "basin", "uv")}
+
+    def merge_active_masks(self, out=None):
+        for k, m in enumerate(self.active_masks_dict.values()):
+            if k == 0:
+                if out is None:
+                    out = m.copy()
+                else:
+                    np.copyto(out, m)
+            else:
+                out |= m
+        return out
+
+
+def test_pass2_traced_matches_reference(reference_dir, monkeypatch):
+    """Pass 2 with the lengths traced along streamlines, against the
+    reference's pass2 with its fast-marching measurement swapped for its own
+    traced-length methods (the alternative it keeps switched off).  Kernels on
+    the oracle; channel thresholds from the same Analysis on a CPU stand-in KDE."""
+    import pandas as pd
+
+    from slm_b200 import analysis as A
+    from test_analysis_stage import fake_bivariate, fake_univariate
+    monkeypatch.setattr(A.kde, "estimate_univariate_pdf", fake_univariate)
+    monkeypatch.setattr(A.kde, "estimate_bivariate_pdf", fake_bivariate)
+    if not hasattr(pd.DataFrame, "append"):  # the reference's DataFrame.append (pandas < 2)
+        monkeypatch.setattr(pd.DataFrame, "append", lambda self, other: pd.concat([self, other]), raising=False)
+    R = _reference_mapping_module(reference_dir)
+    R.lengths.hsl = lambda cl_state, info, data, do_use_ridges, verbose=False: M.hsl(
+        cl_state, info, data, do_use_ridges, verbose, runner=oracle_runner)
+
+    class Info(R.Info):  # NumPy 1.x widened int32 + 2**31 to int64; NumPy 2 raises instead
+        def __init__(self, *a, **k):
+            super().__init__(*a, **k)
+            self.left_flank_addition = np.int64(self.left_flank_addition)
+    R.Info = Info
+    n = 64
+    info0, data0 = incised_pipeline_case(n=n, seed=3, n_incisions=6, max_steps=200)
+    slt, slc = data0.slt_array, data0.slc_array
+    with np.errstate(divide="ignore", invalid="ignore"):
+        sla = np.where(slc > 0, np.sqrt(2.0) * slt / slc, 0.0).astype(np.float32)
+    d = default_parameters()
+    trace = types.SimpleNamespace(**vars(d.trace))
+    trace.subpixel_seed_point_density, trace.jitter_magnitude = 1, 0.0
+    trace.integrator_step_factor, trace.max_length = 0.1, 20.0
+    trace.slc_array, trace.slt_array, trace.sla_array = slc, slt, sla
+    geodata = types.SimpleNamespace(roi_nx=n, roi_ny=n, pad_width=2, roi_pixel_size=2.0)
+    preprocess = types.SimpleNamespace(uv_array=data0.uv_array)
+    params = dict(vars(d.mapping))
+    params.update(coarse_channel_threshold=float(info0.channel_threshold), coarse_segmentation_threshold=40,
+                  fine_segmentation_threshold=10, do_map_channels_segments=True, do_map_hsl=True,
+                  midslope_filter_sigma=2.0, midslope_threshold=0.2, ridge_filter_sigma=2.0, ridge_threshold=0.3,
+                  do_measure_hsl_from_ridges=False, n_hsl_averaging_threshold=1, hsl_averaging_threshold=5.0,
+                  min_channel_threshold=1.0, max_channel_threshold=1000.0, guess_channel_threshold=30.0)
+    # log limits low enough that every subsegment has data (with none, the
+    # reference's distribution raises and its pass 2 stops)
+    analysis_params = {"analysis": dict(A.ANALYSIS_PARAMETERS, n_hist_bins=512, n_pdf_points=64,
+                                        pdf_slt_min=1e-3, pdf_sla_min=1e-3, pdf_slc_min=1e-3)}
+
+    ref_state = ActiveMasks(data0.mask_array, **vars(d.state))
+    ref = R.Mapping.__new__(R.Mapping)
+    ref.__dict__.update(params)
+    ref.__dict__.update(state=ref_state, geodata=geodata, preprocess=preprocess, trace=trace, cl_state=None,
+                        verbose=False, vprogress=False, vbackup=False, print=lambda *a, **k: None,
+                        analysis=A.Analysis(ref_state, analysis_params, geodata, None, trace))
+    ref.select_subsegments = lambda info, data, do_restrict=True: R.Mapping.select_subsegments(ref, info, data)
+
+    def traced(info, data):
+        data.fmm_mean_hsl = 0.0
+        return R.Mapping.measure_hsl_traced(ref, info, data)
+    ref.measure_hsl_fmm = traced
+    ref.remap_hsl = lambda info, data, n_hsl_averaging_threshold=None: R.Mapping.remap_hsl(ref, info, data)
+    ref.pass1()
+    ref.pass2()
+
+    my_state = ActiveMasks(data0.mask_array, **vars(d.state))
+    mine = Mapping(my_state, {"mapping": params}, geodata, preprocess, trace,
+                   analysis=A.Analysis(my_state, analysis_params, geodata, None, trace), runner=oracle_runner,
+                   thin=zhang_suen)
+    mine.pass1()
+    mine.pass2()
+    assert mine.n_coarse_subsegments == ref.n_coarse_subsegments > 1
+    assert np.array_equal(mine.mapping_array, ref.mapping_array)
+    assert np.array_equal(mine.hsl_array, ref.hsl_array) and mine.hsl_array.any()
+    assert np.array_equal(mine.hsl_mean_array, ref.hsl_mean_array) and mine.hsl_mean_array.size > 0
+    assert mine.hsl_stats_df.equals(ref.hsl_stats_df)
