@@ -282,4 +282,5 @@ class Mapping:
         vprint(self.vprogress, "\n**Pass#2 end**")
 
     def pass3(self):
-        raise NotImplementedError("pass 3 filters pass 2's hillslope lengths (mapping.py:562-625)")
+        raise NotImplementedError("pass 3 smooths the hillslope lengths and the aspect with scikit-image's rank "
+                                  "mean / median filters (mapping.py:562-1050), which are not available here")
