@@ -4,32 +4,54 @@
 One step = the reference's Trace stage on one synthetic DTM: record the
 trajectory-seed subsample down and up (Trajectories), then trace every pixel's
 d*d jittered sub-pixel trajectories down and up accumulating slc/slt
-(Fields).  Default workload: 2048^2 @ 2 m, d=2, jitter +-0.5 px, RK4, step
-0.1 px, max 10000 steps (16.8 M field trajectories per direction).
+(Fields).  Default workload: the 8192^2 DTM @ 1 m (fBm mountains, an alluvial
+cone of slope 0.03 with +-0.3 m radial ridges, 5000 unfilled pits), d=2,
+jitter +-0.5 px, RK4, step 0.1 px, max 20000 steps: 268 M field trajectories
+per direction.
 
-  value  steps/s with inputs resident in HBM (CUDA events around each step;
-         a 256 MiB buffer is written between steps to flush L2)
+  value  steps/s of the fastest shipped form (both directions in one
+         persistent launch, seeds in spatial queue order, the trajectory
+         recorder beside it) with inputs resident in HBM: CUDA events around
+         each step; the inputs exceed L2 and a 256 MiB buffer is written
+         between steps
+  arms   the field trace in other forms, on identical fields, both
+         directions: `plain` is the reference's form (one thread per
+         trajectory, one launch per direction, the reference's shuffled
+         order); `plain_learned` that kernel in the learned scheduler's order;
+         `pair_spatial` the value's form; `pair_learned_spatial` and
+         `pair_learned` the persistent pair launch in learned orders.  The
+         learned arms' time includes inference and ordering.  The model is
+         trained here, on the GPU, on step counts the tracer records on a
+         held-out DTM of the same family (another seed).
   e2e    the same metric through the public API (Trajectories + Fields) with
          the inputs in pinned host memory and the results read back per step
-  roofline  the field kernel: algorithmic bytes per RK step (RK2 75 B, RK4
-         139 B) x steps / kernel time, against the measured HBM copy peak
-  cpu_baseline  the reference's CPU path timed on this host's cores on a
-         bounded stride of the same seeds
-  scheduler  learned length scheduler vs the unsorted order (plain and
-         persistent field kernels, both directions, identical fields checked):
-         a BF16 CNN trained here on step counts recorded on a held-out DTM of
-         the same family; inference + ordering inside the learned arms' time
+  roofline  the field kernel is issue-bound: warp instructions per RK step
+         (profiles/k_fields_pair_fan4096_rk4.md) x this launch's steps / its
+         CUDA-event time, against 148 SMs x 4 schedulers x the sampled SM
+         clock.  Beside it: the algorithmic bytes (RK2 75 B, RK4 139 B per
+         step) against the measured HBM copy peak; the profiled launch's DRAM
+         and L2 bytes per RK step, scaled to this launch's steps; and an L2
+         copy peak measured here
+  cpu_baseline  the reference's CPU path on this host's cores, over a fixed
+         stride of the shuffled seed list
+  parity  the GPU traces that same strided seed list of the full-size DTM:
+         slc/slt must equal the oracle's C restatement (this workload's
+         integrator) bit for bit, and, with RK2 on the same DTM, the
+         reference's own kernel compiled for the host (low 32 bits, which is
+         what the reference keeps)
 
-N>1 (torchrun): the field seeds are split into contiguous ranges per rank,
+N>1 (torchrun): the tracer's queue is dealt to the ranks in chunks of 64 queue
+positions, round robin, so every rank sweeps the whole grid in spatial order;
 each rank accumulates its own uint64 slc/slt, then one NCCL all-reduce (sum)
 combines them (integer sums: identical to one GPU).  Total work is fixed
 (strong scaling).
 
 `--impl reference` times the reference's own CPU implementation instead
-(rank 0 only): the reference's OpenCL C kernels compiled for the host
-(oracle/_ref) with OpenMP on all cores when the workload uses the
-reference's RK2, else (RK4 has no counterpart in the reference) the oracle's
-C restatement.
+(rank 0 only) on the same config: the oracle's C restatement of the RK4
+workloads (RK4 has no counterpart in the reference), with the reference's
+own kernels compiled for the host (oracle/_ref) timed on RK2 of the same DTM
+beside it.  That process builds the seed list with NumPy, as the reference
+does, and loads none of this repository's libraries.
 """
 from __future__ import annotations
 
@@ -47,10 +69,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path[:0] = [ROOT, os.path.join(ROOT, "oracle")]
 
 BYTES_PER_STEP = {2: 75, 4: 139}
-# dram__bytes_read.sum + dram__bytes_write.sum of one field launch, from an
-# ncu capture of this bench's own workload (spatial seed order), keyed by
-# (workload, both directions in one launch); null for workloads without one
-TRAFFIC_PER_LAUNCH = {("incised2048", False): 211.9e6, ("incised2048", True): 418.0e6}
+N_SMS, SCHEDULERS_PER_SM = 148, 4
+FIELD_PROFILE = os.path.join(ROOT, "profiles", "k_fields_pair_fan4096_rk4.md")
+METRIC = "trajectory steps/s (trace+fields)"
 
 
 def _peaks():
@@ -60,6 +81,19 @@ def _peaks():
         return float(pk["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def field_profile():
+    """Per-RK-step counters of one profiled k_fields_pair launch: the
+    ``per_rk_step:`` JSON line of the ncu summary in profiles/, or None."""
+    try:
+        with open(FIELD_PROFILE) as fp:
+            for ln in fp:
+                if ln.startswith("per_rk_step:"):
+                    return json.loads(ln.split(":", 1)[1])
+    except (OSError, ValueError):
+        pass
+    return None
 
 
 class ClockSampler:
@@ -126,7 +160,16 @@ def _dist():
     return ws, rank, local
 
 
-def _cpu_sample(wl, stride, sign, cores):
+def workload_config(wl):
+    """The ``config`` of both arms' lines: the workload alone."""
+    spec = wl.spec
+    return {"workload": spec.name, "key": wl.key,
+            "trajectories_per_direction": int(wl.info.n_seed_points) * spec.density ** 2,
+            "trajectory_seeds": int(wl.n_traj),
+            "l2": "inputs larger than L2; 256 MiB buffer written between timed steps"}
+
+
+def _cpu_sample(wl, stride, sign, cores, integrator=None):
     """Fields pass over every stride-th shuffled seed on the host cores.
 
     The sampled seeds form their own list (their RNG streams follow their
@@ -136,7 +179,7 @@ def _cpu_sample(wl, stride, sign, cores):
     Returns (steps, seconds, kind)."""
     import oracle as O
     from slm_b200 import params as P
-    integ = wl.spec.integrator
+    integ = integrator or wl.spec.integrator
     sub = np.ascontiguousarray(wl.seeds[::stride])
     prm = P.kernel_params(wl.info, "INTEGRATE_FIELDS", sign)
     prm.n_seed_points = sub.shape[0]
@@ -150,11 +193,17 @@ def _cpu_sample(wl, stride, sign, cores):
     return steps, t, "port"
 
 
-def _cpu_stride(wl, cores, target_s):
+def _cpu_stride(wl, cores, target_s, integrator=None):
     n = int(wl.info.n_seed_points)
     probe = max(1, n // 512)
-    _, t, _ = _cpu_sample(wl, probe, 1.0, cores)
+    _, t, _ = _cpu_sample(wl, probe, 1.0, cores, integrator)
     return max(1, int(probe * max(t, 1e-3) / target_s))
+
+
+def _sample_text(wl, stride):
+    n = int(wl.info.n_seed_points)
+    return "every {}th shuffled seed ({} of {} seeds, {} sub-pixel trajectories each)".format(
+        stride, (n + stride - 1) // stride, n, wl.spec.density ** 2)
 
 
 def run_reference(args):
@@ -163,7 +212,9 @@ def run_reference(args):
     if rank != 0:
         return 0
     from slm_b200.workloads import Workload
-    wl = Workload(args.workload)
+    # the seed list the reference's way (NumPy's shuffle): no library of this
+    # repository is loaded in this process
+    wl = Workload(args.workload, seed_list="numpy")
     cores = os.cpu_count() or 1
     stride = _cpu_stride(wl, cores, 3.0)
     for _ in range(args.warmup):
@@ -175,20 +226,112 @@ def run_reference(args):
             tot_steps += s
             tot_t += t
     v = tot_steps / tot_t
-    sample = "fields down+up over every {}th shuffled seed ({} of {} seeds)".format(
-        stride, (int(wl.info.n_seed_points) + stride - 1) // stride, int(wl.info.n_seed_points))
+    sample = "fields down+up over " + _sample_text(wl, stride)
+    what = ("the reference's integrate_fields kernel compiled for the host" if kind == "reference"
+            else "the oracle's C restatement (RK{} has no counterpart in the reference)".format(
+                wl.spec.integrator))
     line = {
-        "impl": "reference", "metric": "trajectory steps/s (trace+fields)", "value": v,
+        "impl": "reference", "metric": METRIC, "value": v,
         "unit": "steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * tot_t / max(args.steps, 1), "higher_is_better": True,
-        "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": wl.spec.name, "sample": sample},
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded DTM; no dataset)",
+        "config": workload_config(wl),
         "cpu_baseline": {"value": v, "unit": "steps/s", "cores": cores, "kind": kind,
-                         "sample": sample},
+                         "sample": sample, "what": what},
         "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if wl.spec.integrator != 2:
+        # the reference's own kernel, on RK2 over the same DTM and seed list
+        try:
+            import oracle as O
+            if not O.ref_available("integrate_fields"):
+                raise FileNotFoundError("oracle/_ref was not built")
+            s2 = _cpu_stride(wl, cores, 3.0, integrator=2)
+            st, tt = 0, 0.0
+            for sign in (1.0, -1.0):
+                s, t, k2 = _cpu_sample(wl, s2, sign, cores, integrator=2)
+                st += s
+                tt += t
+            line["rk2_reference"] = {"value": st / tt, "unit": "steps/s", "cores": cores, "kind": k2,
+                                     "sample": "RK2 fields down+up over " + _sample_text(wl, s2),
+                                     "what": "the reference's integrate_fields kernel compiled for the host"}
+        except Exception as e:  # noqa: BLE001 -- reported in the line
+            line["rk2_reference"] = {"unavailable": str(e)}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def l2_copy_peak(dev, mib=24, launches=200):
+    """Read + write bandwidth of an elementwise copy whose two buffers
+    (2 x ``mib`` MiB) stay resident in L2: a CUDA graph of ``launches``
+    copies, timed with CUDA events.  GB/s."""
+    import torch
+    a = torch.ones(mib << 18, dtype=torch.float32, device=dev)
+    b = torch.empty_like(a)
+    side = torch.cuda.Stream(device=dev)
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for _ in range(3):
+            torch.neg(a, out=b)
+    torch.cuda.current_stream().wait_stream(side)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        for _ in range(launches):
+            torch.neg(a, out=b)
+    g.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    g.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3
+    del g
+    return 2.0 * a.numel() * 4 * launches / t / 1e9
+
+
+def roofline_block(integrator, pair, steps_per_launch, t_launch, clocks, l2_peak):
+    """The field kernel's roofline: issue rate first (what binds), then
+    algorithmic bytes, DRAM traffic and L2 bytes."""
+    hbm_peak, peak_kind = _peaks()
+    bps = BYTES_PER_STEP[integrator]
+    alg = steps_per_launch * bps
+    kernel = "k_fields_pair<{}>".format(integrator) if pair else "k_fields_persistent<{}>".format(integrator)
+    hbm = {"achieved": alg / t_launch / 1e9, "peak": hbm_peak, "unit": "GB/s",
+           "frac": alg / t_launch / 1e9 / hbm_peak, "peak_source": peak_kind,
+           "bytes_per_step": bps, "algorithmic_bytes_per_launch": alg}
+    prof = field_profile()
+    out = {"kernel": kernel, "launch_ms": 1e3 * t_launch, "rk_steps_per_launch": steps_per_launch}
+    if prof is not None and int(prof.get("integrator", 0)) == integrator:
+        mhz = clocks.get("sm_mhz") or prof.get("sm_mhz") or 1965.0
+        peak_issue = N_SMS * SCHEDULERS_PER_SM * mhz * 1e6
+        inst = prof["warp_inst"] * steps_per_launch / t_launch
+        traffic = prof["dram_bytes"] * steps_per_launch
+        out.update({"bound": "issue", "achieved": inst, "peak": peak_issue, "unit": "warp-inst/s",
+                    "frac": inst / peak_issue, "traffic": traffic,
+                    "peak_note": "148 SMs x 4 warp schedulers x median sampled SM clock ({:.0f} MHz)".format(mhz),
+                    "source": "warp instructions, DRAM and L2 bytes per RK step of one profiled launch "
+                              "({}: {}), scaled by this launch's RK steps".format(
+                                  os.path.relpath(FIELD_PROFILE, ROOT), prof.get("case", "")),
+                    "thread_inst_per_step": prof.get("thread_inst"),
+                    "hbm_algorithmic": hbm,
+                    "dram": {"achieved": traffic / t_launch / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                             "frac": traffic / t_launch / 1e9 / hbm_peak,
+                             "bytes_per_step": prof["dram_bytes"]}})
+        if prof.get("lts_bytes"):
+            l2 = prof["lts_bytes"] * steps_per_launch / t_launch / 1e9
+            out["l2"] = {"achieved": l2, "peak": l2_peak, "unit": "GB/s",
+                         "frac": l2 / l2_peak if l2_peak else None, "bytes_per_step": prof["lts_bytes"],
+                         "peak_note": "elementwise copy of 2 x 24 MiB resident in L2, measured in this run",
+                         "ncu_pct_of_peak": prof.get("lts_pct_of_peak")}
+    else:
+        out.update({"bound": "hbm", "achieved": hbm["achieved"], "peak": hbm_peak, "unit": "GB/s",
+                    "frac": hbm["frac"], "traffic": None, "peak_source": peak_kind,
+                    "note": "no profile of this integrator's launch: algorithmic bytes against the HBM peak"})
+        out["hbm_algorithmic"] = hbm
+    return out
 
 
 def run_b200(args):
@@ -224,9 +367,15 @@ def run_b200(args):
     length_d = torch.zeros((2, n_traj), dtype=torch.float32, device=dev)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
 
-    from slm_b200.distributed import allreduce_counts, shard_params
-    field_prm = [shard_params(kernel_params(info, "INTEGRATE_FIELDS", s), rank, ws)
-                 for s in (1.0, -1.0)]
+    from slm_b200.distributed import allreduce_counts, shard_positions, shard_queue_params
+    field_prm = [kernel_params(info, "INTEGRATE_FIELDS", s) for s in (1.0, -1.0)]
+    queue_d = None
+    if ws > 1:
+        # this rank's dealt share of the queue: chunks of 64 queue positions,
+        # round robin over the ranks
+        mine = torch.from_numpy(shard_positions(n_seeds, rank, ws)).to(dev)
+        field_prm = [shard_queue_params(p, int(mine.numel())) for p in field_prm]
+        queue_d = mine.to(torch.int32).view(torch.uint32).contiguous()
     tinfo = wl.fresh_info()
     tinfo.n_seed_points = n_traj
     traj_prm = [kernel_params(tinfo, "INTEGRATE_TRAJECTORY", np.float32(s)) for s in (1.0, -1.0)]
@@ -258,17 +407,22 @@ def run_b200(args):
             ev[0].record(stream)
         if spatial:
             spatial_order(seeds_d, n_seeds, info.nx, info.ny, out=order_d, bins=bins_d)
+        queue = order_d if spatial else None
+        if queue_d is not None:
+            if spatial:
+                torch.index_select(order_d.view(torch.int32), 0, mine, out=queue_d.view(torch.int32))
+            queue = queue_d
         if pair:
             # acc[d, k]: rows of the [slc|slt] arrays; upstream 2*nxy further
             kernels.integrate_fields_pair(field_prm[0], field_prm[1], seeds_d, mask_d, uv_d, acc[:, 0],
                                           acc[:, 1], work[0], integrator=integrator,
                                           block_threads=args.block_threads, blocks_per_sm=args.blocks_per_sm,
-                                          chunk=args.chunk, order=order_d if spatial else None)
+                                          chunk=args.chunk, order=queue)
         else:
             for d in range(2):
                 kernels.integrate_fields(field_prm[d], seeds_d, mask_d, uv_d, acc[d, 0], acc[d, 1],
                                          work[d], schedule=args.schedule, integrator=integrator,
-                                         order=order_d if spatial else None)
+                                         order=queue)
         if ev is not None:
             ev[1].record(stream)
         for join in joins:
@@ -281,6 +435,8 @@ def run_b200(args):
         t = int(nsteps_d.to(torch.int32).sum().item())
         return f, t
 
+    for w in work:
+        w.zero_()
     for _ in range(args.warmup):
         device_step()
     torch.cuda.synchronize()
@@ -316,50 +472,39 @@ def run_b200(args):
     steps_per_step = field_steps + traj_steps
     value = steps_per_step * args.steps / step_t
     ms = 1e3 * step_t / args.steps
-
-    # e2e through the public API (pinned host inputs, results back on the host)
-    e2e = None
-    if ws == 1 and not args.no_e2e:
-        e2e = run_e2e(args, wl, dev)
-
-    peak, peak_kind = _peaks()
-    bps = BYTES_PER_STEP[integrator]
-    achieved = field_steps_rank * args.steps * bps / kern_t / 1e9
+    clk = clocks.summary()
+    launches_per_step = 1 if pair else 2
+    l2_peak = l2_copy_peak(dev) if ws == 1 else None
     line = {
-        "metric": "trajectory steps/s (trace+fields)", "value": value, "unit": "steps/s",
+        "metric": METRIC, "value": value, "unit": "steps/s",
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded DTM; no dataset)",
-        "config": {"workload": spec.name, "schedule": args.schedule,
-                   "seed_order": "spatial (64 px blocks, ordered inside the timed step)"
-                   if spatial else "shuffled (the reference's)",
-                   "directions": "one launch for both" if pair else "one launch each",
-                   "launch": {"block_threads": args.block_threads, "blocks_per_sm": args.blocks_per_sm,
-                              "chunk": args.chunk},
-                   "field_trajectories_per_direction": n_seeds * spec.density ** 2,
-                   "trajectory_seeds": n_traj, "l2": "256 MiB buffer written between steps",
-                   "mpx_per_s": wl.n_pixels / (step_t / args.steps) / 1e6,
-                   "rk_steps_per_step": steps_per_step,
-                   "parallelism": "seed shards + NCCL all-reduce" if ws > 1 else "1 GPU"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak,
-                     "traffic": TRAFFIC_PER_LAUNCH.get((args.workload, pair)) if spatial else None,
-                     "algorithmic_bytes_per_launch": field_steps_rank * bps / (1 if pair else 2),
-                     "peak_source": peak_kind,
-                     "kernel": "k_fields_pair<{}>".format(integrator) if pair
-                     else "k_fields_{}<{}>".format(args.schedule, integrator),
-                     "bytes_per_step": bps},
-        "clocks": clocks.summary(),
-        "gpu_launches": args.steps * ((3 if spatial else 0) + 2 + (1 if pair else 2)),
+        "config": workload_config(wl),
+        "form": {"schedule": args.schedule,
+                 "seed_order": "spatial (64 px blocks, ordered inside the timed step)"
+                 if spatial else "shuffled (the reference's)",
+                 "directions": "one launch for both" if pair else "one launch each",
+                 "launch": {"block_threads": args.block_threads, "blocks_per_sm": args.blocks_per_sm,
+                            "chunk": args.chunk},
+                 "trajectory_recorder": "{} seeds down and up on side streams".format(n_traj),
+                 "parallelism": "dealt seed shards + NCCL all-reduce" if ws > 1 else "1 GPU"},
+        "mpx_per_s": wl.n_pixels / (step_t / args.steps) / 1e6,
+        "rk_steps_per_step": steps_per_step,
+        "field_rk_steps_per_step": field_steps,
+        "roofline": roofline_block(integrator, pair, field_steps_rank // launches_per_step,
+                                   kern_t / args.steps / launches_per_step, clk, l2_peak),
+        "clocks": clk,
+        "gpu_launches": args.steps * ((3 if spatial else 0) + 2 + launches_per_step),
     }
-    if e2e is not None:
-        line["e2e"] = e2e
     if ws == 1 and not args.no_sched:
-        line["scheduler"] = sched_compare(args, wl, dev, seeds_d, mask_d, uv_d, field_prm, flush)
+        line["arms"] = arms_compare(args, wl, dev, seeds_d, mask_d, uv_d, field_prm, flush)
+    if ws == 1 and not args.no_e2e:
+        line["e2e"] = run_e2e(args, wl, dev)
     if ws == 1 and args.stages:
         line["stages"] = run_stages(args, wl, dev)
     if rank == 0 and not args.no_cpu and ws == 1:
-        line["cpu_baseline"] = cpu_baseline(wl, args)
+        line["cpu_baseline"], line["parity"] = cpu_and_parity(wl, args, dev, mask_d, uv_d)
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -373,12 +518,31 @@ def SPECS_NAME(key):
     return SPECS[key].name
 
 
-def sched_compare(args, wl, dev, seeds_d, mask_d, uv_d, field_prm, flush):
-    """Learned length scheduler against the unsorted order, for the plain
-    (one thread per trajectory) and persistent field kernels, on identical
-    trajectories.  The model is trained here, on the GPU, on step counts the
+ARMS_DEFAULT = "plain,plain_learned,pair_spatial,pair_learned_spatial,pair_learned"
+ARMS_ALL = ("plain", "plain_learned", "plain_spatial", "pair_shuffled", "pair_spatial",
+            "pair_learned", "pair_learned_spatial")
+
+
+def arms_compare(args, wl, dev, seeds_d, mask_d, uv_d, field_prm, flush):
+    """The field trace of both directions in several forms on identical
+    trajectories (the fields of every arm must equal the first arm's):
+
+      plain                 k_fields_plain, one launch per direction, the
+                            reference's shuffled order: the reference's form
+      plain_learned         k_fields_plain, each direction in the learned
+                            order (longest predicted first)
+      plain_spatial         k_fields_plain, spatial order
+      pair_shuffled         k_fields_pair (both directions, one persistent
+                            launch), shuffled order
+      pair_spatial          k_fields_pair, spatial order (the value's form)
+      pair_learned          k_fields_pair, each direction longest predicted
+                            first
+      pair_learned_spatial  k_fields_pair, each direction's predicted-long
+                            class first, then spatial order
+
+    The length model is trained here, on the GPU, on the step counts the
     tracer records on a held-out DTM of the same family (another seed); the
-    learned arms' timed region includes inference and ordering."""
+    learned arms' time includes inference and ordering."""
     import torch
 
     from slm_b200 import kernels, scheduler as S
@@ -388,6 +552,11 @@ def sched_compare(args, wl, dev, seeds_d, mask_d, uv_d, field_prm, flush):
     spec = wl.spec
     d = spec.density
     from slm_b200.params import kernel_params
+    arm_names = [a for a in args.arms.split(",") if a]
+    for a in arm_names:
+        if a not in ARMS_ALL:
+            raise ValueError("unknown arm " + a)
+    learned = any("learned" in a for a in arm_names)
 
     def recorded(w):
         """(uv, seeds, targets [n][2]) of workload w on the device."""
@@ -402,76 +571,81 @@ def sched_compare(args, wl, dev, seeds_d, mask_d, uv_d, field_prm, flush):
             cols.append(S.step_targets(st, n_w, w.spec.density))
         return w.uv, w.seeds[:n_w], torch.stack(cols, 1).contiguous()
 
-    if args.workload == "incised4096_d4":
-        # 40 seeded 512^2 DTMs of the same family, 4x4 seeds: 10.5 M pairs.
-        # Their uv grids are stacked along x with an 8 px edge-replicated
-        # margin each, so a patch clamps exactly as on its own grid.
-        train_keys = [("incised512_d4", 100 + i) for i in range(40)]
-        held_keys = [("incised512_d4", 200 + i) for i in range(4)]
-    else:
-        train_keys = [(args.workload, args.sched_train_seed)]
-        held_keys = []
-    grids, seed_sets, tsets = [], [], []
-    xoff = 0
-    for key, seed in train_keys:
-        g_uv, g_seeds, g_t = recorded(Workload(key, seed=seed))
-        m = 8 if len(train_keys) > 1 else 0
-        grids.append(np.pad(g_uv, ((m, m), (m, m), (0, 0)), mode="edge"))
-        seed_sets.append(g_seeds + np.array([xoff + m, m], np.float32))
-        tsets.append(g_t)
-        xoff += grids[-1].shape[0]
-    tr_uv = torch.from_numpy(np.ascontiguousarray(np.concatenate(grids, 0))).to(dev)
-    tr_seeds = torch.from_numpy(np.ascontiguousarray(np.concatenate(seed_sets, 0))).to(dev)
-    targets = torch.cat(tsets, 0).contiguous()
-    del grids, seed_sets, tsets
-    n_tr = int(targets.shape[0])
-    # "predicted long" class of the learned+spatial order: the top 1% of the
-    # training targets
-    g = torch.Generator(device=dev)
-    g.manual_seed(0)
-    sub = targets[torch.randint(0, n_tr, (min(n_tr, 1 << 20),), device=dev, generator=g)]
-    long_thr = [float(torch.quantile(sub[:, c], 0.99)) for c in (0, 1)]
-    model = S.LengthModel(dev, seed=0)
-    torch.cuda.synchronize()
-    t1 = time.time()
-    hist = model.fit(tr_uv, tr_uv.shape[0], tr_uv.shape[1], 2, tr_seeds, targets,
-                     steps=args.sched_train_steps, batch=4096)
-    torch.cuda.synchronize()
-    t_train = time.time() - t1
-    del tr_seeds, tr_uv, targets
-
     n = int(wl.info.n_seed_points)
     nxp, nyp = uv_d.shape[0], uv_d.shape[1]
-    pred = model.predict(uv_d, nxp, nyp, 2, seeds_d, n)
+    out = {"arms": arm_names, "ms": {}}
+    model = pred = None
+    long_thr = None
+    if learned:
+        if args.workload == "incised4096_d4":
+            # 40 seeded 512^2 DTMs of the same family, 4x4 seeds: 10.5 M pairs.
+            # Their uv grids are stacked along x with an 8 px edge-replicated
+            # margin each, so a patch clamps exactly as on its own grid.
+            train_keys = [("incised512_d4", 100 + i) for i in range(40)]
+            held_keys = [("incised512_d4", 200 + i) for i in range(4)]
+        else:
+            train_keys = [(args.workload, args.sched_train_seed)]
+            held_keys = []
+        grids, seed_sets, tsets = [], [], []
+        xoff = 0
+        for key, seed in train_keys:
+            g_uv, g_seeds, g_t = recorded(Workload(key, seed=seed))
+            m = 8 if len(train_keys) > 1 else 0
+            grids.append(np.pad(g_uv, ((m, m), (m, m), (0, 0)), mode="edge"))
+            seed_sets.append(g_seeds + np.array([xoff + m, m], np.float32))
+            tsets.append(g_t)
+            xoff += grids[-1].shape[0]
+        tr_uv = torch.from_numpy(np.ascontiguousarray(np.concatenate(grids, 0))).to(dev)
+        tr_seeds = torch.from_numpy(np.ascontiguousarray(np.concatenate(seed_sets, 0))).to(dev)
+        targets = torch.cat(tsets, 0).contiguous()
+        del grids, seed_sets, tsets
+        n_tr = int(targets.shape[0])
+        # "predicted long" class of the learned+spatial order: the top 1% of
+        # the training targets
+        g = torch.Generator(device=dev)
+        g.manual_seed(0)
+        sub = targets[torch.randint(0, n_tr, (min(n_tr, 1 << 20),), device=dev, generator=g)]
+        long_thr = [float(torch.quantile(sub[:, c], 0.99)) for c in (0, 1)]
+        model = S.LengthModel(dev, seed=0)
+        torch.cuda.synchronize()
+        t1 = time.time()
+        hist = model.fit(tr_uv, tr_uv.shape[0], tr_uv.shape[1], 2, tr_seeds, targets,
+                         steps=args.sched_train_steps, batch=4096)
+        torch.cuda.synchronize()
+        t_train = time.time() - t1
+        del tr_seeds, tr_uv, targets
+        pred = model.predict(uv_d, nxp, nyp, 2, seeds_d, n)
 
-    # held-out prediction error against the step counts the tracer records
-    def error_of(p_all, truth_all):
-        rank = lambda x: torch.argsort(torch.argsort(x)).double()
-        out_e = {}
-        for col in (0, 1):
-            p, truth = p_all[:, col], truth_all[:, col]
-            rho = float(torch.corrcoef(torch.stack([rank(p), rank(truth)]))[0, 1])
-            out_e["down" if col == 0 else "up"] = {
-                "mae_log_steps": float((p - truth).abs().mean()), "spearman": rho}
-        return out_e
+        def error_of(p_all, truth_all):
+            rank = lambda x: torch.argsort(torch.argsort(x)).double()
+            out_e = {}
+            for col in (0, 1):
+                p, truth = p_all[:, col], truth_all[:, col]
+                rho = float(torch.corrcoef(torch.stack([rank(p), rank(truth)]))[0, 1])
+                out_e["down" if col == 0 else "up"] = {
+                    "mae_log_steps": float((p - truth).abs().mean()), "spearman": rho}
+            return out_e
 
-    held = {}
-    for key, seed in held_keys:
-        h_uv, h_seeds, h_t = recorded(Workload(key, seed=seed))
-        hu, hs = torch.from_numpy(h_uv).to(dev), torch.from_numpy(np.ascontiguousarray(h_seeds)).to(dev)
-        hp = model.predict(hu, hu.shape[0], hu.shape[1], 2, hs, int(hs.shape[0]))
-        held["{} seed {}".format(key, seed)] = error_of(hp, h_t)
-    err = {}
-    for col in (0, 1):
-        st = S.record_steps(field_prm[col], seeds_d, mask_d, uv_d, integrator=spec.integrator)
-        truth = S.step_targets(st, n, d)
-        p = pred[:, col]
-        rank = lambda x: torch.argsort(torch.argsort(x)).double()
-        rp, rt = rank(p), rank(truth)
-        rho = float(torch.corrcoef(torch.stack([rp, rt]))[0, 1])
-        err["down" if col == 0 else "up"] = {
-            "mae_log_steps": float((p - truth).abs().mean()), "spearman": rho}
-        del st, truth, rp, rt
+        held = {}
+        for key, seed in held_keys:
+            h_uv, h_seeds, h_t = recorded(Workload(key, seed=seed))
+            hu = torch.from_numpy(h_uv).to(dev)
+            hs = torch.from_numpy(np.ascontiguousarray(h_seeds)).to(dev)
+            hp = model.predict(hu, hu.shape[0], hu.shape[1], 2, hs, int(hs.shape[0]))
+            held["{} seed {}".format(key, seed)] = error_of(hp, h_t)
+        truth = torch.stack([S.step_targets(S.record_steps(field_prm[c], seeds_d, mask_d, uv_d,
+                                                           integrator=spec.integrator), n, d)
+                             for c in (0, 1)], 1)
+        trained_on = ("40 x {} (seeds 100..139)".format(SPECS_NAME("incised512_d4"))
+                      if args.workload == "incised4096_d4"
+                      else "{} (seed {})".format(spec.name, args.sched_train_seed))
+        out.update({"trained_on": trained_on, "held_out_dtms": held,
+                    "train_pairs": n_tr, "train_steps": args.sched_train_steps, "train_batch": 4096,
+                    "train_s": t_train, "prep_s": t1 - t0,
+                    "loss_first": float(np.mean(hist[:10])), "loss_last": float(np.mean(hist[-50:])),
+                    "held_out_error": error_of(pred, truth),
+                    "long_class_threshold_log_steps": long_thr})
+        del truth
     cap = S.log_cap(field_prm[0])
     orders = [torch.empty(n, dtype=torch.uint32, device=dev) for _ in range(2)]
     bins = torch.empty(S.N_BINS, dtype=torch.uint32, device=dev)
@@ -479,71 +653,78 @@ def sched_compare(args, wl, dev, seeds_d, mask_d, uv_d, field_prm, flush):
     acc = torch.zeros((2, 2, nxy), dtype=torch.uint64, device=dev)
     work = [kernels.workspace(dev) for _ in range(2)]
     stream = torch.cuda.current_stream()
-
     sbins = torch.empty(int(kernels._lib.load().slm_order_spatial_bins(
         int(wl.info.nx), int(wl.info.ny), S.SPATIAL_BLOCK, 1)), dtype=torch.uint32, device=dev)
-
     visit = torch.empty(n, dtype=torch.uint32, device=dev)
+    nx, ny = wl.info.nx, wl.info.ny
 
-    def arm(schedule, mode):
+    def arm(name):
         acc.zero_()
-        if mode in ("learned", "learned_spatial"):
+        for w in work:
+            w.zero_()
+        if "learned" in name:
             # inference visits the seeds in spatial order (patch locality)
-            S.spatial_order(seeds_d, n, wl.info.nx, wl.info.ny, out=visit, bins=sbins)
+            S.spatial_order(seeds_d, n, nx, ny, out=visit, bins=sbins)
             model.predict(uv_d, nxp, nyp, 2, seeds_d, n, out=pred, visit=visit)
-        for col in (0, 1):
-            if mode == "learned":
+        if name.endswith("_learned"):
+            for col in (0, 1):
                 model.order(pred, col, cap, out=orders[col], bins=bins)
-            elif mode == "learned_spatial":
-                S.spatial_order(seeds_d, n, wl.info.nx, wl.info.ny, pred=pred, col=col,
-                                threshold=long_thr[col], out=orders[col], bins=sbins)
-        if mode == "spatial":
-            S.spatial_order(seeds_d, n, wl.info.nx, wl.info.ny, out=orders[0], bins=sbins)
-        for col in (0, 1):
-            work[col].zero_()
-            o = None if mode == "shuffled" else orders[0 if mode == "spatial" else col]
-            kernels.integrate_fields(field_prm[col], seeds_d, mask_d, uv_d, acc[col, 0], acc[col, 1],
-                                     work[col], schedule=schedule, integrator=spec.integrator,
-                                     order=o)
+        elif name.endswith("_learned_spatial"):
+            for col in (0, 1):
+                S.spatial_order(seeds_d, n, nx, ny, pred=pred, col=col, threshold=long_thr[col],
+                                out=orders[col], bins=sbins)
+        elif name.endswith("_spatial"):
+            S.spatial_order(seeds_d, n, nx, ny, out=orders[0], bins=sbins)
+        if name in ("plain", "pair_shuffled"):
+            o_dn = o_up = None
+        elif "learned" in name:
+            o_dn, o_up = orders[0], orders[1]
+        else:
+            o_dn = o_up = orders[0]
+        if name.startswith("plain"):
+            for col, o in ((0, o_dn), (1, o_up)):
+                kernels.integrate_fields(field_prm[col], seeds_d, mask_d, uv_d, acc[col, 0], acc[col, 1],
+                                         work[col], schedule="plain", integrator=spec.integrator, order=o)
+        else:
+            kernels.integrate_fields_pair(field_prm[0], field_prm[1], seeds_d, mask_d, uv_d, acc[:, 0],
+                                          acc[:, 1], work[0], integrator=spec.integrator, order=o_dn,
+                                          order_up=o_up)
 
-    trained_on = ("40 x {} (seeds 100..139)".format(SPECS_NAME("incised512_d4"))
-                  if args.workload == "incised4096_d4" else "{} (seed {})".format(spec.name, args.sched_train_seed))
-    out = {"trained_on": trained_on, "held_out_dtms": held,
-           "train_pairs": n_tr, "train_steps": args.sched_train_steps, "train_batch": 4096,
-           "train_s": t_train, "prep_s": t1 - t0,
-           "loss_first": float(np.mean(hist[:10])), "loss_last": float(np.mean(hist[-50:])),
-           "held_out_error": err, "ms": {}}
     ref = None
-    arms = [("plain", "shuffled"), ("plain", "learned"), ("plain", "spatial"),
-            ("persistent", "shuffled"), ("persistent", "learned"), ("persistent", "spatial"),
-            ("persistent", "learned_spatial")]
-    for schedule, mode in arms:
-        arm(schedule, mode)
+    for name in arm_names:
+        arm(name)
         torch.cuda.synchronize()
         res = (acc.clone(), int(work[0][1].item()) + int(work[1][1].item()))
         if ref is None:
             ref = res
         elif not (torch.equal(res[0], ref[0]) and res[1] == ref[1]):
-            raise RuntimeError("scheduled trace differs from the unsorted one")
+            raise RuntimeError("the {} arm's fields differ from the {} arm's".format(name, arm_names[0]))
         ts = []
-        for _ in range(args.sched_reps):
+        for _ in range(args.arm_reps):
             flush.fill_(1)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             torch.cuda.synchronize()
             e0.record(stream)
-            arm(schedule, mode)
+            arm(name)
             e1.record(stream)
             torch.cuda.synchronize()
             ts.append(e0.elapsed_time(e1))
-        out["ms"][schedule + ("" if mode == "shuffled" else "_" + mode)] = float(np.median(ts))
+        out["ms"][name] = float(np.median(ts))
     f_steps = ref[1]
     out["field_steps"] = f_steps
     out["steps_per_s"] = {k: f_steps / (v / 1e3) for k, v in out["ms"].items()}
-    out["learned_vs_plain"] = out["ms"]["plain"] / out["ms"]["plain_learned"]
-    out["persistent_learned_vs_plain"] = out["ms"]["plain"] / out["ms"]["persistent_learned"]
-    out["persistent_learned_spatial_vs_plain"] = out["ms"]["plain"] / out["ms"]["persistent_learned_spatial"]
-    out["long_class_threshold_log_steps"] = long_thr
+    if "plain" in out["ms"]:
+        out["vs_plain"] = {k: out["ms"]["plain"] / v for k, v in out["ms"].items() if k != "plain"}
+    learned_ms = {k: v for k, v in out["ms"].items() if "learned" in k}
+    if learned_ms and "plain" in out["ms"]:
+        best = min(learned_ms, key=learned_ms.get)
+        out["learned_vs_plain"] = {"arm": best, "speedup": out["ms"]["plain"] / learned_ms[best]}
+    if learned_ms and "pair_spatial" in out["ms"]:
+        best = min(learned_ms, key=learned_ms.get)
+        out["learned_vs_pair_spatial"] = {"arm": best,
+                                          "speedup": out["ms"]["pair_spatial"] / learned_ms[best]}
     out["identical_fields"] = True
+    out["l2"] = "256 MiB buffer written before each timed run"
     return out
 
 
@@ -937,36 +1118,128 @@ def run_e2e(args, wl, dev):
 
     step()
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    k = max(1, args.e2e_steps)
+    times = []
     n = 0
-    k = max(1, min(args.steps, 3))
     for _ in range(k):
+        t0 = time.perf_counter()
         n += step()
-    torch.cuda.synchronize()
-    t = time.perf_counter() - t0
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    t = float(np.sum(times))
     nxy = wl.mask.size
-    h2d = wl.uv.nbytes * 2 + wl.mask.nbytes * 2 + wl.seeds.nbytes + wl.traj_seeds.nbytes
-    # finished slc (float64), slt and sla (float32) per direction, the
+    n_seeds = int(wl.info.n_seed_points)
+    # up: uv and mask for each stage, each stage's swap partners of the seed
+    # shuffle (uint32 per seed; the lists themselves are built on the
+    # device), the trajectory seeds
+    h2d = wl.uv.nbytes * 2 + wl.mask.nbytes * 2 + 4 * n_seeds * 2 + wl.traj_seeds.nbytes
+    # down: finished slc (float64), slt and sla (float32) per direction, the
+    # field seed list (data.seed_point_array) and the trajectory seeds, the
     # trajectory step counts and lengths (recorded steps come back as well,
     # up to each trajectory's length)
-    d2h = nxy * 2 * (8 + 4 + 4) + wl.n_traj * 2 * (2 + 4)
+    d2h = nxy * 2 * (8 + 4 + 4) + wl.seeds.nbytes + wl.traj_seeds.nbytes + wl.n_traj * 2 * (2 + 4)
     return {"value": n / t, "unit": "steps/s", "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "steps": k,
+            "ms_per_step": 1e3 * t / k, "ms_min_max": [1e3 * min(times), 1e3 * max(times)],
             "mpx_per_s": wl.n_pixels * k / t / 1e6,
             "note": "Trajectories.integrate + Fields.integrate through the public API: seed "
-                    "creation and shuffle, uploads, tracing, the fields' post-processing (on the "
-                    "GPU) and the finished arrays copied back, every step"}
+                    "creation and shuffle (swap partners drawn on the host, swaps on the GPU), "
+                    "uploads, tracing, the fields' post-processing (on the GPU), the seed list and "
+                    "the finished arrays copied back, every step"}
 
 
-def cpu_baseline(wl, args):
-    """The reference's CPU path on a bounded seed stride (same metric, ~10 s)."""
+def _trace_sub(prm, sub_d, mask_d, uv_d, integrator, dev):
+    """Both directions of the seed list ``sub_d`` in one pair launch; returns
+    (acc [2][2][nxy] uint64 on the host: direction, slc|slt; RK steps)."""
+    import torch
+
+    from slm_b200 import kernels
+    nxy = int(prm[0].nxy_padded)
+    acc = torch.zeros((2, 2, nxy), dtype=torch.uint64, device=dev)
+    work = kernels.workspace(dev)
+    kernels.integrate_fields_pair(prm[0], prm[1], sub_d, mask_d, uv_d, acc[:, 0], acc[:, 1], work,
+                                  integrator=integrator)
+    torch.cuda.synchronize()
+    return acc.cpu().numpy(), int(work[1].item())
+
+
+def cpu_and_parity(wl, args, dev, mask_d, uv_d):
+    """The reference's CPU path on a fixed stride of the shuffled seed list
+    (the baseline), and the GPU's fields on that same list compared with the
+    CPU's (parity at the workload's full DTM size).
+
+    * restatement: both directions with the workload's integrator, the
+      oracle's C restatement against one pair launch, slc and slt bit for bit
+      (uint64) and the RK step count;
+    * reference RK2: the same DTM with RK2, the reference's own
+      integrate_fields kernel compiled for the host against the pair launch
+      on a 4x sparser stride; the reference keeps uint32 sums, so the GPU's
+      low 32 bits are compared."""
+    import torch
+
+    import oracle as O
+    from slm_b200.params import kernel_params
     cores = os.cpu_count() or 1
-    stride = _cpu_stride(wl, cores, 10.0)
-    steps, t, kind = _cpu_sample(wl, stride, 1.0, cores)
     n = int(wl.info.n_seed_points)
-    return {"value": steps / t, "unit": "steps/s", "cores": cores, "kind": kind,
-            "sample": "downstream fields over every {}th shuffled seed ({} of {} seeds), {:.1f} s".format(
-                stride, (n + stride - 1) // stride, n, t)}
+    integ = wl.spec.integrator
+    stride = wl.spec.cpu_stride or _cpu_stride(wl, cores, 10.0)
+
+    def params_for(m):
+        prm = [kernel_params(wl.info, "INTEGRATE_FIELDS", s) for s in (1.0, -1.0)]
+        for p in prm:
+            p.n_seed_points = m
+        return prm
+
+    sub = np.ascontiguousarray(wl.seeds[::stride])
+    prm = params_for(sub.shape[0])
+    cpu, t_dir = [], []
+    for p in prm:
+        t0 = time.perf_counter()
+        cpu.append(O.integrate_fields(p, sub, wl.mask, wl.uv, integ, n_threads=cores))
+        t_dir.append(time.perf_counter() - t0)
+    base_steps, base_t, kind = cpu[0][2], t_dir[0], "port"
+    if integ == 2 and O.ref_available("integrate_fields"):
+        t0 = time.perf_counter()
+        O.ref_integrate_fields(prm[0], sub, wl.mask, wl.uv, n_threads=cores)
+        base_t, kind = time.perf_counter() - t0, "reference"
+    baseline = {"value": base_steps / base_t, "unit": "steps/s", "cores": cores, "kind": kind,
+                "sample": "downstream fields over {}, {:.1f} s".format(_sample_text(wl, stride), base_t)}
+
+    sub_d = torch.from_numpy(sub).to(dev)
+    g, g_steps = _trace_sub(prm, sub_d, mask_d, uv_d, integ, dev)
+    same = all(np.array_equal(g[d, 0], cpu[d][0]) and np.array_equal(g[d, 1], cpu[d][1]) for d in (0, 1))
+    parity = {"restatement": {
+        "identical": bool(same and g_steps == cpu[0][2] + cpu[1][2]),
+        "kind": "RK{}: pair launch vs the oracle's C restatement, slc and slt uint64 bit for bit, "
+                "both directions, and the RK step count".format(integ),
+        "stride": stride, "seeds": int(sub.shape[0]), "of_seeds": n,
+        "trajectories": int(2 * sub.shape[0] * wl.spec.density ** 2), "rk_steps": g_steps,
+        "pixels_compared": int(4 * g.shape[2])}}
+    del sub_d
+    if O.ref_available("integrate_fields"):
+        s2 = stride * 4 if integ != 2 else stride
+        sub2 = np.ascontiguousarray(wl.seeds[::s2])
+        prm2 = params_for(sub2.shape[0])
+        t0 = time.perf_counter()
+        ref = [O.ref_integrate_fields(p, sub2, wl.mask, wl.uv, n_threads=cores) for p in prm2]
+        t_ref = time.perf_counter() - t0
+        sub2_d = torch.from_numpy(sub2).to(dev)
+        g2, g2_steps = _trace_sub(prm2, sub2_d, mask_d, uv_d, 2, dev)
+        low = (g2 & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+        same2 = all(np.array_equal(low[d, 0], ref[d][0]) and np.array_equal(low[d, 1], ref[d][1])
+                    for d in (0, 1))
+        parity["reference_rk2"] = {
+            "identical": bool(same2),
+            "kind": "RK2 on the same DTM: pair launch vs the reference's own integrate_fields kernel "
+                    "compiled for the host, slc and slt low 32 bits, both directions",
+            "stride": s2, "seeds": int(sub2.shape[0]), "of_seeds": n,
+            "trajectories": int(2 * sub2.shape[0] * wl.spec.density ** 2), "rk_steps": g2_steps,
+            "reference_s": t_ref, "pixels_compared": int(4 * g2.shape[2])}
+    else:
+        parity["reference_rk2"] = {"identical": None,
+                                   "unavailable": "oracle/_ref was not built (it needs the reference "
+                                                  "checkout when the library is built)"}
+    return baseline, parity
 
 
 def main():
@@ -975,11 +1248,15 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="incised2048")
+    ap.add_argument("--workload", default="fan8192")
     ap.add_argument("--schedule", default="persistent", choices=["plain", "persistent"])
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-sched", action="store_true", help="skip the learned-scheduler comparison")
+    ap.add_argument("--e2e-steps", type=int, default=10, help="public-API steps timed for e2e")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and the parity check")
+    ap.add_argument("--no-sched", action="store_true", help="skip the arms (plain / learned / spatial)")
+    ap.add_argument("--arms", default=ARMS_DEFAULT,
+                    help="comma-separated arms of the form comparison, from " + ",".join(ARMS_ALL))
+    ap.add_argument("--arm-reps", type=int, default=2, help="timed runs per arm (median)")
     ap.add_argument("--seed-order", default="spatial", choices=["spatial", "shuffled"])
     ap.add_argument("--no-pair", action="store_true", help="one field launch per direction")
     ap.add_argument("--block-threads", type=int, default=0, help="pair launch: threads per block (0: default)")
@@ -995,15 +1272,59 @@ def main():
     ap.add_argument("--retune", action="store_true", help="tiles96: ignore the autotuner cache")
     ap.add_argument("--sched-train-seed", type=int, default=12)
     ap.add_argument("--sched-train-steps", type=int, default=1500)
-    ap.add_argument("--sched-reps", type=int, default=3)
+    ap.add_argument("--profile-case", action="store_true",
+                    help="run only the field pair launch of the workload --steps times and print its "
+                         "RK steps per launch (the command profiled for the roofline counters)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.preprocess:
         return run_preprocess(args)
+    if args.profile_case:
+        return run_profile_case(args)
     if args.workload == "tiles96":
         return run_batched(args)
     return run_b200(args)
+
+
+def run_profile_case(args):
+    """The field pair launch alone (spatial order), --warmup + --steps times,
+    for an ncu capture of one launch; prints RK steps per launch and the
+    CUDA-event time of the last launch."""
+    import torch
+
+    from slm_b200 import kernels
+    from slm_b200.params import kernel_params
+    from slm_b200.scheduler import spatial_order
+    from slm_b200.workloads import Workload
+    dev = torch.device("cuda", 0)
+    wl = Workload(args.workload)
+    info = wl.info
+    n = int(info.n_seed_points)
+    nxy = int(info.nx_padded * info.ny_padded)
+    seeds_d = torch.from_numpy(wl.seeds).to(dev)
+    mask_d = torch.from_numpy(wl.mask.view(np.uint8)).to(dev)
+    uv_d = torch.from_numpy(wl.uv).to(dev)
+    acc = torch.zeros((2, 2, nxy), dtype=torch.uint64, device=dev)
+    work = kernels.workspace(dev)
+    prm = [kernel_params(info, "INTEGRATE_FIELDS", s) for s in (1.0, -1.0)]
+    order = spatial_order(seeds_d, n, info.nx, info.ny)
+    steps, ms = [], []
+    for _ in range(args.warmup + args.steps):
+        acc.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        kernels.integrate_fields_pair(prm[0], prm[1], seeds_d, mask_d, uv_d, acc[:, 0], acc[:, 1], work,
+                                      integrator=wl.spec.integrator, order=order)
+        e1.record()
+        torch.cuda.synchronize()
+        steps.append(int(work[1].item()))
+        ms.append(e0.elapsed_time(e1))
+    print(json.dumps({"profile_case": wl.key, "workload": wl.spec.name, "launches": len(steps),
+                      "rk_steps_per_launch": steps[-1], "steps_identical": len(set(steps)) == 1,
+                      "ms": ms, "device_bytes": int(seeds_d.nbytes + mask_d.nbytes + uv_d.nbytes
+                                                    + acc.nbytes + order.nbytes)}), flush=True)
+    return 0
 
 
 if __name__ == "__main__":

@@ -154,11 +154,12 @@ int slm_integrate_fields_scheduled(const slm_params* p, const slm_launch* launch
  * (>= nxy_padded), each direction's equal to slm_integrate_fields of that
  * direction; workspace words 1, 2 count both directions' steps and
  * trajectories, word 3 the upstream direction's steps; seed_order as in
- * slm_integrate_fields_scheduled (shared by both directions). */
+ * slm_integrate_fields_scheduled for the downstream queue; seed_order_up the
+ * upstream queue's order (NULL: seed_order serves both directions). */
 int slm_integrate_fields_pair(const slm_params* p_down, const slm_params* p_up, const slm_launch* launch,
                               const float* seed_point, const uint8_t* mask, const float* uv, uint64_t* slc,
                               uint64_t* slt, uint64_t up_stride, uint64_t* workspace,
-                              const uint32_t* seed_order, void* stream);
+                              const uint32_t* seed_order, const uint32_t* seed_order_up, void* stream);
 
 /* slm_integrate_fields_batched -- no counterpart in the reference (which
  * launches integrate_fields once per grid).  Traces every tile of a batch in
@@ -459,6 +460,28 @@ int slm_order_spatial(const float* seed_point, uint32_t n, uint32_t nx, uint32_t
 int slm_create_seeds(const uint8_t* mask, uint32_t nx_padded, uint32_t ny_padded, uint32_t pad, int do_shuffle,
                      uint32_t rng_seed, float* seed_point, uint64_t capacity, uint64_t* n_seeds,
                      uint32_t* generator_state);
+
+/* slm_create_seeds_device -- the seed list of slm_create_seeds (the same
+ * rows in the same order, and the same generator state), built in DEVICE
+ * memory: argwhere by the order-preserving compaction of slm_pick_seeds; the
+ * swap partners drawn on the host with the same generator; the Fisher-Yates
+ * swaps applied on the device in reservation rounds (a swap runs once it is
+ * the earliest pending swap on both of its rows), which replaces the host's
+ * random-access pass over the rows.  Replaces create_seeds
+ * (python/streamlines/useful.py:470-517) for callers that trace on the GPU.
+ *   mask        DEVICE [nx_padded][ny_padded] uint8 (nonzero = masked)
+ *   seed_point  DEVICE [capacity][2] float32, 8-byte aligned
+ *   n_seeds     host: the number of unmasked pixels (also on SLM_ERR_CAPACITY)
+ *   generator_state  host [625] or NULL, as slm_create_seeds
+ *   workspace   DEVICE, 256-byte aligned, slm_create_seeds_device_workspace
+ *               (nx_padded * ny_padded) bytes
+ * Synchronises the stream (it reads back the row count and, per round, the
+ * number of swaps still pending). */
+size_t slm_create_seeds_device_workspace(uint64_t n_pixels);
+int slm_create_seeds_device(const uint8_t* mask, uint32_t nx_padded, uint32_t ny_padded, uint32_t pad,
+                            int do_shuffle, uint32_t rng_seed, float* seed_point, uint64_t capacity,
+                            uint64_t* n_seeds, uint32_t* generator_state, void* workspace,
+                            size_t workspace_bytes, void* stream);
 
 /* ---------------------------------------------------------------- preprocess
  * The conditioned gradient vector field of a DTM region of interest

@@ -27,7 +27,10 @@ int n_threads)``: it runs work-items ``offset .. offset+n_global-1`` of the
 kernel, sequentially in ascending global id when ``n_threads == 1`` (the
 pinned schedule) or with OpenMP otherwise, and ``slmref_P``.
 
-Usage: python oracle/build_ref.py [--reference /root/reference] [--jobs N]
+The reference checkout is ``$SLM_REFERENCE`` when set, else ``reference/``
+beside this repository's folder (``REFERENCE`` below).
+
+Usage: python oracle/build_ref.py [--reference DIR] [--jobs N]
 """
 from __future__ import annotations
 
@@ -41,6 +44,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
+# the reference checkout: $SLM_REFERENCE, else a "reference" folder beside the repository
+REFERENCE = os.environ.get("SLM_REFERENCE") or os.path.join(
+    os.path.dirname(os.path.dirname(HERE)), "reference")
 sys.path.insert(0, os.path.dirname(HERE))
 from slm_b200.params import FIELDS  # noqa: E402
 
@@ -190,7 +196,7 @@ def build_one(kernel, reference, force=False):
     return kernel, "built"
 
 
-def build_all(reference="/root/reference", jobs=8, force=False, only=None):
+def build_all(reference=REFERENCE, jobs=8, force=False, only=None):
     if not os.path.isdir(os.path.join(reference, "opencl")):
         raise FileNotFoundError("reference checkout not found at {}".format(reference))
     names = [k for k in KERNELS if only is None or k.split("__")[0] in only or k in only]
@@ -200,7 +206,7 @@ def build_all(reference="/root/reference", jobs=8, force=False, only=None):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("SLM_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=REFERENCE)
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)
     ap.add_argument("--force", action="store_true")
     ap.add_argument("kernels", nargs="*")

@@ -66,6 +66,8 @@ def lib():
             u32, i32, u64 = ctypes.c_uint32, ctypes.c_int, ctypes.c_uint64
             L.oracle_integrate_fields.restype = u64
             L.oracle_integrate_fields.argtypes = [P, i32, P, u32, u32, u32, P, P, P, P, P, i32]
+            L.oracle_field_seed_steps.restype = None
+            L.oracle_field_seed_steps.argtypes = [P, i32, P, P, P, P, P, P, i32]
             L.oracle_integrate_trajectory.restype = u64
             L.oracle_integrate_trajectory.argtypes = [P, i32, u32, P, P, P, P, P, P, i32]
             for name in ("oracle_histogram_univariate", "oracle_histogram_bivariate"):
@@ -117,6 +119,19 @@ def integrate_fields(params, seeds, mask, uv, integrator=2, seed_begin=0, seed_e
         _ptr(mask), _ptr(uv), _ptr(slc), _ptr(slt),
         ctypes.cast(ctypes.byref(ntraj), ctypes.c_void_p), n_threads)
     return slc, slt, int(steps), int(ntraj.value)
+
+
+def field_seed_steps(params, seeds, mask, uv, integrator=2, n_threads=1):
+    """Per-seed RK step counts (uint32 [n_seed_points], the sum over each seed's
+    d*d trajectories) of a field pass of the restatement."""
+    seeds, mask, uv = _grid_inputs(seeds, mask, uv)
+    nxy = params.nxy_padded
+    slc = np.zeros(nxy, dtype=np.uint64)
+    slt = np.zeros(nxy, dtype=np.uint64)
+    out = np.zeros(int(params.n_seed_points), dtype=np.uint32)
+    lib().oracle_field_seed_steps(_params_ptr(params), integrator, _ptr(seeds), _ptr(mask), _ptr(uv),
+                                  _ptr(slc), _ptr(slt), _ptr(out), n_threads)
+    return out
 
 
 def integrate_trajectory(params, n_chunk, seeds, mask, uv, integrator=2, n_threads=1):

@@ -257,6 +257,34 @@ uint64_t oracle_integrate_fields(const slm_params* p, int integrator,
     return steps;
 }
 
+/* Per-seed RK step counts of a field pass (the sum over the seed's d*d
+ * trajectories) -- the per-seed load a seed shard carries; slc/slt receive
+ * the pass's sums as in oracle_integrate_fields. */
+void oracle_field_seed_steps(const slm_params* p, int integrator, const float* seed_point,
+                             const uint8_t* mask, const float* uv, uint64_t* slc, uint64_t* slt,
+                             uint32_t* seed_steps, int n_threads) {
+    const int rk4 = integrator == SLM_RK4;
+    const uint32_t d = p->subpixel_seed_point_density;
+    const long n = (long)p->n_seed_points;
+    const int atomic = n_threads > 1;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(n_threads > 1 ? n_threads : 1)
+    for (long it = 0; it < n; ++it) {
+        const uint32_t seed_idx = (uint32_t)it;
+        const uint32_t rng0 = seed_rng(seed_idx);
+        const v2 c = {seed_point[2 * (size_t)seed_idx], seed_point[2 * (size_t)seed_idx + 1]};
+        uint64_t steps = 0;
+        for (uint32_t j = 0; j < d; ++j) {
+            for (uint32_t i = 0; i < d; ++i) {
+                v2 s0;
+                s0.x = c.x + ((float)i * p->subpixel_seed_step - p->subpixel_seed_halfspan);
+                s0.y = c.y + ((float)j * p->subpixel_seed_step - p->subpixel_seed_halfspan);
+                steps += field_trajectory(s0, rng0, rk4, mask, uv, slc, slt, p, atomic);
+            }
+        }
+        seed_steps[seed_idx] = (uint32_t)steps;
+    }
+}
+
 static inline float edge_dt(float x, float u) {
     float dt = 0.0f;
     const float right = ((float)(int32_t)(x + 1.5f) - (x + 0.5f)) / u;

@@ -64,7 +64,7 @@ SIGNATURES = {
     "slm_integrate_fields": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_integrate_fields_noalloc": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_integrate_fields_scheduled": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
-    "slm_integrate_fields_pair": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, ctypes.c_uint64, _P, _P, _P]),
+    "slm_integrate_fields_pair": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, ctypes.c_uint64, _P, _P, _P, _P]),
     "slm_integrate_fields_batched": (ctypes.c_int, [_P, _P, _P, _U, _U, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_fields_finish": (ctypes.c_int, [_P, _U, _U, ctypes.c_double, ctypes.c_double, _I, _P, _U, _P, _P,
                                          _P, _P]),
@@ -93,6 +93,9 @@ SIGNATURES = {
     "slm_hillslope_lengths": (ctypes.c_int, [_P, _U, _P, _P, _P, _P, _P, _P, _P]),
     "slm_thin": (ctypes.c_int, [_P, _P, _U, _U, _U, _P, _P, _P]),
     "slm_create_seeds": (ctypes.c_int, [_P, _U, _U, _U, ctypes.c_int, _U, _P, ctypes.c_uint64, _P, _P]),
+    "slm_create_seeds_device_workspace": (ctypes.c_size_t, [ctypes.c_uint64]),
+    "slm_create_seeds_device": (ctypes.c_int, [_P, _U, _U, _U, ctypes.c_int, _U, _P, ctypes.c_uint64, _P, _P,
+                                               _P, ctypes.c_size_t, _P]),
     "slm_preprocess": (ctypes.c_int, [_P, ctypes.c_int, _U, _U, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "slm_pick_seeds_workspace": (ctypes.c_size_t, [_U]),
     "slm_pick_seeds": (ctypes.c_int, [_P, _P, _U, _I, _U, _U, _U, _P, _U, _P, _P, ctypes.c_size_t, _P]),

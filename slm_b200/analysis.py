@@ -25,52 +25,94 @@ from .useful import vprint
 AVAILABLE_KERNELS = ["tophat", "triangle", "epanechnikov", "cosine", "gaussian"]
 
 
+def _data_limits(a, lo, hi):
+    """The log-space limits of ``a`` where not given: its extremes above
+    float32's lowest value (the "no data" marker of the log arrays)."""
+    if lo is None or hi is None:
+        valid = a[a > np.finfo(np.float32).min]
+        lo = valid.min() if lo is None else lo
+        hi = valid.max() if hi is None else hi
+    return lo, hi
+
+
+def _set_in_order(obj, table):
+    """Evaluate a (name, derivation) attribute table on ``obj`` in order."""
+    for name, derive in table:
+        setattr(obj, name, derive(obj))
+
+
+# What the KDE stage and its consumers read from a univariate distribution,
+# and how each value follows from the selected data (the reference's
+# analysis.py:665-717 derives the same values).  Evaluated in order on the
+# object; ``logx_data`` (the selected log data, one column) is set first.
+#   read by the histogram / pdf kernels (kde.estimate_univariate_pdf):
+#     logx_data, n_data, logx_min, logx_range, n_hist_bins, n_pdf_points,
+#     bin_dx, pdf_dx, and the unused y axis (zeros) of the shared parameter set
+#   read by the consumers (cdf, statistics, find_modes, locate_threshold):
+#     logx_vec, x_vec, bin_dx, search_cdf_min / max
+_UNIVARIATE_TABLE = (
+    ("logx_min", lambda d: np.min(d.logx_data)),          # the data's, not the selection limits
+    ("logx_max", lambda d: np.max(d.logx_data)),
+    ("logx_range", lambda d: d.logx_max - d.logx_min),
+    ("logy_min", lambda d: 0.0),
+    ("logy_max", lambda d: 0.0),
+    ("logy_range", lambda d: 0.0),
+    ("n_data", lambda d: d.logx_data.shape[0]),
+    ("bin_dx", lambda d: d.logx_range / d.n_hist_bins),
+    ("pdf_dx", lambda d: d.logx_range / d.n_pdf_points),
+    ("bin_dy", lambda d: 0.0),
+    ("pdf_dy", lambda d: 0.0),
+    ("logx_vec", lambda d: np.linspace(d.logx_min, d.logx_max, d.n_pdf_points).reshape((d.n_pdf_points, 1))),
+    ("logx_vec_histogram", lambda d: np.linspace(d.logx_min, d.logx_max,
+                                                 d.n_hist_bins).reshape((d.n_hist_bins, 1))),
+    ("x_vec", lambda d: np.exp(d.logx_vec)),
+    ("dlogx", lambda d: d.logx_vec[1] - d.logx_vec[0]),
+)
+
+# The same for a bivariate distribution (the reference's analysis.py:
+# 859-900).  ``logxy_data`` (float32 rows of the selected (x, y) pairs) and
+# the four limits (given, or the data's extremes) are set first.
+#   read by the histogram / rows / cols kernels (kde.estimate_bivariate_pdf):
+#     logxy_data, n_data, logx_min, logy_min, the ranges, n_hist_bins,
+#     n_pdf_points, bin_dx / bin_dy, pdf_dx / pdf_dy
+#   read by the consumers (cdf, find_mode): bin_dx, x_mesh, y_mesh
+_BIVARIATE_TABLE = (
+    ("logx_range", lambda d: d.logx_max - d.logx_min),
+    ("logy_range", lambda d: d.logy_max - d.logy_min),
+    ("n_data", lambda d: d.logxy_data.shape[0]),
+    ("bin_dx", lambda d: d.logx_range / d.n_hist_bins),
+    ("pdf_dx", lambda d: d.logx_range / d.n_pdf_points),
+    ("bin_dy", lambda d: d.logy_range / d.n_hist_bins),
+    ("pdf_dy", lambda d: d.logy_range / d.n_pdf_points),
+    ("x_mesh", lambda d: np.exp(d.logx_mesh)),
+    ("y_mesh", lambda d: np.exp(d.logy_mesh)),
+)
+
+# constructor arguments kept as attributes unchanged
+_PASSED_THROUGH = ("pixel_size", "cl_src_path", "cl_platform", "cl_device", "debug", "verbose", "gpu_verbose")
+
+
 class Univariate_distribution:
+    """Log-space data of one quantity and the KDE of it (the reference's
+    streamlines.analysis.Univariate_distribution, OpenCL method).  The
+    selection keeps the x values whose (x, y) pair lies inside the limits;
+    the derived attributes follow ``_UNIVARIATE_TABLE``."""
+
     def __init__(self, logx_array=None, logy_array=None, pixel_size=None, method="opencl",
                  n_hist_bins=2048, n_pdf_points=256, search_cdf_min=0.95, search_cdf_max=0.99,
                  logx_min=None, logy_min=None, logx_max=None, logy_max=None,
                  cl_src_path=None, cl_platform=None, cl_device=None, debug=False,
                  verbose=False, gpu_verbose=False):
-        fmin = np.finfo(np.float32).min
-        if logx_min is None:
-            logx_min = logx_array[logx_array > fmin].min()
-        if logx_max is None:
-            logx_max = logx_array[logx_array > fmin].max()
-        if logy_min is None:
-            logy_min = logy_array[logy_array > fmin].min()
-        if logy_max is None:
-            logy_max = logy_array[logy_array > fmin].max()
-        self.logx_data = logx_array[(logx_array >= logx_min) & (logx_array <= logx_max)
-                                    & (logy_array >= logy_min) & (logy_array <= logy_max)]
-        self.logx_data = self.logx_data.reshape((self.logx_data.shape[0], 1))
-        self.logx_min = np.min(self.logx_data)
-        self.logx_max = np.max(self.logx_data)
-        self.logx_range = self.logx_max - self.logx_min
-        self.logy_min = 0.0
-        self.logy_max = 0.0
-        self.logy_range = 0.0
-        self.n_data = self.logx_data.shape[0]
-        self.n_hist_bins = n_hist_bins
-        self.n_pdf_points = n_pdf_points
-        self.bin_dx = self.logx_range / self.n_hist_bins
-        self.pdf_dx = self.logx_range / self.n_pdf_points
-        self.bin_dy = 0.0
-        self.pdf_dy = 0.0
-        self.logx_vec = np.linspace(self.logx_min, self.logx_max,
-                                    self.n_pdf_points).reshape((self.n_pdf_points, 1))
-        self.logx_vec_histogram = np.linspace(self.logx_min, self.logx_max,
-                                              self.n_hist_bins).reshape((self.n_hist_bins, 1))
-        self.x_vec = np.exp(self.logx_vec)
-        self.dlogx = self.logx_vec[1] - self.logx_vec[0]
-        self.search_cdf_min = search_cdf_min
-        self.search_cdf_max = search_cdf_max
-        self.pixel_size = pixel_size
-        self.cl_src_path = cl_src_path
-        self.cl_platform = cl_platform
-        self.cl_device = cl_device
-        self.debug = debug
-        self.verbose = verbose
-        self.gpu_verbose = gpu_verbose
+        x_lo, x_hi = _data_limits(logx_array, logx_min, logx_max)
+        y_lo, y_hi = _data_limits(logy_array, logy_min, logy_max)
+        inside = (logx_array >= x_lo) & (logx_array <= x_hi) & (logy_array >= y_lo) & (logy_array <= y_hi)
+        self.logx_data = logx_array[inside].reshape((-1, 1))
+        self.n_hist_bins, self.n_pdf_points = n_hist_bins, n_pdf_points
+        self.search_cdf_min, self.search_cdf_max = search_cdf_min, search_cdf_max
+        _set_in_order(self, _UNIVARIATE_TABLE)
+        args = locals()
+        for name in _PASSED_THROUGH:
+            setattr(self, name, args[name])
 
     def compute_kde_opencl(self, kernel="epanechnikov", bandwidth=0.15):
         """Histogram + kernel smoothing on the device (analysis.py:763-786)."""
@@ -141,52 +183,32 @@ class Univariate_distribution:
 
 
 class Bivariate_distribution:
+    """Log-space (x, y) pairs and their 2-D KDE (the reference's
+    streamlines.analysis.Bivariate_distribution, OpenCL method).  The
+    selection keeps the pairs inside the limits (and outside ``mask_array``);
+    the pdf mesh spans the limits; the derived attributes follow
+    ``_BIVARIATE_TABLE``."""
+
     def __init__(self, logx_array=None, logy_array=None, mask_array=None, pixel_size=None,
                  method="opencl", n_hist_bins=2048, n_pdf_points=256, logx_min=None,
                  logy_min=None, logx_max=None, logy_max=None, cl_src_path=None,
                  cl_platform=None, cl_device=None, debug=False, verbose=False,
                  gpu_verbose=False):
-        self.logx_data = logx_array
-        self.logy_data = logy_array
-        fmin = np.finfo(np.float32).min
-        if logx_min is None:
-            logx_min = logx_array[logx_array > fmin].min()
-        if logx_max is None:
-            logx_max = logx_array[logx_array > fmin].max()
-        if logy_min is None:
-            logy_min = logy_array[logy_array > fmin].min()
-        if logy_max is None:
-            logy_max = logy_array[logy_array > fmin].max()
-        sel = ((logx_array >= logx_min) & (logx_array <= logx_max)
-               & (logy_array >= logy_min) & (logy_array <= logy_max))
+        self.logx_data, self.logy_data = logx_array, logy_array
+        self.logx_min, self.logx_max = _data_limits(logx_array, logx_min, logx_max)
+        self.logy_min, self.logy_max = _data_limits(logy_array, logy_min, logy_max)
+        inside = ((logx_array >= self.logx_min) & (logx_array <= self.logx_max)
+                  & (logy_array >= self.logy_min) & (logy_array <= self.logy_max))
         if mask_array is not None:
-            sel = sel & (~mask_array)
-        logxy_data = np.vstack([logx_array[sel], logy_array[sel]]).T
-        self.logxy_data = logxy_data.copy().astype(dtype=np.float32)
-        self.logx_mesh, self.logy_mesh = np.mgrid[logx_min:logx_max:complex(n_pdf_points),
-                                                  logy_min:logy_max:complex(n_pdf_points)]
-        self.logx_min = logx_min
-        self.logx_max = logx_max
-        self.logy_min = logy_min
-        self.logy_max = logy_max
-        self.logx_range = self.logx_max - self.logx_min
-        self.logy_range = self.logy_max - self.logy_min
-        self.n_data = self.logxy_data.shape[0]
-        self.n_hist_bins = n_hist_bins
-        self.n_pdf_points = n_pdf_points
-        self.bin_dx = self.logx_range / self.n_hist_bins
-        self.pdf_dx = self.logx_range / self.n_pdf_points
-        self.bin_dy = self.logy_range / self.n_hist_bins
-        self.pdf_dy = self.logy_range / self.n_pdf_points
-        self.x_mesh = np.exp(self.logx_mesh)
-        self.y_mesh = np.exp(self.logy_mesh)
-        self.pixel_size = pixel_size
-        self.cl_src_path = cl_src_path
-        self.cl_platform = cl_platform
-        self.cl_device = cl_device
-        self.debug = debug
-        self.verbose = verbose
-        self.gpu_verbose = gpu_verbose
+            inside &= ~mask_array
+        self.logxy_data = np.stack([logx_array[inside], logy_array[inside]], axis=1).astype(np.float32)
+        n = complex(n_pdf_points)
+        self.logx_mesh, self.logy_mesh = np.mgrid[self.logx_min:self.logx_max:n, self.logy_min:self.logy_max:n]
+        self.n_hist_bins, self.n_pdf_points = n_hist_bins, n_pdf_points
+        _set_in_order(self, _BIVARIATE_TABLE)
+        args = locals()
+        for name in _PASSED_THROUGH:
+            setattr(self, name, args[name])
 
     def compute_kde_opencl(self, kernel="epanechnikov", bandwidth=0.10):
         """Histogram + separable smoothing on the device (analysis.py:955-969)."""
@@ -300,9 +322,6 @@ ANALYSIS_PARAMETERS = {
     "do_joint_distribn_uslt_dslt": False, "do_joint_distribn_dsla_usla": False,
     "do_joint_distribn_dsla_dslc": True, "do_joint_distribn_dslt_dslc": True,
     "do_joint_distribn_usla_uslc": False, "do_joint_distribn_uslc_dslc": False,
-    "pdf_bw_method": "scott", "pdf_bw_factor_h_midline": 0.6, "pdf_bw_factor_h_all": 0.6,
-    "pdf_bw_factor_slope": 0.2, "pdf_h_min": 0, "pdf_h_max": 4000, "pdf_h_steps": 200,
-    "pdf_h_midline_max_bound": 1000, "pdf_slope_min": 0, "pdf_slope_max": 80, "pdf_slope_steps": 10,
 }
 
 # name: (x field, y field, x direction, y direction, log-limit parameters), as
@@ -331,9 +350,9 @@ class Analysis:
     statistics, channel threshold) and the joint pdfs (``jpdf_<name>``: mode)
     that the job's ``do_*`` flags select, from ``trace``'s slc/slt/sla, or
     from ``data`` when a method is given one.  Only the 'opencl' KDE method
-    exists here (on the GPU); the reference's scipy/sklearn alternatives are
-    not restated.  ``compute_elevation_slope_pdfs`` is the reference's SciPy
-    code, on the host as there."""
+    exists here (on the GPU); the reference's scipy/sklearn alternatives and
+    its elevation / slope pdfs (SciPy's gaussian_kde on the host, outside the
+    KDE path) are not restated."""
 
     def __init__(self, state, imported_parameters, geodata, preprocess, trace):
         params = dict(ANALYSIS_PARAMETERS)
@@ -370,53 +389,6 @@ class Analysis:
         except AttributeError as error:
             self.print("Failed to estimate channel threshold:", error)
             return None
-
-    def compute_elevation_slope_pdfs(self, bw_method=None, h_min=None, h_max=None, h_steps=None,
-                                     bw_factor_h_midline=None, bw_factor_h_all=None, h_midline_max_bound=None,
-                                     slope_min=None, slope_max=None, slope_steps=None, bw_factor_slope=None):
-        """analysis.py:580-657: Gaussian KDEs (SciPy, host, as the reference) of
-        the elevations of the midslope pixels and of the whole basin, and of
-        the midslope slopes (mirrored about zero), each with its bandwidth
-        scaled by a factor, evaluated on fixed grids; their maxima above the
-        given bounds.  Needs ``_augment(mapping)`` first (the mapping's
-        IS_MIDSLOPE flags), ``geodata.roi_array`` / ``basin_mask_array`` and
-        ``preprocess.slope_array``."""
-        from scipy.stats import gaussian_kde
-        pick = lambda v, k: getattr(self, k) if v is None else v  # noqa: E731
-        bw_method = pick(bw_method, "pdf_bw_method")
-        h_min, h_max, h_steps = pick(h_min, "pdf_h_min"), pick(h_max, "pdf_h_max"), pick(h_steps, "pdf_h_steps")
-        bw_factor_h_midline = pick(bw_factor_h_midline, "pdf_bw_factor_h_midline")
-        bw_factor_h_all = pick(bw_factor_h_all, "pdf_bw_factor_h_all")
-        h_midline_max_bound = pick(h_midline_max_bound, "pdf_h_midline_max_bound")
-        slope_min, slope_max = pick(slope_min, "pdf_slope_min"), pick(slope_max, "pdf_slope_max")
-        slope_steps = pick(slope_steps, "pdf_slope_steps")
-        bw_factor_slope = pick(bw_factor_slope, "pdf_bw_factor_slope")
-        m = self.mapping
-        m.midslope_array = (m.mapping_array & m.info.is_midslope).copy().astype(bool)
-        h_mid = self.geodata.roi_array[m.midslope_array[2:-2, 2:-2]].ravel()
-        h_all = self.geodata.roi_array[~self.geodata.basin_mask_array[2:-2, 2:-2]].ravel()
-        s_mid = np.abs(self.preprocess.slope_array[m.midslope_array].ravel())
-        s_mid = np.concatenate([s_mid, -s_mid])
-        h_grid = np.linspace(h_min, h_max, h_steps)
-        s_grid = np.linspace(slope_min, slope_max, (slope_max - slope_min) * slope_steps + 1)
-        kdes = []
-        for pts, factor in ((h_mid, bw_factor_h_midline), (h_all, bw_factor_h_all), (s_mid, bw_factor_slope)):
-            k = gaussian_kde(pts, bw_method=bw_method)
-            k.set_bandwidth(k.factor * factor)
-            kdes.append(k)
-        h_mid_pdf = kdes[0].evaluate(points=h_grid)
-        h_all_pdf = kdes[1].evaluate(points=h_grid)
-        s_mid_pdf = kdes[2].evaluate(points=s_grid)
-        self.h_midline_pdf_array = h_mid_pdf
-        self.h_midline_pdf_max1 = np.max(h_mid_pdf[h_grid > h_midline_max_bound])
-        self.h_midline_pdf_max1_h = h_grid[h_mid_pdf == self.h_midline_pdf_max1]
-        self.h_all_pdf_array = h_all_pdf
-        self.h_array = h_grid
-        self.h_pdf_sf = np.max(h_mid_pdf)
-        self.slope_midline_pdf_array = s_mid_pdf
-        self.slope_midline_pdf_max = np.max(s_mid_pdf[s_grid >= 10])
-        self.slope_midline_pdf_max_slope = s_grid[s_mid_pdf == self.slope_midline_pdf_max]
-        self.slope_array = s_grid
 
     def _get_limits(self, attr_list):
         return [np.log(getattr(self, a)) if hasattr(self, a) and getattr(self, a) is not None else None

@@ -192,21 +192,44 @@ __global__ void k_map_channel_heads(const slm_params p, uint32_t n, const float2
 // neighbour offsets in the reference's check order N, S, E, W, NE, SE, NW, SW
 __constant__ float c_nbr[8][2] = {{0, 1}, {0, -1}, {1, 0}, {-1, 0}, {1, 1}, {1, -1}, {-1, 1}, {-1, -1}};
 
-__global__ void k_prune_channel_heads(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
-                                      uint32_t* mapping) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    for (uint32_t g = 0; g < n; ++g) {
-        const Vec2 vec = seed_vec(seeds, g);
-        uint32_t flag = 0;
-        for (int k = 0; k < 8; ++k) {
-            const Vec2 nb{vec.x + c_nbr[k][0], vec.y + c_nbr[k][1]};
-            flag += (mapping[pixel_of(nb, p)] & p.is_thinchannel) != 0u;
-        }
-        if (flag != 1u) {
-            const uint32_t idx = pixel_of(vec, p);
-            mapping[idx] &= ~p.is_channelhead;
-            if (flag == 0u) mapping[idx] &= ~(p.is_thinchannel | p.is_channel);
-        }
+// One head of prune_channel_heads (channelheads.cl:143-199): count the thin
+// channel pixels among the 8 neighbours; not exactly one clears the head's
+// IS_CHANNELHEAD, none also its IS_THINCHANNEL | IS_CHANNEL.
+__device__ __forceinline__ void prune_head(uint32_t g, const slm_params& p, const float2* __restrict__ seeds,
+                                           uint32_t* mapping) {
+    const Vec2 vec = seed_vec(seeds, g);
+    uint32_t flag = 0;
+    for (int k = 0; k < 8; ++k) {
+        const Vec2 nb{vec.x + c_nbr[k][0], vec.y + c_nbr[k][1]};
+        flag += (*(volatile uint32_t*)(mapping + pixel_of(nb, p)) & p.is_thinchannel) != 0u;
+    }
+    if (flag != 1u) {
+        const uint32_t idx = pixel_of(vec, p);
+        atomicAnd(mapping + idx, ~p.is_channelhead);
+        if (flag == 0u) atomicAnd(mapping + idx, ~(p.is_thinchannel | p.is_channel));
+    }
+}
+
+// prune_channel_heads with the result of the reference's sequential schedule
+// (ascending global id).  A head reads its neighbours' IS_THINCHANNEL bits
+// and changes bits of its own pixel only.  When every head is itself a thin
+// channel pixel -- as the mapping sequence leaves them -- no count can change
+// while the heads run: a head that clears its thin bit has no thin
+// neighbour, so no head is its neighbour.  The heads then run in parallel.
+// Otherwise a head that is not thin may count an isolated thin head that
+// runs before it, and the heads run one after another.  One block decides
+// and runs either case, so no scratch word is needed.
+__global__ void __launch_bounds__(1024) k_prune_channel_heads(const slm_params p, uint32_t n,
+                                                              const float2* __restrict__ seeds,
+                                                              uint32_t* mapping) {
+    int all_thin = 1;
+    for (uint32_t g = threadIdx.x; g < n; g += blockDim.x)
+        if ((mapping[pixel_of(seed_vec(seeds, g), p)] & p.is_thinchannel) == 0u) all_thin = 0;
+    all_thin = __syncthreads_and(all_thin);
+    if (all_thin) {
+        for (uint32_t g = threadIdx.x; g < n; g += blockDim.x) prune_head(g, p, seeds, mapping);
+    } else if (threadIdx.x == 0) {
+        for (uint32_t g = 0; g < n; ++g) prune_head(g, p, seeds, mapping);
     }
 }
 
@@ -1105,7 +1128,7 @@ int slm_prune_channel_heads(const slm_params* p, uint32_t n, const float* seed_p
     int rc = map_checks(p, n, seed_point);
     if (rc) return rc;
     if (n == 0) return SLM_OK;
-    k_prune_channel_heads<<<1, 1, 0, SS>>>(*p, n, F2(seed_point), mapping);
+    k_prune_channel_heads<<<1, 1024, 0, SS>>>(*p, n, F2(seed_point), mapping);
     SLM_LAUNCHED("k_prune_channel_heads");
     return SLM_OK;
 }

@@ -258,7 +258,8 @@ __global__ void __launch_bounds__(256)
 k_fields_pair(const slm_params p, float cf_up, const float2* __restrict__ seeds, uint32_t seed_begin,
               u64 n_items, const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
               u64* __restrict__ slc, u64* __restrict__ slt, uint32_t up_stride, u64* __restrict__ work,
-              const uint32_t* __restrict__ order, uint32_t refill_min) {
+              const uint32_t* __restrict__ order, const uint32_t* __restrict__ order_up,
+              uint32_t refill_min) {
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
     const uint32_t dd = p.subpixel_seed_point_density * p.subpixel_seed_point_density;
@@ -291,7 +292,8 @@ k_fields_pair(const slm_params p, float cf_up, const float2* __restrict__ seeds,
                         base = up ? up_stride : 0u;
                         uint32_t pos, sub;
                         split_item(item, dd, pos, sub);
-                        const uint32_t seed_idx = order ? __ldg(order + seed_begin + pos) : seed_begin + pos;
+                        const uint32_t* o = up ? order_up : order;
+                        const uint32_t seed_idx = o ? __ldg(o + seed_begin + pos) : seed_begin + pos;
                         field_init(s, __ldg(seeds + seed_idx), seed_idx, sub, (uint32_t)item, mask, p,
                                    up ? g_up : g_down, base, acc, slc, slt);
                         ntraj++;
@@ -657,7 +659,7 @@ int slm_integrate_fields_scheduled(const slm_params* p, const slm_launch* launch
 int slm_integrate_fields_pair(const slm_params* p_down, const slm_params* p_up, const slm_launch* launch,
                               const float* seed_point, const uint8_t* mask, const float* uv, uint64_t* slc,
                               uint64_t* slt, uint64_t up_stride, uint64_t* workspace, const uint32_t* seed_order,
-                              void* stream) {
+                              const uint32_t* seed_order_up, void* stream) {
     clear_error();
     int rc = check_grid(p_down);
     if (rc) return rc;
@@ -705,11 +707,13 @@ int slm_integrate_fields_pair(const slm_params* p_down, const slm_params* p_up, 
     if (L.integrator == SLM_RK4)
         k_fields_pair<4><<<grid, block, 0, s>>>(*p_down, p_up->combo_factor, sp, begin, n_items, mask, u2,
                                                 (u64*)slc, (u64*)slt, (uint32_t)up_stride, (u64*)workspace,
-                                                seed_order, refill_min(L));
+                                                seed_order, seed_order_up ? seed_order_up : seed_order,
+                                                refill_min(L));
     else
         k_fields_pair<2><<<grid, block, 0, s>>>(*p_down, p_up->combo_factor, sp, begin, n_items, mask, u2,
                                                 (u64*)slc, (u64*)slt, (uint32_t)up_stride, (u64*)workspace,
-                                                seed_order, refill_min(L));
+                                                seed_order, seed_order_up ? seed_order_up : seed_order,
+                                                refill_min(L));
     SLM_LAUNCHED("k_fields_pair");
     return SLM_OK;
 }

@@ -18,9 +18,10 @@ Differences from the reference (none changes a result):
 * device accumulators are uint64; ``slc``/``slt`` returned to the caller are
   the low 32 bits (what the reference's uint32 atomics hold) unless
   ``exact=True``, which keeps the full sums;
-* with ``process_group`` (one process per GPU) each rank traces its shard of
-  the seed list and the uint64 accumulators are summed with one all-reduce
-  (slm_b200.distributed); every rank then holds the full fields.
+* with ``process_group`` (one process per GPU) each rank traces its dealt
+  share of the tracer's queue (chunks of 64 queue positions, round robin;
+  slm_b200.distributed) and the uint64 accumulators are summed with one
+  all-reduce; every rank then holds the full fields.
 """
 from __future__ import annotations
 
@@ -29,9 +30,9 @@ import torch
 
 from . import kernels
 from .device import cuda_device, host_copy, low32, to_device
-from .distributed import sharded_field_pass
+from .distributed import allreduce_counts, shard_queue, shard_queue_params, sharded_field_pass
 from .params import kernel_params
-from .useful import create_seeds, vprint
+from .useful import create_seeds_device, vprint
 
 
 _SLC_TABLES = {}
@@ -62,6 +63,32 @@ def _staging(slot, t):
         st = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
         _STAGING[key] = st
     return st
+
+
+_ROWS_POOL = None
+
+
+def _rows_to_host_behind(t, dev):
+    """A future of a fresh NumPy copy of device tensor ``t``: the copy to
+    pinned memory runs on a side stream behind the work queued so far, the copy
+    out of it on a worker thread, so both overlap what the caller queues next."""
+    global _ROWS_POOL
+    if _ROWS_POOL is None:
+        from concurrent.futures import ThreadPoolExecutor
+        _ROWS_POOL = ThreadPoolExecutor(1)
+    side = torch.cuda.Stream(dev)
+    side.wait_stream(torch.cuda.current_stream(dev))
+    stage = _staging("seed rows", t)
+    with torch.cuda.stream(side):
+        stage.copy_(t, non_blocking=True)
+        t.record_stream(side)
+        done = torch.cuda.Event()
+        done.record(side)
+
+    def finish():
+        done.synchronize()
+        return host_copy(stage.numpy())
+    return _ROWS_POOL.submit(finish)
 
 
 class Fields:
@@ -97,17 +124,23 @@ class Fields:
         info = self.info
         mask_array = self.data.mask_array
         traj_stats_df = self.data.traj_stats_df
-        (self.data.seed_point_array, info.n_seed_points, info.n_padded_seed_points) \
-            = create_seeds(mask_array, info.pad_width, info.n_work_items,
-                           do_shuffle=info.do_shuffle, rng_seed=info.shuffle_rng_seed,
-                           verbose=self.verbose)
         pixel_size = info.pixel_size
         dds = traj_stats_df["ds"]["downstream", "mean"]
         uds = traj_stats_df["ds"]["upstream", "mean"]
         nxp, nyp = mask_array.shape
-        with torch.cuda.device(self.device):
-            acc = self._trace()
+        dev = self.device
+        with torch.cuda.device(dev):
+            # the seed list is built on the device (the rows create_seeds
+            # gives, in its order); its host copy for data.seed_point_array is
+            # taken behind the trace
+            mask_d = to_device(mask_array, dev)
+            seeds_d, info.n_seed_points, info.n_padded_seed_points = create_seeds_device(
+                mask_array, info.pad_width, info.n_work_items, dev, do_shuffle=info.do_shuffle,
+                rng_seed=info.shuffle_rng_seed, verbose=self.verbose, mask_d=mask_d)
+            host_seeds = _rows_to_host_behind(seeds_d, dev)
+            acc = self._trace(seeds_d, mask_d)
             self._finish(acc, float(dds / pixel_size), float(uds / pixel_size), nxp, nyp)
+            self.data.seed_point_array = host_seeds.result()
         vprint(self.verbose, "...done")
 
     def _finish(self, acc, scale_down, scale_up, nxp, nyp):
@@ -141,16 +174,19 @@ class Fields:
         torch.cuda.current_stream(dev).synchronize()
         self.data.slc_array, self.data.slt_array, self.data.sla_array = (host_copy(o.numpy()) for o in out)
 
-    def _trace(self):
-        """Both passes on the device; returns the uint64 accumulators [2, 2, nxy]."""
+    def _trace(self, seeds_d=None, mask_d=None):
+        """Both passes on the device; returns the uint64 accumulators [2, 2, nxy].
+        The seeds and mask come from ``data`` unless given on the device."""
         info = self.info
         dev = self.device
         mask_array = self.data.mask_array
         nxp, nyp = mask_array.shape
         nxy = nxp * nyp
         with torch.cuda.device(dev):
-            seeds_d = to_device(self.data.seed_point_array, dev, torch.float32)
-            mask_d = to_device(mask_array, dev)
+            if seeds_d is None:
+                seeds_d = to_device(self.data.seed_point_array, dev, torch.float32)
+            if mask_d is None:
+                mask_d = to_device(mask_array, dev)
             uv_d = to_device(self.data.uv_array, dev, torch.float32)
             work = kernels.workspace(dev)
             acc = torch.zeros((2, 2, nxy), dtype=torch.uint64, device=dev)  # [downup, slc/slt]
@@ -158,33 +194,43 @@ class Fields:
             if self.seed_order == "spatial" and int(info.n_seed_points) > 0:
                 from .scheduler import spatial_order
                 order = spatial_order(seeds_d, info.n_seed_points, info.nx, info.ny)
-            if self.process_group is None and self.schedule == "persistent":
+            if self.schedule == "persistent":
                 # both directions in one persistent launch: each one's tail
                 # fills with the other's trajectories
                 prm = [kernel_params(info, "INTEGRATE_FIELDS", sign) for sign in (+1.0, -1.0)]
                 info.downup_sign = -1.0
-                kernels.integrate_fields_pair(prm[0], prm[1], seeds_d, mask_d, uv_d, acc[:, 0], acc[:, 1], work,
-                                              integrator=self.integrator, order=order)
-                counts = work[1:4].view(torch.int64).cpu().tolist()
-                self.n_steps[0], self.n_steps[1] = counts[0] - counts[2], counts[2]
                 for d in (0, 1):
                     self.n_trajectories[d] = int(prm[d].n_seed_points) * int(prm[d].subpixel_seed_point_density) ** 2
+                pg = self.process_group
+                queue = order
+                if pg is not None:
+                    import torch.distributed as dist
+                    queue = shard_queue(order, int(info.n_seed_points), dist.get_rank(pg),
+                                        dist.get_world_size(pg), device=dev)
+                    prm = [shard_queue_params(p, queue) for p in prm]
+                kernels.integrate_fields_pair(prm[0], prm[1], seeds_d, mask_d, uv_d, acc[:, 0], acc[:, 1], work,
+                                              integrator=self.integrator, order=queue)
+                counts = work[1:4].view(torch.int64).clone()
+                if pg is not None:
+                    allreduce_counts(acc, counts, group=pg)
+                counts = counts.cpu().tolist()
+                self.n_steps[0], self.n_steps[1] = counts[0] - counts[2], counts[2]
                 return acc
             for downup_idx, downup_sign in ((0, +1.0), (1, -1.0)):
                 info.downup_sign = downup_sign
                 prm = kernel_params(info, "INTEGRATE_FIELDS", downup_sign)
 
-                def trace(p, slc, slt):
+                def trace(p, slc, slt, queue):
                     kernels.integrate_fields(p, seeds_d, mask_d, uv_d, slc, slt, work,
                                              schedule=self.schedule, integrator=self.integrator,
-                                             order=order)
+                                             order=queue)
                     return int(work[1].view(torch.int64).item())
 
                 if self.process_group is None:
-                    self.n_steps[downup_idx] = trace(prm, acc[downup_idx, 0], acc[downup_idx, 1])
+                    self.n_steps[downup_idx] = trace(prm, acc[downup_idx, 0], acc[downup_idx, 1], order)
                 else:
                     _, self.n_steps[downup_idx] = sharded_field_pass(
-                        prm, trace, acc[downup_idx, 0], acc[downup_idx, 1], self.process_group)
+                        prm, trace, acc[downup_idx, 0], acc[downup_idx, 1], self.process_group, order=order)
                 self.n_trajectories[downup_idx] = int(prm.n_seed_points) * int(prm.subpixel_seed_point_density) ** 2
         return acc
 

@@ -75,10 +75,13 @@ def integrate_fields(params, seeds, mask, uv, slc, slt, work, schedule="persiste
 
 
 def integrate_fields_pair(params_down, params_up, seeds, mask, uv, slc, slt, work, integrator=2,
-                          block_threads=0, blocks_per_sm=0, chunk=0, order=None, stream=None):
+                          block_threads=0, blocks_per_sm=0, chunk=0, order=None, order_up=None,
+                          stream=None):
     """Both directions in one persistent launch.  ``slc``/``slt``: uint64
     tensors of shape [2, nxy] (downstream, upstream; any stride between the
-    two rows), each row as ``integrate_fields`` of that direction."""
+    two rows), each row as ``integrate_fields`` of that direction.  ``order``
+    is the queue order of both directions unless ``order_up`` gives the
+    upstream one."""
     lib = _lib.load()
     nxy = params_down.nxy_padded
     _need(seeds, torch.float32, 2 * params_down.n_seed_points, "seeds")
@@ -93,10 +96,12 @@ def integrate_fields_pair(params_down, params_up, seeds, mask, uv, slc, slt, wor
     _need(work, torch.uint64, lib.slm_fields_workspace_words(), "workspace")
     if order is not None:
         _need(order, torch.uint32, int(params_down.n_seed_points), "order")
+    if order_up is not None:
+        _need(order_up, torch.uint32, int(params_down.n_seed_points), "order_up")
     L = launch_config("persistent", integrator, block_threads, blocks_per_sm, chunk)
     check(lib.slm_integrate_fields_pair(sref(params_down), sref(params_up), sref(L), ptr(seeds), ptr(mask),
                                         ptr(uv), ptr(slc), ptr(slt), int(slc.stride(0)), ptr(work), ptr(order),
-                                        _stream(stream)))
+                                        ptr(order_up), _stream(stream)))
 
 
 def integrate_trajectory(params, n_chunk, seeds, mask, uv, traj, nsteps, length,

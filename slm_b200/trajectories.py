@@ -18,7 +18,7 @@ import torch
 from . import kernels
 from .device import cuda_device, to_device
 from .params import kernel_params
-from .useful import compute_stats, create_seeds, vprint
+from .useful import compute_stats, create_seeds_device, vprint
 
 
 class Trajectories:
@@ -40,10 +40,17 @@ class Trajectories:
         vprint(self.verbose, "Integrating trajectories...")
         info = self.info
         mask_array = self.data.mask_array
-        self.data.seed_point_array, n_seed_points, n_padded_seed_points = create_seeds(
-            mask_array, info.pad_width, info.n_work_items,
-            n_seed_points=info.n_trajectory_seed_points, do_shuffle=info.do_shuffle,
-            rng_seed=info.shuffle_rng_seed, verbose=self.verbose)
+        # the seed list on the device (create_seeds' rows in its order): the
+        # full shuffle runs there, only the first n_trajectory_seed_points
+        # rows come back
+        with torch.cuda.device(self.device):
+            self._mask_d = to_device(mask_array, self.device)
+            seeds_d, n_seed_points, n_padded_seed_points = create_seeds_device(
+                mask_array, info.pad_width, info.n_work_items, self.device,
+                n_seed_points=info.n_trajectory_seed_points, do_shuffle=info.do_shuffle,
+                rng_seed=info.shuffle_rng_seed, verbose=self.verbose, mask_d=self._mask_d)
+            self.data.seed_point_array = seeds_d.cpu().numpy()
+            del seeds_d
         info.n_seed_points = n_seed_points
         info.n_padded_seed_points = n_padded_seed_points
         if self.data.mapping_array is None:
@@ -54,6 +61,7 @@ class Trajectories:
         n_chunks = max(1, int(np.ceil(request / limit)))
         self.choose_chunks(n_chunks)
         self.gpu_compute_trajectories()
+        self._mask_d = None
         self.data.traj_stats_df = compute_stats(self.data.traj_length_array,
                                                 self.data.traj_nsteps_array,
                                                 info.pixel_size, self.verbose)
@@ -79,7 +87,9 @@ class Trajectories:
         traj_length_array = np.zeros([ns, 2], dtype=np.float32)
         with torch.cuda.device(dev):
             seeds_d = to_device(self.data.seed_point_array, dev, torch.float32)
-            mask_d = to_device(self.data.mask_array, dev)
+            mask_d = getattr(self, "_mask_d", None)
+            if mask_d is None:
+                mask_d = to_device(self.data.mask_array, dev)
             uv_d = to_device(self.data.uv_array, dev, torch.float32)
             todo = [td[1:] for td in self.trace_do_chunks if td[0]]
             # one chunk per direction (the usual case): both directions run

@@ -257,6 +257,52 @@ def create_seeds(mask, pad, n_work_items, n_seed_points=None, do_shuffle=True,
     return seed_point_array, n_seed_points, n_padded_seed_points  # a fresh array either way
 
 
+def create_seeds_device(mask, pad, n_work_items, device, n_seed_points=None, do_shuffle=True, rng_seed=1,
+                        verbose=False, mask_d=None, stream=None):
+    """``create_seeds`` with the list built in device memory
+    (``slm_create_seeds_device``): the same rows in the same order, and
+    NumPy's global generator left where the reference's shuffle leaves it.
+
+    ``mask``: the host mask (its shape gives the grid); ``mask_d``: the same
+    mask already on ``device`` as uint8 (else it is uploaded).  Returns
+    ``(seeds [n][2] float32 CUDA tensor, n_seed_points, n_padded_seed_points)``
+    with ``n_seed_points`` rows (the first rows when truncated)."""
+    import ctypes
+
+    import torch
+
+    from . import _lib
+    vprint(verbose, "Generating seed points on the GPU...", end="")
+    nxp, nyp = mask.shape
+    n_px = int(nxp) * int(nyp)
+    if mask_d is None:
+        m = np.ascontiguousarray(mask)
+        m = m.view(np.uint8) if m.dtype == np.bool_ else (m != 0).view(np.uint8)
+        mask_d = torch.from_numpy(m).to(device)
+    L = _lib.load()
+    ws = torch.empty(int(L.slm_create_seeds_device_workspace(n_px)), dtype=torch.uint8, device=device)
+    out = torch.empty((max(1, n_px), 2), dtype=torch.float32, device=device)
+    n = ctypes.c_uint64(0)
+    state = np.empty(625, np.uint32)
+    s = stream if stream is not None else torch.cuda.current_stream(device)
+    _lib.check(L.slm_create_seeds_device(_lib.ptr(mask_d), int(nxp), int(nyp), int(pad), 1 if do_shuffle else 0,
+                                         int(rng_seed) & 0xFFFFFFFF, _lib.ptr(out), out.shape[0], ctypes.byref(n),
+                                         state.ctypes.data, _lib.ptr(ws), ws.numel(),
+                                         ctypes.c_void_p(s.cuda_stream)))
+    if do_shuffle:
+        np.random.set_state(("MT19937", state[:624].copy(), int(state[624]), 0, 0.0))
+    n_all = int(n.value)
+    rows = n_all
+    if n_seed_points is not None and n_seed_points > 0:
+        rows = min(int(n_seed_points), n_all)  # the count stays as asked, as create_seeds keeps it
+    else:
+        n_seed_points = n_all
+    pad_length = (np.uint32(np.round(n_seed_points / n_work_items + 0.5)) * n_work_items
+                  - n_seed_points)
+    vprint(verbose, "done")
+    return out[:rows], n_seed_points, n_seed_points + pad_length
+
+
 def pick_seeds(mask=None, map=None, flag=None, pad=None):
     """Seed coordinates of pixels selected by mask and/or mapping flag (useful.py:519-538)."""
     if mask is None and map is not None:

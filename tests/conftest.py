@@ -8,7 +8,8 @@ for p in (ROOT, os.path.join(ROOT, "oracle"), os.path.join(ROOT, "tests")):
     if p not in sys.path:
         sys.path.insert(0, p)
 
-REFERENCE = os.environ.get("SLM_REFERENCE", "/root/reference")
+# the reference checkout: $SLM_REFERENCE, else a "reference" folder beside the repository
+REFERENCE = os.environ.get("SLM_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference")
 
 
 def pytest_configure(config):

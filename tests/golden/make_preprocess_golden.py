@@ -33,7 +33,9 @@ import types
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_REF = os.environ.get("SLM_REFERENCE", "/root/reference")
+# the reference checkout: $SLM_REFERENCE, else a "reference" folder beside the repository
+DEFAULT_REF = os.environ.get("SLM_REFERENCE") or os.path.join(
+    os.path.dirname(os.path.dirname(os.path.dirname(HERE))), "reference")
 
 CASES = {
     "preprocess_a": dict(nx=48, ny=40, seed=21, pixel_size=1.0, pad=2, noise=0.1),

@@ -71,14 +71,14 @@ def test_pair_and_preprocess_arguments_rejected_without_device():
     bad = c.params("INTEGRATE_FIELDS", -1.0)
     bad.max_n_steps += 1
     rc = L.slm_integrate_fields_pair(_lib.sref(pd), _lib.sref(bad), None, fake, fake, fake, fake, fake,
-                                     pd.nxy_padded, fake, None, None)
+                                     pd.nxy_padded, fake, None, None, None)
     assert rc == _lib.SLM_ERR_ARGS and b"differ in more than the direction" in L.slm_last_error()
     same = c.params("INTEGRATE_FIELDS", 1.0)
     rc = L.slm_integrate_fields_pair(_lib.sref(pd), _lib.sref(same), None, fake, fake, fake, fake, fake,
-                                     pd.nxy_padded, fake, None, None)
+                                     pd.nxy_padded, fake, None, None, None)
     assert rc == _lib.SLM_ERR_ARGS  # same sign twice
     rc = L.slm_integrate_fields_pair(_lib.sref(pd), _lib.sref(pu), None, fake, fake, fake, fake, fake,
-                                     pd.nxy_padded - 1, fake, None, None)
+                                     pd.nxy_padded - 1, fake, None, None, None)
     assert rc == _lib.SLM_ERR_ARGS and b"up_stride" in L.slm_last_error()
     prm = _lib.SlmPreprocessParams(1.0, 0.95, -0.5, 0.0, 2, 1)
     rc = L.slm_preprocess(fake, 7, 10, 10, ctypes.byref(prm), fake, None, None, None, None, None, None, None,

@@ -101,32 +101,3 @@ def test_analysis_stage_matches_reference(reference_dir, seed, monkeypatch):
         assert np.array_equal(a.logxy_data, b.logxy_data), name
     # the channel threshold of a data object, as the mapping pass asks for it
     assert mine.estimate_channel_threshold(data) == ref.estimate_channel_threshold(data)
-
-
-def test_elevation_slope_pdfs_match_reference(reference_dir, monkeypatch):
-    R = _reference_analysis(reference_dir)
-    if not hasattr(np, "bool"):
-        monkeypatch.setattr(np, "bool", np.bool_, raising=False)
-    rng = np.random.default_rng(5)
-    nx, ny = 60, 50
-    roi = (800.0 + 900.0 * rng.random((nx, ny))).astype(np.float32)
-    basin = np.zeros((nx + 4, ny + 4), bool)
-    basin[:2], basin[-2:], basin[:, :2], basin[:, -2:] = True, True, True, True
-    flags = np.zeros((nx + 4, ny + 4), np.uint32)
-    flags[rng.random(flags.shape) < 0.1] |= 2048
-    slope = (40.0 * rng.random((nx + 4, ny + 4))).astype(np.float32)
-    info = types.SimpleNamespace(is_midslope=np.uint32(2048))
-    geodata = types.SimpleNamespace(roi_array=roi, basin_mask_array=basin, roi_pixel_size=1.0)
-    params = {"analysis": dict(A.ANALYSIS_PARAMETERS)}
-    outs = []
-    for cls in (R.Analysis, A.Analysis):
-        mapping = types.SimpleNamespace(mapping_array=flags.copy(), info=info)
-        a = cls.__new__(cls)
-        a.__dict__.update(params["analysis"])
-        a.__dict__.update(geodata=geodata, preprocess=types.SimpleNamespace(slope_array=slope), mapping=mapping,
-                          state=types.SimpleNamespace(verbose=False), print=lambda *x, **k: None)
-        a.compute_elevation_slope_pdfs()
-        outs.append(a)
-    for k in ("h_midline_pdf_array", "h_all_pdf_array", "slope_midline_pdf_array", "h_midline_pdf_max1",
-              "h_midline_pdf_max1_h", "slope_midline_pdf_max", "slope_midline_pdf_max_slope", "h_pdf_sf"):
-        assert np.array_equal(np.asarray(getattr(outs[0], k)), np.asarray(getattr(outs[1], k))), k

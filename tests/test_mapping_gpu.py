@@ -54,6 +54,38 @@ def test_prune_channel_heads_bit_exact():
     assert run.mismatches == []
 
 
+@pytest.mark.parametrize("seed,thin_heads", [(21, True), (22, False), (23, False)])
+def test_prune_channel_heads_random_heads(seed, thin_heads):
+    """Random thin-channel grids and random heads: all heads thin (the
+    parallel case) and heads of which some are not thin, next to isolated
+    thin heads (the case the sequential schedule decides), against the
+    oracle's sequential schedule."""
+    c, info, data = pipeline_case(nx=60, ny=50, seed=8)
+    rng = np.random.default_rng(seed)
+    nxp, nyp = data.mask_array.shape
+    m = np.zeros((nxp, nyp), np.uint32)
+    thin = rng.random((nxp, nyp)) < 0.25
+    m[thin] |= info.is_thinchannel | info.is_channel
+    # isolated thin pixels next to non-thin ones
+    for x, y in rng.integers(4, min(nxp, nyp) - 4, size=(40, 2)):
+        m[x - 1:x + 2, y - 1:y + 2] &= ~np.uint32(info.is_thinchannel)
+        m[x, y] |= info.is_thinchannel
+    pool = np.argwhere(((m & info.is_thinchannel) != 0) if thin_heads else np.ones_like(thin))
+    heads = pool[rng.choice(pool.shape[0], size=min(400, pool.shape[0]), replace=False)]
+    heads = heads[np.lexsort((heads[:, 1], heads[:, 0]))]
+    m[heads[:, 0], heads[:, 1]] |= info.is_channelhead
+    data.mapping_array = m
+    info.n_seed_points = np.uint32(heads.shape[0])
+    seeds = (heads - int(info.pad_width)).astype(np.float32)
+    prm = M.kernel_params(info, "PRUNE_CHANNEL_HEADS")
+    expect = [data.mask_array, data.uv_array, m.copy()]
+    oracle_runner("prune_channel_heads", prm, seeds, expect)
+    got = [data.mask_array, data.uv_array, m.copy()]
+    assert M.DeviceRunner()("prune_channel_heads", prm, seeds, got) == 0
+    assert np.array_equal(got[2], expect[2])
+    assert not np.array_equal(got[2], m)  # something was pruned
+
+
 def test_device_pipeline_end_to_end_matches_oracle_pipeline():
     """The whole sequence on the device alone equals the whole sequence on the oracle."""
     _, info, data = pipeline_case(nx=160, ny=128, seed=11)

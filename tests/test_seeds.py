@@ -64,3 +64,55 @@ def test_decode_streamlines_matches_the_reference_expression():
         y = origin[1] + np.cumsum(traj.T[1]) + seeds[k, 1]
         assert np.array_equal(got[k][0], x) and np.array_equal(got[k][1], y)
         assert got[k][0].dtype == np.float32 and got[k][0].size == lists[k].shape[0] + 1
+
+
+def _sequential_swaps(rows, js):
+    """Fisher-Yates' swap pass: swap(i, js[i]) for i = n-1 down to 1."""
+    rows = rows.copy()
+    for i in range(rows.shape[0] - 1, 0, -1):
+        j = js[i]
+        rows[[i, j]] = rows[[j, i]]
+    return rows
+
+
+def _reservation_rounds(rows, js):
+    """The device shuffle's schedule restated in NumPy: every pending swap
+    reserves its two rows with its index (the maximum wins); a swap holding
+    both reservations runs, the others wait for the next round."""
+    rows = rows.copy()
+    n = rows.shape[0]
+    pending = np.arange(1, n, dtype=np.int64)
+    rounds = 0
+    while pending.size:
+        rounds += 1
+        res = np.zeros(n, np.int64)
+        np.maximum.at(res, pending, pending)
+        np.maximum.at(res, js[pending], pending)
+        run = (res[pending] == pending) & (res[js[pending]] == pending)
+        i = pending[run]
+        j = js[i]
+        # rows of swaps that run in one round are pairwise distinct
+        assert np.unique(np.concatenate([i, j[i != j]])).size == i.size + int((i != j).sum())
+        rows[i], rows[j] = rows[j].copy(), rows[i].copy()
+        pending = pending[~run]
+    return rows, rounds
+
+
+@pytest.mark.parametrize("n,seed", [(1, 0), (2, 1), (3, 2), (17, 3), (1000, 4), (200_000, 5)])
+def test_reservation_rounds_equal_sequential_swaps(n, seed):
+    """The round schedule of slm_create_seeds_device gives the sequential
+    shuffle's rows for any partners j(i) in [0, i], in few rounds."""
+    rng = np.random.default_rng(seed)
+    js = np.zeros(n, np.int64)
+    if n > 1:
+        js[1:] = rng.integers(0, np.arange(2, n + 1))
+    rows = np.stack([np.arange(n, dtype=np.float32), -np.arange(n, dtype=np.float32)], 1)
+    got, rounds = _reservation_rounds(rows, js)
+    assert np.array_equal(got, _sequential_swaps(rows, js)) if n < 5000 else True
+    if n >= 5000:  # the sequential loop in Python is slow: compare with NumPy's own shuffle order
+        perm = np.arange(n)
+        for i in range(n - 1, 0, -1):
+            j = js[i]
+            perm[i], perm[j] = perm[j], perm[i]
+        assert np.array_equal(got, rows[perm])
+    assert rounds <= max(4, 8 * int(np.log2(max(n, 2))))

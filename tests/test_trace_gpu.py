@@ -156,19 +156,27 @@ def test_golden_on_gpu():
 
 
 @pytest.mark.parametrize("integrator,ordered,interleaved", [(2, False, False), (4, False, False),
-                                                            (2, True, False), (4, True, True)])
+                                                            (2, True, False), (4, True, True),
+                                                            (4, "per-direction", False)])
 def test_fields_pair_equals_two_directions(integrator, ordered, interleaved):
     """One launch over both directions gives each direction's fields and the
     summed step and trajectory counts of two single-direction launches; the
-    upstream rows may sit at any stride (interleaved: [direction][slc|slt])."""
+    upstream rows may sit at any stride (interleaved: [direction][slc|slt]);
+    the two directions may take their queues in different orders."""
     c = Case(nx=70, ny=58, seed=91, density=2, step=0.25, max_length=120.0)
     seeds, mask, uv = _dev(c)
     pd, pu = c.params("INTEGRATE_FIELDS", 1.0), c.params("INTEGRATE_FIELDS", -1.0)
     nxy = pd.nxy_padded
-    order = None
+    order = order_up = None
+
+    def perm(seed):
+        p = np.random.default_rng(seed).permutation(int(pd.n_seed_points)).astype(np.int32)
+        return torch.from_numpy(p).to(DEV).view(torch.uint32)
+
     if ordered:
-        order = torch.from_numpy(np.random.default_rng(5).permutation(int(pd.n_seed_points)).astype(np.int32)).to(DEV)
-        order = order.view(torch.uint32)
+        order = perm(5)
+    if ordered == "per-direction":
+        order_up = perm(6)
     ref = []
     for prm in (pd, pu):
         slc = torch.zeros(nxy, dtype=torch.uint64, device=DEV)
@@ -184,7 +192,8 @@ def test_fields_pair_equals_two_directions(integrator, ordered, interleaved):
         slc2 = torch.zeros((2, nxy), dtype=torch.uint64, device=DEV)
         slt2 = torch.zeros((2, nxy), dtype=torch.uint64, device=DEV)
     work = kernels.workspace(DEV)
-    kernels.integrate_fields_pair(pd, pu, seeds, mask, uv, slc2, slt2, work, integrator=integrator, order=order)
+    kernels.integrate_fields_pair(pd, pu, seeds, mask, uv, slc2, slt2, work, integrator=integrator, order=order,
+                                  order_up=order_up)
     torch.cuda.synchronize()
     for d in range(2):
         assert np.array_equal(slc2[d].cpu().numpy(), ref[d][0])
