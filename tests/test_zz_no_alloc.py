@@ -18,8 +18,6 @@ import torch
 from cases import Case
 from slm_b200 import _lib
 
-pytestmark = pytest.mark.gpu
-
 
 def _call(fn_name, prm, launch, seeds, mask, uv, slc, slt, work=None):
     L = _lib.load()
@@ -33,8 +31,22 @@ def _call(fn_name, prm, launch, seeds, mask, uv, slc, slt, work=None):
     _lib.check(fn(*args))
 
 
-@pytest.mark.parametrize("schedule", [_lib.SLM_SCHED_PERSISTENT, _lib.SLM_SCHED_PLAIN])
-def test_noalloc_matches_workspace_entry_point(schedule):
+def test_noalloc_scratch_holds_the_tracer_workspace():
+    """The static array must hold every scratch word the field tracer uses, so
+    a tracer that grows its scratch fails here (CPU) before it could fail a
+    caller (the entry point returns SLM_ERR_CAPACITY then)."""
+    import os
+    import re
+    hdr = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "slm_b200.h")
+    limit = int(re.search(r"#define SLM_NOALLOC_SCRATCH_WORDS (\d+)", open(hdr).read()).group(1))
+    assert _lib.load().slm_fields_workspace_words() <= limit
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("schedule,integrator", [(_lib.SLM_SCHED_PERSISTENT, _lib.SLM_RK2),
+                                                 (_lib.SLM_SCHED_PLAIN, _lib.SLM_RK2),
+                                                 (_lib.SLM_SCHED_PERSISTENT, _lib.SLM_RK4)])
+def test_noalloc_matches_workspace_entry_point(schedule, integrator):
     c = Case(nx=72, ny=60, seed=61, density=2, jitter=1.0, step=0.25, max_length=90.0)
     dev = "cuda"
     seeds = torch.from_numpy(c.seeds).to(dev)
@@ -43,7 +55,7 @@ def test_noalloc_matches_workspace_entry_point(schedule):
     nxy = int(c.info.nx_padded * c.info.ny_padded)
     launch = _lib.SlmLaunch()
     launch.schedule = schedule
-    launch.integrator = _lib.SLM_RK2
+    launch.integrator = integrator
     work = torch.zeros(_lib.load().slm_fields_workspace_words(), dtype=torch.uint64, device=dev)
     for sign in (1.0, -1.0):
         prm = c.params("INTEGRATE_FIELDS", sign)
