@@ -983,6 +983,31 @@ def run_stages(args, wl, dev):
                                 pixel_size=spec.pixel_size, n_hist_bins=1024, n_pdf_points=256)
     timed("kde_bivariate_s", lambda: bd.compute_kde_opencl(kernel="gaussian", bandwidth=0.1))
     out["kde_bivariate_points"] = int(bd.n_data)
+
+    # the Mapping stage's passes 1 and 2 with the grids on the GPU: the
+    # coarse channels at the 94th-percentile threshold, then per coarse
+    # subsegment its KDE threshold, fine channels, traced hillslope lengths
+    # and their statistics
+    import types
+
+    from slm_b200 import analysis as A
+    from slm_b200.mapping_stage import Mapping
+    from slm_b200.useful import default_parameters
+    dflt = default_parameters()
+    state = types.SimpleNamespace(**vars(dflt.state))
+    state.reset_active_masks = lambda: None
+    state.merge_active_masks = lambda: wl.mask.copy()
+    state.add_active_mask = lambda item: None
+    trace_ns = types.SimpleNamespace(**vars(wl.defaults.trace))
+    trace_ns.slc_array, trace_ns.slt_array, trace_ns.sla_array = data2.slc_array, data2.slt_array, data2.sla_array
+    geodata = types.SimpleNamespace(roi_nx=spec.n, roi_ny=spec.n, pad_width=2, roi_pixel_size=spec.pixel_size)
+    stage = Mapping(state, {"mapping": dict(coarse_channel_threshold=float(thr), coarse_segmentation_threshold=200)},
+                    geodata, types.SimpleNamespace(uv_array=wl.uv), trace_ns,
+                    analysis=A.Analysis(state, None, geodata, None, trace_ns), device=dev)
+    timed("mapping_pass1_s", stage.pass1)
+    timed("mapping_pass2_s", stage.pass2)
+    out["mapping_coarse_subsegments"] = int(stage.n_coarse_subsegments)
+    out["mapping_pass2_subsegments_with_lengths"] = int(len(stage.hsl_mean_array))
     out["ok"] = bool(ok)
     return out
 

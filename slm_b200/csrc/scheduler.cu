@@ -75,13 +75,15 @@ __global__ void k_dx2_to_da1(const float* __restrict__ dx2, uint32_t n, float* _
 // C[M,N] (+)= op(A)[M,K] op(B)[K,N]; op(A) = A (row-major MxK) or A^T (A is KxM),
 // op(B) = B (KxN) or B^T (B is NxK).  Epilogue (when not accumulating): + bias[N],
 // ReLU, keep the pre-activation in Z, round the output to bf16.
-// 64x64 tiles, 256 threads, 4x4 outputs each; split-K over gridDim.z with
-// atomicAdd into a zeroed C when accumulate is set.
+// 64x64 tiles, 256 threads, 4x4 outputs each.  With ``partial`` (accumulate),
+// K is split over gridDim.z: slice z writes its tile to partial[z][M][N] and
+// k_split_sum adds the slices into C in slice order, so the sums do not
+// depend on the order blocks run in.
 template <bool TA, bool TB>
 __global__ void __launch_bounds__(256)
 k_gemm(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ C,
        float* __restrict__ Z, const float* __restrict__ bias, int M, int N, int K,
-       int relu, int round_out, int accumulate) {
+       int relu, int round_out, float* __restrict__ partial) {
     __shared__ float As[16][64 + 4];
     __shared__ float Bs[16][64 + 4];
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -125,8 +127,8 @@ k_gemm(const float* __restrict__ A, const float* __restrict__ B, float* __restri
             const int gn = n0 + tx * 4 + j;
             if (gn >= N) continue;
             const size_t o = (size_t)gm * N + gn;
-            if (accumulate) {
-                atomicAdd(C + o, acc[i][j]);
+            if (partial) {
+                partial[(size_t)blockIdx.z * M * N + o] = acc[i][j];
             } else {
                 float v = acc[i][j] + (bias ? bias[gn] : 0.0f);
                 if (Z) Z[o] = v;
@@ -136,6 +138,15 @@ k_gemm(const float* __restrict__ A, const float* __restrict__ B, float* __restri
             }
         }
     }
+}
+
+// C[o] += partial[0][o] + partial[1][o] + ... in slice order
+__global__ void k_split_sum(const float* __restrict__ partial, int slices, size_t mn, float* __restrict__ C) {
+    const size_t o = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= mn) return;
+    float v = C[o];
+    for (int z = 0; z < slices; ++z) v += partial[(size_t)z * mn + o];
+    C[o] = v;
 }
 
 // dZ = dA * (Z > 0)
@@ -529,17 +540,23 @@ int slm_cnn_rearrange(const float* src, uint32_t n, float* dst, int backward, vo
 }
 
 int slm_gemm(int trans_a, int trans_b, int M, int N, int K, const float* A, const float* B, float* C,
-             float* Z, const float* bias, int relu, int round_out, int split_k, void* stream) {
+             float* Z, const float* bias, int relu, int round_out, int split_k, float* partial, void* stream) {
     clear_error();
     SLM_REQUIRE(M > 0 && N > 0 && K > 0 && A && B && C, "bad GEMM arguments");
-    const int accumulate = split_k > 0 ? 1 : 0;
+    SLM_REQUIRE(split_k <= 0 || partial, "split_k needs a partial buffer of split_k*M*N floats");
+    float* part = split_k > 0 ? partial : nullptr;
     dim3 grid((N + 63) / 64, (M + 63) / 64, split_k > 0 ? split_k : 1);
     cudaStream_t s = (cudaStream_t)stream;
-    if (trans_a && trans_b) k_gemm<true, true><<<grid, 256, 0, s>>>(A, B, C, Z, bias, M, N, K, relu, round_out, accumulate);
-    else if (trans_a) k_gemm<true, false><<<grid, 256, 0, s>>>(A, B, C, Z, bias, M, N, K, relu, round_out, accumulate);
-    else if (trans_b) k_gemm<false, true><<<grid, 256, 0, s>>>(A, B, C, Z, bias, M, N, K, relu, round_out, accumulate);
-    else k_gemm<false, false><<<grid, 256, 0, s>>>(A, B, C, Z, bias, M, N, K, relu, round_out, accumulate);
+    if (trans_a && trans_b) k_gemm<true, true><<<grid, 256, 0, s>>>(A, B, C, Z, bias, M, N, K, relu, round_out, part);
+    else if (trans_a) k_gemm<true, false><<<grid, 256, 0, s>>>(A, B, C, Z, bias, M, N, K, relu, round_out, part);
+    else if (trans_b) k_gemm<false, true><<<grid, 256, 0, s>>>(A, B, C, Z, bias, M, N, K, relu, round_out, part);
+    else k_gemm<false, false><<<grid, 256, 0, s>>>(A, B, C, Z, bias, M, N, K, relu, round_out, part);
     SLM_LAUNCHED("k_gemm");
+    if (part) {
+        const size_t mn = (size_t)M * N;
+        k_split_sum<<<(unsigned)((mn + 255) / 256), 256, 0, s>>>(part, split_k, mn, C);
+        SLM_LAUNCHED("k_split_sum");
+    }
     return SLM_OK;
 }
 

@@ -23,10 +23,19 @@ from .device import cuda_device
 from .params import kernel_params
 
 
+_TORCH = {np.dtype(np.uint8): torch.uint8, np.dtype(np.float32): torch.float32,
+          np.dtype(np.uint32): torch.uint32, np.dtype(np.float64): torch.float64}
+
+
 class DeviceMapping:
     """Device copies of the mapping grids of one ``data`` object."""
 
     def __init__(self, info, data, device=None):
+        """``data``: NumPy arrays (uploaded once), or CUDA tensors already on
+        ``device`` (used in place; ``mapping_array`` is then updated there):
+        ``mask_array`` [nxp, nyp] bool/uint8, ``uv_array`` [nxp, nyp, 2],
+        ``mapping_array`` uint32, ``slt_array`` / ``slc_array`` [nxp, nyp, 2]
+        (only the downstream half is read)."""
         self.info, self.data = info, data
         self.dev = device if device is not None else cuda_device(0, 0)
         self.L = _lib.load()
@@ -34,9 +43,14 @@ class DeviceMapping:
         nxp, nyp = data.mask_array.shape
         self.shape = (nxp, nyp)
         self.n = nxp * nyp
-        up = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).to(dev)
-        self.mask = up(data.mask_array.view(np.uint8) if data.mask_array.dtype == np.bool_
-                       else data.mask_array, np.uint8)
+
+        def up(a, dt):
+            if isinstance(a, torch.Tensor):
+                t = a if a.dtype != torch.bool else a.view(torch.uint8)
+                return t.to(dev, _TORCH[np.dtype(dt)]).contiguous()
+            return torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).to(dev)
+        m = data.mask_array
+        self.mask = up(m.view(np.uint8) if isinstance(m, np.ndarray) and m.dtype == np.bool_ else m, np.uint8)
         self.uv = up(data.uv_array, np.float32)
         self.mapping = up(data.mapping_array, np.uint32).reshape(-1)
         self.slt_dn = up(data.slt_array[:, :, 0], np.float32)

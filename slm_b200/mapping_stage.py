@@ -1,51 +1,252 @@
-"""The Mapping stage's first pass: coarse channels, subsegments, midslopes, ridges.
+"""The Mapping stage: passes 1 and 2 with the region's grids on the compute device.
 
-Mirrors ``streamlines.mapping.Mapping.pass1`` (python/streamlines/mapping.py:
-235-345) over this package's mapping wrappers:
+What the passes compute (the reference's ``streamlines.mapping.Mapping``,
+python/streamlines/mapping.py:235-560, computes the same arrays):
 
-1. crop every grid to the bounding box of the merged active mask;
-2. flag midslopes and ridges from the sla angle (``map_midslopes``,
-   ``map_ridges``);
-3. map channels and segments with the coarse thresholds
-   (``map_channels_segments``);
-4. record the coarse subsegment labels, the list of them, and the mask that
-   selects them;
-5. merge the flags back into the full ROI grid, then erase this pass's
-   channel-head and thin-channel bits.
+Pass 1 maps the whole region coarsely.  Inside the window around the
+unmasked pixels it flags midslopes and ridges (from the sla angle), maps
+channels and segments with the coarse thresholds, and keeps the segment
+labels as the region's coarse subsegments.
 
-The per-subsegment hillslope-length helpers follow: ``select_subsegments``,
-``measure_hsl_traced`` (the lengths kernel), ``parse_hsl`` (per-subsegment
-statistics) and ``remap_hsl`` (mapping.py:819-976).
+Pass 2 revisits each coarse subsegment L, in ascending label order.  Its
+pixels, grown by 2 pixels for a left flank (L < 0) or 1 for a right flank,
+form the working region; the channel threshold comes from the KDE of that
+region's downstream slt (clamped to [min, max], else the guess or half of
+it); channels and segments are mapped there with the fine thresholds; the
+hillslope length of every unmasked midslope pixel is traced along its
+streamline to the channel; each fine subsegment's lengths give count / mean
+/ standard deviation, and its mean is painted on its pixels.  Only the
+subsegment's own (ungrown) pixels take the new lengths and flags back.
 
-Kernels run through ``runner`` (default: the GPU, ``mapping.DeviceRunner``;
-tests pass the oracle).  ``pass2`` runs the reference's second pass with the
-hillslope lengths traced along streamlines, the alternative the reference
-keeps beside its fast-marching measurement (skfmm, absent here).  The third
-pass is not restated.
+How this implementation is organised:
+
+* ``_Roi`` holds the region's grids -- flags (uint32), coarse labels
+  (int32), hillslope lengths (float32), the job's base mask, the
+  downstream fields the mapping reads -- as tensors on one device, for both
+  passes and every subsegment.
+* ``_Window`` is an axis-aligned window of the region (a bounding box
+  widened by the pad): crops, the Info of its kernels, and the write-back.
+* An engine maps channels and segments in a window and traces the lengths:
+  ``DeviceEngine`` keeps the window's grids on the GPU from the crop to the
+  lengths (``DeviceMapping`` fed with device tensors);  ``WrapperEngine``
+  runs the reference-shaped wrappers with a kernel runner (the oracle, to
+  check the passes against the reference on the CPU).
+* Region growing is a 3x3 max-pool per pixel of growth (binary dilation with
+  the 8-neighbour structure), bounding boxes come from row / column
+  reductions, and the write-back is a masked scatter, all on the device.
+  The per-subsegment statistics, over the few midslope lengths, use pandas
+  as the reference does, so the means painted are the reference's; the KDE's
+  data selection runs on host copies of the window (the KDE itself runs on
+  the GPU).
+
+The hillslope lengths are the ones traced along streamlines, the
+alternative the reference keeps beside its fast-marching measurement
+(skfmm, absent here).  Pass 3 (scikit-image's rank filters, absent) is not
+built.
 """
 from __future__ import annotations
 
+import types
+
 import numpy as np
+import torch
+import torch.nn.functional as F
 
 from . import mapping as M
-from .useful import Data, Info, default_parameters, dilate, get_bbox, vprint
+from .useful import Info, default_parameters, vprint
 
 MAPPING_PARAMETERS = dict(vars(default_parameters().mapping))
 MAPPING_PARAMETERS.update(do_map_channels_segments=True, do_map_hsl=True, midslope_filter_sigma=5.0,
                           midslope_threshold=0.03, ridge_filter_sigma=2.0, ridge_threshold=0.8,
                           n_hsl_averaging_threshold=1, hsl_averaging_threshold=5.0)
 
+HSL_COLUMNS = ("count", "mean [m]", "stddev [m]")
 
+
+# ------------------------------------------------------------------ grid helpers
+def grow(region, n_pixels):
+    """``region`` (bool [X, Y]) grown by ``n_pixels`` with the 8-neighbour
+    structure; outside the grid counts as not in the region."""
+    x = region.to(torch.float32)[None, None]
+    for _ in range(int(n_pixels)):
+        x = F.max_pool2d(x, 3, stride=1, padding=1)
+    return x[0, 0] > 0
+
+
+def bounding_box(on):
+    """(x_min, x_max, y_min, y_max) of the True pixels of ``on`` (bool [X, Y])."""
+    xs = torch.nonzero(on.any(dim=1)).flatten()
+    ys = torch.nonzero(on.any(dim=0)).flatten()
+    if xs.numel() == 0:
+        raise ValueError("no unmasked pixel to map")
+    return int(xs[0]), int(xs[-1]), int(ys[0]), int(ys[-1])
+
+
+class _Window:
+    """The bounding box of ``on`` widened by ``pad`` on every side."""
+
+    def __init__(self, on, pad):
+        x0, x1, y0, y1 = bounding_box(on)
+        self.pad = pad
+        self.nx, self.ny = x1 + 1 - x0, y1 + 1 - y0  # the box itself
+        self.box = (x0, x1, y0, y1)
+        self.sl = (slice(x0 - pad, x1 + pad + 1), slice(y0 - pad, y1 + pad + 1))
+
+    def info(self, stage, coarse_label=None):
+        info = Info(stage.state, stage.trace, stage.geodata.roi_pixel_size, mapping=stage,
+                    coarse_label=coarse_label)
+        info.set_xy(self.nx, self.ny, self.pad)
+        return info
+
+    def of(self, t):
+        return t[self.sl]
+
+
+class _Roi:
+    """The region's grids on one device."""
+
+    def __init__(self, nxp, nyp, trace, uv, base_mask, device):
+        dev = device
+        self.device = dev
+        self.mapping = torch.zeros((nxp, nyp), dtype=torch.int64, device=dev)  # uint32 flags held in int64
+        self.coarse = torch.zeros((nxp, nyp), dtype=torch.int32, device=dev)
+        self.hsl = torch.zeros((nxp, nyp), dtype=torch.float32, device=dev)
+        self.base = torch.from_numpy(np.ascontiguousarray(base_mask)).to(dev)
+        self.uv = torch.from_numpy(np.ascontiguousarray(uv, dtype=np.float32)).to(dev)
+        self.slt = torch.from_numpy(np.ascontiguousarray(trace.slt_array, dtype=np.float32)).to(dev)
+        self.slc = torch.from_numpy(np.ascontiguousarray(trace.slc_array, dtype=np.float64)).to(dev)
+        self.sla_h = np.asarray(trace.sla_array)
+        self.slt_h = np.asarray(trace.slt_array)
+        self.uv_h = np.asarray(uv)
+
+
+def _u32(t):
+    """int64 flag tensor -> uint32 NumPy array."""
+    return t.to(torch.int64).cpu().numpy().astype(np.uint32)
+
+
+# ------------------------------------------------------------------ engines
+class WrapperEngine:
+    """The mapping sequence through the reference-shaped wrappers
+    (mapping.map_channels_segments), each kernel through ``runner``."""
+
+    def __init__(self, runner):
+        self.runner = runner
+
+    def map(self, info, win, roi, mask, mapping):
+        """Channels and segments in the window; returns (ok, flags int64
+        tensor, labels int32 tensor) on the region's device."""
+        sl = win.sl
+        data = types.SimpleNamespace(
+            mask_array=np.ascontiguousarray(mask.cpu().numpy()), uv_array=np.ascontiguousarray(roi.uv_h[sl]),
+            mapping_array=_u32(mapping), slt_array=np.ascontiguousarray(roi.slt_h[sl]),
+            slc_array=np.ascontiguousarray(roi.slc[sl].cpu().numpy()), label_array=None,
+            count_array=None, link_array=None, channel_label_array=None)
+        ok = M.map_channels_segments(None, info, data, runner=self.runner)
+        self.data = data
+        lab = data.label_array if data.label_array is not None else np.zeros(mask.shape, np.int32)
+        return (ok, torch.from_numpy(data.mapping_array.astype(np.int64)).to(roi.device),
+                torch.from_numpy(np.ascontiguousarray(lab, dtype=np.int32)).to(roi.device))
+
+    def lengths(self, info, mapping, n):
+        """The doubled hillslope lengths of the window's unmasked midslope
+        pixels (row-major order), or None when there is none."""
+        d = self.data
+        d.mapping_array = _u32(mapping)
+        d.subsegment_hsl_array = np.zeros(n, dtype=np.float32)
+        if not M.hsl(None, info, d, False, runner=self.runner):
+            return None
+        return d.subsegment_hsl_array
+
+
+class DeviceEngine:
+    """The mapping sequence with the window's grids resident on the GPU
+    (``mapping_device.DeviceMapping`` over device tensors)."""
+
+    def __init__(self, device=None):
+        self.device = device
+
+    def map(self, info, win, roi, mask, mapping):
+        from .mapping_device import DeviceMapping
+        sl = win.sl
+        data = types.SimpleNamespace(mask_array=mask, uv_array=roi.uv[sl], mapping_array=mapping.to(torch.uint32),
+                                     slt_array=roi.slt[sl], slc_array=roi.slc[sl])
+        self.dm = DeviceMapping(info, data, device=roi.device)
+        with torch.cuda.device(roi.device):
+            ok = self.dm.map_channels_segments()
+        if self.dm.status:
+            raise RuntimeError("mapping kernel status {:#x}".format(self.dm.status))
+        shape = mask.shape
+        return (ok, self.dm.mapping.view(shape).to(torch.int64),
+                self.dm.label.view(shape).view(torch.int32).clone())
+
+    def lengths(self, info, mapping, n):
+        self.dm.mapping.copy_(mapping.reshape(-1).to(torch.uint32))
+        if n == 0:
+            return None
+        with torch.cuda.device(self.dm.dev):
+            return self.dm.hsl(False)
+
+
+# ------------------------------------------------------------------ subsegment statistics
+def length_statistics(fine_labels, lengths, coarse_label):
+    """Count, mean and standard deviation of the lengths of each nonzero
+    fine label, one row per distinct label in ascending order, indexed by
+    (fine, coarse) -- pandas' groupby statistics, as the reference's
+    parse_hsl (mapping.py:920-944) takes them.  None when they cannot be
+    formed."""
+    import pandas as pd
+    fine_labels = np.asarray(fine_labels, dtype=np.int32)
+    table = pd.DataFrame({"fine": fine_labels, "length": np.asarray(lengths, dtype=np.float32)})
+    table = table[table.fine != 0]
+    distinct = np.unique(fine_labels)
+    rows = pd.DataFrame(distinct[distinct != 0].astype(np.int32), columns=["fine"])
+    try:
+        by = table.groupby("fine")["length"]
+        for column, stat in zip(HSL_COLUMNS, (by.count(), by.mean(), by.std())):
+            rows = rows.join(stat.rename(column), on="fine")
+    except Exception:  # noqa: BLE001 - a failed subsegment is skipped, as in the reference
+        return None
+    rows["coarse"] = coarse_label
+    return rows.set_index(["fine", "coarse"])
+
+
+def paint_means(labels, stats, min_count, device):
+    """Each listed fine subsegment's mean length on its pixels (0 when it has
+    fewer than ``min_count`` lengths, and on unlisted pixels); float32."""
+    out = torch.zeros(labels.shape, dtype=torch.float32, device=device)
+    if stats is None or len(stats) == 0:
+        return out
+    fine = stats.index.get_level_values("fine").to_numpy(np.int64)
+    value = np.where(stats["count"].to_numpy() >= min_count, stats["mean [m]"].to_numpy(), 0.0)
+    order = np.argsort(fine, kind="stable")
+    keys = torch.from_numpy(fine[order]).to(device)
+    vals = torch.from_numpy(value[order].astype(np.float32)).to(device)
+    lab = labels.to(torch.int64)
+    k = torch.searchsorted(keys, lab).clamp_(max=keys.numel() - 1)
+    hit = keys[k] == lab
+    out[hit] = vals[k[hit]]
+    return out
+
+
+# ------------------------------------------------------------------ the stage
 class Mapping:
     """``state``: the job state (``reset_active_masks()``,
-    ``merge_active_masks()``, the state parameters Info reads);
-    ``imported_parameters``: the job's parameters (its 'mapping' section, or
-    that section itself); ``geodata``: ``roi_nx``, ``roi_ny``, ``pad_width``,
-    ``roi_pixel_size``; ``preprocess``: ``uv_array``; ``trace``: the trace
-    parameters and ``slc_array`` / ``slt_array`` / ``sla_array``."""
+    ``merge_active_masks()``, ``add_active_mask()``, and the state
+    parameters Info reads); ``imported_parameters``: the job's parameters
+    (its 'mapping' section, or that section itself); ``geodata``:
+    ``roi_nx``, ``roi_ny``, ``pad_width``, ``roi_pixel_size``;
+    ``preprocess``: ``uv_array``; ``trace``: the trace parameters and
+    ``slc_array`` / ``slt_array`` / ``sla_array``; ``analysis``: its
+    ``estimate_channel_threshold`` (pass 2).
+
+    ``runner``: a kernel runner (e.g. the oracle) -- the passes then run
+    through the reference-shaped wrappers on the CPU; by default the grids
+    live on the GPU (``device``) and the mapping sequence runs there.
+    ``thin``: the one-pixel thinning of the midslope and ridge filters."""
 
     def __init__(self, state, imported_parameters, geodata, preprocess, trace, analysis=None, runner=None,
-                 thin=None):
+                 thin=None, device=None):
         params = dict(MAPPING_PARAMETERS)
         if imported_parameters:
             params.update(imported_parameters.get("mapping", imported_parameters))
@@ -53,233 +254,158 @@ class Mapping:
             setattr(self, k, v)
         self.state, self.geodata, self.preprocess, self.trace, self.analysis = \
             state, geodata, preprocess, trace, analysis
-        self.runner = runner
         self.thin = thin
-        self.cl_state = None
         self.verbose = getattr(state, "verbose", False)
-        self.vprogress = self.verbose
+        if runner is not None and not isinstance(runner, M.DeviceRunner):
+            self.engine, self.device = WrapperEngine(runner), torch.device("cpu")
+        else:
+            from .device import cuda_device
+            self.device = device if device is not None else cuda_device(0, 0)
+            self.engine = DeviceEngine(self.device)
+        self._roi = None
+        self.coarse_subsegments_list_array = np.zeros(0, np.int32)
+        self.n_coarse_subsegments = 0
+        self.hsl_mean_array = np.array([], dtype=np.float32)
+        self.hsl_stats_df = None
 
     def print(self, *args, **kwargs):
         vprint(self.verbose, *args, **kwargs)
 
-    def _runner(self):
-        if self.runner is None:
-            self.runner = M.DeviceRunner()
-        return self.runner
+    # the region's grids as the reference keeps them: NumPy arrays
+    @property
+    def mapping_array(self):
+        return _u32(self._roi.mapping)
 
-    def pass1(self):
-        vprint(self.vprogress, "\n**Pass#1 begin**")
-        pad = self.geodata.pad_width
-        nxp = self.geodata.roi_nx + pad * 2
-        nyp = self.geodata.roi_ny + pad * 2
-        self.mapping_array = np.zeros((nxp, nyp), dtype=np.uint32)
-        self.coarse_subsegment_array = np.zeros((nxp, nyp), dtype=np.int32)
-        self.merged_coarse_mask_array = np.ones((nxp, nyp), dtype=bool)
-        info = Info(self.state, self.trace, self.geodata.roi_pixel_size, mapping=self)
+    @property
+    def coarse_subsegment_array(self):
+        return self._roi.coarse.cpu().numpy()
+
+    @property
+    def merged_coarse_mask_array(self):
+        return ~np.isin(self.coarse_subsegment_array, self.coarse_subsegments_list_array)
+
+    @property
+    def hsl_array(self):
+        return self._roi.hsl.cpu().numpy()
+
+    def _base_mask(self):
         self.state.reset_active_masks()
-        mask_array = self.state.merge_active_masks()
-        bbox, nxb, nyb = get_bbox(~mask_array)
-        info.set_xy(nxb, nyb, pad)
+        return self.state.merge_active_masks()
+
+    def _clear(self, flags):
+        """Erase bits from every pixel of the region's flags."""
+        self._roi.mapping &= ~int(flags)
+
+    # ---------------------------------------------------------------- pass 1
+    def pass1(self):
+        self.print("\n**Pass#1 begin**")
+        g = self.geodata
+        pad = g.pad_width
+        base = self._base_mask()
+        roi = self._roi = _Roi(g.roi_nx + 2 * pad, g.roi_ny + 2 * pad, self.trace, self.preprocess.uv_array,
+                               base, self.device)
+        win = _Window(~roi.base, pad)
+        info = win.info(self)
         info.set_thresholds(channel_threshold=self.coarse_channel_threshold,
                             segmentation_threshold=self.coarse_segmentation_threshold)
-        data = Data(info=info, bbox=bbox, pad=pad, mapping_array=self.mapping_array, mask_array=mask_array,
-                    uv_array=self.preprocess.uv_array, slc_array=self.trace.slc_array,
-                    slt_array=self.trace.slt_array, sla_array=self.trace.sla_array)
-        M.map_midslopes(info, data, self.midslope_filter_sigma, self.midslope_threshold, thin=self.thin)
-        M.map_ridges(info, data, self.ridge_filter_sigma, self.ridge_threshold, thin=self.thin)
+        # midslope and ridge flags from the sla angle (host filters) in a fresh window grid
+        sl = win.sl
+        filt = types.SimpleNamespace(mask_array=base[sl].copy(), sla_array=roi.sla_h[sl],
+                                     mapping_array=np.zeros((win.nx + 2 * pad, win.ny + 2 * pad), np.uint32))
+        M.map_midslopes(info, filt, self.midslope_filter_sigma, self.midslope_threshold, thin=self.thin)
+        M.map_ridges(info, filt, self.ridge_filter_sigma, self.ridge_threshold, thin=self.thin)
         info.set_flags(self)
+        flags = torch.from_numpy(filt.mapping_array.astype(np.int64)).to(roi.device)
+        mask_w = win.of(roi.base)
         if self.do_map_channels_segments:
-            if not M.map_channels_segments(self.cl_state, info, data, verbose=self.verbose,
-                                           runner=self._runner()):
+            ok, flags, labels = self.engine.map(info, win, roi, mask_w, flags)
+            if not ok:
                 self.print("A problem during mapping channels & segments")
-            self.mapping_array[data.bounds_grid] = data.mapping_array
-            self.coarse_subsegment_array[data.bounds_grid] = data.label_array
-            coarse = np.unique(data.label_array[~data.mask_array])
-            self.coarse_subsegments_list_array = np.sort(coarse[coarse != 0])
-            self.n_coarse_subsegments = self.coarse_subsegments_list_array.shape[0]
-            for label in self.coarse_subsegments_list_array:
-                self.merged_coarse_mask_array[self.coarse_subsegment_array == label] = False
-        self.state.reset_active_masks()
+            win.of(roi.mapping).copy_(flags)
+            win.of(roi.coarse).copy_(labels)
+            present = torch.unique(labels[~mask_w]).cpu().numpy()
+            self.coarse_subsegments_list_array = np.sort(present[present != 0]).astype(np.int32)
+            self.n_coarse_subsegments = int(self.coarse_subsegments_list_array.shape[0])
+        elif not self.do_map_hsl:
+            # the flags alone reach the region, on its unmasked pixels
+            target = win.of(roi.mapping)
+            target[~mask_w] |= flags[~mask_w]
+        base = self._base_mask()
         if self.do_map_hsl:
-            del info, data
-            mask_array = self.state.merge_active_masks()
-            bbox, nxb, nyb = get_bbox(~mask_array)
-            info = Info(self.state, self.trace, self.geodata.roi_pixel_size, mapping=self)
-            info.set_xy(nxb, nyb, pad)
+            win = _Window(torch.from_numpy(~base).to(roi.device), pad)
+            info = win.info(self)
             info.set_thresholds(segmentation_threshold=self.fine_segmentation_threshold)
-            data = Data(info=info, bbox=bbox, pad=pad, mapping_array=self.mapping_array, mask_array=mask_array)
         self.info = info
-        bounds = data.bounds_grid
-        self.mapping_array[bounds][~mask_array[bounds]] |= data.mapping_array[~mask_array[bounds]]
-        self.mapping_array[(self.mapping_array & info.is_channelhead) != 0] ^= info.is_channelhead
-        self.mapping_array[(self.mapping_array & info.is_thinchannel) != 0] ^= info.is_thinchannel
-        vprint(self.vprogress, "**Pass#1 end**")
+        self._clear(info.is_channelhead | info.is_thinchannel)
+        self.print("**Pass#1 end**")
 
-    # ---------------------------------------------- hillslope lengths of subsegments
-    def select_subsegments(self, info, data, do_restrict=True):
-        """mapping.py:819-839: the (fine) subsegment label of every unmasked
-        midslope pixel (every unmasked pixel when not restricted), and the
-        nonzero labels among them."""
-        if do_restrict:
-            if self.do_measure_hsl_from_ridges:
-                pass  # the reference selects nothing new for ridges here
-            else:
-                sel = ((data.mapping_array & info.is_midslope) > 0) & (~data.mask_array)
-                data.subsegment_label_array = data.label_array[sel].astype(np.int32)
-        else:
-            data.subsegment_label_array = data.label_array[~data.mask_array].astype(np.int32)
-        unique = np.unique(data.subsegment_label_array)
-        data.selected_subsegments_array = unique[unique != 0].astype(np.int32)
-        self.n_subsegments = unique.size
-
-    def measure_hsl_traced(self, info, data):
-        """mapping.py:910-918: the hillslope length of every selected pixel,
-        traced on the GPU (``slm_hillslope_lengths``)."""
-        data.subsegment_hsl_array = np.zeros_like(data.subsegment_label_array, dtype=np.float32)
-        return M.hsl(self.cl_state, info, data, self.do_measure_hsl_from_ridges, self.verbose,
-                     runner=self._runner())
-
-    def parse_hsl(self, info, data):
-        """mapping.py:920-944: count, mean and standard deviation of the
-        lengths per selected subsegment, as a DataFrame indexed by
-        (fine, coarse) label."""
-        import pandas as pd
-        n = data.subsegment_hsl_array.shape[0]
-        df = pd.DataFrame(np.zeros((n,), dtype=[("fine", np.int32), ("length", np.float32)]))
-        df["fine"] = data.subsegment_label_array
-        df["length"] = data.subsegment_hsl_array
-        df = df[df.fine != 0]
-        try:
-            stats_df = pd.DataFrame(data.selected_subsegments_array, columns=["fine"])
-            for stat, column in (("count", "count"), ("mean", "mean [m]"), ("std", "stddev [m]")):
-                stats_df = stats_df.join(getattr(df.groupby("fine"), stat)(), on="fine")
-                stats_df.rename(index=str, columns={"length": column}, inplace=True)
-        except Exception:  # noqa: BLE001 - the reference reports failure, not the error
-            self.print("Problem constructing HSL stats dataframe")
-            return False
-        stats_df["coarse"] = getattr(info, "coarse_label", None)
-        stats_df.set_index(["fine", "coarse"], inplace=True)
-        data.hsl_stats_df = stats_df
-        return True
-
-    def remap_hsl(self, info, data, n_hsl_averaging_threshold=None):
-        """mapping.py:946-976: each subsegment's mean length painted on its
-        pixels (0 where it has fewer than ``n_hsl_averaging_threshold``
-        lengths); the mean of the painted values of at least
-        ``hsl_averaging_threshold`` metres."""
-        if n_hsl_averaging_threshold is None:
-            n_hsl_averaging_threshold = self.n_hsl_averaging_threshold
-        stats_df = data.hsl_stats_df
-        try:
-            data.hsl_array = np.zeros((info.nx_padded, info.ny_padded), dtype=np.float32)
-            for idx, row in stats_df.iterrows():
-                data.hsl_array[data.label_array == idx[0]] = (row["mean [m]"] if row["count"] >= n_hsl_averaging_threshold
-                                                              else 0)
-        except Exception:  # noqa: BLE001
-            self.print("Problem with HSL stats dataframe")
-            return False
-        if stats_df.empty:
-            return False
-        hsl = data.hsl_array[~np.isnan(data.hsl_array)]
-        hsl = hsl[hsl >= self.hsl_averaging_threshold]
-        if hsl.shape[0] == 0:
-            return False
-        data.trace_mean_hsl = np.mean(hsl)
-        return True
-
-    def make_coarse_subsegment_masks(self, coarse_subsegment, is_left_or_right, raw_mask, dilated_mask):
-        """mapping.py:348-386: the mask of one coarse subsegment (raw), and
-        that dilated by 2 pixels for a left flank or 1 for a right flank,
-        never into the pad; returns the dilated mask's bounding box."""
-        raw_mask.fill(True)
-        raw_mask[self.coarse_subsegment_array == coarse_subsegment] = False
-        dilate(~raw_mask, n_iterations=(2 if is_left_or_right == "left" else 1), out=dilated_mask)
-        np.invert(dilated_mask, out=dilated_mask)
-        pad = self.geodata.pad_width
-        dilated_mask[:pad, :] = True
-        dilated_mask[:, :pad] = True
-        dilated_mask[-pad:, :] = True
-        dilated_mask[:, -pad:] = True
-        return get_bbox(~dilated_mask)
-
+    # ---------------------------------------------------------------- pass 2
     def pass2(self, hsl_method="traced"):
-        """mapping.py:388-560, per coarse subsegment: its dilated mask and
-        crop, the channel threshold from the crop's dslt pdf (clamped as
-        ``mapping.subsegment_channel_threshold`` does), fine channels and
-        segments, the hillslope lengths and their statistics, then the merge
-        of the subsegment's lengths and flags into the ROI grids.
-
-        The reference measures the lengths by fast marching (skfmm, absent
-        here).  Its own alternative, kept in the same method but switched
-        off, measures them along streamlines from the midslopes
-        (``select_subsegments``, ``measure_hsl_traced``, ``parse_hsl``,
-        ``remap_hsl``); that is the ``"traced"`` method, the only one here.
-        Needs ``pass1`` and an ``analysis`` (``estimate_channel_threshold``)."""
+        """Per coarse subsegment (pass 1's labels, ascending): see the module
+        docstring.  Needs ``pass1`` and an ``analysis``."""
         import pandas as pd
         if hsl_method != "traced":
             raise NotImplementedError("hsl_method {!r}: fast marching needs skfmm, which is not available "
                                       "here; use 'traced'".format(hsl_method))
-        vprint(self.vprogress, "\n**Pass#2 begin**")
-        self.vbackup = getattr(self.state, "verbose", False)
+        if self.do_measure_hsl_from_ridges:
+            raise NotImplementedError("traced hillslope lengths start from the midslopes; the reference's "
+                                      "traced measurement selects no seeds when measuring from ridges")
+        self.print("\n**Pass#2 begin**")
+        roi = self._roi
         pad = self.geodata.pad_width
-        nxp = self.geodata.roi_nx + pad * 2
-        nyp = self.geodata.roi_ny + pad * 2
-        pixel_size = self.geodata.roi_pixel_size
+        quiet = getattr(self.state, "verbose", False)
+        # the job's masks, without pass 1's mask of its coarse subsegments
         self.state.add_active_mask({"merged_coarse": self.merged_coarse_mask_array})
-        raw_mask_array = np.zeros((nxp, nyp), dtype=bool)
-        dilated_mask_array = np.zeros((nxp, nyp), dtype=bool)
-        merged_mask_array = np.zeros((nxp, nyp), dtype=bool)
-        self.hsl_array = np.zeros((nxp, nyp), dtype=np.float32)
-        self.hsl_mean_array = np.array([], dtype=np.float32)
-        self.hsl_stats_df = None
-        for idx, coarse_subsegment in enumerate(self.coarse_subsegments_list_array):
-            if idx > 0:
-                merged_mask_array.fill(False)
-            self.state.reset_active_masks()
-            is_left_or_right = "left" if coarse_subsegment < 0 else "right"
-            bbox, nxb, nyb = self.make_coarse_subsegment_masks(coarse_subsegment, is_left_or_right,
-                                                               raw_mask_array, dilated_mask_array)
-            info = Info(self.state, self.trace, pixel_size, mapping=self, coarse_label=coarse_subsegment)
-            info.set_xy(nxb, nyb, pad)
-            self.state.add_active_mask({"dilated_segment": dilated_mask_array})
-            self.state.merge_active_masks(out=merged_mask_array)
-            data = Data(info=info, bbox=bbox, pad=pad, mapping_array=self.mapping_array,
-                        mask_array=merged_mask_array, uv_array=self.preprocess.uv_array,
-                        slc_array=self.trace.slc_array, slt_array=self.trace.slt_array,
-                        sla_array=self.trace.sla_array)
-            t = self.analysis.estimate_channel_threshold(data, verbose=self.vbackup)
+        frame = torch.ones_like(roi.base)
+        frame[pad:-pad, pad:-pad] = False
+        means, tables = [], []
+        roi.hsl.zero_()
+        for label in self.coarse_subsegments_list_array:
+            base = torch.from_numpy(self._base_mask()).to(roi.device)
+            own = roi.coarse == int(label)
+            region = grow(own, 2 if label < 0 else 1) & ~frame
+            win = _Window(region, pad)
+            info = win.info(self, coarse_label=label)
+            mask_w = win.of(base | ~region)
+            t = self.analysis.estimate_channel_threshold(types.SimpleNamespace(
+                mask_array=mask_w.cpu().numpy(), slt_array=roi.slt_h[win.sl], sla_array=roi.sla_h[win.sl]),
+                verbose=quiet)
             if t is None or t > self.max_channel_threshold:
                 t = self.guess_channel_threshold
             elif t < self.min_channel_threshold:
                 t = self.guess_channel_threshold / 2
-            data.channel_threshold = t
-            info.set_thresholds(channel_threshold=data.channel_threshold,
-                                segmentation_threshold=self.fine_segmentation_threshold)
-            if not M.map_channels_segments(self.cl_state, info, data, verbose=self.verbose, runner=self._runner()):
-                del data
+            info.set_thresholds(channel_threshold=t, segmentation_threshold=self.fine_segmentation_threshold)
+            ok, flags, labels = self.engine.map(info, win, roi, mask_w, win.of(roi.mapping).clone())
+            if not ok:
                 continue
-            # this pass's channel heads are remembered as WAS_CHANNELHEAD
-            data.mapping_array[(data.mapping_array & info.is_channelhead) == info.is_channelhead] \
-                |= info.was_channelhead
-            self.select_subsegments(info, data)
-            if not self.measure_hsl_traced(info, data) or not self.parse_hsl(info, data) \
-                    or not self.remap_hsl(info, data):
-                del data
+            # this pass's channel heads are kept as WAS_CHANNELHEAD
+            head = int(info.is_channelhead)
+            flags = torch.where((flags & head) == head, flags | int(info.was_channelhead), flags)
+            picked = ((flags & int(info.is_midslope)) > 0) & ~mask_w
+            fine = labels[picked].cpu().numpy()
+            lengths = self.engine.lengths(info, flags, int(fine.shape[0]))
+            if lengths is None:
                 continue
-            self.hsl_mean_array = np.append(self.hsl_mean_array, data.trace_mean_hsl)
-            keep = data.hsl_stats_df[(data.hsl_stats_df["count"] > 1) & (data.hsl_stats_df["mean [m]"] > 5.0)]
-            self.hsl_stats_df = keep.copy() if self.hsl_stats_df is None else pd.concat([self.hsl_stats_df, keep])
-            self.state.remove_active_mask("dilated_segment")
-            self.state.add_active_mask({"raw_segment": raw_mask_array})
-            self.state.merge_active_masks(out=merged_mask_array)
-            bounds = data.bounds_grid
-            data.hsl_array[np.isnan(data.hsl_array)] = 0.0
-            self.hsl_array[bounds][~merged_mask_array[bounds]] = data.hsl_array[~merged_mask_array[bounds]]
-            self.mapping_array[bounds][~merged_mask_array[bounds]] |= data.mapping_array[~merged_mask_array[bounds]]
-            self.state.remove_active_mask("raw_segment")
-            del data
-        self.hsl_array[np.isnan(self.hsl_array)] = 0.0
-        vprint(self.vprogress, "\n**Pass#2 end**")
+            stats = length_statistics(fine, lengths, label)
+            if stats is None:
+                continue
+            painted = paint_means(labels, stats, self.n_hsl_averaging_threshold, roi.device)
+            kept = painted[~torch.isnan(painted)]
+            kept = kept[kept >= self.hsl_averaging_threshold].cpu().numpy()
+            if len(stats) == 0 or kept.shape[0] == 0:
+                continue
+            means.append(np.mean(kept))
+            tables.append(stats[(stats["count"] > 1) & (stats["mean [m]"] > 5.0)])
+            # only the subsegment's own unmasked pixels take the results
+            take = win.of(own & ~base)
+            win.of(roi.hsl)[take] = torch.nan_to_num(painted, nan=0.0)[take]
+            target = win.of(roi.mapping)
+            target[take] |= flags[take]
+        roi.hsl.nan_to_num_(nan=0.0)
+        self.hsl_mean_array = np.array(means, dtype=np.float32) if means else np.array([], dtype=np.float32)
+        self.hsl_stats_df = pd.concat(tables) if tables else None
+        self.state.reset_active_masks()
+        self.print("\n**Pass#2 end**")
 
     def pass3(self):
         raise NotImplementedError("pass 3 smooths the hillslope lengths and the aspect with scikit-image's rank "

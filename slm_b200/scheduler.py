@@ -121,8 +121,9 @@ class LengthModel:
         return b[:n].view(*shape)
 
     def _gemm(self, ta, tb, M, N, K, A, B, C, Z=None, bias=None, relu=0, rnd=0, split=0, stream=None):
+        partial = self._buf("split_k", (int(split) * int(M) * int(N),)) if split > 0 else None
         check(self.L.slm_gemm(int(ta), int(tb), int(M), int(N), int(K), ptr(A), ptr(B), ptr(C), ptr(Z),
-                              ptr(bias), int(relu), int(rnd), int(split), _stream(stream)))
+                              ptr(bias), int(relu), int(rnd), int(split), ptr(partial), _stream(stream)))
 
     @staticmethod
     def _split(M, N, K):

@@ -236,3 +236,54 @@ def test_mapping_stage_pass1_on_the_gpu():
     assert np.array_equal(gpu.mapping_array, cpu.mapping_array)
     assert np.array_equal(gpu.coarse_subsegment_array, cpu.coarse_subsegment_array)
     assert gpu.n_coarse_subsegments == cpu.n_coarse_subsegments > 0
+
+
+@pytest.mark.gpu
+def test_mapping_stage_pass2_on_the_gpu():
+    """Passes 1 and 2 with the region's grids on the GPU (device engine: the
+    mapping sequence and the traced lengths with the windows resident there)
+    equal the same passes through the wrappers on the oracle; the channel
+    thresholds come from the device KDE on both sides."""
+    import types
+
+    from mapping_cases import incised_pipeline_case
+    from slm_b200 import analysis as A
+    from slm_b200.mapping_stage import Mapping
+    from slm_b200.skeleton import zhang_suen
+    from slm_b200.useful import default_parameters
+    from test_mapping_stage import ActiveMasks
+    n = 64
+    info0, data0 = incised_pipeline_case(n=n, seed=3, n_incisions=6, max_steps=200)
+    slt, slc = data0.slt_array, data0.slc_array
+    with np.errstate(divide="ignore", invalid="ignore"):
+        sla = np.where(slc > 0, np.sqrt(2.0) * slt / slc, 0.0).astype(np.float32)
+    d = default_parameters()
+    trace = types.SimpleNamespace(**vars(d.trace))
+    trace.subpixel_seed_point_density, trace.jitter_magnitude = 1, 0.0
+    trace.integrator_step_factor, trace.max_length = 0.1, 20.0
+    trace.slc_array, trace.slt_array, trace.sla_array = slc, slt, sla
+    geodata = types.SimpleNamespace(roi_nx=n, roi_ny=n, pad_width=2, roi_pixel_size=2.0)
+    preprocess = types.SimpleNamespace(uv_array=data0.uv_array)
+    params = dict(vars(d.mapping))
+    params.update(coarse_channel_threshold=float(info0.channel_threshold), coarse_segmentation_threshold=40,
+                  fine_segmentation_threshold=10, midslope_filter_sigma=2.0, midslope_threshold=0.2,
+                  ridge_filter_sigma=2.0, ridge_threshold=0.3, do_measure_hsl_from_ridges=False,
+                  n_hsl_averaging_threshold=1, hsl_averaging_threshold=5.0, min_channel_threshold=1.0,
+                  max_channel_threshold=1000.0, guess_channel_threshold=30.0)
+    analysis_params = {"analysis": dict(A.ANALYSIS_PARAMETERS, n_hist_bins=512, n_pdf_points=64,
+                                        pdf_slt_min=1e-3, pdf_sla_min=1e-3, pdf_slc_min=1e-3)}
+    out = []
+    for runner in (None, oracle_runner):
+        state = ActiveMasks(data0.mask_array, **vars(d.state))
+        m = Mapping(state, {"mapping": params}, geodata, preprocess, trace,
+                    analysis=A.Analysis(state, analysis_params, geodata, None, trace), runner=runner,
+                    thin=zhang_suen)
+        m.pass1()
+        m.pass2()
+        out.append(m)
+    gpu, cpu = out
+    assert gpu.n_coarse_subsegments == cpu.n_coarse_subsegments > 1
+    assert np.array_equal(gpu.mapping_array, cpu.mapping_array)
+    assert np.array_equal(gpu.hsl_array, cpu.hsl_array) and gpu.hsl_array.any()
+    assert np.array_equal(gpu.hsl_mean_array, cpu.hsl_mean_array)
+    assert gpu.hsl_stats_df.equals(cpu.hsl_stats_df)

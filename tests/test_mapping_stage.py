@@ -120,13 +120,17 @@ def test_pass1_matches_reference(reference_dir, seed, do_map_hsl):
 
 
 @pytest.mark.parametrize("seed", [3, 4])
-def test_traced_hillslope_length_helpers_match_reference(reference_dir, seed):
-    """select_subsegments, measure_hsl_traced (the lengths kernel on the
-    oracle), parse_hsl and remap_hsl against the reference's methods on the
-    same mapped grids."""
+def test_traced_hillslope_length_statistics_match_reference(reference_dir, seed):
+    """The traced lengths of the midslope pixels (the lengths kernel on the
+    oracle), their per-subsegment statistics (length_statistics) and the
+    painted means (paint_means) against the reference's select_subsegments,
+    measure_hsl_traced, parse_hsl and remap_hsl on the same mapped grids."""
     import copy
 
+    import torch
+
     from mapping_cases import midslope_case
+    from slm_b200 import mapping_stage as MS
     R = _reference_mapping_module(reference_dir)
     R.lengths.hsl = lambda cl_state, info, data, do_use_ridges, verbose=False: M.hsl(
         cl_state, info, data, do_use_ridges, verbose, runner=oracle_runner)
@@ -137,20 +141,26 @@ def test_traced_hillslope_length_helpers_match_reference(reference_dir, seed):
     params = dict(do_measure_hsl_from_ridges=False, n_hsl_averaging_threshold=2, hsl_averaging_threshold=5.0)
     ref = R.Mapping.__new__(R.Mapping)
     ref.__dict__.update(params, cl_state=None, verbose=False, print=lambda *a, **k: None)
-    mine = Mapping(types.SimpleNamespace(verbose=False), {"mapping": params}, None, None, None,
-                   runner=oracle_runner)
-    rd, md = copy.deepcopy(data), copy.deepcopy(data)
-    for obj, d in ((ref, rd), (mine, md)):
-        obj.select_subsegments(info, d)
-        assert obj.measure_hsl_traced(info, d)
-        assert obj.parse_hsl(info, d)
-        assert obj.remap_hsl(info, d)
-    assert np.array_equal(md.subsegment_label_array, rd.subsegment_label_array)
-    assert np.array_equal(md.selected_subsegments_array, rd.selected_subsegments_array)
-    assert np.array_equal(md.subsegment_hsl_array.view(np.uint32), rd.subsegment_hsl_array.view(np.uint32))
-    assert md.hsl_stats_df.equals(rd.hsl_stats_df)
-    assert np.array_equal(md.hsl_array, rd.hsl_array) and md.trace_mean_hsl == rd.trace_mean_hsl
-    assert len(md.hsl_stats_df) > 3 and md.hsl_array.any()
+    rd = copy.deepcopy(data)
+    ref.select_subsegments(info, rd)
+    assert ref.measure_hsl_traced(info, rd)
+    assert ref.parse_hsl(info, rd)
+    assert ref.remap_hsl(info, rd)
+    # the same through this package: the engine's lengths, then the statistics
+    md = copy.deepcopy(data)
+    picked = ((md.mapping_array & info.is_midslope) > 0) & ~md.mask_array
+    fine = md.label_array[picked]
+    engine = MS.WrapperEngine(oracle_runner)
+    engine.data = md
+    lengths = engine.lengths(info, torch.from_numpy(md.mapping_array.astype(np.int64)), int(fine.shape[0]))
+    assert np.array_equal(lengths.view(np.uint32), rd.subsegment_hsl_array.view(np.uint32))
+    stats = MS.length_statistics(fine, lengths, 7)
+    assert stats.equals(rd.hsl_stats_df)
+    painted = MS.paint_means(torch.from_numpy(md.label_array), stats, 2, "cpu").numpy()
+    assert np.array_equal(painted, rd.hsl_array)
+    kept = painted[~np.isnan(painted)]
+    assert np.mean(kept[kept >= 5.0]) == rd.trace_mean_hsl
+    assert len(stats) > 3 and painted.any()
 
 
 class ActiveMasks:

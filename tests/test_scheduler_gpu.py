@@ -203,6 +203,91 @@ def test_learned_order_beats_shuffled():
         assert rho > 0.3, rho
 
 
+def test_training_is_deterministic():
+    """Split-K sums its K-slices in a fixed order: two trainings from the same
+    seed on the same batches give identical weights."""
+    uv_h, seeds_h = _uv_grid(5, nx=64, ny=60)
+    uv, seeds = torch.from_numpy(uv_h).to(DEV), torch.from_numpy(seeds_h).to(DEV)
+    t = torch.rand((seeds.shape[0], 2), generator=torch.Generator().manual_seed(3)).to(DEV) * 5.0
+    weights = []
+    for _ in range(2):
+        m = S.LengthModel(DEV, seed=0)
+        m.fit(uv, uv.shape[0], uv.shape[1], 2, seeds, t, steps=60, batch=512)
+        torch.cuda.synchronize()
+        weights.append(m.master.clone())
+    assert torch.equal(weights[0], weights[1])
+
+
+def _time_ms(fn, reps=5):
+    ts = []
+    for _ in range(reps + 1):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return float(np.median(ts[1:]))
+
+
+def test_learned_order_timed_on_the_kernels():
+    """The learned order on the real field kernels of a held-out DTM (time
+    includes inference and ordering): with one thread per trajectory it is
+    faster than the shuffled order; on the persistent pair launch its
+    predicted-long-first order is timed against the spatial order (printed;
+    the spatial order is this tracer's default because the persistent queue
+    leaves ordering little to gain)."""
+    m, hist, ev, _, prm, (seeds, mask, uv) = _trained_and_eval()
+    n = int(ev.info.n_seed_points)
+    nxy = int(prm.nxy_padded)
+    p = [kernel_params(ev.info, "INTEGRATE_FIELDS", sg) for sg in (1.0, -1.0)]
+    acc = torch.zeros((2, 2, nxy), dtype=torch.uint64, device=DEV)
+    work = kernels.workspace(DEV)
+    cap = S.log_cap(prm)
+    thr = [float(torch.quantile(m.predict(uv, uv.shape[0], uv.shape[1], 2, seeds, n)[:, c], 0.99)) for c in (0, 1)]
+
+    def plain(order_fn):
+        acc.zero_()
+        orders = order_fn()
+        for c in (0, 1):
+            kernels.integrate_fields(p[c], seeds, mask, uv, acc[c, 0], acc[c, 1], work, schedule="plain",
+                                     integrator=ev.spec.integrator, order=orders[c])
+
+    def learned():
+        pred = m.predict(uv, uv.shape[0], uv.shape[1], 2, seeds, n)
+        return [m.order(pred, c, cap) for c in (0, 1)]
+
+    def pair(order_fn):
+        acc.zero_()
+        o = order_fn()
+        kernels.integrate_fields_pair(p[0], p[1], seeds, mask, uv, acc[:, 0], acc[:, 1], work,
+                                      integrator=ev.spec.integrator, order=o[0], order_up=o[1])
+
+    def spatial():
+        o = S.spatial_order(seeds, n, ev.info.nx, ev.info.ny)
+        return [o, o]
+
+    def learned_spatial():
+        pred = m.predict(uv, uv.shape[0], uv.shape[1], 2, seeds, n)
+        return [S.spatial_order(seeds, n, ev.info.nx, ev.info.ny, pred=pred, col=c, threshold=thr[c])
+                for c in (0, 1)]
+
+    results = {}
+    ref = None
+    for name, fn in (("plain_shuffled", lambda: plain(lambda: [None, None])), ("plain_learned", lambda: plain(learned)),
+                     ("pair_spatial", lambda: pair(spatial)), ("pair_learned_spatial", lambda: pair(learned_spatial))):
+        fn()
+        torch.cuda.synchronize()
+        if ref is None:
+            ref = acc.clone()
+        assert torch.equal(acc, ref), name
+        results[name] = _time_ms(fn)
+    print("learned order, ms:", results)
+    assert results["plain_learned"] < results["plain_shuffled"], results
+    assert results["pair_learned_spatial"] < 1.25 * results["pair_spatial"], results
+
+
 @pytest.mark.parametrize("block", [64, 4])  # 64: bins counted in shared memory; 4: 5625 bins, global
 @pytest.mark.parametrize("with_pred", [False, True])
 def test_spatial_order(block, with_pred):
