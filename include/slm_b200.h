@@ -208,6 +208,13 @@ int slm_integrate_fields_noalloc(const slm_params* p, const slm_launch* launch,
                                  const float* seed_point, const uint8_t* mask, const float* uv,
                                  uint32_t* mapping, uint64_t* slc, uint64_t* slt, void* stream);
 
+/* slm_selftest_div6 -- no counterpart in the reference: checks on the
+ * device, over all 2^32 float bit patterns, that the tracer's division-free
+ * x / 6 (the RK4 step's weighted sum) equals the IEEE quotient.  counts:
+ * two device uint64 words; [0] receives the number of inputs that differ
+ * (NaN equals NaN), [1] the largest such bit pattern plus one (0: none). */
+int slm_selftest_div6(uint64_t* counts, void* stream);
+
 /* slm_fields_finish: the host arithmetic of Fields.integrate
  * (fields.py:146-167, 293-310) on the device, so only the finished fields
  * leave the GPU.  acc [2 directions][slc, slt][nxy_padded] uint64 raw sums

@@ -858,3 +858,35 @@ extern "C" int slm_integrate_fields_noalloc(const slm_params* p, const slm_launc
     return slm_integrate_fields(p, launch, seed_point, mask, uv, mapping, slc, slt,
                                 reinterpret_cast<uint64_t*>(scratch), stream);
 }
+
+// ------------------------------------------------------------------ self-test
+namespace slm {
+// counts[0] += inputs whose div6 differs from the IEEE quotient (NaN equals
+// NaN); counts[1] = the largest such input bit pattern + 1 (0: none)
+__global__ void k_selftest_div6(u64* counts) {
+    u64 bad = 0, last = 0;
+    for (u64 b = (u64)blockIdx.x * blockDim.x + threadIdx.x; b < (1ull << 32); b += (u64)gridDim.x * blockDim.x) {
+        const float x = __uint_as_float((uint32_t)b);
+        const float want = __fdiv_rn(x, 6.0f), got = div6(x);
+        const bool same = __float_as_uint(want) == __float_as_uint(got) || (want != want && got != got);
+        if (!same) {
+            bad++;
+            last = b + 1;
+        }
+    }
+    if (bad) {
+        atomicAdd(counts, bad);
+        atomicMax(counts + 1, last);
+    }
+}
+}  // namespace slm
+
+extern "C" int slm_selftest_div6(uint64_t* counts, void* stream) {
+    clear_error();
+    SLM_REQUIRE(counts && aligned(counts, 8), "counts must be two 8-byte aligned device words");
+    cudaStream_t s = (cudaStream_t)stream;
+    SLM_CUDA(cudaMemsetAsync(counts, 0, 2 * sizeof(uint64_t), s));
+    k_selftest_div6<<<(unsigned)(num_sms() * 8), 256, 0, s>>>((u64*)counts);
+    SLM_LAUNCHED("k_selftest_div6");
+    return SLM_OK;
+}

@@ -128,6 +128,19 @@ __device__ __forceinline__ Quant make_quant(uint32_t r) {
     return q;
 }
 
+// x / 6 correctly rounded without a division: the product by the constant
+// 1/6 held as two floats, C_h = RN(1/6) and C_l = RN(1/6 - C_h), formed as
+// RN(C_h x + RN(C_l x)) with one fused multiply-add -- Brisebarre and
+// Muller's correctly rounded multiplication by a constant ("Correctly
+// rounded multiplication by arbitrary precision constants", IEEE
+// Transactions on Computers 57(2), 2008).  For 1/6 in binary32 it gives the
+// IEEE quotient x / 6.0f for every float input; slm_selftest_div6 checks
+// that over all 2^32 bit patterns on the device.
+__device__ __forceinline__ float div6(float x) {
+    const float c_hi = 0x1.555556p-3f, c_lo = -0x1.555556p-28f;
+    return __fmaf_rn(c_hi, x, __fmul_rn(c_lo, x));
+}
+
 __device__ __forceinline__ float quant(float v, float res) {
     return __fdiv_rn((float)cvt_i8(v * res), res);
 }
@@ -210,8 +223,8 @@ __device__ __forceinline__ Step rk_step(Vec2 a, float dt, uint32_t& rng,
         Vec2 k4 = sample_uv(d, uv, p, g);
         if (JITTER) k4 = jitter(k4, rng, p.jitter_magnitude);
         const float h4x = k4.x * cf * dt, h4y = k4.y * cf * dt;
-        s.d2.x = quant(__fdiv_rn(h1x + 2.0f * h2x + 2.0f * h3x + h4x, 6.0f));
-        s.d2.y = quant(__fdiv_rn(h1y + 2.0f * h2y + 2.0f * h3y + h4y, 6.0f));
+        s.d2.x = quant(div6(h1x + 2.0f * h2x + 2.0f * h3x + h4x));
+        s.d2.y = quant(div6(h1y + 2.0f * h2y + 2.0f * h3y + h4y));
     }
     s.next.x = a.x + s.d2.x;
     s.next.y = a.y + s.d2.y;

@@ -201,3 +201,17 @@ def test_fields_pair_equals_two_directions(integrator, ordered, interleaved):
     assert int(work[1].item()) == ref[0][2] + ref[1][2]
     assert int(work[2].item()) == ref[0][3] + ref[1][3]
     assert int(work[3].item()) == ref[1][2]
+
+
+def test_division_free_sixth_is_exact_for_every_float():
+    """The RK4 step's x / 6 is a product by 1/6 held as two floats (one fused
+    multiply-add, no division); over all 2^32 float bit patterns it equals
+    the IEEE quotient x / 6.0f (NaN for NaN)."""
+    import ctypes
+
+    from slm_b200 import _lib
+    counts = torch.zeros(2, dtype=torch.uint64, device=DEV)
+    _lib.check(_lib.load().slm_selftest_div6(_lib.ptr(counts), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    torch.cuda.synchronize()
+    bad, last = (int(v) for v in counts.view(torch.int64).cpu().tolist())
+    assert bad == 0, "{} inputs differ, e.g. bit pattern {:#010x}".format(bad, last - 1)
