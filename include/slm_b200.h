@@ -209,8 +209,9 @@ int slm_integrate_fields_noalloc(const slm_params* p, const slm_launch* launch,
                                  uint32_t* mapping, uint64_t* slc, uint64_t* slt, void* stream);
 
 /* slm_selftest_div6 -- no counterpart in the reference: checks on the
- * device, over all 2^32 float bit patterns, that the tracer's division-free
- * x / 6 (the RK4 step's weighted sum) equals the IEEE quotient.  counts:
+ * device, over all 2^32 float bit patterns, that the tracer's x / 6 (the
+ * RK4 step's weighted sum; a product by a two-float constant where that is
+ * exact, else a division) equals the IEEE quotient.  counts:
  * two device uint64 words; [0] receives the number of inputs that differ
  * (NaN equals NaN), [1] the largest such bit pattern plus one (0: none). */
 int slm_selftest_div6(uint64_t* counts, void* stream);

@@ -128,17 +128,23 @@ __device__ __forceinline__ Quant make_quant(uint32_t r) {
     return q;
 }
 
-// x / 6 correctly rounded without a division: the product by the constant
-// 1/6 held as two floats, C_h = RN(1/6) and C_l = RN(1/6 - C_h), formed as
-// RN(C_h x + RN(C_l x)) with one fused multiply-add -- Brisebarre and
-// Muller's correctly rounded multiplication by a constant ("Correctly
-// rounded multiplication by arbitrary precision constants", IEEE
-// Transactions on Computers 57(2), 2008).  For 1/6 in binary32 it gives the
-// IEEE quotient x / 6.0f for every float input; slm_selftest_div6 checks
-// that over all 2^32 bit patterns on the device.
+// x / 6 correctly rounded, for finite |x| >= 2^-120 without a division: the
+// product by the constant 1/6 held as two floats, C_h = RN(1/6) and
+// C_l = RN(1/6 - C_h), formed as RN(C_h x + RN(C_l x)) with one fused
+// multiply-add -- Brisebarre and Muller's correctly rounded multiplication
+// by a constant ("Correctly rounded multiplication by arbitrary precision
+// constants", IEEE Transactions on Computers 57(2), 2008).  For 1/6 in
+// binary32 it equals the IEEE quotient x / 6.0f for every finite x with
+// |x| >= 2^-121 (checked over all 2^32 bit patterns: it differs only below
+// that, where C_l x underflows, and at +-infinity).  Those inputs, and NaN,
+// take the IEEE division; the RK4 step's sums are far inside the range.
+// slm_selftest_div6 repeats the exhaustive check on the device.
 __device__ __forceinline__ float div6(float x) {
     const float c_hi = 0x1.555556p-3f, c_lo = -0x1.555556p-28f;
-    return __fmaf_rn(c_hi, x, __fmul_rn(c_lo, x));
+    const float ax = fabsf(x);
+    if (__builtin_expect(ax >= 0x1p-120f && ax <= 0x1.fffffep+127f, 1))
+        return __fmaf_rn(c_hi, x, __fmul_rn(c_lo, x));
+    return __fdiv_rn(x, 6.0f);
 }
 
 __device__ __forceinline__ float quant(float v, float res) {

@@ -205,8 +205,9 @@ def test_fields_pair_equals_two_directions(integrator, ordered, interleaved):
 
 def test_division_free_sixth_is_exact_for_every_float():
     """The RK4 step's x / 6 is a product by 1/6 held as two floats (one fused
-    multiply-add, no division); over all 2^32 float bit patterns it equals
-    the IEEE quotient x / 6.0f (NaN for NaN)."""
+    multiply-add, no division) for finite |x| >= 2^-120, a division
+    otherwise; over all 2^32 float bit patterns it equals the IEEE quotient
+    x / 6.0f (NaN for NaN)."""
     import ctypes
 
     from slm_b200 import _lib
