@@ -68,3 +68,17 @@ def pinned_empty(shape, dtype):
 def low32(t_u64):
     """Low 32 bits of a uint64 device tensor, as uint32 (the reference's wrap-around)."""
     return t_u64.view(torch.int32).view(-1, 2)[:, 0].contiguous().view(torch.uint32)
+
+
+def traced(name):
+    """Decorator: the call runs inside an NVTX range ``name``, so profiler
+    timelines (nsys, ncu's range filters) show the stages of the path."""
+    import functools
+
+    def wrap(fn):
+        @functools.wraps(fn)
+        def inner(*args, **kwargs):
+            with torch.cuda.nvtx.range(name):
+                return fn(*args, **kwargs)
+        return inner
+    return wrap

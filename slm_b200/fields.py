@@ -29,7 +29,7 @@ import numpy as np
 import torch
 
 from . import kernels
-from .device import cuda_device, host_copy, low32, to_device
+from .device import cuda_device, host_copy, low32, to_device, traced
 from .distributed import allreduce_counts, shard_queue, shard_queue_params, sharded_field_pass
 from .params import kernel_params
 from .useful import create_seeds_device, vprint
@@ -118,6 +118,7 @@ class Fields:
     # largest slc count whose pow is looked up in a host-computed table
     SLC_TABLE_MAX = 1 << 22
 
+    @traced("slm.Fields.integrate")
     def integrate(self):
         """Trace all seeds down and up, then post-process slt/slc/sla (fields.py:69-167)."""
         vprint(self.verbose, "Integrating streamline fields...")
@@ -143,6 +144,7 @@ class Fields:
             self.data.seed_point_array = host_seeds.result()
         vprint(self.verbose, "...done")
 
+    @traced("slm.Fields.finish")
     def _finish(self, acc, scale_down, scale_up, nxp, nyp):
         """slm_fields_finish on the device; finished arrays copied to the host."""
         from . import _lib
@@ -174,6 +176,7 @@ class Fields:
         torch.cuda.current_stream(dev).synchronize()
         self.data.slc_array, self.data.slt_array, self.data.sla_array = (host_copy(o.numpy()) for o in out)
 
+    @traced("slm.Fields.trace")
     def _trace(self, seeds_d=None, mask_d=None):
         """Both passes on the device; returns the uint64 accumulators [2, 2, nxy].
         The seeds and mask come from ``data`` unless given on the device."""

@@ -53,6 +53,7 @@ import torch
 import torch.nn.functional as F
 
 from . import mapping as M
+from .device import traced
 from .useful import Info, default_parameters, vprint
 
 MAPPING_PARAMETERS = dict(vars(default_parameters().mapping))
@@ -297,6 +298,7 @@ class Mapping:
         self._roi.mapping &= ~int(flags)
 
     # ---------------------------------------------------------------- pass 1
+    @traced("slm.Mapping.pass1")
     def pass1(self):
         self.print("\n**Pass#1 begin**")
         g = self.geodata
@@ -340,6 +342,7 @@ class Mapping:
         self.print("**Pass#1 end**")
 
     # ---------------------------------------------------------------- pass 2
+    @traced("slm.Mapping.pass2")
     def pass2(self, hsl_method="traced"):
         """Per coarse subsegment (pass 1's labels, ascending): see the module
         docstring.  Needs ``pass1`` and an ``analysis``."""

@@ -30,7 +30,7 @@ import torch
 
 from . import _lib
 from ._lib import SlmPreprocessParams, check, ptr
-from .device import cuda_device
+from .device import cuda_device, traced
 
 DEFAULTS = {"do_normalize_speed": True, "vecsum_threshold": 0.95, "divergence_threshold": -0.5,
             "curl_threshold": 0.0}
@@ -129,6 +129,7 @@ class Preprocess:
             setattr(self, k, v)
         self.state, self.geodata, self.device = state, geodata, device
 
+    @traced("slm.Preprocess.do")
     def do(self):
         if getattr(self.state, "do_condition", True):
             self.conditioned_gradient_vector_field()

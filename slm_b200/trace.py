@@ -18,6 +18,7 @@ from __future__ import annotations
 
 import numpy as np
 
+from .device import traced
 from .fields import Fields
 from .trajectories import Trajectories
 from .useful import Data, Info, default_parameters, get_bbox, vprint
@@ -48,6 +49,7 @@ class Trace:
     def print(self, *args, **kwargs):
         vprint(getattr(self.state, "verbose", False), *args, **kwargs)
 
+    @traced("slm.Trace.do")
     def do(self):
         self.print("\n**Trace begin**")
         self.compute_trajectories()

@@ -16,7 +16,7 @@ import numpy as np
 import torch
 
 from . import kernels
-from .device import cuda_device, to_device
+from .device import cuda_device, to_device, traced
 from .params import kernel_params
 from .useful import compute_stats, create_seeds_device, vprint
 
@@ -36,6 +36,7 @@ class Trajectories:
         self.integrator = integrator
         self.n_steps = 0
 
+    @traced("slm.Trajectories.integrate")
     def integrate(self):
         vprint(self.verbose, "Integrating trajectories...")
         info = self.info
