@@ -416,14 +416,17 @@ int slm_cnn_gather(const float* uv, uint32_t nx_padded, uint32_t ny_padded, uint
 int slm_cnn_rearrange(const float* src, uint32_t n, float* dst, int backward, void* stream);
 /* C[M][N] = op(A) op(B) (+ bias[N], ReLU, pre-activation into Z, bf16 round
  * of the output), fp32; op(A) = A [M][K] or, trans_a, A^T with A [K][M];
- * op(B) = B [K][N] or, trans_b, B^T with B [N][K].  split_k > 0 instead adds
- * the product into C over split_k K-slices (bias, Z, relu and round_out are
- * then ignored): each slice's tile goes to partial [split_k][M][N] (device
- * workspace) and the slices are added into C in slice order, so the result
- * does not depend on the order the blocks run in. */
+ * op(B) = B [K][N] or, trans_b, B^T with B [N][K]; N <= 256.  The products
+ * run on the tensor cores (tcgen05) with A and B rounded to bfloat16 and fp32
+ * accumulation.  split_k > 0 instead adds the product into C over split_k
+ * K-slices (bias, Z, relu and round_out are then ignored): each slice's tile
+ * goes to partial [split_k][M][N] (device workspace) and the slices are
+ * added into C in slice order, so the result does not depend on the order
+ * the blocks run in.  status: a device word; bit 0 is set if a tensor-core
+ * wait ran out (the launch then leaves C incomplete). */
 int slm_gemm(int trans_a, int trans_b, int M, int N, int K, const float* A, const float* B,
              float* C, float* Z, const float* bias, int relu, int round_out, int split_k,
-             float* partial, void* stream);
+             float* partial, uint32_t* status, void* stream);
 /* dz[i] = z[i] > 0 ? da[i] : 0 */
 int slm_relu_backward(const float* da, const float* z, uint64_t n, float* dz, void* stream);
 /* db[c] += sum_r dz[r][c] */

@@ -4,8 +4,8 @@ backward and inference kernels; never by the product path).
 
 The network has no counterpart in the reference; this is a plain NumPy
 restatement of its definition in float64, with the same bfloat16 roundings
-as the device (inputs, weights, hidden activations), straight-through in the
-backward pass:
+as the device (inputs, weights, hidden activations, and the gradients where
+they enter a product), straight-through in the backward pass:
 
     x1[s, t, f]  = bf16(uv[clamp(cx-8+4ti+di), clamp(cy-8+4tj+dj), c]),
                    t = 4ti+tj, f = 2(4di+dj)+c, (cx, cy) = seed pixel + pad
@@ -89,12 +89,16 @@ def loss_and_grad(w, x1, target, rounding=True):
     loss = float((d * d).sum() / n_el)
     dy = 2.0 * d / n_el
     W = c["W"]
-    g = {"w3": c["x3"].T @ dy, "b3": dy.sum(0)}
-    dz2 = (dy @ W["w3"].T).reshape(-1, 4, 64) * (c["z2"] > 0)
-    g["w2"] = c["x2"].reshape(-1, 128).T @ dz2.reshape(-1, 64)
+    # every GEMM operand is bfloat16 (the tensor cores' input type): the
+    # gradients are rounded where they enter a product, the bias gradients
+    # sum them unrounded
+    r = (lambda a: bf16(a.astype(np.float32)).astype(np.float64)) if rounding else (lambda a: a)
+    g = {"w3": c["x3"].T @ r(dy), "b3": dy.sum(0)}
+    dz2 = (r(dy) @ W["w3"].T).reshape(-1, 4, 64) * (c["z2"] > 0)
+    g["w2"] = c["x2"].reshape(-1, 128).T @ r(dz2.reshape(-1, 64))
     g["b2"] = dz2.reshape(-1, 64).sum(0)
-    dz1 = _rearrange_back(dz2 @ W["w2"].T) * (c["z1"] > 0)
-    g["w1"] = x1.reshape(-1, 32).T @ dz1.reshape(-1, 32)
+    dz1 = _rearrange_back((r(dz2.reshape(-1, 64)) @ W["w2"].T).reshape(-1, 4, 128)) * (c["z1"] > 0)
+    g["w1"] = x1.reshape(-1, 32).T @ r(dz1.reshape(-1, 32))
     g["b1"] = dz1.reshape(-1, 32).sum(0)
     return loss, g
 

@@ -107,7 +107,7 @@ SIGNATURES = {
     "slm_signed_labels": (ctypes.c_int, [_P, _U, _U, _P]),
     "slm_cnn_gather": (ctypes.c_int, [_P, _U, _U, _U, _P, _P, _U, _P, _P]),
     "slm_cnn_rearrange": (ctypes.c_int, [_P, _U, _P, _I, _P]),
-    "slm_gemm": (ctypes.c_int, [_I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _I, _I, _P, _P]),
+    "slm_gemm": (ctypes.c_int, [_I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _I, _I, _P, _P, _P]),
     "slm_relu_backward": (ctypes.c_int, [_P, _P, ctypes.c_uint64, _P, _P]),
     "slm_bias_grad": (ctypes.c_int, [_P, ctypes.c_uint64, _I, _P, _P]),
     "slm_mse": (ctypes.c_int, [_P, _P, _P, ctypes.c_uint64, ctypes.c_float, _P, _P, _P]),

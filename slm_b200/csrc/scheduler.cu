@@ -14,9 +14,10 @@
 // (cx-8+4ti+di, cy-8+4tj+dj) clamped to the padded grid; X2[u][g], u = 2*ui+uj,
 // g = 32*(2*ei+ej) + o reads A1[4*(2ui+ei) + (2uj+ej)][o]; X3[h] = A2[h/64][h%64].
 //
-// Training runs as batched GEMMs on fp32 tiles (k_gemm: C = op(A) op(B), with
-// split-K for the weight gradients); inference is one fused kernel per warp of
-// 16 seeds on the tensor cores (mma.sync m16n8k16 bf16 -> fp32).
+// Training runs as batched GEMMs on the tensor cores (slm_gemm, gemm_tc.cu:
+// tcgen05 with bf16 operands and fp32 accumulators in tensor memory, split-K
+// for the weight gradients); inference is one fused kernel per warp of 16
+// seeds (mma.sync m16n8k16 bf16 -> fp32).
 #include <cuda_bf16.h>
 #include "capi_util.cuh"
 
@@ -69,84 +70,6 @@ __global__ void k_dx2_to_da1(const float* __restrict__ dx2, uint32_t n, float* _
     const uint32_t ui = u >> 1, uj = u & 1u, ei = e >> 1, ej = e & 1u;
     const uint32_t t = 4u * (2u * ui + ei) + (2u * uj + ej);
     da1[((size_t)s * 16 + t) * 32 + o] = dx2[tid];
-}
-
-// ------------------------------------------------------------------ GEMM
-// C[M,N] (+)= op(A)[M,K] op(B)[K,N]; op(A) = A (row-major MxK) or A^T (A is KxM),
-// op(B) = B (KxN) or B^T (B is NxK).  Epilogue (when not accumulating): + bias[N],
-// ReLU, keep the pre-activation in Z, round the output to bf16.
-// 64x64 tiles, 256 threads, 4x4 outputs each.  With ``partial`` (accumulate),
-// K is split over gridDim.z: slice z writes its tile to partial[z][M][N] and
-// k_split_sum adds the slices into C in slice order, so the sums do not
-// depend on the order blocks run in.
-template <bool TA, bool TB>
-__global__ void __launch_bounds__(256)
-k_gemm(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ C,
-       float* __restrict__ Z, const float* __restrict__ bias, int M, int N, int K,
-       int relu, int round_out, float* __restrict__ partial) {
-    __shared__ float As[16][64 + 4];
-    __shared__ float Bs[16][64 + 4];
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
-    const int kchunk = (K + gridDim.z - 1) / gridDim.z;
-    const int kb = blockIdx.z * kchunk, ke = min(K, kb + kchunk);
-    float acc[4][4] = {};
-    for (int k0 = kb; k0 < ke; k0 += 16) {
-        for (int i = threadIdx.x; i < 16 * 64; i += 256) {
-            const int kk = i / 64, mm = i % 64;
-            const int gk = k0 + kk, gm = m0 + mm;
-            float va = 0.0f;
-            if (gk < ke && gm < M) va = TA ? A[(size_t)gk * M + gm] : A[(size_t)gm * K + gk];
-            As[kk][mm] = va;
-            const int gn = n0 + mm;
-            float vb = 0.0f;
-            if (gk < ke && gn < N) vb = TB ? B[(size_t)gn * K + gk] : B[(size_t)gk * N + gn];
-            Bs[kk][mm] = vb;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < 16; ++kk) {
-            float a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const int gm = m0 + ty * 4 + i;
-        if (gm >= M) continue;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int gn = n0 + tx * 4 + j;
-            if (gn >= N) continue;
-            const size_t o = (size_t)gm * N + gn;
-            if (partial) {
-                partial[(size_t)blockIdx.z * M * N + o] = acc[i][j];
-            } else {
-                float v = acc[i][j] + (bias ? bias[gn] : 0.0f);
-                if (Z) Z[o] = v;
-                if (relu) v = fmaxf(v, 0.0f);
-                if (round_out) v = bf16r(v);
-                C[o] = v;
-            }
-        }
-    }
-}
-
-// C[o] += partial[0][o] + partial[1][o] + ... in slice order
-__global__ void k_split_sum(const float* __restrict__ partial, int slices, size_t mn, float* __restrict__ C) {
-    const size_t o = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= mn) return;
-    float v = C[o];
-    for (int z = 0; z < slices; ++z) v += partial[(size_t)z * mn + o];
-    C[o] = v;
 }
 
 // dZ = dA * (Z > 0)
@@ -536,27 +459,6 @@ int slm_cnn_rearrange(const float* src, uint32_t n, float* dst, int backward, vo
     if (backward) k_dx2_to_da1<<<grid, 256, 0, (cudaStream_t)stream>>>(src, n, dst);
     else k_a1_to_x2<<<grid, 256, 0, (cudaStream_t)stream>>>(src, n, dst);
     SLM_LAUNCHED("k_a1_to_x2/k_dx2_to_da1");
-    return SLM_OK;
-}
-
-int slm_gemm(int trans_a, int trans_b, int M, int N, int K, const float* A, const float* B, float* C,
-             float* Z, const float* bias, int relu, int round_out, int split_k, float* partial, void* stream) {
-    clear_error();
-    SLM_REQUIRE(M > 0 && N > 0 && K > 0 && A && B && C, "bad GEMM arguments");
-    SLM_REQUIRE(split_k <= 0 || partial, "split_k needs a partial buffer of split_k*M*N floats");
-    float* part = split_k > 0 ? partial : nullptr;
-    dim3 grid((N + 63) / 64, (M + 63) / 64, split_k > 0 ? split_k : 1);
-    cudaStream_t s = (cudaStream_t)stream;
-    if (trans_a && trans_b) k_gemm<true, true><<<grid, 256, 0, s>>>(A, B, C, Z, bias, M, N, K, relu, round_out, part);
-    else if (trans_a) k_gemm<true, false><<<grid, 256, 0, s>>>(A, B, C, Z, bias, M, N, K, relu, round_out, part);
-    else if (trans_b) k_gemm<false, true><<<grid, 256, 0, s>>>(A, B, C, Z, bias, M, N, K, relu, round_out, part);
-    else k_gemm<false, false><<<grid, 256, 0, s>>>(A, B, C, Z, bias, M, N, K, relu, round_out, part);
-    SLM_LAUNCHED("k_gemm");
-    if (part) {
-        const size_t mn = (size_t)M * N;
-        k_split_sum<<<(unsigned)((mn + 255) / 256), 256, 0, s>>>(part, split_k, mn, C);
-        SLM_LAUNCHED("k_split_sum");
-    }
     return SLM_OK;
 }
 

@@ -162,10 +162,14 @@ class WrapperEngine:
 
 class DeviceEngine:
     """The mapping sequence with the window's grids resident on the GPU
-    (``mapping_device.DeviceMapping`` over device tensors)."""
+    (``mapping_device.DeviceMapping`` over device tensors).  ``status`` ORs
+    the kernels' status words (1: a walk the reference leaves unbounded hit
+    its cap; 2: a read the reference would make outside the grid was
+    skipped), as ``mapping.DeviceRunner`` does."""
 
     def __init__(self, device=None):
         self.device = device
+        self.status = 0
 
     def map(self, info, win, roi, mask, mapping):
         from .mapping_device import DeviceMapping
@@ -175,8 +179,7 @@ class DeviceEngine:
         self.dm = DeviceMapping(info, data, device=roi.device)
         with torch.cuda.device(roi.device):
             ok = self.dm.map_channels_segments()
-        if self.dm.status:
-            raise RuntimeError("mapping kernel status {:#x}".format(self.dm.status))
+        self.status |= self.dm.status
         shape = mask.shape
         return (ok, self.dm.mapping.view(shape).to(torch.int64),
                 self.dm.label.view(shape).view(torch.int32).clone())

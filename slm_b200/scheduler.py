@@ -98,6 +98,16 @@ class LengthModel:
         self.G = _views(self.grad)
         self._bufs = {}
         self.L = _lib.load()
+        # bit 0: a tensor-core GEMM's wait ran out (checked by check_status)
+        self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
+
+    def check_status(self):
+        """Raise if any training GEMM since the last check gave up waiting for
+        its tensor-core work (its outputs are then incomplete)."""
+        st = int(self.status.item())
+        if st:
+            self.status.zero_()
+            raise RuntimeError("tensor-core GEMM status {:#x}: a wait for the MMAs ran out".format(st))
 
     # ------------------------------------------------------------ persistence
     def state(self):
@@ -123,7 +133,8 @@ class LengthModel:
     def _gemm(self, ta, tb, M, N, K, A, B, C, Z=None, bias=None, relu=0, rnd=0, split=0, stream=None):
         partial = self._buf("split_k", (int(split) * int(M) * int(N),)) if split > 0 else None
         check(self.L.slm_gemm(int(ta), int(tb), int(M), int(N), int(K), ptr(A), ptr(B), ptr(C), ptr(Z),
-                              ptr(bias), int(relu), int(rnd), int(split), ptr(partial), _stream(stream)))
+                              ptr(bias), int(relu), int(rnd), int(split), ptr(partial), ptr(self.status),
+                              _stream(stream)))
 
     @staticmethod
     def _split(M, N, K):
@@ -210,7 +221,9 @@ class LengthModel:
             frac = it / max(1, steps - 1)
             self.adam(lr * 0.5 * (1.0 + math.cos(math.pi * frac)), stream=stream)
             hist.append(loss)
-        return torch.cat(hist).cpu().numpy()
+        out = torch.cat(hist).cpu().numpy()
+        self.check_status()
+        return out
 
     # ------------------------------------------------------------ inference
     def predict(self, uv, nxp, nyp, pad, seeds, n, out=None, visit=None, stream=None):

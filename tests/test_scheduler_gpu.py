@@ -29,26 +29,33 @@ def _weights(seed):
 
 
 @pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
-@pytest.mark.parametrize("mnk", [(1, 1, 1), (70, 33, 45), (128, 64, 200), (5, 130, 17)])
+@pytest.mark.parametrize("mnk", [(1, 1, 1), (70, 33, 45), (128, 64, 200), (5, 130, 17), (300, 256, 130),
+                                 (4096, 2, 256), (32, 32, 5000)])
 def test_gemm_matches_torch(ta, tb, mnk):
     M, N, K = mnk
     g = torch.Generator().manual_seed(M * 7 + N * 3 + K)
     A = torch.randn((K, M) if ta else (M, K), generator=g).to(DEV)
     B = torch.randn((N, K) if tb else (K, N), generator=g).to(DEV)
     bias = torch.randn(N, generator=g).to(DEV)
-    ref = (A.T if ta else A).double() @ (B.T if tb else B).double() + bias.double()
+    # the tensor cores take A and B as bfloat16: the exact products of the
+    # rounded operands, summed in fp32 (tolerance relative to sum |a b|)
+    Ar, Br = S.bf16_round(A).double(), S.bf16_round(B).double()
+    opA, opB = (Ar.T if ta else Ar), (Br.T if tb else Br)
+    ref = opA @ opB + bias.double()
+    mag = opA.abs() @ opB.abs()
     m = S.LengthModel(DEV)
     C = torch.empty(M, N, device=DEV)
     Z = torch.empty(M, N, device=DEV)
     m._gemm(ta, tb, M, N, K, A, B, C, Z, bias, relu=1, rnd=1)
     torch.cuda.synchronize()
-    tol = 1e-5 * K ** 0.5 * (1 + ref.abs())
+    tol = 1e-5 * (mag + bias.double().abs()) + 1e-30
     assert torch.all((Z.double() - ref).abs() <= tol)
     assert torch.equal(C, S.bf16_round(torch.relu(Z)))
     C2 = torch.zeros(M, N, device=DEV)
     m._gemm(ta, tb, M, N, K, A, B, C2, split=3)
     torch.cuda.synchronize()
-    assert torch.all((C2.double() - (ref - bias.double())).abs() <= tol)
+    assert torch.all((C2.double() - (ref - bias.double())).abs() <= 1e-5 * mag + 1e-30)
+    m.check_status()
 
 
 def _uv_grid(seed, nx=40, ny=36, pad=2):
