@@ -1133,16 +1133,19 @@ def run_e2e(args, wl, dev):
     integ = wl.spec.integrator
 
     def step():
+        # as the Trace stage runs them: the fields' seed list is built on a
+        # worker thread (Fields.prepare_seeds) while the trajectories run
+        info2 = wl.fresh_info()
+        data2 = Data(info=info2, mask_array=mask_h, uv_array=uv_h,
+                     mapping_array=np.zeros(mask_h.shape, np.uint32))
+        f = Fields(0, dev.index, info=info2, data=data2, schedule=args.schedule, integrator=integ)
+        f.prepare_seeds()
         info = wl.fresh_info()
         data = Data(info=info, mask_array=mask_h, uv_array=uv_h,
                     mapping_array=np.zeros(mask_h.shape, np.uint32))
         tr = Trajectories(0, dev.index, info=info, data=data, integrator=integ)
         tr.integrate()
-        info2 = wl.fresh_info()
-        data2 = Data(info=info2, mask_array=mask_h, uv_array=uv_h,
-                     mapping_array=np.zeros(mask_h.shape, np.uint32),
-                     traj_stats_df=tr.data.traj_stats_df)
-        f = Fields(0, dev.index, info=info2, data=data2, schedule=args.schedule, integrator=integ)
+        data2.traj_stats_df = tr.data.traj_stats_df
         f.integrate()
         return tr.n_steps + sum(f.n_steps)
 
@@ -1172,8 +1175,10 @@ def run_e2e(args, wl, dev):
             "d2h_bytes_per_step": int(d2h), "steps": k,
             "ms_per_step": 1e3 * t / k, "ms_min_max": [1e3 * min(times), 1e3 * max(times)],
             "mpx_per_s": wl.n_pixels * k / t / 1e6,
-            "note": "Trajectories.integrate + Fields.integrate through the public API: seed "
-                    "creation and shuffle (swap partners drawn on the host, swaps on the GPU), "
+            "note": "Trajectories.integrate + Fields.integrate through the public API, as the Trace "
+                    "stage runs them (the fields' seed list built on a worker thread while the "
+                    "trajectories run): seed creation and shuffle for each (swap partners drawn "
+                    "on the host, swaps on the GPU), "
                     "uploads, tracing, the fields' post-processing (on the GPU), the seed list and "
                     "the finished arrays copied back, every step"}
 

@@ -481,10 +481,11 @@ int slm_create_seeds(const uint8_t* mask, uint32_t nx_padded, uint32_t ny_padded
 /* slm_create_seeds_device -- the seed list of slm_create_seeds (the same
  * rows in the same order, and the same generator state), built in DEVICE
  * memory: argwhere by the order-preserving compaction of slm_pick_seeds; the
- * swap partners drawn on the host with the same generator; the Fisher-Yates
- * swaps applied on the device in reservation rounds (a swap runs once it is
- * the earliest pending swap on both of its rows), which replaces the host's
- * random-access pass over the rows.  Replaces create_seeds
+ * swap partners drawn on the host with the same generator, by a thread of
+ * its own; the Fisher-Yates swaps applied on the device in reservation
+ * rounds (a swap runs once it is the earliest pending swap on both of its
+ * rows), chunk by chunk (4 M swaps, in sequential order) as their partners
+ * are drawn, which replaces the host's random-access pass over the rows.  Replaces create_seeds
  * (python/streamlines/useful.py:470-517) for callers that trace on the GPU.
  *   mask        DEVICE [nx_padded][ny_padded] uint8 (nonzero = masked)
  *   seed_point  DEVICE [capacity][2] float32, 8-byte aligned

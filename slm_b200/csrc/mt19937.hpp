@@ -68,14 +68,16 @@ struct Mt19937 {
     // js[i] = interval(i) for i = top .. 1, in that order: the same draws as
     // calling interval() in a loop, consumed a tempered 624-word block at a
     // time without a data-dependent branch (a rejected draw's value is
-    // written and then overwritten by the next draw for the same i).  After
-    // each block, *final_above (if given) is set to the lowest index whose
-    // js is final (release order): the index still being drawn is not.
+    // written and then overwritten by the next draw for the same i).  The
+    // mask only changes when i drops below a power of two, so the inner loop
+    // runs with it fixed while i > mask/2: a compare and a subtract per draw
+    // on the loop-carried path.  After each block, *final_above (if given) is
+    // set to the lowest index whose js is final (release order): the index
+    // still being drawn is not.  top < 2^32.
     void intervals_down(uint64_t top, uint32_t* js, std::atomic<uint64_t>* final_above = nullptr) {
         uint32_t block[624];
-        uint64_t i = top;
-        uint32_t mask = i ? (0xffffffffu >> __builtin_clz((uint32_t)i)) : 0u;
-        while (i >= 1) {
+        uint32_t i = (uint32_t)top;
+        while (i >= 1u) {
             if (pos == 624) regenerate();
             for (int k = pos; k < 624; ++k) {
                 uint32_t y = key[k];
@@ -86,16 +88,17 @@ struct Mt19937 {
                 block[k] = y;
             }
             int k = pos;
-            for (; k < 624 && i >= 1; ++k) {
-                const uint32_t v = block[k] & mask;
-                const uint64_t take = v <= (uint32_t)i ? 1u : 0u;
-                js[i] = v;
-                i -= take;
-                const uint32_t ii = (uint32_t)i;
-                mask = ii ? (0xffffffffu >> __builtin_clz(ii)) : 0u;
+            while (k < 624 && i >= 1u) {
+                const uint32_t mask = 0xffffffffu >> __builtin_clz(i);
+                const uint32_t low = mask >> 1;  // the mask holds while i > low
+                for (; k < 624 && i > low; ++k) {
+                    const uint32_t v = block[k] & mask;
+                    js[i] = v;
+                    i -= (uint32_t)(v <= i);
+                }
             }
             pos = k;
-            if (final_above) final_above->store(i + 1, std::memory_order_release);
+            if (final_above) final_above->store((uint64_t)i + 1, std::memory_order_release);
         }
     }
 };

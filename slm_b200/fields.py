@@ -32,7 +32,7 @@ from . import kernels
 from .device import cuda_device, host_copy, low32, to_device, traced
 from .distributed import allreduce_counts, shard_queue, shard_queue_params, sharded_field_pass
 from .params import kernel_params
-from .useful import create_seeds_device, vprint
+from .useful import create_seeds_device, create_seeds_device_state, vprint
 
 
 _SLC_TABLES = {}
@@ -66,6 +66,7 @@ def _staging(slot, t):
 
 
 _ROWS_POOL = None
+_SEEDS_POOL = None
 
 
 def _rows_to_host_behind(t, dev):
@@ -114,9 +115,47 @@ class Fields:
         self.seed_order = seed_order
         self.n_steps = [0, 0]
         self.n_trajectories = [0, 0]
+        self._seeds_future = None
 
     # largest slc count whose pow is looked up in a host-computed table
     SLC_TABLE_MAX = 1 << 22
+
+    def prepare_seeds(self):
+        """Start building this call's seed list now, on a worker thread and a
+        side stream, and return at once; ``integrate`` waits for it instead
+        of building the list itself.  The Trace stage calls this before it
+        runs the trajectories, so the list (host partner draws and device
+        swaps) overlaps them.  The list is the one ``integrate`` would build;
+        NumPy's global generator is set where ``integrate`` would set it."""
+        global _SEEDS_POOL
+        if _SEEDS_POOL is None:
+            from concurrent.futures import ThreadPoolExecutor
+            _SEEDS_POOL = ThreadPoolExecutor(1)
+        info, dev, mask_array, verbose = self.info, self.device, self.data.mask_array, self.verbose
+
+        def build():
+            with torch.cuda.device(dev):
+                side = torch.cuda.Stream(dev)
+                with torch.cuda.stream(side):
+                    mask_d = to_device(mask_array, dev)
+                    seeds_d, n, npad, state = create_seeds_device_state(
+                        mask_array, info.pad_width, info.n_work_items, dev, do_shuffle=info.do_shuffle,
+                        rng_seed=info.shuffle_rng_seed, verbose=verbose, mask_d=mask_d, stream=side)
+                    done = torch.cuda.Event()
+                    done.record(side)
+            return mask_d, seeds_d, n, npad, state, done
+        self._seeds_future = _SEEDS_POOL.submit(build)
+
+    def _take_prepared_seeds(self, dev):
+        mask_d, seeds_d, n, npad, state, done = self._seeds_future.result()
+        self._seeds_future = None
+        cur = torch.cuda.current_stream(dev)
+        cur.wait_event(done)
+        mask_d.record_stream(cur)
+        seeds_d.record_stream(cur)
+        if state is not None:
+            np.random.set_state(state)
+        return mask_d, seeds_d, n, npad
 
     @traced("slm.Fields.integrate")
     def integrate(self):
@@ -134,10 +173,13 @@ class Fields:
             # the seed list is built on the device (the rows create_seeds
             # gives, in its order); its host copy for data.seed_point_array is
             # taken behind the trace
-            mask_d = to_device(mask_array, dev)
-            seeds_d, info.n_seed_points, info.n_padded_seed_points = create_seeds_device(
-                mask_array, info.pad_width, info.n_work_items, dev, do_shuffle=info.do_shuffle,
-                rng_seed=info.shuffle_rng_seed, verbose=self.verbose, mask_d=mask_d)
+            if self._seeds_future is not None:
+                mask_d, seeds_d, info.n_seed_points, info.n_padded_seed_points = self._take_prepared_seeds(dev)
+            else:
+                mask_d = to_device(mask_array, dev)
+                seeds_d, info.n_seed_points, info.n_padded_seed_points = create_seeds_device(
+                    mask_array, info.pad_width, info.n_work_items, dev, do_shuffle=info.do_shuffle,
+                    rng_seed=info.shuffle_rng_seed, verbose=self.verbose, mask_d=mask_d)
             host_seeds = _rows_to_host_behind(seeds_d, dev)
             acc = self._trace(seeds_d, mask_d)
             self._finish(acc, float(dds / pixel_size), float(uds / pixel_size), nxp, nyp)

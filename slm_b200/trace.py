@@ -2,7 +2,8 @@
 
 Mirrors ``streamlines.trace.Trace`` (python/streamlines/trace.py:31-170), the
 caller of the two hot-path wrappers: ``do()`` runs ``compute_trajectories``
-then ``compute_fields``.  Each crops the merged active mask and the uv field
+then ``compute_fields``, with the fields' seed list built on a worker thread
+while the trajectories run (``Fields.prepare_seeds``).  Each crops the merged active mask and the uv field
 to the bounding box of the unmasked pixels (widened by the pad), runs
 ``slm_b200.trajectories.Trajectories`` / ``slm_b200.fields.Fields`` on the
 crop, and writes the results back into full padded ROI arrays, as the
@@ -52,8 +53,11 @@ class Trace:
     @traced("slm.Trace.do")
     def do(self):
         self.print("\n**Trace begin**")
+        # the fields' seed list is built while the trajectories run
+        job = self._fields_job()
+        job[0].prepare_seeds()
         self.compute_trajectories()
-        self.compute_fields()
+        self.compute_fields(job)
         self.print("**Trace end**\n")
 
     def _crop(self):
@@ -84,17 +88,25 @@ class Trace:
         self.streamline_arrays_list = trajectories.data.streamline_arrays_list
         self.traj_stats_df = trajectories.data.traj_stats_df
 
-    def compute_fields(self):
-        """trace.py:130-170: the slc / slt / sla fields of the cropped region,
-        written back into full padded arrays."""
+    def _fields_job(self):
+        """The Fields wrapper of the cropped region and its Data (the
+        trajectory statistics are added when the fields are computed)."""
         mask_array, bbox, pad, nxp, nyp, info = self._crop()
         data = Data(info=info, bbox=bbox, pad=pad, mask_array=mask_array, uv_array=self.preprocess.uv_array,
-                    mapping_array=np.zeros((nxp, nyp), dtype=np.uint32), traj_stats_df=self.traj_stats_df)
+                    mapping_array=np.zeros((nxp, nyp), dtype=np.uint32), traj_stats_df=None)
         fields = Fields(self.state.cl_platform, self.state.cl_device,
                         cl_src_path=getattr(self.state, "cl_src_path", None), info=info, data=data,
                         verbose=getattr(self.state, "verbose", False),
                         gpu_verbose=getattr(self.state, "gpu_verbose", False),
                         schedule=self.schedule, integrator=self.integrator)
+        return fields, data, nxp, nyp
+
+    def compute_fields(self, job=None):
+        """trace.py:130-170: the slc / slt / sla fields of the cropped region,
+        written back into full padded arrays.  ``job``: a ``_fields_job()``
+        whose seed list may already be under way."""
+        fields, data, nxp, nyp = job if job is not None else self._fields_job()
+        data.traj_stats_df = self.traj_stats_df
         fields.integrate()
         self.slc_array = np.zeros((nxp, nyp, 2), dtype=np.uint32)
         self.slt_array = np.zeros((nxp, nyp, 2), dtype=np.float32)

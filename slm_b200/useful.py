@@ -267,6 +267,20 @@ def create_seeds_device(mask, pad, n_work_items, device, n_seed_points=None, do_
     mask already on ``device`` as uint8 (else it is uploaded).  Returns
     ``(seeds [n][2] float32 CUDA tensor, n_seed_points, n_padded_seed_points)``
     with ``n_seed_points`` rows (the first rows when truncated)."""
+    seeds, n, npad, state = create_seeds_device_state(mask, pad, n_work_items, device, n_seed_points, do_shuffle,
+                                                      rng_seed, verbose, mask_d, stream)
+    if state is not None:
+        np.random.set_state(state)
+    return seeds, n, npad
+
+
+def create_seeds_device_state(mask, pad, n_work_items, device, n_seed_points=None, do_shuffle=True, rng_seed=1,
+                              verbose=False, mask_d=None, stream=None):
+    """``create_seeds_device`` without touching NumPy's global generator: the
+    generator state the reference's shuffle leaves (for
+    ``numpy.random.set_state``; None without a shuffle) is returned as a
+    fourth value instead, so the list can be built on another thread and the
+    state applied where the reference's shuffle would run."""
     import ctypes
 
     import torch
@@ -289,8 +303,7 @@ def create_seeds_device(mask, pad, n_work_items, device, n_seed_points=None, do_
                                          int(rng_seed) & 0xFFFFFFFF, _lib.ptr(out), out.shape[0], ctypes.byref(n),
                                          state.ctypes.data, _lib.ptr(ws), ws.numel(),
                                          ctypes.c_void_p(s.cuda_stream)))
-    if do_shuffle:
-        np.random.set_state(("MT19937", state[:624].copy(), int(state[624]), 0, 0.0))
+    gen_state = ("MT19937", state[:624].copy(), int(state[624]), 0, 0.0) if do_shuffle else None
     n_all = int(n.value)
     rows = n_all
     if n_seed_points is not None and n_seed_points > 0:
@@ -300,7 +313,7 @@ def create_seeds_device(mask, pad, n_work_items, device, n_seed_points=None, do_
     pad_length = (np.uint32(np.round(n_seed_points / n_work_items + 0.5)) * n_work_items
                   - n_seed_points)
     vprint(verbose, "done")
-    return out[:rows], n_seed_points, n_seed_points + pad_length
+    return out[:rows], n_seed_points, n_seed_points + pad_length, gen_state
 
 
 def pick_seeds(mask=None, map=None, flag=None, pad=None):

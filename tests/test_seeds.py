@@ -23,7 +23,8 @@ def numpy_seeds(mask, pad, do_shuffle, rng_seed):
 
 @pytest.mark.parametrize("shape,pad,seed,frac", [((7, 9), 2, 1, 0.2), ((130, 77), 2, 0, 0.1),
                                                  ((300, 257), 3, 12345, 0.5), ((1, 1), 0, 5, 0.0),
-                                                 ((64, 64), 2, 2 ** 32 - 1, 0.97), ((40, 33), 0, 7, 1.0)])
+                                                 ((64, 64), 2, 2 ** 32 - 1, 0.97), ((40, 33), 0, 7, 1.0),
+                                                 ((1100, 1000), 2, 3, 0.0)])
 @pytest.mark.parametrize("do_shuffle", [True, False])
 def test_native_seeds_match_numpy(shape, pad, seed, frac, do_shuffle):
     rng = np.random.default_rng(sum(shape) + seed % 1000)

@@ -3,8 +3,8 @@
 slm_create_seeds is pinned to NumPy's own argwhere + legacy shuffle
 (tests/test_seeds.py); the device list must hold the same rows in the same
 order and leave the same generator state, including the edge cases: no
-unmasked pixel, one, two, a truncated list, and grids up to 2052^2 (4.2 M
-rows, ~45 reservation rounds).
+unmasked pixel, one, two, a truncated list, and grids up to 4100^2 (16.6 M
+rows: the swaps go to the device in chunks of 4 M as they are drawn).
 """
 import ctypes
 
@@ -48,6 +48,7 @@ def _mask(shape, frac, seed):
     ((300, 257), 0.1, 7, True),
     ((1030, 1030), 0.02, 8, True),
     ((2052, 2052), 0.01, 9, True),
+    ((4100, 4100), 0.01, 11, True),   # 16.6 M rows: four chunks of swaps, drawn while earlier ones run
 ])
 def test_device_seeds_equal_host_seeds(shape, frac, seed, do_shuffle):
     mask = _mask(shape, frac, seed)

@@ -144,3 +144,29 @@ def test_trace_stage_on_a_cropped_region():
     assert not t.slc_array[outside].any() and t.slc_array[b].any()
     x, y = t.seed_point_array[:, 0] + pad, t.seed_point_array[:, 1] + pad
     assert (x >= bbox[0]).all() and (x <= bbox[1]).all() and (y >= bbox[2]).all() and (y <= bbox[3]).all()
+
+
+def test_fields_prepared_seed_list_is_the_same():
+    """Fields.prepare_seeds (the list built on a worker thread while the caller
+    traces trajectories) gives the same seed list, fields and generator state
+    as building the list inside integrate()."""
+    c = Case(nx=70, ny=66, seed=83, density=2, step=0.25, max_length=60.0, n_traj_seeds=200)
+    tr = Trajectories(0, 0, info=c.info, data=_data(c))
+    tr.integrate()
+    stats = tr.data.traj_stats_df
+    out = []
+    for prepared in (False, True):
+        cc = Case(nx=70, ny=66, seed=83, density=2, step=0.25, max_length=60.0)
+        f = Fields(0, 0, info=cc.info, data=_data(cc))
+        if prepared:
+            f.prepare_seeds()
+            ct = Case(nx=70, ny=66, seed=83, n_traj_seeds=200)
+            Trajectories(0, 0, info=ct.info, data=_data(ct)).integrate()  # runs while the list is built
+        f.data.traj_stats_df = stats
+        np.random.seed(777)
+        f.integrate()
+        out.append((f.data.seed_point_array, f.data.slc_array, f.data.slt_array, np.random.get_state()))
+    a, b = out
+    assert np.array_equal(a[0], b[0])
+    assert np.array_equal(a[1], b[1]) and np.array_equal(a[2].view(np.uint32), b[2].view(np.uint32))
+    assert np.array_equal(a[3][1], b[3][1]) and a[3][2] == b[3][2]

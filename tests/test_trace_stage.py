@@ -36,6 +36,9 @@ class FakeFields:
                  gpu_verbose=False, schedule="persistent", integrator=2):
         self.data = data
 
+    def prepare_seeds(self):
+        pass
+
     def integrate(self):
         d = self.data
         u = d.uv_array.astype(np.float64)
