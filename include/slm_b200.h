@@ -216,6 +216,15 @@ int slm_integrate_fields_noalloc(const slm_params* p, const slm_launch* launch,
  * (NaN equals NaN), [1] the largest such bit pattern plus one (0: none). */
 int slm_selftest_div6(uint64_t* counts, void* stream);
 
+/* slm_selftest_cvt_i8 -- no counterpart in the reference: checks on the
+ * device, over all 2^32 float bit patterns, that the tracer's float -> char
+ * conversion (one range test around the device's saturating conversion)
+ * equals the x86 conversion the reference's compress/approximate follow
+ * (essentials.cl:71-109): truncation in range, INT32_MIN's low byte (0)
+ * for NaN and out of range.  counts: DEVICE [2] uint64: mismatches, and the
+ * largest mismatching bit pattern + 1 (0: none).  Asynchronous. */
+int slm_selftest_cvt_i8(uint64_t* counts, void* stream);
+
 /* slm_fields_finish: the host arithmetic of Fields.integrate
  * (fields.py:146-167, 293-310) on the device, so only the finished fields
  * leave the GPU.  acc [2 directions][slc, slt][nxy_padded] uint64 raw sums

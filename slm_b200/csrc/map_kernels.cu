@@ -172,12 +172,20 @@ __global__ void k_map_channel_heads(const slm_params p, uint32_t n, const float2
     Vec2 vec = seed_vec(seeds, g);
     float dt = p.dt_max;
     uint32_t idx = pixel_of(vec, p), prev_idx = idx, n_steps = 0;
+    // Every state the loop continues from lies in the start pixel, and
+    // (vec, dt) determines the rest of the walk: once that state repeats
+    // (Brent) the walk circles inside the pixel until the step bound, where
+    // it returns without a change.  Walks stuck on flats and in pits end here
+    // instead of running max_n_steps steps.
+    StateCycle cyc;
+    cyc.init(vec, dt);
     while (prev_idx == idx && !mask[idx] && n_steps < p.max_n_steps) {
         const Step s = rk_plain(vec, dt, uv, p);
         idx = s.idx;
         const Move m = rk_move(s, vec, idx, p);
         n_steps++;
         dt = next_dt(dt, m.err, p);
+        if (prev_idx == idx && cyc.repeated(vec, dt)) return;
     }
     if (n_steps >= p.max_n_steps) return;
     if (!mask[idx]) {

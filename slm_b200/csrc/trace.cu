@@ -13,6 +13,7 @@
 // (a step is at most integrator_step_factor px, so a trajectory usually visits
 // a pixel several times in a row) and adds the merged count and length sum
 // with one 64-bit atomic each when it moves to another pixel.
+#include <cstring>
 #include <mutex>
 #include "capi_util.cuh"
 #include "trace_common.cuh"
@@ -117,18 +118,19 @@ __device__ __forceinline__ void field_start(FieldLane& s, u64 item, uint32_t see
 
 // One pass of the while loop of jittered_trajectory with
 // runge_kutta_step_write_sl_data (rungekutta.cl:163-186).  The Euler branch
-// of that loop is unreachable (get_array_idx clamps into the grid).
-template <int ORDER>
+// of that loop is unreachable (get_array_idx clamps into the grid).  P2:
+// trajectory_resolution and GRID_SCALE are powers of two (slm_pow2_steps).
+template <int ORDER, bool P2 = false>
 __device__ __forceinline__ void field_step(FieldLane& s, const uint8_t* __restrict__ mask,
                                            const float2* __restrict__ uv, const slm_params& p,
                                            const Geo& g, uint32_t base, Acc& acc,
                                            u64* __restrict__ slc, u64* __restrict__ slt) {
-    const Step st = rk_step<ORDER, true>(s.a, s.dt, s.rng, uv, p, g);
+    const Step st = rk_step<ORDER, true, P2>(s.a, s.dt, s.rng, uv, p, g);
     if (__ldg(mask + st.idx)) {
         s.alive = false;
         return;
     }
-    const float err = vlen(div_gs(st.d2.x - st.d1.x, g), div_gs(st.d2.y - st.d1.y, g));
+    const float err = vlen(div_gs<P2>(st.d2.x - st.d1.x, g), div_gs<P2>(st.d2.y - st.d1.y, g));
     const float dl = vlen(st.d2.x, st.d2.y);
     s.a = st.next;
     if (dl < p.integration_halt_threshold) {
@@ -253,7 +255,7 @@ k_fields_persistent(const slm_params p, const float2* __restrict__ seeds, uint32
 // direction value of the step) and its accumulator offset (0, or up_stride
 // for the upstream slc/slt); every trajectory is the single-direction
 // kernels'.
-template <int ORDER>
+template <int ORDER, bool P2>
 __global__ void __launch_bounds__(256)
 k_fields_pair(const slm_params p, float cf_up, const float2* __restrict__ seeds, uint32_t seed_begin,
               u64 n_items, const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
@@ -306,7 +308,7 @@ k_fields_pair(const slm_params p, float cf_up, const float2* __restrict__ seeds,
             continue;
         }
         if (s.alive) {
-            field_step<ORDER>(s, mask, uv, p, up ? g_up : g_down, base, acc, slc, slt);
+            field_step<ORDER, P2>(s, mask, uv, p, up ? g_up : g_down, base, acc, slc, slt);
             steps++;
             steps_up += up;
         }
@@ -545,6 +547,19 @@ __global__ void k_fields_finish(const u64* __restrict__ acc, uint32_t nxy, uint3
 
 using namespace slm;
 
+// True when the step's two power-of-two shortcuts hold for the whole launch:
+// trajectory_resolution is a power of two (Quant) and GRID_SCALE is one whose
+// reciprocal is a normal float (pow2_reciprocal), the same tests the device
+// makes per step; the pair launch then runs the form without them.
+static bool pow2_steps(const slm_params& p) {
+    const uint32_t r = p.trajectory_resolution;
+    uint32_t b;
+    std::memcpy(&b, &p.grid_scale, sizeof b);
+    const uint32_t e = (b >> 23) & 0xffu;
+    const bool gs_pow2 = (b >> 31) == 0u && (b & 0x7fffffu) == 0u && e >= 1u && e <= 253u;
+    return r != 0u && (r & (r - 1u)) == 0u && gs_pow2;
+}
+
 static int check_grid(const slm_params* p) {
     SLM_REQUIRE(p != nullptr, "params is NULL");
     SLM_REQUIRE(p->nx_padded >= 2 && p->ny_padded >= 2, "grid too small: %u x %u",
@@ -694,26 +709,31 @@ int slm_integrate_fields_pair(const slm_params* p_down, const slm_params* p_up, 
     const u64 n_items = (u64)(p_down->n_seed_points - begin) * dd;
     const float2* sp = reinterpret_cast<const float2*>(seed_point);
     const float2* u2 = reinterpret_cast<const float2*>(uv);
+    const bool p2 = pow2_steps(*p_down);
     int per_sm = L.blocks_per_sm;
     if (per_sm <= 0) {
         int occ = 0;
-        if (L.integrator == SLM_RK4)
-            SLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fields_pair<4>, block, 0));
-        else
-            SLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fields_pair<2>, block, 0));
+        const void* fn = L.integrator == SLM_RK4 ? (p2 ? (const void*)k_fields_pair<4, true>
+                                                       : (const void*)k_fields_pair<4, false>)
+                                                 : (p2 ? (const void*)k_fields_pair<2, true>
+                                                       : (const void*)k_fields_pair<2, false>);
+        SLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, block, 0));
         per_sm = occ > 0 ? occ : 1;
     }
     const unsigned grid = (unsigned)(num_sms() * per_sm);
-    if (L.integrator == SLM_RK4)
-        k_fields_pair<4><<<grid, block, 0, s>>>(*p_down, p_up->combo_factor, sp, begin, n_items, mask, u2,
-                                                (u64*)slc, (u64*)slt, (uint32_t)up_stride, (u64*)workspace,
-                                                seed_order, seed_order_up ? seed_order_up : seed_order,
-                                                refill_min(L));
-    else
-        k_fields_pair<2><<<grid, block, 0, s>>>(*p_down, p_up->combo_factor, sp, begin, n_items, mask, u2,
-                                                (u64*)slc, (u64*)slt, (uint32_t)up_stride, (u64*)workspace,
-                                                seed_order, seed_order_up ? seed_order_up : seed_order,
-                                                refill_min(L));
+    const uint32_t* o_up = seed_order_up ? seed_order_up : seed_order;
+#define SLM_PAIR_LAUNCH(ORD, P2)                                                                          \
+    k_fields_pair<ORD, P2><<<grid, block, 0, s>>>(*p_down, p_up->combo_factor, sp, begin, n_items, mask, u2, \
+                                                  (u64*)slc, (u64*)slt, (uint32_t)up_stride,              \
+                                                  (u64*)workspace, seed_order, o_up, refill_min(L))
+    if (L.integrator == SLM_RK4) {
+        if (p2) SLM_PAIR_LAUNCH(4, true);
+        else SLM_PAIR_LAUNCH(4, false);
+    } else {
+        if (p2) SLM_PAIR_LAUNCH(2, true);
+        else SLM_PAIR_LAUNCH(2, false);
+    }
+#undef SLM_PAIR_LAUNCH
     SLM_LAUNCHED("k_fields_pair");
     return SLM_OK;
 }
@@ -881,6 +901,26 @@ __global__ void k_selftest_div6(u64* counts) {
 }
 }  // namespace slm
 
+// counts[0] += inputs whose cvt_i8 differs from the x86 conversion the
+// reference's float -> char follows (cvttss2si: truncation in range, INT32_MIN
+// for NaN and out of range; the low byte kept); counts[1] as for div6
+__global__ void k_selftest_cvt_i8(u64* counts) {
+    u64 bad = 0, last = 0;
+    for (u64 b = (u64)blockIdx.x * blockDim.x + threadIdx.x; b < (1ull << 32); b += (u64)gridDim.x * blockDim.x) {
+        const float x = __uint_as_float((uint32_t)b);
+        int32_t w = (int32_t)0x80000000;
+        if (x >= -2147483648.0f && x < 2147483648.0f) w = __float2int_rz(x);
+        if ((int8_t)(w & 0xff) != cvt_i8(x)) {
+            bad++;
+            last = b + 1;
+        }
+    }
+    if (bad) {
+        atomicAdd(counts, bad);
+        atomicMax(counts + 1, last);
+    }
+}
+
 extern "C" int slm_selftest_div6(uint64_t* counts, void* stream) {
     clear_error();
     SLM_REQUIRE(counts && aligned(counts, 8), "counts must be two 8-byte aligned device words");
@@ -888,5 +928,15 @@ extern "C" int slm_selftest_div6(uint64_t* counts, void* stream) {
     SLM_CUDA(cudaMemsetAsync(counts, 0, 2 * sizeof(uint64_t), s));
     k_selftest_div6<<<(unsigned)(num_sms() * 8), 256, 0, s>>>((u64*)counts);
     SLM_LAUNCHED("k_selftest_div6");
+    return SLM_OK;
+}
+
+extern "C" int slm_selftest_cvt_i8(uint64_t* counts, void* stream) {
+    clear_error();
+    SLM_REQUIRE(counts && aligned(counts, 8), "counts must be two 8-byte aligned device words");
+    cudaStream_t s = (cudaStream_t)stream;
+    SLM_CUDA(cudaMemsetAsync(counts, 0, 2 * sizeof(uint64_t), s));
+    k_selftest_cvt_i8<<<(unsigned)(num_sms() * 8), 256, 0, s>>>((u64*)counts);
+    SLM_LAUNCHED("k_selftest_cvt_i8");
     return SLM_OK;
 }

@@ -25,10 +25,12 @@ typedef unsigned long long u64;
 
 struct Vec2 { float x, y; };
 
-// float -> char the way x86 converts (cvttss2si, keep the low byte)
+// float -> char the way x86 converts (cvttss2si, keep the low byte): x86
+// gives INT32_MIN for NaN and out-of-range values.  The device conversion
+// saturates (NaN -> 0, below -2^31 -> INT32_MIN, from 2^31 up -> INT32_MAX),
+// which has the same low byte (0) except from 2^31 up, the one case tested.
 __device__ __forceinline__ int8_t cvt_i8(float v) {
-    const int32_t i = (v >= -2147483648.0f && v < 2147483648.0f) ? __float2int_rz(v)
-                                                                 : (int32_t)0x80000000;
+    const int32_t i = (v < 2147483648.0f) ? __float2int_rz(v) : (int32_t)0x80000000;
     return (int8_t)(i & 0xff);
 }
 
@@ -67,8 +69,11 @@ __device__ __forceinline__ Geo geo_of(const slm_params& p) {
 }
 
 // x / GRID_SCALE: a multiplication when GRID_SCALE is a power of two (both
-// are the correctly rounded value of the same quotient)
+// are the correctly rounded value of the same quotient).  P2: the caller has
+// checked that it is (slm_pow2_steps), so the test is left out.
+template <bool P2 = false>
 __device__ __forceinline__ float div_gs(float x, const Geo& g) {
+    if (P2) return x * g.gs_inv;
     return g.gs_inv != 0.0f ? x * g.gs_inv : __fdiv_rn(x, g.gs);
 }
 
@@ -111,17 +116,21 @@ __device__ __forceinline__ Vec2 sample_uv(Vec2 a, const float2* __restrict__ uv,
 
 // Quantisation scale.  When trajectory_resolution is a power of two (128 by
 // default) dividing by it is exactly a multiplication by its reciprocal.
+// P2: the caller has checked that it is, so the test is left out.
+template <bool P2 = false>
 struct Quant {
     float res, inv;
     bool pow2;
     __device__ __forceinline__ float operator()(float v) const {
         const float c = (float)cvt_i8(v * res);
+        if (P2) return c * inv;
         return pow2 ? c * inv : __fdiv_rn(c, res);
     }
 };
 
-__device__ __forceinline__ Quant make_quant(uint32_t r) {
-    Quant q;
+template <bool P2 = false>
+__device__ __forceinline__ Quant<P2> make_quant(uint32_t r) {
+    Quant<P2> q;
     q.res = (float)r;
     q.inv = __fdiv_rn(1.0f, (float)r);
     q.pow2 = r != 0u && (r & (r - 1u)) == 0u;
@@ -194,14 +203,15 @@ struct Step {
 };
 
 // RK2 (computestep.cl:42-57 / 86-106), or the RK4 extension (same
-// quantisation; d1 = approx(h k1) for the error estimate).
-template <int ORDER, bool JITTER>
+// quantisation; d1 = approx(h k1) for the error estimate).  P2: the
+// trajectory resolution is a power of two (checked by the caller).
+template <int ORDER, bool JITTER, bool P2 = false>
 __device__ __forceinline__ Step rk_step(Vec2 a, float dt, uint32_t& rng,
                                         const float2* __restrict__ uv, const slm_params& p,
                                         const Geo& g) {
     Step s;
     const float cf = g.cf;
-    const Quant quant = make_quant(p.trajectory_resolution);
+    const Quant<P2> quant = make_quant<P2>(p.trajectory_resolution);
     Vec2 k1 = sample_uv(a, uv, p, g);
     if (JITTER) k1 = jitter(k1, rng, p.jitter_magnitude);
     s.u1 = k1;

@@ -216,3 +216,19 @@ def test_division_free_sixth_is_exact_for_every_float():
     torch.cuda.synchronize()
     bad, last = (int(v) for v in counts.view(torch.int64).cpu().tolist())
     assert bad == 0, "{} inputs differ, e.g. bit pattern {:#010x}".format(bad, last - 1)
+
+
+def test_float_to_char_matches_x86_for_every_float():
+    """The step quantisation's float -> char (one range test around the
+    device's saturating conversion) equals the x86 conversion the reference
+    follows over all 2^32 float bit patterns: truncation in range, low byte
+    of INT32_MIN (0) for NaN and out of range."""
+    import ctypes
+
+    from slm_b200 import _lib
+    counts = torch.zeros(2, dtype=torch.uint64, device=DEV)
+    _lib.check(_lib.load().slm_selftest_cvt_i8(_lib.ptr(counts),
+                                               ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    torch.cuda.synchronize()
+    bad, last = (int(v) for v in counts.view(torch.int64).cpu().tolist())
+    assert bad == 0, "{} inputs differ, e.g. bit pattern {:#010x}".format(bad, last - 1)
