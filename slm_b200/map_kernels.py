@@ -45,16 +45,20 @@ def _to_dev(a, dev):
     return torch.from_numpy(a).to(dev)
 
 
-def run_device(name, params, seeds_d, n, bufs, device=None, stream=None):
+def run_device(name, params, seeds_d, n, bufs, device=None, stream=None, status=None):
     """Run kernel ``name`` on device tensors (the kernel's buffers after
-    ``seed_point``, in its order); returns the status word."""
+    ``seed_point``, in its order); returns the status word.  ``status``: a
+    device uint32 word the kernel ORs its status bits into, left on the
+    device (the call then returns 0 without waiting for the kernel)."""
     L = _lib.load()
     fn_name, written, extra = SPECS[name]
     fn = getattr(L, fn_name)
     dev = device if device is not None else cuda_device(0, 0)
     st = stream if stream is not None else ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
     args = [sref(params), int(n), ptr(seeds_d)] + [ptr(b) for b in bufs]
-    status = torch.zeros(1, dtype=torch.uint32, device=dev)
+    keep = status is not None
+    if not keep:
+        status = torch.zeros(1, dtype=torch.uint32, device=dev)
     if extra == "status":
         check(fn(*(args + [ptr(status), st])))
     elif extra == "workspace":
@@ -72,7 +76,7 @@ def run_device(name, params, seeds_d, n, bufs, device=None, stream=None):
         check(rc)
     else:
         check(fn(*(args + [st])))
-    return int(status.cpu().numpy()[0])
+    return 0 if keep else int(status.cpu().numpy()[0])
 
 
 def run(name, params, seeds, arrays, device=None):

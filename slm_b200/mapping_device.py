@@ -64,7 +64,34 @@ class DeviceMapping:
         self.flag = torch.zeros(1, dtype=torch.uint32, device=dev)
         self.pick_ws = torch.empty(int(self.L.slm_pick_seeds_workspace(self.n)), dtype=torch.uint8, device=dev)
         self.seeds = torch.empty((max(1, self.n), 2), dtype=torch.float32, device=dev)
-        self.status = 0
+        # status words of the kernels that report one, read back once
+        self._status = 0
+        self._slots = torch.zeros(32, dtype=torch.uint32, device=dev)
+        self._n_slots = 0
+        self._no_status = torch.zeros(1, dtype=torch.uint32, device=dev)
+        self._prm = None
+
+    @property
+    def status(self):
+        """OR of the status words of the kernels run so far (1: a walk the
+        reference leaves unbounded hit its cap; 2: a read the reference would
+        make outside the grid was skipped)."""
+        if self._n_slots:
+            self._status |= int(np.bitwise_or.reduce(self._slots[:self._n_slots].cpu().numpy()))
+            self._slots.zero_()
+            self._n_slots = 0
+        return self._status
+
+    def _params(self, n):
+        """The launch parameters with n seeds.  They are formed from ``info``
+        once: the mapping sequence changes only the seed count."""
+        info = self.info
+        info.n_seed_points = np.uint32(n)
+        if self._prm is None:
+            self._prm = kernel_params(info, "MAPPING")
+        prm = self._prm.copy()
+        prm.n_seed_points = int(info.n_seed_points)
+        return prm
 
     def _stream(self):
         return ctypes.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
@@ -83,10 +110,15 @@ class DeviceMapping:
         check(self.L.slm_flag_op(ptr(self.mapping), ptr(select), self.n, int(op), int(a), int(b), self._stream()))
 
     def run(self, kernel, seeds, n, bufs):
-        info = self.info
-        info.n_seed_points = np.uint32(n)
-        prm = kernel_params(info, kernel.upper())
-        self.status |= map_kernels.run_device(kernel, prm, seeds, n, bufs, self.dev, self._stream())
+        prm = self._params(n)
+        if map_kernels.SPECS[kernel][2] == "status":
+            if self._n_slots == self._slots.numel():
+                self.status  # noqa: B018 - folds the words read so far
+            slot = self._slots[self._n_slots:self._n_slots + 1]
+            self._n_slots += 1
+        else:
+            slot = self._no_status
+        map_kernels.run_device(kernel, prm, seeds, n, bufs, self.dev, self._stream(), status=slot)
 
     # ------------------------------------------------------------ the sequence
     def map_channels_segments(self, do_map_channels_from_scratch=True, do_map_segments=True):

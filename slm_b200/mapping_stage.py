@@ -74,6 +74,37 @@ def grow(region, n_pixels):
     return x[0, 0] > 0
 
 
+def label_boxes(grid, labels):
+    """(x_min, x_max, y_min, y_max) of the pixels of each of ``labels`` (an
+    ascending int array) in the int grid ``grid`` [X, Y]; a host int64 array
+    [len(labels), 4].  A label with no pixel gets (X + Y, -1, X + Y, -1)."""
+    dev = grid.device
+    keys = torch.from_numpy(np.asarray(labels, dtype=np.int64)).to(dev)
+    n, (X, Y) = keys.numel(), grid.shape
+    out = torch.empty((4, n), dtype=torch.int64, device=dev)
+    if n == 0:
+        return out.t().cpu().numpy()
+    flat = grid.reshape(-1).to(torch.int64)
+    pos = torch.searchsorted(keys, flat).clamp_(max=n - 1)
+    at = torch.nonzero(keys[pos] == flat).flatten()
+    k = pos[at]
+    xs, ys = at // Y, at % Y
+    for row, v, how, init in ((0, xs, "amin", X + Y), (1, xs, "amax", -1), (2, ys, "amin", X + Y),
+                              (3, ys, "amax", -1)):
+        out[row].fill_(init).scatter_reduce_(0, k, v, how)
+    return out.t().cpu().numpy()
+
+
+def _paste(dst, dst_origin, src, src_origin):
+    """Copy ``src`` into ``dst`` where they overlap; each array's origin is
+    the grid position of its element (0, 0)."""
+    lo = [max(d, s_) for d, s_ in zip(dst_origin, src_origin)]
+    hi = [min(d + n, s_ + m) for d, n, s_, m in zip(dst_origin, dst.shape, src_origin, src.shape)]
+    if lo[0] < hi[0] and lo[1] < hi[1]:
+        dst[lo[0] - dst_origin[0]:hi[0] - dst_origin[0], lo[1] - dst_origin[1]:hi[1] - dst_origin[1]] = \
+            src[lo[0] - src_origin[0]:hi[0] - src_origin[0], lo[1] - src_origin[1]:hi[1] - src_origin[1]]
+
+
 def bounding_box(on):
     """(x_min, x_max, y_min, y_max) of the True pixels of ``on`` (bool [X, Y])."""
     xs = torch.nonzero(on.any(dim=1)).flatten()
@@ -84,10 +115,12 @@ def bounding_box(on):
 
 
 class _Window:
-    """The bounding box of ``on`` widened by ``pad`` on every side."""
+    """The bounding box of ``on`` widened by ``pad`` on every side; ``origin``:
+    the grid position of ``on``'s element (0, 0) when ``on`` is a crop."""
 
-    def __init__(self, on, pad):
+    def __init__(self, on, pad, origin=(0, 0)):
         x0, x1, y0, y1 = bounding_box(on)
+        x0, x1, y0, y1 = x0 + origin[0], x1 + origin[0], y0 + origin[1], y1 + origin[1]
         self.pad = pad
         self.nx, self.ny = x1 + 1 - x0, y1 + 1 - y0  # the box itself
         self.box = (x0, x1, y0, y1)
@@ -201,18 +234,16 @@ def length_statistics(fine_labels, lengths, coarse_label):
     formed."""
     import pandas as pd
     fine_labels = np.asarray(fine_labels, dtype=np.int32)
-    table = pd.DataFrame({"fine": fine_labels, "length": np.asarray(lengths, dtype=np.float32)})
-    table = table[table.fine != 0]
-    distinct = np.unique(fine_labels)
-    rows = pd.DataFrame(distinct[distinct != 0].astype(np.int32), columns=["fine"])
+    lengths = np.asarray(lengths, dtype=np.float32)
+    keep = fine_labels != 0
     try:
-        by = table.groupby("fine")["length"]
-        for column, stat in zip(HSL_COLUMNS, (by.count(), by.mean(), by.std())):
-            rows = rows.join(stat.rename(column), on="fine")
+        rows = pd.Series(lengths[keep]).groupby(fine_labels[keep]).agg(["count", "mean", "std"])
     except Exception:  # noqa: BLE001 - a failed subsegment is skipped, as in the reference
         return None
-    rows["coarse"] = coarse_label
-    return rows.set_index(["fine", "coarse"])
+    rows.columns = list(HSL_COLUMNS)
+    coarse = np.full(len(rows), coarse_label, dtype=np.asarray(coarse_label).dtype)
+    rows.index = pd.MultiIndex.from_arrays([rows.index.to_numpy(np.int32), coarse], names=["fine", "coarse"])
+    return rows
 
 
 def paint_means(labels, stats, min_count, device):
@@ -366,13 +397,24 @@ class Mapping:
         frame[pad:-pad, pad:-pad] = False
         means, tables = [], []
         roi.hsl.zero_()
-        for label in self.coarse_subsegments_list_array:
-            base = torch.from_numpy(self._base_mask()).to(roi.device)
-            own = roi.coarse == int(label)
-            region = grow(own, 2 if label < 0 else 1) & ~frame
-            win = _Window(region, pad)
+        # the job's masks do not change inside the loop
+        base = torch.from_numpy(self._base_mask()).to(roi.device)
+        coarse_labels = self.coarse_subsegments_list_array
+        nxp, nyp = roi.coarse.shape
+        for label, (x0, x1, y0, y1) in zip(coarse_labels, label_boxes(roi.coarse, coarse_labels)):
+            # the subsegment grown by 1 px (2 for a left flank), off the
+            # frame, worked out on the crop its growth can reach
+            g = 2 if label < 0 else 1
+            cx, cy = max(0, int(x0) - g), max(0, int(y0) - g)
+            crop = (slice(cx, min(nxp, int(x1) + g + 1)), slice(cy, min(nyp, int(y1) + g + 1)))
+            region_c = grow(roi.coarse[crop] == int(label), g) & ~frame[crop]
+            win = _Window(region_c, pad, origin=(cx, cy))
             info = win.info(self, coarse_label=label)
-            mask_w = win.of(base | ~region)
+            region = torch.zeros((win.sl[0].stop - win.sl[0].start, win.sl[1].stop - win.sl[1].start),
+                                 dtype=torch.bool, device=roi.device)
+            _paste(region, (win.sl[0].start, win.sl[1].start), region_c, (cx, cy))
+            mask_w = win.of(base) | ~region
+            own_w = win.of(roi.coarse) == int(label)
             t = self.analysis.estimate_channel_threshold(types.SimpleNamespace(
                 mask_array=mask_w.cpu().numpy(), slt_array=roi.slt_h[win.sl], sla_array=roi.sla_h[win.sl]),
                 verbose=quiet)
@@ -403,7 +445,7 @@ class Mapping:
             means.append(np.mean(kept))
             tables.append(stats[(stats["count"] > 1) & (stats["mean [m]"] > 5.0)])
             # only the subsegment's own unmasked pixels take the results
-            take = win.of(own & ~base)
+            take = own_w & ~win.of(base)
             win.of(roi.hsl)[take] = torch.nan_to_num(painted, nan=0.0)[take]
             target = win.of(roi.mapping)
             target[take] |= flags[take]
