@@ -1133,13 +1133,14 @@ def run_e2e(args, wl, dev):
     integ = wl.spec.integrator
 
     def step():
-        # as the Trace stage runs them: the fields' seed list is built on a
-        # worker thread (Fields.prepare_seeds) while the trajectories run
+        # as the Trace stage runs them: the fields' seed list and passes run
+        # on a worker thread and a side stream (Fields.prepare) while the
+        # trajectories run; integrate() then post-processes
         info2 = wl.fresh_info()
         data2 = Data(info=info2, mask_array=mask_h, uv_array=uv_h,
                      mapping_array=np.zeros(mask_h.shape, np.uint32))
         f = Fields(0, dev.index, info=info2, data=data2, schedule=args.schedule, integrator=integ)
-        f.prepare_seeds()
+        f.prepare()
         info = wl.fresh_info()
         data = Data(info=info, mask_array=mask_h, uv_array=uv_h,
                     mapping_array=np.zeros(mask_h.shape, np.uint32))
@@ -1175,10 +1176,10 @@ def run_e2e(args, wl, dev):
             "d2h_bytes_per_step": int(d2h), "steps": k,
             "ms_per_step": 1e3 * t / k, "ms_min_max": [1e3 * min(times), 1e3 * max(times)],
             "mpx_per_s": wl.n_pixels * k / t / 1e6,
-            "note": "Trajectories.integrate + Fields.integrate through the public API, as the Trace "
-                    "stage runs them (the fields' seed list built on a worker thread while the "
-                    "trajectories run): seed creation and shuffle for each (swap partners drawn "
-                    "on the host, swaps on the GPU), "
+            "note": "Trajectories.integrate + Fields.prepare/integrate through the public API, as "
+                    "the Trace stage runs them (the fields' seed list and passes on a worker thread "
+                    "and a side stream while the trajectories run): seed creation and shuffle for "
+                    "each (swap partners drawn on the host, swaps on the GPU), "
                     "uploads, tracing, the fields' post-processing (on the GPU), the seed list and "
                     "the finished arrays copied back, every step"}
 

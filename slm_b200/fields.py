@@ -115,23 +115,27 @@ class Fields:
         self.seed_order = seed_order
         self.n_steps = [0, 0]
         self.n_trajectories = [0, 0]
-        self._seeds_future = None
+        self._prepared = None
 
     # largest slc count whose pow is looked up in a host-computed table
     SLC_TABLE_MAX = 1 << 22
 
-    def prepare_seeds(self):
-        """Start building this call's seed list now, on a worker thread and a
-        side stream, and return at once; ``integrate`` waits for it instead
-        of building the list itself.  The Trace stage calls this before it
-        runs the trajectories, so the list (host partner draws and device
-        swaps) overlaps them.  The list is the one ``integrate`` would build;
-        NumPy's global generator is set where ``integrate`` would set it."""
+    def prepare(self, trace=True):
+        """Start the work of ``integrate`` that does not need the trajectory
+        statistics -- the seed list and, with ``trace``, both tracing passes
+        -- on a worker thread and a side stream, and return at once;
+        ``integrate`` waits for it and finishes (the statistics scale only the
+        post-processing).  The Trace stage calls this before it runs the
+        trajectories, so this work overlaps them.  The results are those of
+        ``integrate`` alone; NumPy's global generator is set where
+        ``integrate`` would set it.  With a process group only the seed list
+        is prepared (the passes' collectives stay on the caller's thread)."""
         global _SEEDS_POOL
         if _SEEDS_POOL is None:
             from concurrent.futures import ThreadPoolExecutor
             _SEEDS_POOL = ThreadPoolExecutor(1)
         info, dev, mask_array, verbose = self.info, self.device, self.data.mask_array, self.verbose
+        trace = trace and self.process_group is None
 
         def build():
             with torch.cuda.device(dev):
@@ -141,21 +145,31 @@ class Fields:
                     seeds_d, n, npad, state = create_seeds_device_state(
                         mask_array, info.pad_width, info.n_work_items, dev, do_shuffle=info.do_shuffle,
                         rng_seed=info.shuffle_rng_seed, verbose=verbose, mask_d=mask_d, stream=side)
+                    acc = host_seeds = None
+                    if trace:
+                        info.n_seed_points, info.n_padded_seed_points = n, npad
+                        host_seeds = _rows_to_host_behind(seeds_d, dev)
+                        acc = self._trace(seeds_d, mask_d)
                     done = torch.cuda.Event()
                     done.record(side)
-            return mask_d, seeds_d, n, npad, state, done
-        self._seeds_future = _SEEDS_POOL.submit(build)
+            return mask_d, seeds_d, n, npad, state, done, acc, host_seeds
+        self._prepared = _SEEDS_POOL.submit(build)
 
-    def _take_prepared_seeds(self, dev):
-        mask_d, seeds_d, n, npad, state, done = self._seeds_future.result()
-        self._seeds_future = None
+    def prepare_seeds(self):
+        """``prepare`` without the tracing passes: only the seed list."""
+        self.prepare(trace=False)
+
+    def _take_prepared(self, dev):
+        mask_d, seeds_d, n, npad, state, done, acc, host_seeds = self._prepared.result()
+        self._prepared = None
         cur = torch.cuda.current_stream(dev)
         cur.wait_event(done)
-        mask_d.record_stream(cur)
-        seeds_d.record_stream(cur)
+        for t in (mask_d, seeds_d, acc):
+            if t is not None:
+                t.record_stream(cur)
         if state is not None:
             np.random.set_state(state)
-        return mask_d, seeds_d, n, npad
+        return mask_d, seeds_d, n, npad, acc, host_seeds
 
     @traced("slm.Fields.integrate")
     def integrate(self):
@@ -173,15 +187,18 @@ class Fields:
             # the seed list is built on the device (the rows create_seeds
             # gives, in its order); its host copy for data.seed_point_array is
             # taken behind the trace
-            if self._seeds_future is not None:
-                mask_d, seeds_d, info.n_seed_points, info.n_padded_seed_points = self._take_prepared_seeds(dev)
+            acc = host_seeds = None
+            if self._prepared is not None:
+                mask_d, seeds_d, info.n_seed_points, info.n_padded_seed_points, acc, host_seeds = \
+                    self._take_prepared(dev)
             else:
                 mask_d = to_device(mask_array, dev)
                 seeds_d, info.n_seed_points, info.n_padded_seed_points = create_seeds_device(
                     mask_array, info.pad_width, info.n_work_items, dev, do_shuffle=info.do_shuffle,
                     rng_seed=info.shuffle_rng_seed, verbose=self.verbose, mask_d=mask_d)
-            host_seeds = _rows_to_host_behind(seeds_d, dev)
-            acc = self._trace(seeds_d, mask_d)
+            if acc is None:
+                host_seeds = _rows_to_host_behind(seeds_d, dev)
+                acc = self._trace(seeds_d, mask_d)
             self._finish(acc, float(dds / pixel_size), float(uds / pixel_size), nxp, nyp)
             self.data.seed_point_array = host_seeds.result()
         vprint(self.verbose, "...done")

@@ -2,8 +2,10 @@
 
 Mirrors ``streamlines.trace.Trace`` (python/streamlines/trace.py:31-170), the
 caller of the two hot-path wrappers: ``do()`` runs ``compute_trajectories``
-then ``compute_fields``, with the fields' seed list built on a worker thread
-while the trajectories run (``Fields.prepare_seeds``).  Each crops the merged active mask and the uv field
+then ``compute_fields``, with the fields' seed list and tracing passes run
+on a worker thread and a side stream while the trajectories run
+(``Fields.prepare``; the trajectory statistics are needed only by the
+fields' post-processing).  Each crops the merged active mask and the uv field
 to the bounding box of the unmasked pixels (widened by the pad), runs
 ``slm_b200.trajectories.Trajectories`` / ``slm_b200.fields.Fields`` on the
 crop, and writes the results back into full padded ROI arrays, as the
@@ -53,9 +55,9 @@ class Trace:
     @traced("slm.Trace.do")
     def do(self):
         self.print("\n**Trace begin**")
-        # the fields' seed list is built while the trajectories run
+        # the fields' seed list and passes run while the trajectories run
         job = self._fields_job()
-        job[0].prepare_seeds()
+        job[0].prepare()
         self.compute_trajectories()
         self.compute_fields(job)
         self.print("**Trace end**\n")

@@ -146,10 +146,12 @@ def test_trace_stage_on_a_cropped_region():
     assert (x >= bbox[0]).all() and (x <= bbox[1]).all() and (y >= bbox[2]).all() and (y <= bbox[3]).all()
 
 
-def test_fields_prepared_seed_list_is_the_same():
-    """Fields.prepare_seeds (the list built on a worker thread while the caller
-    traces trajectories) gives the same seed list, fields and generator state
-    as building the list inside integrate()."""
+@pytest.mark.parametrize("trace", [False, True])
+def test_fields_prepared_work_is_the_same(trace):
+    """Fields.prepare (the seed list, and with trace both passes, on a worker
+    thread and a side stream while the caller traces trajectories) gives the
+    same seed list, fields, step counts and generator state as integrate()
+    alone."""
     c = Case(nx=70, ny=66, seed=83, density=2, step=0.25, max_length=60.0, n_traj_seeds=200)
     tr = Trajectories(0, 0, info=c.info, data=_data(c))
     tr.integrate()
@@ -159,14 +161,18 @@ def test_fields_prepared_seed_list_is_the_same():
         cc = Case(nx=70, ny=66, seed=83, density=2, step=0.25, max_length=60.0)
         f = Fields(0, 0, info=cc.info, data=_data(cc))
         if prepared:
-            f.prepare_seeds()
+            f.prepare(trace=trace)
             ct = Case(nx=70, ny=66, seed=83, n_traj_seeds=200)
-            Trajectories(0, 0, info=ct.info, data=_data(ct)).integrate()  # runs while the list is built
+            Trajectories(0, 0, info=ct.info, data=_data(ct)).integrate()  # runs meanwhile
         f.data.traj_stats_df = stats
         np.random.seed(777)
         f.integrate()
-        out.append((f.data.seed_point_array, f.data.slc_array, f.data.slt_array, np.random.get_state()))
+        out.append((f.data.seed_point_array, f.data.slc_array, f.data.slt_array, f.data.sla_array,
+                    np.random.get_state(), list(f.n_steps)))
     a, b = out
     assert np.array_equal(a[0], b[0])
-    assert np.array_equal(a[1], b[1]) and np.array_equal(a[2].view(np.uint32), b[2].view(np.uint32))
-    assert np.array_equal(a[3][1], b[3][1]) and a[3][2] == b[3][2]
+    assert np.array_equal(a[1], b[1])
+    assert np.array_equal(a[2].view(np.uint32), b[2].view(np.uint32))
+    assert np.array_equal(a[3].view(np.uint32), b[3].view(np.uint32))
+    assert np.array_equal(a[4][1], b[4][1]) and a[4][2] == b[4][2]
+    assert a[5] == b[5]
