@@ -1140,11 +1140,13 @@ def run_e2e(args, wl, dev):
         data2 = Data(info=info2, mask_array=mask_h, uv_array=uv_h,
                      mapping_array=np.zeros(mask_h.shape, np.uint32))
         f = Fields(0, dev.index, info=info2, data=data2, schedule=args.schedule, integrator=integ)
-        f.prepare()
+        launched = threading.Event()
+        f.prepare(after=launched)
         info = wl.fresh_info()
         data = Data(info=info, mask_array=mask_h, uv_array=uv_h,
                     mapping_array=np.zeros(mask_h.shape, np.uint32))
         tr = Trajectories(0, dev.index, info=info, data=data, integrator=integ)
+        tr.launched = launched
         tr.integrate()
         data2.traj_stats_df = tr.data.traj_stats_df
         f.integrate()

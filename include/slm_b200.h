@@ -345,7 +345,14 @@ int slm_subsegment_flanks(const slm_params* p, uint32_t n_seeds, const float* se
                           const uint32_t* channel_label, const uint32_t* link, uint32_t* label,
                           void* stream);
 /* fix_right_flanks / fix_left_flanks (opencl/segment.cl:441-504, 530-594;
- * segment.py:210-232) */
+ * segment.py:210-232), with the result of the items run in ascending order.
+ * One persistent launch walks every item once, taking items in ascending
+ * order and waiting (bounded) for the final label of a lower-index item whose
+ * pixel it reads.  If a wait runs out, or when the environment variable
+ * SLM_FLANK_ROUNDS is set to a nonzero value, the labels are restored and the
+ * multi-launch form runs: paths stored (within the workspace beyond the
+ * minimum slm_fix_flanks_workspace(n, nxy, 0); SLM_ERR_CAPACITY with
+ * *required_bytes when one path does not fit), then resolved in rounds. */
 size_t slm_fix_flanks_workspace(uint32_t n_seeds, uint32_t nxy_padded, uint64_t n_path_steps);
 int slm_fix_right_flanks(const slm_params* p, uint32_t n_seeds, const float* seed_point,
                          const uint8_t* mask, const float* uv, const uint32_t* mapping,

@@ -25,16 +25,20 @@
 //   fix_right_flanks, fix_left_flanks  every work-item writes only its own
 //       pixel's label and reads labels along its RK path, so its result depends
 //       only on the final labels of lower-index items owning pixels on that
-//       path.  Paths are traced in parallel (k_flank_paths, compressed to the
-//       steps whose (compute pixel, moved-to pixel) pair changes), then items
-//       are resolved in rounds (k_flank_round): an item resolves once every
+//       path.  One persistent launch (k_flank_resolve) takes items in
+//       ascending order and walks each once, waiting for the final label of a
+//       lower-index owner it reads.  Fallback (a bounded wait ran out): paths
+//       are traced in parallel (k_flank_paths, compressed to the steps whose
+//       (compute pixel, moved-to pixel) pair changes), then items are
+//       resolved in rounds (k_flank_round): an item resolves once every
 //       lower-index owner it reads has resolved in an earlier round.  The
-//       lowest unresolved item always can, so the rounds end.
+//       lowest unresolved item always can, so both forms end.
 //
 // Every loop is bounded; a cap that the reference would exceed (it would loop
 // on) or a neighbour index outside the grid sets a bit in the caller's status
 // word instead of trapping.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 #include "capi_util.cuh"
@@ -850,6 +854,195 @@ __global__ void k_flank_round(const slm_params p, uint32_t g0, uint32_t n, uint3
     atomicAdd(n_resolved, 1u);
 }
 
+// ------------------------------------------------------------------ fix flanks in one pass
+// fix_right_flanks (side 0) / fix_left_flanks (side 1) with every walk traced
+// once, in the pinned schedule's result.  Persistent warps take items in
+// ascending index from a queue (warp-aggregated atomicAdd), so every item
+// below one a lane holds has been taken.  A lane walks its item as the
+// reference does; a label it reads belongs to its own pixel (its running
+// value), to no item or a higher-index one (the initial label), or to a
+// lower-index item, whose final label it must wait for.  A lane that has to
+// wait does nothing this pass and tries the same read on the next; a read
+// has no side effect, so trying again changes nothing.  The lowest
+// unresolved item taken waits on nothing unresolved, so some lane always
+// advances.  Its label is published with a fence before its resolved flag.
+//
+// A walk whose (vec, dt) state repeats (Brent) is periodic; every read but
+// that of its own pixel gives the same value each lap, so a lap is a
+// function of the running label at its start.  Once that label repeats at a
+// lap start, whole multiples of its period of laps are skipped (the state
+// and the label come back unchanged).
+//
+// Every wait is bounded: a lane that has waited FLANK_WAIT_LIMIT passes in
+// a row sets bit 0 of *status and gives up its item; the caller then runs the
+// multi-launch form (k_flank_paths + k_flank_round) instead.
+#define FLANK_WAIT_LIMIT (1u << 22)
+
+// label of pixel q as item g (own pixel h, running label lab_h) reads it;
+// false: its lower-index owner has not resolved yet
+__device__ __forceinline__ bool flank_read_live(uint32_t q, uint32_t g, uint32_t h, uint32_t lab_h,
+                                                const uint32_t* __restrict__ owner,
+                                                const uint32_t* __restrict__ label_init, const uint32_t* label,
+                                                const uint32_t* resolved, uint32_t& out) {
+    if (q == h) { out = lab_h; return true; }
+    const uint32_t o = owner[q];
+    if (o == NO_OWNER || o > g) { out = label_init[q]; return true; }
+    if (((volatile const uint32_t*)resolved)[o] == 0u) return false;
+    __threadfence();
+    out = ((volatile const uint32_t*)label)[q];
+    return true;
+}
+
+struct FlankWalk {
+    Vec2 vec, tv;
+    float dt, tdt;
+    uint32_t g, h, at, n_steps, lab_h;
+    uint32_t power, lam;               // Brent's checkpoint
+    uint32_t lap_len, next_lap, laps;  // lap bookkeeping once periodic (lap_len > 0)
+    uint32_t seen[8];                  // running label at the first lap starts
+    uint32_t waited;
+    bool alive, finishing, skipped;
+};
+
+__global__ void __launch_bounds__(256)
+k_flank_resolve(const slm_params p, uint32_t n, uint32_t side, const float2* __restrict__ seeds,
+                const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
+                const uint32_t* __restrict__ mapping, const uint32_t* __restrict__ owner,
+                const uint32_t* __restrict__ label_init, uint32_t* label, uint32_t* resolved,
+                uint32_t* queue_head, uint32_t* status) {
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    const uint32_t lfa = p.left_flank_addition, thin = p.is_thinchannel;
+    FlankWalk w;
+    w.alive = false;
+    bool drained = false;
+    for (uint32_t pass = 0;; ++pass) {
+        // a lane that gave up stops every warp (the caller falls back)
+        if ((pass & 255u) == 0u) {
+            uint32_t stop = 0;
+            if (lane == 0) stop = *(volatile const uint32_t*)status;
+            if (__shfl_sync(FULL, stop, 0)) break;
+        }
+        if (!drained) {
+            const unsigned idle = __ballot_sync(FULL, !w.alive);
+            if (idle) {
+                const int leader = __ffs(idle) - 1;
+                uint32_t head = 0;
+                if ((int)lane == leader) head = atomicAdd(queue_head, (uint32_t)__popc(idle));
+                head = __shfl_sync(FULL, head, leader);
+                if ((u64)head + __popc(idle) >= n) drained = true;
+                if (!w.alive) {
+                    const uint32_t g = head + __popc(idle & ((1u << lane) - 1u));
+                    if (g < n) {
+                        w.g = g;
+                        w.vec = seed_vec(seeds, g);
+                        w.h = pixel_of(w.vec, p);
+                        w.at = w.h;
+                        w.dt = p.dt_max;
+                        w.n_steps = 0;
+                        w.lab_h = label_init[w.h];
+                        w.tv = w.vec;
+                        w.tdt = w.dt;
+                        w.power = 1;
+                        w.lam = 0;
+                        w.lap_len = 0;
+                        w.waited = 0;
+                        w.alive = true;
+                        w.finishing = false;
+                        w.skipped = false;
+                    }
+                }
+            }
+        }
+        if (!__any_sync(FULL, w.alive)) {
+            if (drained) break;
+            continue;
+        }
+        if (!w.alive) continue;
+        bool blocked = false;
+        uint32_t v = 0;
+        if (!w.finishing) {
+            // the loop test at the current pixel, then one step
+            if (mask[w.at] || (mapping[w.at] & thin) || w.n_steps >= p.max_n_steps) {
+                w.finishing = true;
+            } else if (!flank_read_live(w.at, w.g, w.h, w.lab_h, owner, label_init, label, resolved, v)) {
+                blocked = true;
+            } else if (side ? ((v & lfa) == 0u) : ((v & lfa) != 0u)) {
+                w.finishing = true;
+            } else {
+                const Step st = rk_plain(w.vec, w.dt, uv, p);
+                if (!flank_read_live(st.idx, w.g, w.h, w.lab_h, owner, label_init, label, resolved, v)) {
+                    blocked = true;
+                } else {
+                    if ((w.lab_h & ~lfa) != (v & ~lfa)) w.lab_h = v;
+                    uint32_t idx = st.idx;
+                    const bool stuck = seg_move(st, w.vec, idx, w.dt, w.n_steps, p);
+                    w.at = idx;
+                    if (stuck) {
+                        w.finishing = true;
+                    } else if (w.lap_len == 0u) {
+                        w.lam++;
+                        if (__float_as_uint(w.vec.x) == __float_as_uint(w.tv.x) &&
+                            __float_as_uint(w.vec.y) == __float_as_uint(w.tv.y) &&
+                            __float_as_uint(w.dt) == __float_as_uint(w.tdt)) {
+                            w.lap_len = w.lam;
+                            w.next_lap = w.n_steps;
+                            w.laps = 0;
+                        } else if (w.lam == w.power) {
+                            w.tv = w.vec;
+                            w.tdt = w.dt;
+                            w.power <<= 1;
+                            w.lam = 0;
+                        }
+                    }
+                    if (w.lap_len && !w.skipped && w.n_steps == w.next_lap) {
+                        for (uint32_t i = 0; i < w.laps && i < 8u; ++i)
+                            if (w.seen[i] == w.lab_h) {
+                                const uint32_t per = w.laps - i;
+                                const uint32_t full = (p.max_n_steps - w.n_steps) / w.lap_len;
+                                w.n_steps += (full / per) * per * w.lap_len;
+                                w.skipped = true;
+                                break;
+                            }
+                        if (!w.skipped) {
+                            if (w.laps < 8u) w.seen[w.laps] = w.lab_h;
+                            else w.skipped = true;  // no repeat within 8 laps: step on to the bound
+                            w.laps++;
+                            w.next_lap += w.lap_len;
+                        }
+                    }
+                }
+            }
+        }
+        if (w.finishing && !blocked) {
+            // after the loop: the label at the last pixel, then the flank bit
+            if (!flank_read_live(w.at, w.g, w.h, w.lab_h, owner, label_init, label, resolved, v)) {
+                blocked = true;
+            } else {
+                if ((w.lab_h & ~lfa) != (v & ~lfa)) w.lab_h = v;
+                flank_read_live(w.at, w.g, w.h, w.lab_h, owner, label_init, label, resolved, v);
+                if (side) {
+                    if (((~v) & lfa) && !(mapping[w.at] & thin)) w.lab_h &= ~lfa;
+                } else {
+                    if (v & lfa) w.lab_h |= lfa;
+                }
+                label[w.h] = w.lab_h;
+                __threadfence();
+                ((volatile uint32_t*)resolved)[w.g] = 1u;
+                w.alive = false;
+            }
+        }
+        if (blocked) {
+            if (++w.waited >= FLANK_WAIT_LIMIT) {
+                atomicOr(status, 1u);
+                w.alive = false;
+            }
+        } else {
+            w.waited = 0;
+        }
+    }
+}
+
 // ------------------------------------------------------------------ hillslopes
 __global__ void k_hillslopes(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
                              const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
@@ -1323,11 +1516,37 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
     uint32_t* resolved = hpix + n;
     uint32_t* owner = resolved + n;
     uint32_t* label_init = owner + nxy;
-    uint32_t* n_resolved = label_init + nxy;
-    uintptr_t pa = reinterpret_cast<uintptr_t>(n_resolved + 1);
+    uint32_t* n_resolved = label_init + nxy;  // [0] rounds: resolved count; [1] queue head; [2] status
+    uintptr_t pa = reinterpret_cast<uintptr_t>(n_resolved + 4);
     pa = (pa + 15) & ~(uintptr_t)15;
     uint2* pairs = reinterpret_cast<uint2*>(pa);
     const u64 cap_pairs = (workspace_bytes - fixed) / sizeof(uint2);
+    SLM_CUDA(cudaMemsetAsync(owner, 0xff, (size_t)nxy * sizeof(uint32_t), SS));
+    SLM_CUDA(cudaMemsetAsync(resolved, 0, (size_t)n * sizeof(uint32_t), SS));
+    SLM_CUDA(cudaMemcpyAsync(label_init, label, (size_t)nxy * sizeof(uint32_t), cudaMemcpyDeviceToDevice, SS));
+    k_owner_map<<<blocks_for(n, 256), 256, 0, SS>>>(*p, n, F2(seed_point), owner, hpix);
+    SLM_LAUNCHED("k_owner_map");
+    if (required_bytes) *required_bytes = fixed;
+    // The one-pass form (k_flank_resolve); the multi-launch form below if a
+    // wait there ran out, or when SLM_FLANK_ROUNDS is set (for tests).
+    const char* force = std::getenv("SLM_FLANK_ROUNDS");
+    if (!(force && force[0] && force[0] != '0')) {
+        SLM_CUDA(cudaMemsetAsync(n_resolved, 0, 4 * sizeof(uint32_t), SS));
+        int occ = 0;
+        SLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_flank_resolve, 256, 0));
+        const unsigned grid = (unsigned)(num_sms() * (occ > 0 ? occ : 1));
+        k_flank_resolve<<<grid, 256, 0, SS>>>(*p, n, left ? 1u : 0u, F2(seed_point), mask, F2(uv), mapping, owner,
+                                              label_init, label, resolved, n_resolved + 1, n_resolved + 2);
+        SLM_LAUNCHED("k_flank_resolve");
+        uint32_t st = 0;
+        SLM_CUDA(cudaMemcpyAsync(&st, n_resolved + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, SS));
+        SLM_CUDA(cudaStreamSynchronize(SS));
+        if (st == 0u) return SLM_OK;
+        // start over from the initial labels
+        SLM_CUDA(cudaMemcpyAsync(label, label_init, (size_t)nxy * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                                 SS));
+        SLM_CUDA(cudaMemsetAsync(resolved, 0, (size_t)n * sizeof(uint32_t), SS));
+    }
     k_flank_paths<<<blocks_for(n, 128), 128, 0, SS>>>(*p, 0u, n, F2(seed_point), mask, F2(uv), mapping,
                                                      n_pairs, nullptr, 0ull, nullptr);
     SLM_LAUNCHED("k_flank_paths");
@@ -1364,11 +1583,6 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
             a = b;
         }
     }
-    SLM_CUDA(cudaMemsetAsync(owner, 0xff, (size_t)nxy * sizeof(uint32_t), SS));
-    SLM_CUDA(cudaMemsetAsync(resolved, 0, (size_t)n * sizeof(uint32_t), SS));
-    SLM_CUDA(cudaMemcpyAsync(label_init, label, (size_t)nxy * sizeof(uint32_t), cudaMemcpyDeviceToDevice, SS));
-    k_owner_map<<<blocks_for(n, 256), 256, 0, SS>>>(*p, n, F2(seed_point), owner, hpix);
-    SLM_LAUNCHED("k_owner_map");
     uint32_t round = 1;
     for (const auto& c : chunks) {
         const uint32_t a = c.first, m = c.second - c.first;

@@ -67,6 +67,7 @@ def _staging(slot, t):
 
 _ROWS_POOL = None
 _SEEDS_POOL = None
+PREPARE_WAIT_S = 60.0  # longest wait of Fields.prepare's passes for their ``after`` event
 
 
 def _rows_to_host_behind(t, dev):
@@ -120,7 +121,7 @@ class Fields:
     # largest slc count whose pow is looked up in a host-computed table
     SLC_TABLE_MAX = 1 << 22
 
-    def prepare(self, trace=True):
+    def prepare(self, trace=True, after=None):
         """Start the work of ``integrate`` that does not need the trajectory
         statistics -- the seed list and, with ``trace``, both tracing passes
         -- on a worker thread and a side stream, and return at once;
@@ -129,7 +130,10 @@ class Fields:
         trajectories, so this work overlaps them.  The results are those of
         ``integrate`` alone; NumPy's global generator is set where
         ``integrate`` would set it.  With a process group only the seed list
-        is prepared (the passes' collectives stay on the caller's thread)."""
+        is prepared (the passes' collectives stay on the caller's thread).
+        ``after``: a ``threading.Event``; the passes start once it is set (at
+        most PREPARE_WAIT_S later), so work the caller queues first is not
+        held behind the persistent launch, which fills every SM."""
         global _SEEDS_POOL
         if _SEEDS_POOL is None:
             from concurrent.futures import ThreadPoolExecutor
@@ -149,6 +153,8 @@ class Fields:
                     if trace:
                         info.n_seed_points, info.n_padded_seed_points = n, npad
                         host_seeds = _rows_to_host_behind(seeds_d, dev)
+                        if after is not None:
+                            after.wait(PREPARE_WAIT_S)
                         acc = self._trace(seeds_d, mask_d)
                     done = torch.cuda.Event()
                     done.record(side)

@@ -19,6 +19,8 @@ reference does:
 """
 from __future__ import annotations
 
+import threading
+
 import numpy as np
 
 from .device import traced
@@ -55,10 +57,12 @@ class Trace:
     @traced("slm.Trace.do")
     def do(self):
         self.print("\n**Trace begin**")
-        # the fields' seed list and passes run while the trajectories run
+        # the fields' seed list and passes run while the trajectories run;
+        # the passes start once the recording kernels are queued
+        launched = threading.Event()
         job = self._fields_job()
-        job[0].prepare()
-        self.compute_trajectories()
+        job[0].prepare(after=launched)
+        self.compute_trajectories(launched=launched)
         self.compute_fields(job)
         self.print("**Trace end**\n")
 
@@ -72,8 +76,9 @@ class Trace:
         info.set_xy(bnx, bny, pad)
         return mask_array, bbox, pad, nxp, nyp, info
 
-    def compute_trajectories(self):
-        """trace.py:93-128: the recorded trajectories of the cropped region."""
+    def compute_trajectories(self, launched=None):
+        """trace.py:93-128: the recorded trajectories of the cropped region.
+        ``launched``: an event set once the recording kernels are queued."""
         mask_array, bbox, pad, nxp, nyp, info = self._crop()
         data = Data(info=info, bbox=bbox, pad=pad, mapping_array=np.zeros((nxp, nyp), dtype=np.uint32),
                     mask_array=mask_array, uv_array=self.preprocess.uv_array)
@@ -84,6 +89,7 @@ class Trace:
                                     verbose=getattr(self.state, "verbose", False),
                                     gpu_verbose=getattr(self.state, "gpu_verbose", False),
                                     integrator=self.integrator)
+        trajectories.launched = launched
         trajectories.integrate()
         offset_xy = np.array((bbox[0] - pad, bbox[2] - pad))
         self.seed_point_array = trajectories.data.seed_point_array + offset_xy

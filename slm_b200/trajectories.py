@@ -35,9 +35,23 @@ class Trajectories:
         self.gpu_verbose = gpu_verbose
         self.integrator = integrator
         self.n_steps = 0
+        # set (.set()) once the recording kernels are queued: the Trace stage
+        # holds the fields' passes until then, so these small launches are not
+        # queued behind a launch that fills every SM
+        self.launched = None
 
     @traced("slm.Trajectories.integrate")
     def integrate(self):
+        try:
+            self._integrate()
+        finally:
+            self._signal_launched()
+
+    def _signal_launched(self):
+        if self.launched is not None:
+            self.launched.set()
+
+    def _integrate(self):
         vprint(self.verbose, "Integrating trajectories...")
         info = self.info
         mask_array = self.data.mask_array
@@ -112,6 +126,7 @@ class Trajectories:
                     kernels.integrate_trajectory(prm, n_chunk_ki, seeds_d, mask_d, uv_d, trajs[j],
                                                  nsteps[j], lengths[j], integrator=self.integrator,
                                                  stream=streams[j])
+                self._signal_launched()
                 for st in streams:
                     cur.wait_stream(st)
             for j, (_, downup_idx, downup_sign, _chunk_idx, seeds_chunk_offset, n_chunk_seeds,
@@ -124,6 +139,7 @@ class Trajectories:
                     prm = kernel_params(info, "INTEGRATE_TRAJECTORY", downup_sign)
                     kernels.integrate_trajectory(prm, n_chunk_ki, seeds_d, mask_d, uv_d, traj_d,
                                                  nsteps_d, length_d, integrator=self.integrator)
+                    self._signal_launched()
                 n = max(n_chunk_seeds, 0)
                 chunk_nsteps = nsteps_d[:n].cpu().numpy()
                 chunk_length = length_d[:n].cpu().numpy()

@@ -111,11 +111,33 @@ def test_mapping_pipeline_incised_bit_exact(seed):
     assert run.mismatches == [], run.mismatches
 
 
+@pytest.mark.parametrize("form", ["one_pass", "rounds"])
+@pytest.mark.parametrize("case", ["pipeline", "incised"])
+def test_flank_fix_forms_bit_exact(monkeypatch, form, case):
+    """fix_right/left_flanks in both forms -- one persistent pass that waits on
+    lower-index owners (the default), and stored paths resolved in rounds
+    (SLM_FLANK_ROUNDS=1, the fallback) -- give the oracle's labels."""
+    if form == "rounds":
+        monkeypatch.setenv("SLM_FLANK_ROUNDS", "1")
+    else:
+        monkeypatch.delenv("SLM_FLANK_ROUNDS", raising=False)
+    if case == "pipeline":
+        _, info, data = pipeline_case(nx=160, ny=128, seed=21, channel_pct=91.0)
+    else:
+        info, data = incised_pipeline_case(seed=5)
+    run = DeviceVsOracle()
+    assert M.map_channels_segments(None, info, data, runner=run)
+    assert run.mismatches == [], run.mismatches
+    assert [n for n, _ in run.calls].count("fix_right_flanks") == 1
+
+
 def test_flank_fix_in_chunks_bit_exact(monkeypatch):
-    """A path budget far below the total makes fix_right/left_flanks run their
-    items in many index-ordered chunks; labels equal the oracle's."""
+    """A path budget far below the total makes the rounds form of
+    fix_right/left_flanks run its items in many index-ordered chunks; labels
+    equal the oracle's."""
     from slm_b200 import map_kernels
     monkeypatch.setattr(map_kernels, "FLANK_PATH_BUDGET", 2048)
+    monkeypatch.setenv("SLM_FLANK_ROUNDS", "1")
     c, info, data = pipeline_case(nx=120, ny=96, seed=12)
     run = DeviceVsOracle()
     assert M.map_channels_segments(None, info, data, runner=run)

@@ -1,4 +1,6 @@
 """The drop-in stage wrappers (Trajectories, Fields) on the GPU against the oracle."""
+import threading
+
 import numpy as np
 import pytest
 
@@ -161,9 +163,13 @@ def test_fields_prepared_work_is_the_same(trace):
         cc = Case(nx=70, ny=66, seed=83, density=2, step=0.25, max_length=60.0)
         f = Fields(0, 0, info=cc.info, data=_data(cc))
         if prepared:
-            f.prepare(trace=trace)
+            launched = threading.Event()
+            f.prepare(trace=trace, after=launched)
             ct = Case(nx=70, ny=66, seed=83, n_traj_seeds=200)
-            Trajectories(0, 0, info=ct.info, data=_data(ct)).integrate()  # runs meanwhile
+            t2 = Trajectories(0, 0, info=ct.info, data=_data(ct))
+            t2.launched = launched
+            t2.integrate()  # runs meanwhile
+            assert launched.is_set()
         f.data.traj_stats_df = stats
         np.random.seed(777)
         f.integrate()
