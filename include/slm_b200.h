@@ -344,15 +344,26 @@ int slm_subsegment_flanks(const slm_params* p, uint32_t n_seeds, const float* se
                           const uint8_t* mask, const float* uv, const uint32_t* mapping,
                           const uint32_t* channel_label, const uint32_t* link, uint32_t* label,
                           void* stream);
+/* slm_exclusive_scan_u64 -- no counterpart in the reference (the prefix sum
+ * behind the mapping kernels' stored walks): out[i] = in[0] + ... + in[i-1]
+ * for i <= n (out[n] = the total).  in [n], out [n+1], scratch
+ * [slm_exclusive_scan_u64_scratch(n) bytes]: DEVICE, 8-byte aligned.
+ * Asynchronous. */
+size_t slm_exclusive_scan_u64_scratch(uint32_t n);
+int slm_exclusive_scan_u64(const uint64_t* in, uint32_t n, uint64_t* out, void* scratch, size_t scratch_bytes,
+                           void* stream);
+
 /* fix_right_flanks / fix_left_flanks (opencl/segment.cl:441-504, 530-594;
  * segment.py:210-232), with the result of the items run in ascending order.
- * One persistent launch walks every item once, taking items in ascending
- * order and waiting (bounded) for the final label of a lower-index item whose
- * pixel it reads.  If a wait runs out, or when the environment variable
- * SLM_FLANK_ROUNDS is set to a nonzero value, the labels are restored and the
- * multi-launch form runs: paths stored (within the workspace beyond the
- * minimum slm_fix_flanks_workspace(n, nxy, 0); SLM_ERR_CAPACITY with
- * *required_bytes when one path does not fit), then resolved in rounds. */
+ * The walks are traced in parallel and stored compressed (within the
+ * workspace beyond the minimum slm_fix_flanks_workspace(n, nxy, 0), in
+ * index-ordered chunks when they do not all fit; SLM_ERR_CAPACITY with
+ * *required_bytes when one path does not), then each chunk is settled in
+ * one persistent launch that takes items in ascending order and waits
+ * (bounded) for the final label of a lower-index item whose pixel it reads.
+ * If a wait runs out, or when the environment variable SLM_FLANK_ROUNDS is
+ * nonzero, the labels are restored and the items resolve in rounds
+ * instead. */
 size_t slm_fix_flanks_workspace(uint32_t n_seeds, uint32_t nxy_padded, uint64_t n_path_steps);
 int slm_fix_right_flanks(const slm_params* p, uint32_t n_seeds, const float* seed_point,
                          const uint8_t* mask, const float* uv, const uint32_t* mapping,

@@ -854,71 +854,135 @@ __global__ void k_flank_round(const slm_params p, uint32_t g0, uint32_t n, uint3
     atomicAdd(n_resolved, 1u);
 }
 
-// ------------------------------------------------------------------ fix flanks in one pass
-// fix_right_flanks (side 0) / fix_left_flanks (side 1) with every walk traced
-// once, in the pinned schedule's result.  Persistent warps take items in
-// ascending index from a queue (warp-aggregated atomicAdd), so every item
-// below one a lane holds has been taken.  A lane walks its item as the
-// reference does; a label it reads belongs to its own pixel (its running
-// value), to no item or a higher-index one (the initial label), or to a
-// lower-index item, whose final label it must wait for.  A lane that has to
-// wait does nothing this pass and tries the same read on the next; a read
-// has no side effect, so trying again changes nothing.  The lowest
-// unresolved item taken waits on nothing unresolved, so some lane always
-// advances.  Its label is published with a fence before its resolved flag.
+// ------------------------------------------------------------------ fix flanks, settled in one launch
+// The stored paths of a chunk of flank items resolved in one persistent
+// launch instead of rounds.  Warps take items in ascending index from a
+// queue (warp-aggregated atomicAdd), so every item below one a lane holds
+// has been taken.  A lane scans its item's stored path as k_flank_round does;
+// at a read of a lower-index owner that has not resolved it stops, notes that
+// owner and its place in the path (the start of a period record when inside
+// one, with the running label there), and on later passes only polls the
+// owner's flag until it can go on.  The lowest unresolved item taken waits on
+// nothing unresolved, so some lane always advances.  A label is published
+// with a fence before its resolved flag.  The RK walks are traced in parallel
+// beforehand (k_flank_paths), so only the path scans lie on a chain of waits.
 //
-// A walk whose (vec, dt) state repeats (Brent) is periodic; every read but
-// that of its own pixel gives the same value each lap, so a lap is a
-// function of the running label at its start.  Once that label repeats at a
-// lap start, whole multiples of its period of laps are skipped (the state
-// and the label come back unchanged).
-//
-// Every wait is bounded: a lane that has waited FLANK_WAIT_LIMIT passes in
-// a row sets bit 0 of *status and gives up its item; the caller then runs the
-// multi-launch form (k_flank_paths + k_flank_round) instead.
+// Every wait is bounded: a lane that polls FLANK_WAIT_LIMIT times in a row
+// sets bit 0 of *status, and every warp stops; the caller then resolves the
+// items in rounds (k_flank_round) from the initial labels.
 #define FLANK_WAIT_LIMIT (1u << 22)
 
-// label of pixel q as item g (own pixel h, running label lab_h) reads it;
-// false: its lower-index owner has not resolved yet
-__device__ __forceinline__ bool flank_read_live(uint32_t q, uint32_t g, uint32_t h, uint32_t lab_h,
-                                                const uint32_t* __restrict__ owner,
-                                                const uint32_t* __restrict__ label_init, const uint32_t* label,
-                                                const uint32_t* resolved, uint32_t& out) {
+// the label of pixel q as item g reads it (flank_read's rules, with the
+// owner's flag instead of its round); false and *wait_o when the owner has
+// not resolved.  Out of line, as flank_read.
+__device__ __noinline__ bool settle_read(uint32_t q, uint32_t g, uint32_t h, uint32_t lab_h,
+                                        const uint32_t* __restrict__ owner,
+                                        const uint32_t* __restrict__ label_init, const uint32_t* label,
+                                        const uint32_t* resolved, uint32_t& out, uint32_t& wait_o) {
     if (q == h) { out = lab_h; return true; }
     const uint32_t o = owner[q];
     if (o == NO_OWNER || o > g) { out = label_init[q]; return true; }
-    if (((volatile const uint32_t*)resolved)[o] == 0u) return false;
+    if (((volatile const uint32_t*)resolved)[o] == 0u) { wait_o = o; return false; }
     __threadfence();
     out = ((volatile const uint32_t*)label)[q];
     return true;
 }
 
-struct FlankWalk {
-    Vec2 vec, tv;
-    float dt, tdt;
-    uint32_t g, h, at, n_steps, lab_h;
-    uint32_t power, lam;               // Brent's checkpoint
-    uint32_t lap_len, next_lap, laps;  // lap bookkeeping once periodic (lap_len > 0)
-    uint32_t seen[8];                  // running label at the first lap starts
-    uint32_t waited;
-    bool alive, finishing, skipped;
+struct SettleLane {
+    u64 k, k_end;
+    uint32_t g, h, at, lab_h, wait_o, waited;
+    bool alive, waiting;
 };
 
+// Scan item state `w` on from w.k; 0: resolved (label written), 2: blocked
+// (w.k, w.at, w.lab_h at the place to resume, w.wait_o set).
+__device__ int settle_scan(SettleLane& w, uint32_t side, const slm_params& p, u64 base,
+                           const uint2* __restrict__ pairs, const uint8_t* __restrict__ mask,
+                           const uint32_t* __restrict__ mapping, const uint32_t* __restrict__ owner,
+                           const uint32_t* __restrict__ label_init, uint32_t* label, uint32_t* resolved) {
+    const uint32_t lfa = p.left_flank_addition, thin = p.is_thinchannel;
+    uint32_t v = 0;
+    // one pair of the walk's label scan: 0 go on, 1 the walk stops, 2 wait
+    auto scan = [&](uint2 e) -> int {
+        if (!settle_read(w.at, w.g, w.h, w.lab_h, owner, label_init, label, resolved, v, w.wait_o)) return 2;
+        const bool flank_ok = side ? (v & lfa) != 0u : ((~v) & lfa) != 0u;
+        if (mask[w.at] || !flank_ok || (mapping[w.at] & thin)) return 1;
+        if (!settle_read(e.x, w.g, w.h, w.lab_h, owner, label_init, label, resolved, v, w.wait_o)) return 2;
+        if ((w.lab_h & ~lfa) != (v & ~lfa)) w.lab_h = v;
+        w.at = e.y;
+        return 0;
+    };
+    while (w.k < w.k_end) {
+        const uint2 e = pairs[w.k - base];
+        if ((e.x & FLANK_PERIOD) == 0u) {
+            const int st = scan(e);
+            if (st == 2) return 2;
+            if (st == 1) { w.k = w.k_end; break; }
+            ++w.k;
+            continue;
+        }
+        // a period record, as k_flank_round runs it; a wait inside it
+        // restarts the record
+        const uint32_t E = e.x & ~FLANK_PERIOD, nfut = e.y;
+        const uint2* pat = pairs + (w.k + 1 - base);
+        const uint32_t at0 = w.at, lab0 = w.lab_h;
+        const uint32_t full = nfut / E, rem = nfut % E;
+        uint32_t seen[8];
+        bool skipped = false;
+        int st = 0;
+        for (uint32_t lap = 0; lap < full && st == 0; ++lap) {
+            if (!skipped && lap < 8) {
+                for (uint32_t j = 0; j < lap; ++j)
+                    if (seen[j] == w.lab_h) {
+                        const uint32_t per = lap - j;
+                        lap += ((full - lap) / per) * per;
+                        skipped = true;
+                        break;
+                    }
+                if (!skipped) seen[lap] = w.lab_h;
+                if (lap >= full) break;
+            }
+            for (uint32_t i = 0; i < E && st == 0; ++i) st = scan(pat[i]);
+        }
+        for (uint32_t i = 0; i < rem && st == 0; ++i) st = scan(pat[i]);
+        if (st == 2) {
+            w.at = at0;
+            w.lab_h = lab0;
+            return 2;
+        }
+        if (st == 1) { w.k = w.k_end; break; }
+        w.k += (u64)E + 1u;
+    }
+    // after the walk: the label at the last pixel, then the flank bit
+    if (!settle_read(w.at, w.g, w.h, w.lab_h, owner, label_init, label, resolved, v, w.wait_o)) return 2;
+    if ((w.lab_h & ~lfa) != (v & ~lfa)) w.lab_h = v;
+    settle_read(w.at, w.g, w.h, w.lab_h, owner, label_init, label, resolved, v, w.wait_o);
+    if (side) {
+        if (((~v) & lfa) && !(mapping[w.at] & thin)) w.lab_h &= ~lfa;
+    } else {
+        if (v & lfa) w.lab_h |= lfa;
+    }
+    label[w.h] = w.lab_h;
+    __threadfence();
+    ((volatile uint32_t*)resolved)[w.g] = 1u;
+    return 0;
+}
+
+// Items g0 .. g0+n-1 (their paths stored at pairs[offsets[g] - base]).
 __global__ void __launch_bounds__(256)
-k_flank_resolve(const slm_params p, uint32_t n, uint32_t side, const float2* __restrict__ seeds,
-                const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
-                const uint32_t* __restrict__ mapping, const uint32_t* __restrict__ owner,
-                const uint32_t* __restrict__ label_init, uint32_t* label, uint32_t* resolved,
-                uint32_t* queue_head, uint32_t* status) {
+k_flank_settle(const slm_params p, uint32_t g0, uint32_t n, uint32_t side, const u64* __restrict__ offsets,
+               u64 base, const uint2* __restrict__ pairs, const uint32_t* __restrict__ hpix,
+               const uint8_t* __restrict__ mask, const uint32_t* __restrict__ mapping,
+               const uint32_t* __restrict__ owner, const uint32_t* __restrict__ label_init, uint32_t* label,
+               uint32_t* resolved, uint32_t* queue_head, uint32_t* status) {
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
-    const uint32_t lfa = p.left_flank_addition, thin = p.is_thinchannel;
-    FlankWalk w;
+    SettleLane w;
     w.alive = false;
     bool drained = false;
     for (uint32_t pass = 0;; ++pass) {
         // a lane that gave up stops every warp (the caller falls back)
-        if ((pass & 255u) == 0u) {
+        if ((pass & 63u) == 0u) {
             uint32_t stop = 0;
             if (lane == 0) stop = *(volatile const uint32_t*)status;
             if (__shfl_sync(FULL, stop, 0)) break;
@@ -932,24 +996,17 @@ k_flank_resolve(const slm_params p, uint32_t n, uint32_t side, const float2* __r
                 head = __shfl_sync(FULL, head, leader);
                 if ((u64)head + __popc(idle) >= n) drained = true;
                 if (!w.alive) {
-                    const uint32_t g = head + __popc(idle & ((1u << lane) - 1u));
-                    if (g < n) {
-                        w.g = g;
-                        w.vec = seed_vec(seeds, g);
-                        w.h = pixel_of(w.vec, p);
+                    const uint32_t t = head + __popc(idle & ((1u << lane) - 1u));
+                    if (t < n) {
+                        w.g = g0 + t;
+                        w.k = offsets[w.g];
+                        w.k_end = offsets[w.g + 1];
+                        w.h = hpix[w.g];
                         w.at = w.h;
-                        w.dt = p.dt_max;
-                        w.n_steps = 0;
                         w.lab_h = label_init[w.h];
-                        w.tv = w.vec;
-                        w.tdt = w.dt;
-                        w.power = 1;
-                        w.lam = 0;
-                        w.lap_len = 0;
                         w.waited = 0;
+                        w.waiting = false;
                         w.alive = true;
-                        w.finishing = false;
-                        w.skipped = false;
                     }
                 }
             }
@@ -959,87 +1016,21 @@ k_flank_resolve(const slm_params p, uint32_t n, uint32_t side, const float2* __r
             continue;
         }
         if (!w.alive) continue;
-        bool blocked = false;
-        uint32_t v = 0;
-        if (!w.finishing) {
-            // the loop test at the current pixel, then one step
-            if (mask[w.at] || (mapping[w.at] & thin) || w.n_steps >= p.max_n_steps) {
-                w.finishing = true;
-            } else if (!flank_read_live(w.at, w.g, w.h, w.lab_h, owner, label_init, label, resolved, v)) {
-                blocked = true;
-            } else if (side ? ((v & lfa) == 0u) : ((v & lfa) != 0u)) {
-                w.finishing = true;
-            } else {
-                const Step st = rk_plain(w.vec, w.dt, uv, p);
-                if (!flank_read_live(st.idx, w.g, w.h, w.lab_h, owner, label_init, label, resolved, v)) {
-                    blocked = true;
-                } else {
-                    if ((w.lab_h & ~lfa) != (v & ~lfa)) w.lab_h = v;
-                    uint32_t idx = st.idx;
-                    const bool stuck = seg_move(st, w.vec, idx, w.dt, w.n_steps, p);
-                    w.at = idx;
-                    if (stuck) {
-                        w.finishing = true;
-                    } else if (w.lap_len == 0u) {
-                        w.lam++;
-                        if (__float_as_uint(w.vec.x) == __float_as_uint(w.tv.x) &&
-                            __float_as_uint(w.vec.y) == __float_as_uint(w.tv.y) &&
-                            __float_as_uint(w.dt) == __float_as_uint(w.tdt)) {
-                            w.lap_len = w.lam;
-                            w.next_lap = w.n_steps;
-                            w.laps = 0;
-                        } else if (w.lam == w.power) {
-                            w.tv = w.vec;
-                            w.tdt = w.dt;
-                            w.power <<= 1;
-                            w.lam = 0;
-                        }
-                    }
-                    if (w.lap_len && !w.skipped && w.n_steps == w.next_lap) {
-                        for (uint32_t i = 0; i < w.laps && i < 8u; ++i)
-                            if (w.seen[i] == w.lab_h) {
-                                const uint32_t per = w.laps - i;
-                                const uint32_t full = (p.max_n_steps - w.n_steps) / w.lap_len;
-                                w.n_steps += (full / per) * per * w.lap_len;
-                                w.skipped = true;
-                                break;
-                            }
-                        if (!w.skipped) {
-                            if (w.laps < 8u) w.seen[w.laps] = w.lab_h;
-                            else w.skipped = true;  // no repeat within 8 laps: step on to the bound
-                            w.laps++;
-                            w.next_lap += w.lap_len;
-                        }
-                    }
+        if (w.waiting) {
+            if (((volatile const uint32_t*)resolved)[w.wait_o] == 0u) {
+                if (++w.waited >= FLANK_WAIT_LIMIT) {
+                    atomicOr(status, 1u);
+                    w.alive = false;
                 }
+                continue;
             }
-        }
-        if (w.finishing && !blocked) {
-            // after the loop: the label at the last pixel, then the flank bit
-            if (!flank_read_live(w.at, w.g, w.h, w.lab_h, owner, label_init, label, resolved, v)) {
-                blocked = true;
-            } else {
-                if ((w.lab_h & ~lfa) != (v & ~lfa)) w.lab_h = v;
-                flank_read_live(w.at, w.g, w.h, w.lab_h, owner, label_init, label, resolved, v);
-                if (side) {
-                    if (((~v) & lfa) && !(mapping[w.at] & thin)) w.lab_h &= ~lfa;
-                } else {
-                    if (v & lfa) w.lab_h |= lfa;
-                }
-                label[w.h] = w.lab_h;
-                __threadfence();
-                ((volatile uint32_t*)resolved)[w.g] = 1u;
-                w.alive = false;
-            }
-        }
-        if (blocked) {
-            if (++w.waited >= FLANK_WAIT_LIMIT) {
-                atomicOr(status, 1u);
-                w.alive = false;
-            }
-        } else {
+            w.waiting = false;
             w.waited = 0;
         }
+        if (settle_scan(w, side, p, base, pairs, mask, mapping, owner, label_init, label, resolved) == 2)
+            w.waiting = true;
+        else
+            w.alive = false;
     }
 }
 
@@ -1129,6 +1120,94 @@ __global__ void k_exclusive_scan(const u64* __restrict__ in, uint32_t n, u64* __
         carry += tot;
     }
     if (threadIdx.x == 0) out[n] = carry;
+}
+
+// Exclusive scan of n u64 for large n, in tiles of SCAN_TILE: per-tile sums,
+// an exclusive scan of those (k_exclusive_scan), then each tile rescanned
+// with its offset.  out[n] = the total.
+constexpr uint32_t SCAN_PER = 8;
+constexpr uint32_t SCAN_TILE = 1024 * SCAN_PER;
+
+__global__ void __launch_bounds__(1024) k_tile_sums(const u64* __restrict__ in, uint32_t n, u64* __restrict__ sums) {
+    __shared__ u64 warp_sum[32];
+    const u64 t0 = (u64)blockIdx.x * SCAN_TILE + (u64)threadIdx.x * SCAN_PER;
+    u64 v = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < SCAN_PER; ++k)
+        if (t0 + k < n) v += in[t0 + k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        u64 w = warp_sum[threadIdx.x];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+        if (threadIdx.x == 0) sums[blockIdx.x] = w;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_tile_scan(const u64* __restrict__ in, uint32_t n,
+                                                    const u64* __restrict__ tile_off, uint32_t n_tiles,
+                                                    u64* __restrict__ out) {
+    __shared__ u64 warp_off[32];
+    const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    const u64 t0 = (u64)blockIdx.x * SCAN_TILE + (u64)threadIdx.x * SCAN_PER;
+    u64 x[SCAN_PER];
+    u64 tot = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < SCAN_PER; ++k) {
+        x[k] = t0 + k < n ? in[t0 + k] : 0ull;
+        tot += x[k];
+    }
+    // inclusive scan of the thread totals within the warp, then across warps
+    u64 inc = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const u64 y = __shfl_up_sync(0xffffffffu, inc, o);
+        if ((int)lane >= o) inc += y;
+    }
+    if (lane == 31) warp_off[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+        u64 w = warp_off[lane];
+        u64 wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const u64 y = __shfl_up_sync(0xffffffffu, wi, o);
+            if ((int)lane >= o) wi += y;
+        }
+        warp_off[lane] = wi - w;  // exclusive
+    }
+    __syncthreads();
+    u64 run = tile_off[blockIdx.x] + warp_off[wid] + (inc - tot);
+#pragma unroll
+    for (uint32_t k = 0; k < SCAN_PER; ++k) {
+        if (t0 + k < n) out[t0 + k] = run;
+        run += x[k];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = tile_off[n_tiles];
+}
+
+// scratch words exclusive_scan needs for n elements
+static inline size_t scan_scratch_words(uint32_t n) { return 2 * ((size_t)(n + SCAN_TILE - 1) / SCAN_TILE + 1); }
+
+static int exclusive_scan(const u64* in, uint32_t n, u64* out, u64* scratch, cudaStream_t s) {
+    const uint32_t n_tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (n_tiles <= 8) {
+        k_exclusive_scan<<<1, 1024, 0, s>>>(in, n, out);
+        SLM_LAUNCHED("k_exclusive_scan");
+        return SLM_OK;
+    }
+    u64* sums = scratch;
+    u64* off = scratch + n_tiles + 1;
+    k_tile_sums<<<n_tiles, 1024, 0, s>>>(in, n, sums);
+    SLM_LAUNCHED("k_tile_sums");
+    k_exclusive_scan<<<1, 1024, 0, s>>>(sums, n_tiles, off);
+    SLM_LAUNCHED("k_exclusive_scan");
+    k_tile_scan<<<n_tiles, 1024, 0, s>>>(in, n, off, n_tiles, out);
+    SLM_LAUNCHED("k_tile_scan");
+    return SLM_OK;
 }
 
 // ------------------------------------------------------------------ parallel flag_downchannels
@@ -1494,10 +1573,23 @@ int slm_subsegment_flanks(const slm_params* p, uint32_t n, const float* seed_poi
     return SLM_OK;
 }
 
+size_t slm_exclusive_scan_u64_scratch(uint32_t n) { return scan_scratch_words(n) * sizeof(u64); }
+
+int slm_exclusive_scan_u64(const uint64_t* in, uint32_t n, uint64_t* out, void* scratch, size_t scratch_bytes,
+                           void* stream) {
+    clear_error();
+    SLM_REQUIRE(in && out && scratch, "NULL buffer");
+    SLM_REQUIRE(aligned(in, 8) && aligned(out, 8) && aligned(scratch, 8), "buffers must be 8-byte aligned");
+    SLM_REQUIRE(scratch_bytes >= slm_exclusive_scan_u64_scratch(n), "scratch holds %zu bytes, needs %zu",
+                scratch_bytes, slm_exclusive_scan_u64_scratch(n));
+    return exclusive_scan(reinterpret_cast<const u64*>(in), n, reinterpret_cast<u64*>(out),
+                          reinterpret_cast<u64*>(scratch), SS);
+}
+
 size_t slm_fix_flanks_workspace(uint32_t n_seeds, uint32_t nxy_padded, uint64_t n_pairs) {
     return (size_t)(2 * (size_t)n_seeds + 1) * sizeof(u64) + (size_t)n_seeds * 2 * sizeof(uint32_t)
          + (size_t)nxy_padded * 2 * sizeof(uint32_t) + sizeof(uint32_t) + 256
-         + (size_t)n_pairs * sizeof(uint2);
+         + scan_scratch_words(n_seeds) * sizeof(u64) + (size_t)n_pairs * sizeof(uint2);
 }
 
 static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, const uint8_t* mask,
@@ -1519,47 +1611,26 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
     uint32_t* n_resolved = label_init + nxy;  // [0] rounds: resolved count; [1] queue head; [2] status
     uintptr_t pa = reinterpret_cast<uintptr_t>(n_resolved + 4);
     pa = (pa + 15) & ~(uintptr_t)15;
-    uint2* pairs = reinterpret_cast<uint2*>(pa);
+    u64* scan_scratch = reinterpret_cast<u64*>(pa);
+    uint2* pairs = reinterpret_cast<uint2*>(scan_scratch + scan_scratch_words(n));
     const u64 cap_pairs = (workspace_bytes - fixed) / sizeof(uint2);
     SLM_CUDA(cudaMemsetAsync(owner, 0xff, (size_t)nxy * sizeof(uint32_t), SS));
     SLM_CUDA(cudaMemsetAsync(resolved, 0, (size_t)n * sizeof(uint32_t), SS));
     SLM_CUDA(cudaMemcpyAsync(label_init, label, (size_t)nxy * sizeof(uint32_t), cudaMemcpyDeviceToDevice, SS));
     k_owner_map<<<blocks_for(n, 256), 256, 0, SS>>>(*p, n, F2(seed_point), owner, hpix);
     SLM_LAUNCHED("k_owner_map");
-    if (required_bytes) *required_bytes = fixed;
-    // The one-pass form (k_flank_resolve); the multi-launch form below if a
-    // wait there ran out, or when SLM_FLANK_ROUNDS is set (for tests).
-    const char* force = std::getenv("SLM_FLANK_ROUNDS");
-    if (!(force && force[0] && force[0] != '0')) {
-        SLM_CUDA(cudaMemsetAsync(n_resolved, 0, 4 * sizeof(uint32_t), SS));
-        int occ = 0;
-        SLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_flank_resolve, 256, 0));
-        const unsigned grid = (unsigned)(num_sms() * (occ > 0 ? occ : 1));
-        k_flank_resolve<<<grid, 256, 0, SS>>>(*p, n, left ? 1u : 0u, F2(seed_point), mask, F2(uv), mapping, owner,
-                                              label_init, label, resolved, n_resolved + 1, n_resolved + 2);
-        SLM_LAUNCHED("k_flank_resolve");
-        uint32_t st = 0;
-        SLM_CUDA(cudaMemcpyAsync(&st, n_resolved + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, SS));
-        SLM_CUDA(cudaStreamSynchronize(SS));
-        if (st == 0u) return SLM_OK;
-        // start over from the initial labels
-        SLM_CUDA(cudaMemcpyAsync(label, label_init, (size_t)nxy * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
-                                 SS));
-        SLM_CUDA(cudaMemsetAsync(resolved, 0, (size_t)n * sizeof(uint32_t), SS));
-    }
     k_flank_paths<<<blocks_for(n, 128), 128, 0, SS>>>(*p, 0u, n, F2(seed_point), mask, F2(uv), mapping,
                                                      n_pairs, nullptr, 0ull, nullptr);
     SLM_LAUNCHED("k_flank_paths");
-    k_exclusive_scan<<<1, 1024, 0, SS>>>(n_pairs, n, offsets);
-    SLM_LAUNCHED("k_exclusive_scan");
+    rc = exclusive_scan(n_pairs, n, offsets, scan_scratch, SS);
+    if (rc) return rc;
     u64 total = 0;
     SLM_CUDA(cudaMemcpyAsync(&total, offsets + n, sizeof(u64), cudaMemcpyDeviceToHost, SS));
     SLM_CUDA(cudaStreamSynchronize(SS));
     if (required_bytes) *required_bytes = slm_fix_flanks_workspace(n, nxy, total);
     // Items run in index order, chunk after chunk, each chunk's paths stored
     // at once: an item reads only initial labels and the final labels of
-    // lower-index owners, which earlier chunks have resolved; rounds keep
-    // counting across chunks, so those owners count as resolved before.
+    // lower-index owners, which earlier chunks have resolved.
     std::vector<std::pair<uint32_t, uint32_t>> chunks;
     if (total <= cap_pairs) {
         chunks.emplace_back(0u, n);
@@ -1583,6 +1654,41 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
             a = b;
         }
     }
+    // Each chunk settled in one persistent launch (k_flank_settle); in rounds
+    // (k_flank_round) from the initial labels if a wait there ran out, or when
+    // the environment variable SLM_FLANK_ROUNDS is nonzero (for tests).
+    const char* force = std::getenv("SLM_FLANK_ROUNDS");
+    bool settle = !(force && force[0] && force[0] != '0');
+    if (settle) {
+        int occ = 0;
+        SLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_flank_settle, 256, 0));
+        const unsigned grid = (unsigned)(num_sms() * (occ > 0 ? occ : 1));
+        SLM_CUDA(cudaMemsetAsync(n_resolved + 2, 0, sizeof(uint32_t), SS));
+        for (const auto& c : chunks) {
+            const uint32_t a = c.first, m = c.second - c.first;
+            u64 base = 0;
+            SLM_CUDA(cudaMemcpyAsync(&base, offsets + a, sizeof(u64), cudaMemcpyDeviceToHost, SS));
+            SLM_CUDA(cudaStreamSynchronize(SS));
+            k_flank_paths<<<blocks_for(m, 128), 128, 0, SS>>>(*p, a, m, F2(seed_point), mask, F2(uv), mapping,
+                                                             nullptr, offsets, base, pairs);
+            SLM_LAUNCHED("k_flank_paths");
+            SLM_CUDA(cudaMemsetAsync(n_resolved + 1, 0, sizeof(uint32_t), SS));
+            k_flank_settle<<<grid, 256, 0, SS>>>(*p, a, m, left ? 1u : 0u, offsets, base, pairs, hpix, mask,
+                                                 mapping, owner, label_init, label, resolved, n_resolved + 1,
+                                                 n_resolved + 2);
+            SLM_LAUNCHED("k_flank_settle");
+        }
+        uint32_t st = 0;
+        SLM_CUDA(cudaMemcpyAsync(&st, n_resolved + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, SS));
+        SLM_CUDA(cudaStreamSynchronize(SS));
+        if (st == 0u) return SLM_OK;
+        // start over from the initial labels, in rounds
+        SLM_CUDA(cudaMemcpyAsync(label, label_init, (size_t)nxy * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                                 SS));
+        SLM_CUDA(cudaMemsetAsync(resolved, 0, (size_t)n * sizeof(uint32_t), SS));
+    }
+    // rounds keep counting across chunks, so owners of earlier chunks count
+    // as resolved before
     uint32_t round = 1;
     for (const auto& c : chunks) {
         const uint32_t a = c.first, m = c.second - c.first;

@@ -131,9 +131,11 @@ class Fields:
         ``integrate`` alone; NumPy's global generator is set where
         ``integrate`` would set it.  With a process group only the seed list
         is prepared (the passes' collectives stay on the caller's thread).
-        ``after``: a ``threading.Event``; the passes start once it is set (at
-        most PREPARE_WAIT_S later), so work the caller queues first is not
-        held behind the persistent launch, which fills every SM."""
+        ``after``: a ``trajectories.LaunchSignal`` (or any object with
+        ``wait(timeout)``); the passes are queued once it is set (at most
+        PREPARE_WAIT_S later) and run after its CUDA ``event``, so the
+        caller's small launches are not held behind the persistent launch,
+        which fills every SM."""
         global _SEEDS_POOL
         if _SEEDS_POOL is None:
             from concurrent.futures import ThreadPoolExecutor
@@ -155,6 +157,9 @@ class Fields:
                         host_seeds = _rows_to_host_behind(seeds_d, dev)
                         if after is not None:
                             after.wait(PREPARE_WAIT_S)
+                            ev = getattr(after, "event", None)
+                            if ev is not None:
+                                side.wait_event(ev)
                         acc = self._trace(seeds_d, mask_d)
                     done = torch.cuda.Event()
                     done.record(side)

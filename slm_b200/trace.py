@@ -19,13 +19,11 @@ reference does:
 """
 from __future__ import annotations
 
-import threading
-
 import numpy as np
 
 from .device import traced
 from .fields import Fields
-from .trajectories import Trajectories
+from .trajectories import LaunchSignal, Trajectories
 from .useful import Data, Info, default_parameters, get_bbox, vprint
 
 
@@ -58,8 +56,8 @@ class Trace:
     def do(self):
         self.print("\n**Trace begin**")
         # the fields' seed list and passes run while the trajectories run;
-        # the passes start once the recording kernels are queued
-        launched = threading.Event()
+        # the passes run once the recording kernels have run
+        launched = LaunchSignal()
         job = self._fields_job()
         job[0].prepare(after=launched)
         self.compute_trajectories(launched=launched)

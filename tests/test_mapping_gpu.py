@@ -111,12 +111,13 @@ def test_mapping_pipeline_incised_bit_exact(seed):
     assert run.mismatches == [], run.mismatches
 
 
-@pytest.mark.parametrize("form", ["one_pass", "rounds"])
+@pytest.mark.parametrize("form", ["settle", "rounds"])
 @pytest.mark.parametrize("case", ["pipeline", "incised"])
 def test_flank_fix_forms_bit_exact(monkeypatch, form, case):
-    """fix_right/left_flanks in both forms -- one persistent pass that waits on
-    lower-index owners (the default), and stored paths resolved in rounds
-    (SLM_FLANK_ROUNDS=1, the fallback) -- give the oracle's labels."""
+    """fix_right/left_flanks in both forms -- the stored paths settled in one
+    persistent launch that waits on lower-index owners (the default), and
+    resolved in rounds (SLM_FLANK_ROUNDS=1, the fallback) -- give the
+    oracle's labels."""
     if form == "rounds":
         monkeypatch.setenv("SLM_FLANK_ROUNDS", "1")
     else:
@@ -309,3 +310,25 @@ def test_mapping_stage_pass2_on_the_gpu():
     assert np.array_equal(gpu.hsl_array, cpu.hsl_array) and gpu.hsl_array.any()
     assert np.array_equal(gpu.hsl_mean_array, cpu.hsl_mean_array)
     assert gpu.hsl_stats_df.equals(cpu.hsl_stats_df)
+
+
+@pytest.mark.parametrize("n", [0, 1, 1000, 65536, 65537, 300001, 10_000_000])
+def test_exclusive_scan_u64(n):
+    """The tiled exclusive scan behind the stored flank paths (one block up
+    to 8 tiles of 8192, three launches above) against NumPy's cumsum."""
+    import ctypes
+
+    import torch
+
+    from slm_b200 import _lib
+    L = _lib.load()
+    rng = np.random.default_rng(n)
+    x = rng.integers(0, 5000, n, dtype=np.uint64)
+    dev = torch.device("cuda", 0)
+    xin = torch.from_numpy(x.view(np.int64)).to(dev) if n else torch.zeros(1, dtype=torch.int64, device=dev)
+    out = torch.full((n + 1,), -1, dtype=torch.int64, device=dev)
+    scratch = torch.empty(max(1, int(L.slm_exclusive_scan_u64_scratch(n))), dtype=torch.uint8, device=dev)
+    _lib.check(L.slm_exclusive_scan_u64(_lib.ptr(xin), n, _lib.ptr(out), _lib.ptr(scratch), scratch.numel(),
+                                        ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    want = np.concatenate([[0], np.cumsum(x, dtype=np.uint64)])
+    assert np.array_equal(out.cpu().numpy().view(np.uint64), want)
