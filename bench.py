@@ -1123,7 +1123,7 @@ def run_e2e(args, wl, dev):
 
     from slm_b200.device import pinned_empty
     from slm_b200.fields import Fields
-    from slm_b200.trajectories import LaunchSignal, Trajectories
+    from slm_b200.trajectories import Trajectories
     from slm_b200.useful import Data
 
     uv_h = pinned_empty(wl.uv.shape, np.float32)
@@ -1140,13 +1140,11 @@ def run_e2e(args, wl, dev):
         data2 = Data(info=info2, mask_array=mask_h, uv_array=uv_h,
                      mapping_array=np.zeros(mask_h.shape, np.uint32))
         f = Fields(0, dev.index, info=info2, data=data2, schedule=args.schedule, integrator=integ)
-        launched = LaunchSignal()
-        f.prepare(after=launched)
+        f.prepare()
         info = wl.fresh_info()
         data = Data(info=info, mask_array=mask_h, uv_array=uv_h,
                     mapping_array=np.zeros(mask_h.shape, np.uint32))
         tr = Trajectories(0, dev.index, info=info, data=data, integrator=integ)
-        tr.launched = launched
         tr.integrate()
         data2.traj_stats_df = tr.data.traj_stats_df
         f.integrate()

@@ -67,7 +67,6 @@ def _staging(slot, t):
 
 _ROWS_POOL = None
 _SEEDS_POOL = None
-PREPARE_WAIT_S = 60.0  # longest wait of Fields.prepare's passes for their ``after`` event
 
 
 def _rows_to_host_behind(t, dev):
@@ -121,7 +120,7 @@ class Fields:
     # largest slc count whose pow is looked up in a host-computed table
     SLC_TABLE_MAX = 1 << 22
 
-    def prepare(self, trace=True, after=None):
+    def prepare(self, trace=True):
         """Start the work of ``integrate`` that does not need the trajectory
         statistics -- the seed list and, with ``trace``, both tracing passes
         -- on a worker thread and a side stream, and return at once;
@@ -130,12 +129,7 @@ class Fields:
         trajectories, so this work overlaps them.  The results are those of
         ``integrate`` alone; NumPy's global generator is set where
         ``integrate`` would set it.  With a process group only the seed list
-        is prepared (the passes' collectives stay on the caller's thread).
-        ``after``: a ``trajectories.LaunchSignal`` (or any object with
-        ``wait(timeout)``); the passes are queued once it is set (at most
-        PREPARE_WAIT_S later) and run after its CUDA ``event``, so the
-        caller's small launches are not held behind the persistent launch,
-        which fills every SM."""
+        is prepared (the passes' collectives stay on the caller's thread)."""
         global _SEEDS_POOL
         if _SEEDS_POOL is None:
             from concurrent.futures import ThreadPoolExecutor
@@ -155,11 +149,6 @@ class Fields:
                     if trace:
                         info.n_seed_points, info.n_padded_seed_points = n, npad
                         host_seeds = _rows_to_host_behind(seeds_d, dev)
-                        if after is not None:
-                            after.wait(PREPARE_WAIT_S)
-                            ev = getattr(after, "event", None)
-                            if ev is not None:
-                                side.wait_event(ev)
                         acc = self._trace(seeds_d, mask_d)
                     done = torch.cuda.Event()
                     done.record(side)

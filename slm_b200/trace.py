@@ -23,7 +23,7 @@ import numpy as np
 
 from .device import traced
 from .fields import Fields
-from .trajectories import LaunchSignal, Trajectories
+from .trajectories import Trajectories
 from .useful import Data, Info, default_parameters, get_bbox, vprint
 
 
@@ -55,12 +55,10 @@ class Trace:
     @traced("slm.Trace.do")
     def do(self):
         self.print("\n**Trace begin**")
-        # the fields' seed list and passes run while the trajectories run;
-        # the passes run once the recording kernels have run
-        launched = LaunchSignal()
+        # the fields' seed list and passes run while the trajectories run
         job = self._fields_job()
-        job[0].prepare(after=launched)
-        self.compute_trajectories(launched=launched)
+        job[0].prepare()
+        self.compute_trajectories()
         self.compute_fields(job)
         self.print("**Trace end**\n")
 
@@ -74,9 +72,8 @@ class Trace:
         info.set_xy(bnx, bny, pad)
         return mask_array, bbox, pad, nxp, nyp, info
 
-    def compute_trajectories(self, launched=None):
-        """trace.py:93-128: the recorded trajectories of the cropped region.
-        ``launched``: an event set once the recording kernels are queued."""
+    def compute_trajectories(self):
+        """trace.py:93-128: the recorded trajectories of the cropped region."""
         mask_array, bbox, pad, nxp, nyp, info = self._crop()
         data = Data(info=info, bbox=bbox, pad=pad, mapping_array=np.zeros((nxp, nyp), dtype=np.uint32),
                     mask_array=mask_array, uv_array=self.preprocess.uv_array)
@@ -87,7 +84,6 @@ class Trace:
                                     verbose=getattr(self.state, "verbose", False),
                                     gpu_verbose=getattr(self.state, "gpu_verbose", False),
                                     integrator=self.integrator)
-        trajectories.launched = launched
         trajectories.integrate()
         offset_xy = np.array((bbox[0] - pad, bbox[2] - pad))
         self.seed_point_array = trajectories.data.seed_point_array + offset_xy

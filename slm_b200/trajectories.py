@@ -35,27 +35,9 @@ class Trajectories:
         self.gpu_verbose = gpu_verbose
         self.integrator = integrator
         self.n_steps = 0
-        # a LaunchSignal, set once the recording kernels are queued: the Trace
-        # stage holds the fields' passes until they have run, so these small
-        # launches do not queue behind a persistent launch that fills every SM
-        self.launched = None
 
     @traced("slm.Trajectories.integrate")
     def integrate(self):
-        try:
-            self._integrate()
-        finally:
-            self._signal_launched()
-
-    def _signal_launched(self):
-        if self.launched is not None and not self.launched.is_set():
-            ev = None
-            if torch.cuda.is_available():
-                ev = torch.cuda.Event()
-                ev.record(torch.cuda.current_stream(self.device))
-            self.launched.set(ev)
-
-    def _integrate(self):
         vprint(self.verbose, "Integrating trajectories...")
         info = self.info
         mask_array = self.data.mask_array
@@ -132,7 +114,6 @@ class Trajectories:
                                                  stream=streams[j])
                 for st in streams:
                     cur.wait_stream(st)
-                self._signal_launched()
             for j, (_, downup_idx, downup_sign, _chunk_idx, seeds_chunk_offset, n_chunk_seeds,
                     n_chunk_ki) in enumerate(todo):
                 b = j if concurrent else 0
@@ -143,7 +124,6 @@ class Trajectories:
                     prm = kernel_params(info, "INTEGRATE_TRAJECTORY", downup_sign)
                     kernels.integrate_trajectory(prm, n_chunk_ki, seeds_d, mask_d, uv_d, traj_d,
                                                  nsteps_d, length_d, integrator=self.integrator)
-                    self._signal_launched()
                 n = max(n_chunk_seeds, 0)
                 chunk_nsteps = nsteps_d[:n].cpu().numpy()
                 chunk_length = length_d[:n].cpu().numpy()
@@ -165,27 +145,6 @@ class Trajectories:
         self.data.streamline_arrays_list = streamline_arrays_list
         self.data.traj_nsteps_array = traj_nsteps_array[0:ns].copy()
         self.data.traj_length_array = traj_length_array[0:ns].copy()
-
-
-class LaunchSignal:
-    """Set by ``Trajectories`` once its recording kernels are queued, with a
-    CUDA event that completes when they have run (``event``); ``wait`` as
-    ``threading.Event.wait``."""
-
-    def __init__(self):
-        import threading
-        self._flag = threading.Event()
-        self.event = None
-
-    def set(self, event=None):
-        self.event = event
-        self._flag.set()
-
-    def is_set(self):
-        return self._flag.is_set()
-
-    def wait(self, timeout=None):
-        return self._flag.wait(timeout)
 
 
 def decode_streamlines(seed_point_array, streamline_arrays_list, trajectory_resolution, origin=(0.0, 0.0),

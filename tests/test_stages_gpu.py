@@ -5,7 +5,7 @@ import pytest
 import oracle as O
 from cases import Case
 from slm_b200.fields import Fields
-from slm_b200.trajectories import LaunchSignal, Trajectories
+from slm_b200.trajectories import Trajectories
 from slm_b200.useful import Data, compute_stats, create_seeds
 
 pytestmark = pytest.mark.gpu
@@ -161,13 +161,9 @@ def test_fields_prepared_work_is_the_same(trace):
         cc = Case(nx=70, ny=66, seed=83, density=2, step=0.25, max_length=60.0)
         f = Fields(0, 0, info=cc.info, data=_data(cc))
         if prepared:
-            launched = LaunchSignal()
-            f.prepare(trace=trace, after=launched)
+            f.prepare(trace=trace)
             ct = Case(nx=70, ny=66, seed=83, n_traj_seeds=200)
-            t2 = Trajectories(0, 0, info=ct.info, data=_data(ct))
-            t2.launched = launched
-            t2.integrate()  # runs meanwhile
-            assert launched.is_set()
+            Trajectories(0, 0, info=ct.info, data=_data(ct)).integrate()  # runs meanwhile
         f.data.traj_stats_df = stats
         np.random.seed(777)
         f.integrate()

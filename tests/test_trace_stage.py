@@ -36,7 +36,7 @@ class FakeFields:
                  gpu_verbose=False, schedule="persistent", integrator=2):
         self.data = data
 
-    def prepare(self, trace=True, after=None):
+    def prepare(self, trace=True):
         pass
 
     def integrate(self):
