@@ -29,7 +29,12 @@ SPECS = {
     "hillslopes": ("slm_hillslopes", (4,), None),
     "hillslope_lengths": ("slm_hillslope_lengths", (4,), None),
 }
-FLANK_PATH_BUDGET = 4 << 30  # bytes of stored flank paths per chunk
+# bytes of stored flank paths per chunk.  None: 1 KiB per item (at least
+# 1 GiB), at most half the device's free memory and FLANK_PATH_MAX -- one
+# chunk at 8192^2 holds ~40 GB of paths, and each extra chunk retraces its
+# walks and ends in a tail of waits
+FLANK_PATH_BUDGET = None
+FLANK_PATH_MAX = 64 << 30
 _MIN_WS = {
     "count_downchannels": lambda L, p, n: L.slm_count_downchannels_workspace(n, 0),
     "flag_downchannels": lambda L, p, n: L.slm_flag_downchannels_workspace(n, p.nxy_padded),
@@ -66,7 +71,11 @@ def run_device(name, params, seeds_d, n, bufs, device=None, stream=None, status=
         size = int(_MIN_WS[name](L, params, n))
         if name.startswith("fix_"):
             # the flank fix stores paths chunk by chunk within this budget
-            size += FLANK_PATH_BUDGET
+            budget = FLANK_PATH_BUDGET
+            if budget is None:
+                free, _ = torch.cuda.mem_get_info(dev)
+                budget = min(max(1 << 30, int(n) << 10), FLANK_PATH_MAX, free // 2)
+            size += int(budget)
         ws = torch.empty(size, dtype=torch.uint8, device=dev)
         rc = fn(*(args + [ptr(ws), size, ctypes.byref(need), st]))
         if rc == _lib.SLM_ERR_CAPACITY:
