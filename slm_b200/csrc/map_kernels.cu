@@ -680,8 +680,8 @@ __global__ void k_owner_map(const slm_params p, uint32_t n, const float2* __rest
 // Items g0 .. g0+n-1; paths are stored at pairs[offsets[g] - base] (a chunk
 // of the item range at a time, so the stored paths fit the workspace).
 __global__ void k_flank_paths(const slm_params p, uint32_t g0, uint32_t n, const float2* __restrict__ seeds,
-                              const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
-                              const uint32_t* __restrict__ mapping, u64* __restrict__ n_pairs,
+                              const uint8_t* __restrict__ stop, const float2* __restrict__ uv,
+                              u64* __restrict__ n_pairs,
                               const u64* __restrict__ offsets, u64 base, uint2* __restrict__ pairs) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
@@ -699,7 +699,7 @@ __global__ void k_flank_paths(const slm_params p, uint32_t g0, uint32_t n, const
     Vec2 tv = vec;
     float tdt = dt;
     uint32_t power = 1, lam = 0;
-    while (!mask[idx] && ((~mapping[idx]) & p.is_thinchannel) && n_steps < p.max_n_steps) {
+    while (!stop[idx] && n_steps < p.max_n_steps) {
         const Step s = rk_plain(vec, dt, uv, p);
         const uint32_t q = s.idx;
         idx = q;
@@ -897,17 +897,22 @@ struct SettleLane {
 // Scan item state `w` on from w.k; 0: resolved (label written), 2: blocked
 // (w.k, w.at, w.lab_h at the place to resume, w.wait_o set).
 __device__ int settle_scan(SettleLane& w, uint32_t side, const slm_params& p, u64 base,
-                           const uint2* __restrict__ pairs, const uint8_t* __restrict__ mask,
+                           const uint2* __restrict__ pairs, const uint8_t* __restrict__ stop,
                            const uint32_t* __restrict__ mapping, const uint32_t* __restrict__ owner,
                            const uint32_t* __restrict__ label_init, uint32_t* label, uint32_t* resolved) {
     const uint32_t lfa = p.left_flank_addition, thin = p.is_thinchannel;
     uint32_t v = 0;
     // one pair of the walk's label scan: 0 go on, 1 the walk stops, 2 wait
+    // (stop[q]: mask or thin channel at q; when the compute pixel is the
+    // current one its label is the one just read)
     auto scan = [&](uint2 e) -> int {
+        if (stop[w.at]) return 1;
         if (!settle_read(w.at, w.g, w.h, w.lab_h, owner, label_init, label, resolved, v, w.wait_o)) return 2;
         const bool flank_ok = side ? (v & lfa) != 0u : ((~v) & lfa) != 0u;
-        if (mask[w.at] || !flank_ok || (mapping[w.at] & thin)) return 1;
-        if (!settle_read(e.x, w.g, w.h, w.lab_h, owner, label_init, label, resolved, v, w.wait_o)) return 2;
+        if (!flank_ok) return 1;
+        if (e.x != w.at &&
+            !settle_read(e.x, w.g, w.h, w.lab_h, owner, label_init, label, resolved, v, w.wait_o))
+            return 2;
         if ((w.lab_h & ~lfa) != (v & ~lfa)) w.lab_h = v;
         w.at = e.y;
         return 0;
@@ -968,11 +973,18 @@ __device__ int settle_scan(SettleLane& w, uint32_t side, const slm_params& p, u6
     return 0;
 }
 
+// stop[q] = 1 where a flank walk's loop test ends regardless of labels
+__global__ void k_flank_stop(uint32_t nxy, const uint8_t* __restrict__ mask, const uint32_t* __restrict__ mapping,
+                             uint32_t thin, uint8_t* __restrict__ stop) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nxy; q += gridDim.x * blockDim.x)
+        stop[q] = (mask[q] || (mapping[q] & thin)) ? 1 : 0;
+}
+
 // Items g0 .. g0+n-1 (their paths stored at pairs[offsets[g] - base]).
 __global__ void __launch_bounds__(256)
 k_flank_settle(const slm_params p, uint32_t g0, uint32_t n, uint32_t side, const u64* __restrict__ offsets,
                u64 base, const uint2* __restrict__ pairs, const uint32_t* __restrict__ hpix,
-               const uint8_t* __restrict__ mask, const uint32_t* __restrict__ mapping,
+               const uint8_t* __restrict__ stop, const uint32_t* __restrict__ mapping,
                const uint32_t* __restrict__ owner, const uint32_t* __restrict__ label_init, uint32_t* label,
                uint32_t* resolved, uint32_t* queue_head, uint32_t* status) {
     const unsigned FULL = 0xffffffffu;
@@ -1027,7 +1039,7 @@ k_flank_settle(const slm_params p, uint32_t g0, uint32_t n, uint32_t side, const
             w.waiting = false;
             w.waited = 0;
         }
-        if (settle_scan(w, side, p, base, pairs, mask, mapping, owner, label_init, label, resolved) == 2)
+        if (settle_scan(w, side, p, base, pairs, stop, mapping, owner, label_init, label, resolved) == 2)
             w.waiting = true;
         else
             w.alive = false;
@@ -1589,7 +1601,8 @@ int slm_exclusive_scan_u64(const uint64_t* in, uint32_t n, uint64_t* out, void* 
 size_t slm_fix_flanks_workspace(uint32_t n_seeds, uint32_t nxy_padded, uint64_t n_pairs) {
     return (size_t)(2 * (size_t)n_seeds + 1) * sizeof(u64) + (size_t)n_seeds * 2 * sizeof(uint32_t)
          + (size_t)nxy_padded * 2 * sizeof(uint32_t) + sizeof(uint32_t) + 256
-         + scan_scratch_words(n_seeds) * sizeof(u64) + (size_t)n_pairs * sizeof(uint2);
+         + scan_scratch_words(n_seeds) * sizeof(u64) + ((size_t)nxy_padded + 16)
+         + (size_t)n_pairs * sizeof(uint2);
 }
 
 static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, const uint8_t* mask,
@@ -1612,15 +1625,20 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
     uintptr_t pa = reinterpret_cast<uintptr_t>(n_resolved + 4);
     pa = (pa + 15) & ~(uintptr_t)15;
     u64* scan_scratch = reinterpret_cast<u64*>(pa);
-    uint2* pairs = reinterpret_cast<uint2*>(scan_scratch + scan_scratch_words(n));
+    uint8_t* stop = reinterpret_cast<uint8_t*>(scan_scratch + scan_scratch_words(n));
+    pa = reinterpret_cast<uintptr_t>(stop + nxy);
+    pa = (pa + 15) & ~(uintptr_t)15;
+    uint2* pairs = reinterpret_cast<uint2*>(pa);
     const u64 cap_pairs = (workspace_bytes - fixed) / sizeof(uint2);
     SLM_CUDA(cudaMemsetAsync(owner, 0xff, (size_t)nxy * sizeof(uint32_t), SS));
     SLM_CUDA(cudaMemsetAsync(resolved, 0, (size_t)n * sizeof(uint32_t), SS));
     SLM_CUDA(cudaMemcpyAsync(label_init, label, (size_t)nxy * sizeof(uint32_t), cudaMemcpyDeviceToDevice, SS));
     k_owner_map<<<blocks_for(n, 256), 256, 0, SS>>>(*p, n, F2(seed_point), owner, hpix);
     SLM_LAUNCHED("k_owner_map");
-    k_flank_paths<<<blocks_for(n, 128), 128, 0, SS>>>(*p, 0u, n, F2(seed_point), mask, F2(uv), mapping,
-                                                     n_pairs, nullptr, 0ull, nullptr);
+    k_flank_stop<<<(unsigned)(num_sms() * 8), 256, 0, SS>>>(nxy, mask, mapping, p->is_thinchannel, stop);
+    SLM_LAUNCHED("k_flank_stop");
+    k_flank_paths<<<blocks_for(n, 128), 128, 0, SS>>>(*p, 0u, n, F2(seed_point), stop, F2(uv), n_pairs, nullptr,
+                                                     0ull, nullptr);
     SLM_LAUNCHED("k_flank_paths");
     rc = exclusive_scan(n_pairs, n, offsets, scan_scratch, SS);
     if (rc) return rc;
@@ -1669,11 +1687,11 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
             u64 base = 0;
             SLM_CUDA(cudaMemcpyAsync(&base, offsets + a, sizeof(u64), cudaMemcpyDeviceToHost, SS));
             SLM_CUDA(cudaStreamSynchronize(SS));
-            k_flank_paths<<<blocks_for(m, 128), 128, 0, SS>>>(*p, a, m, F2(seed_point), mask, F2(uv), mapping,
-                                                             nullptr, offsets, base, pairs);
+            k_flank_paths<<<blocks_for(m, 128), 128, 0, SS>>>(*p, a, m, F2(seed_point), stop, F2(uv), nullptr,
+                                                             offsets, base, pairs);
             SLM_LAUNCHED("k_flank_paths");
             SLM_CUDA(cudaMemsetAsync(n_resolved + 1, 0, sizeof(uint32_t), SS));
-            k_flank_settle<<<grid, 256, 0, SS>>>(*p, a, m, left ? 1u : 0u, offsets, base, pairs, hpix, mask,
+            k_flank_settle<<<grid, 256, 0, SS>>>(*p, a, m, left ? 1u : 0u, offsets, base, pairs, hpix, stop,
                                                  mapping, owner, label_init, label, resolved, n_resolved + 1,
                                                  n_resolved + 2);
             SLM_LAUNCHED("k_flank_settle");
@@ -1695,8 +1713,8 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
         u64 base = 0;
         SLM_CUDA(cudaMemcpyAsync(&base, offsets + a, sizeof(u64), cudaMemcpyDeviceToHost, SS));
         SLM_CUDA(cudaStreamSynchronize(SS));
-        k_flank_paths<<<blocks_for(m, 128), 128, 0, SS>>>(*p, a, m, F2(seed_point), mask, F2(uv), mapping,
-                                                         nullptr, offsets, base, pairs);
+        k_flank_paths<<<blocks_for(m, 128), 128, 0, SS>>>(*p, a, m, F2(seed_point), stop, F2(uv), nullptr,
+                                                         offsets, base, pairs);
         SLM_LAUNCHED("k_flank_paths");
         uint32_t done = 0;
         for (uint32_t r0 = round; done < m; ++round) {
