@@ -48,6 +48,7 @@
 #define MAP_ST_OOB 2u
 #define MAP_LOOP_CAP (1u << 26)
 #define CONNECT_REC_MAX 256
+#define CNT_PREFETCH 16u
 #define NO_OWNER 0xffffffffu
 #define FLANK_PERIOD 0x80000000u
 
@@ -434,8 +435,19 @@ __global__ void k_count_replay(const slm_params p, uint32_t n, const float2* __r
         uint32_t nd = 0;  // decoded events (for the pattern ring)
         count[head] = counter++;
         bool stopped = false;
-        for (u64 k = offsets[g]; k < offsets[g + 1] && !stopped; ++k) {
+        const u64 k_end = offsets[g + 1];
+        for (u64 k = offsets[g]; k < k_end && !stopped; ++k) {
             const uint32_t wd = events[k];
+            // one thread walks the events: bring the pixels of the event
+            // CNT_PREFETCH ahead into L2 so their loads do not wait on DRAM
+            if (k + CNT_PREFETCH < k_end) {
+                const uint32_t ahead = events[k + CNT_PREFETCH];
+                if (ahead < p.nxy_padded) {  // a pixel, or a count word that is still in the grid
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(count + ahead));
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(mapping + ahead));
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(link + ahead));
+                }
+            }
             if ((wd & CNT_REPEAT) == 0u) {
                 if (!count_event(p, wd, counter, prev, mapping, count, link)) { last = wd; stopped = true; break; }
                 last8[nd % CNT_PMAX] = wd;
@@ -1091,12 +1103,21 @@ __global__ void k_hillslope_lengths(const slm_params p, uint32_t n, const float2
     uint32_t idx = pixel_of(vec, p), n_steps = 0;
     float dt = p.dt_max, l = 0.0f;
     bool moved_off = false;
+    // (vec, dt, moved_off) determines the rest of the walk (l only
+    // accumulates).  Once it repeats (Brent; the checkpoint restarts when
+    // moved_off turns), every lap passes the same tests, so the walk circles
+    // to its step bound on a pixel that is not a thin channel and writes
+    // nothing: it returns now.
+    StateCycle cyc;
+    cyc.init(vec, dt);
     while (((~mapping[idx]) & p.is_thinchannel) && n_steps < p.max_n_steps) {
         const Step s = rk_plain(vec, dt, uv, p);
         idx = s.idx;
         if (mask[idx]) return;
+        bool turned = false;
         if (!moved_off && ((~mapping[idx]) & from_flag)) {
             moved_off = true;
+            turned = true;
         } else if (moved_off && (mapping[idx] & from_flag)) {
             return;
         }
@@ -1105,6 +1126,8 @@ __global__ void k_hillslope_lengths(const slm_params p, uint32_t n, const float2
         n_steps++;
         if (m.stuck) return;
         dt = next_dt(dt, m.err, p);
+        if (turned) cyc.init(vec, dt);
+        else if (cyc.repeated(vec, dt)) return;
     }
     if (mapping[idx] & p.is_thinchannel) traj_length[g] = l * p.pixel_size;
 }
