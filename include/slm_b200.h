@@ -355,12 +355,13 @@ int slm_exclusive_scan_u64(const uint64_t* in, uint32_t n, uint64_t* out, void* 
 
 /* fix_right_flanks / fix_left_flanks (opencl/segment.cl:441-504, 530-594;
  * segment.py:210-232), with the result of the items run in ascending order.
- * The walks are traced in parallel and stored compressed (within the
- * workspace beyond the minimum slm_fix_flanks_workspace(n, nxy, 0), in
- * index-ordered chunks when they do not all fit; SLM_ERR_CAPACITY with
- * *required_bytes when one path does not), then each chunk is settled in
- * one persistent launch that takes items in ascending order and waits
- * (bounded) for the final label of a lower-index item whose pixel it reads.
+ * The walks are traced in parallel, once, into linked blocks of the path
+ * store (the workspace beyond the minimum slm_fix_flanks_workspace(n, nxy,
+ * 0)), then settled in one persistent launch that takes items in ascending
+ * order and waits (bounded) for the final label of a lower-index item whose
+ * pixel it reads.  When the store is too small the walks are traced again
+ * into index-ordered contiguous chunks of it (SLM_ERR_CAPACITY with
+ * *required_bytes when one path does not fit) and settled chunk by chunk.
  * If a wait runs out, or when the environment variable SLM_FLANK_ROUNDS is
  * nonzero, the labels are restored and the items resolve in rounds
  * instead. */

@@ -40,6 +40,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 #include "capi_util.cuh"
 #include "trace_common.cuh"
@@ -686,24 +687,75 @@ __global__ void k_owner_map(const slm_params p, uint32_t n, const float2* __rest
     owner[h] = g;
 }
 
+// Stored flank paths: linked blocks of FLANK_BLOCK entries, FLANK_BLOCK - 1
+// pairs and the index of the next block.
+constexpr uint32_t FLANK_BLOCK = 32;
+constexpr uint32_t NO_BLOCK = 0xffffffffu;
+
+// A block index for each calling lane of the warp (one atomic per call site
+// and warp); NO_BLOCK when the pool of cap blocks is used up.
+__device__ __forceinline__ uint32_t take_block(uint32_t* taken, uint32_t cap) {
+    const unsigned m = __activemask();
+    const unsigned lane = threadIdx.x & 31u;
+    const int leader = __ffs(m) - 1;
+    uint32_t b = 0;
+    if ((int)lane == leader) b = atomicAdd(taken, (uint32_t)__popc(m));
+    b = __shfl_sync(m, b, leader) + __popc(m & ((1u << lane) - 1u));
+    return b < cap ? b : NO_BLOCK;
+}
+
+// Where a flank walk's pairs go: counted only (out == NULL), a contiguous
+// range, or linked blocks taken from a pool as needed (counting goes on
+// after the pool runs out; *overflow is then set).
+struct ContigSink {
+    uint2* out;
+    u64 k;
+    __device__ void put(uint2 e) {
+        if (out) out[k] = e;
+        ++k;
+    }
+};
+
+struct LinkedSink {
+    uint2* pool;
+    uint32_t* taken;
+    uint32_t* overflow;
+    uint32_t cap, cur, f;
+    uint32_t* head;
+    u64 k;
+    bool ok;
+    __device__ void put(uint2 e) {
+        ++k;
+        if (!ok) return;
+        if (cur == NO_BLOCK || f == FLANK_BLOCK - 1) {
+            const uint32_t b = take_block(taken, cap);
+            if (b == NO_BLOCK) {
+                ok = false;
+                atomicOr(overflow, 1u);
+                return;
+            }
+            if (cur == NO_BLOCK) *head = b;
+            else pool[(u64)cur * FLANK_BLOCK + (FLANK_BLOCK - 1)] = make_uint2(b, 0u);
+            cur = b;
+            f = 0;
+        }
+        pool[(u64)cur * FLANK_BLOCK + f++] = e;
+    }
+};
+
 // Steps of a flank walk up to its label-independent end (mask, thin channel,
 // step cap, stuck), as (compute pixel, moved-to pixel) pairs; consecutive
 // equal pairs are stored once.  With pairs == nullptr only counts.
 // Items g0 .. g0+n-1; paths are stored at pairs[offsets[g] - base] (a chunk
 // of the item range at a time, so the stored paths fit the workspace).
-__global__ void k_flank_paths(const slm_params p, uint32_t g0, uint32_t n, const float2* __restrict__ seeds,
-                              const uint8_t* __restrict__ stop, const float2* __restrict__ uv,
-                              u64* __restrict__ n_pairs,
-                              const u64* __restrict__ offsets, u64 base, uint2* __restrict__ pairs) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const uint32_t g = g0 + t;
+// The walk of item g into `sink`; returns its pair count.
+template <class Sink>
+__device__ u64 flank_walk(const slm_params& p, uint32_t g, const float2* __restrict__ seeds,
+                          const uint8_t* __restrict__ stop, const float2* __restrict__ uv, Sink& sink) {
     Vec2 vec = seed_vec(seeds, g);
     uint32_t idx = pixel_of(vec, p), n_steps = 0;
     float dt = p.dt_max;
-    u64 k = 0;
     uint2 last = make_uint2(NO_OWNER, NO_OWNER);
-    uint2* out = pairs ? pairs + (offsets[g] - base) : nullptr;
     // As in count_downchannels: once (vec, dt) repeats bit for bit the
     // per-step pairs repeat with the period, so the rest of the walk is
     // stored as one period record {0x80000000|E, n} + the E pairs of a lap
@@ -718,8 +770,7 @@ __global__ void k_flank_paths(const slm_params p, uint32_t g0, uint32_t n, const
         const bool stuck = seg_move(s, vec, idx, dt, n_steps, p);
         if (q != last.x || idx != last.y) {
             last = make_uint2(q, idx);
-            if (out) out[k] = last;
-            k++;
+            sink.put(last);
         }
         if (stuck) break;
         lam++;
@@ -735,8 +786,7 @@ __global__ void k_flank_paths(const slm_params p, uint32_t g0, uint32_t n, const
                 if (pass == 1) {
                     const uint32_t nfut = (R / L) * E + partial;
                     if (nfut == 0) break;
-                    if (out) out[k] = make_uint2(FLANK_PERIOD | E, nfut);
-                    k++;
+                    sink.put(make_uint2(FLANK_PERIOD | E, nfut));
                 }
                 for (uint32_t t2 = 1; t2 <= L; ++t2) {
                     const Step s2 = rk_plain(v2, d2, uv, p);
@@ -749,8 +799,7 @@ __global__ void k_flank_paths(const slm_params p, uint32_t g0, uint32_t n, const
                             E++;
                             if (t2 <= Rm) partial++;
                         } else {
-                            if (out) out[k] = l2;
-                            k++;
+                            sink.put(l2);
                         }
                     }
                 }
@@ -764,7 +813,36 @@ __global__ void k_flank_paths(const slm_params p, uint32_t g0, uint32_t n, const
             lam = 0;
         }
     }
+    return sink.k;
+}
+
+// Items g0 .. g0+n-1: with pairs == NULL the pair counts into n_pairs[g],
+// else the pairs into pairs[offsets[g] - base ..].
+__global__ void k_flank_paths(const slm_params p, uint32_t g0, uint32_t n, const float2* __restrict__ seeds,
+                              const uint8_t* __restrict__ stop, const float2* __restrict__ uv,
+                              u64* __restrict__ n_pairs, const u64* __restrict__ offsets, u64 base,
+                              uint2* __restrict__ pairs) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint32_t g = g0 + t;
+    ContigSink sink{pairs ? pairs + (offsets[g] - base) : nullptr, 0};
+    const u64 k = flank_walk(p, g, seeds, stop, uv, sink);
     if (!pairs) n_pairs[g] = k;
+}
+
+// Items 0 .. n-1 in one pass: each path into linked blocks from the pool
+// (head block heads[g], NO_BLOCK for an empty path), its count into
+// n_pairs[g]; pool_ctr[0] counts the blocks taken, pool_ctr[1] is set when
+// the pool ran out (the counts are still exact).
+__global__ void k_flank_paths_linked(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
+                                     const uint8_t* __restrict__ stop, const float2* __restrict__ uv,
+                                     u64* __restrict__ n_pairs, uint32_t* __restrict__ heads,
+                                     uint2* __restrict__ pool, uint32_t cap_blocks, uint32_t* pool_ctr) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    heads[g] = NO_BLOCK;
+    LinkedSink sink{pool, pool_ctr, pool_ctr + 1, cap_blocks, NO_BLOCK, 0, heads + g, 0, true};
+    n_pairs[g] = flank_walk(p, g, seeds, stop, uv, sink);
 }
 
 // The label of pixel q as flank item g sees it: item g's own running value if
@@ -900,18 +978,56 @@ __device__ __noinline__ bool settle_read(uint32_t q, uint32_t g, uint32_t h, uin
     return true;
 }
 
-struct SettleLane {
+// A stored path read pair by pair: a contiguous range (pairs[k], k <
+// k_end), or linked blocks of FLANK_BLOCK entries, FLANK_BLOCK - 1 pairs and
+// the index of the next block, with `left` pairs still to read.
+struct ContigPath {
+    const uint2* pairs;  // the chunk's store, indexed from the chunk's base
     u64 k, k_end;
+    __device__ bool more() const { return k < k_end; }
+    __device__ uint2 get() { return pairs[k]; }
+    __device__ void next() { ++k; }
+    __device__ void end() { k = k_end; }
+};
+
+struct LinkedPath {
+    const uint2* pool;
+    uint32_t blk, off;
+    u64 left;
+    __device__ bool more() const { return left > 0; }
+    __device__ void follow() {
+        if (off == FLANK_BLOCK - 1) {
+            blk = pool[(u64)blk * FLANK_BLOCK + off].x;
+            off = 0;
+        }
+    }
+    __device__ uint2 get() {
+        follow();
+        return pool[(u64)blk * FLANK_BLOCK + off];
+    }
+    __device__ void next() {
+        follow();
+        ++off;
+        --left;
+    }
+    __device__ void end() { left = 0; }
+};
+
+template <class P>
+struct SettleLane {
+    P path;
     uint32_t g, h, at, lab_h, wait_o, waited;
     bool alive, waiting;
 };
 
-// Scan item state `w` on from w.k; 0: resolved (label written), 2: blocked
-// (w.k, w.at, w.lab_h at the place to resume, w.wait_o set).
-__device__ int settle_scan(SettleLane& w, uint32_t side, const slm_params& p, u64 base,
-                           const uint2* __restrict__ pairs, const uint8_t* __restrict__ stop,
-                           const uint32_t* __restrict__ mapping, const uint32_t* __restrict__ owner,
-                           const uint32_t* __restrict__ label_init, uint32_t* label, uint32_t* resolved) {
+// Scan item state `w` on from its place in its path; 0: resolved (label
+// written), 2: blocked (w.path, w.at, w.lab_h at the place to resume,
+// w.wait_o set).
+template <class P>
+__device__ int settle_scan(SettleLane<P>& w, uint32_t side, const slm_params& p,
+                           const uint8_t* __restrict__ stop, const uint32_t* __restrict__ mapping,
+                           const uint32_t* __restrict__ owner, const uint32_t* __restrict__ label_init,
+                           uint32_t* label, uint32_t* resolved) {
     const uint32_t lfa = p.left_flank_addition, thin = p.is_thinchannel;
     uint32_t v = 0;
     // one pair of the walk's label scan: 0 go on, 1 the walk stops, 2 wait
@@ -929,19 +1045,20 @@ __device__ int settle_scan(SettleLane& w, uint32_t side, const slm_params& p, u6
         w.at = e.y;
         return 0;
     };
-    while (w.k < w.k_end) {
-        const uint2 e = pairs[w.k - base];
+    while (w.path.more()) {
+        const uint2 e = w.path.get();
         if ((e.x & FLANK_PERIOD) == 0u) {
             const int st = scan(e);
             if (st == 2) return 2;
-            if (st == 1) { w.k = w.k_end; break; }
-            ++w.k;
+            if (st == 1) { w.path.end(); break; }
+            w.path.next();
             continue;
         }
-        // a period record, as k_flank_round runs it; a wait inside it
-        // restarts the record
+        // a period record, as k_flank_round runs it (n pairs cycling through
+        // the next E); a wait inside it restarts the record
         const uint32_t E = e.x & ~FLANK_PERIOD, nfut = e.y;
-        const uint2* pat = pairs + (w.k + 1 - base);
+        P pat = w.path;
+        pat.next();
         const uint32_t at0 = w.at, lab0 = w.lab_h;
         const uint32_t full = nfut / E, rem = nfut % E;
         uint32_t seen[8];
@@ -959,16 +1076,25 @@ __device__ int settle_scan(SettleLane& w, uint32_t side, const slm_params& p, u6
                 if (!skipped) seen[lap] = w.lab_h;
                 if (lap >= full) break;
             }
-            for (uint32_t i = 0; i < E && st == 0; ++i) st = scan(pat[i]);
+            P it = pat;
+            for (uint32_t i = 0; i < E && st == 0; ++i) {
+                st = scan(it.get());
+                it.next();
+            }
         }
-        for (uint32_t i = 0; i < rem && st == 0; ++i) st = scan(pat[i]);
+        P it = pat;
+        for (uint32_t i = 0; i < rem && st == 0; ++i) {
+            st = scan(it.get());
+            it.next();
+        }
         if (st == 2) {
             w.at = at0;
             w.lab_h = lab0;
             return 2;
         }
-        if (st == 1) { w.k = w.k_end; break; }
-        w.k += (u64)E + 1u;
+        if (st == 1) { w.path.end(); break; }
+        w.path = pat;
+        for (uint32_t i = 0; i < E; ++i) w.path.next();
     }
     // after the walk: the label at the last pixel, then the flank bit
     if (!settle_read(w.at, w.g, w.h, w.lab_h, owner, label_init, label, resolved, v, w.wait_o)) return 2;
@@ -992,24 +1118,28 @@ __global__ void k_flank_stop(uint32_t nxy, const uint8_t* __restrict__ mask, con
         stop[q] = (mask[q] || (mapping[q] & thin)) ? 1 : 0;
 }
 
-// Items g0 .. g0+n-1 (their paths stored at pairs[offsets[g] - base]).
+// Items g0 .. g0+n-1: with LinkedPath, item g's path starts at block
+// heads[g] and holds n_pairs[g] pairs in `store`; with ContigPath it is
+// store[offsets[g] - base .. offsets[g + 1] - base).
+template <class P>
 __global__ void __launch_bounds__(256)
 k_flank_settle(const slm_params p, uint32_t g0, uint32_t n, uint32_t side, const u64* __restrict__ offsets,
-               u64 base, const uint2* __restrict__ pairs, const uint32_t* __restrict__ hpix,
+               u64 base, const uint32_t* __restrict__ heads, const u64* __restrict__ n_pairs,
+               const uint2* __restrict__ store, const uint32_t* __restrict__ hpix,
                const uint8_t* __restrict__ stop, const uint32_t* __restrict__ mapping,
                const uint32_t* __restrict__ owner, const uint32_t* __restrict__ label_init, uint32_t* label,
                uint32_t* resolved, uint32_t* queue_head, uint32_t* status) {
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
-    SettleLane w;
+    SettleLane<P> w;
     w.alive = false;
     bool drained = false;
     for (uint32_t pass = 0;; ++pass) {
         // a lane that gave up stops every warp (the caller falls back)
         if ((pass & 63u) == 0u) {
-            uint32_t stop = 0;
-            if (lane == 0) stop = *(volatile const uint32_t*)status;
-            if (__shfl_sync(FULL, stop, 0)) break;
+            uint32_t stop_all = 0;
+            if (lane == 0) stop_all = *(volatile const uint32_t*)status;
+            if (__shfl_sync(FULL, stop_all, 0)) break;
         }
         if (!drained) {
             const unsigned idle = __ballot_sync(FULL, !w.alive);
@@ -1023,8 +1153,16 @@ k_flank_settle(const slm_params p, uint32_t g0, uint32_t n, uint32_t side, const
                     const uint32_t t = head + __popc(idle & ((1u << lane) - 1u));
                     if (t < n) {
                         w.g = g0 + t;
-                        w.k = offsets[w.g];
-                        w.k_end = offsets[w.g + 1];
+                        if constexpr (std::is_same<P, LinkedPath>::value) {
+                            w.path.pool = store;
+                            w.path.blk = heads[w.g];
+                            w.path.off = 0;
+                            w.path.left = n_pairs[w.g];
+                        } else {
+                            w.path.pairs = store;
+                            w.path.k = offsets[w.g] - base;
+                            w.path.k_end = offsets[w.g + 1] - base;
+                        }
                         w.h = hpix[w.g];
                         w.at = w.h;
                         w.lab_h = label_init[w.h];
@@ -1051,7 +1189,7 @@ k_flank_settle(const slm_params p, uint32_t g0, uint32_t n, uint32_t side, const
             w.waiting = false;
             w.waited = 0;
         }
-        if (settle_scan(w, side, p, base, pairs, stop, mapping, owner, label_init, label, resolved) == 2)
+        if (settle_scan(w, side, p, stop, mapping, owner, label_init, label, resolved) == 2)
             w.waiting = true;
         else
             w.alive = false;
@@ -1622,10 +1760,18 @@ int slm_exclusive_scan_u64(const uint64_t* in, uint32_t n, uint64_t* out, void* 
 }
 
 size_t slm_fix_flanks_workspace(uint32_t n_seeds, uint32_t nxy_padded, uint64_t n_pairs) {
-    return (size_t)(2 * (size_t)n_seeds + 1) * sizeof(u64) + (size_t)n_seeds * 2 * sizeof(uint32_t)
-         + (size_t)nxy_padded * 2 * sizeof(uint32_t) + sizeof(uint32_t) + 256
+    return (size_t)(2 * (size_t)n_seeds + 1) * sizeof(u64) + (size_t)n_seeds * 3 * sizeof(uint32_t)
+         + (size_t)nxy_padded * 2 * sizeof(uint32_t) + 8 * sizeof(uint32_t) + 256
          + scan_scratch_words(n_seeds) * sizeof(u64) + ((size_t)nxy_padded + 16)
          + (size_t)n_pairs * sizeof(uint2);
+}
+
+// restore the labels and flags before the rounds start over
+static int flank_restart(uint32_t* label, const uint32_t* label_init, uint32_t* resolved, uint32_t n,
+                         uint32_t nxy, cudaStream_t s) {
+    SLM_CUDA(cudaMemcpyAsync(label, label_init, (size_t)nxy * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    SLM_CUDA(cudaMemsetAsync(resolved, 0, (size_t)n * sizeof(uint32_t), s));
+    return SLM_OK;
 }
 
 static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, const uint8_t* mask,
@@ -1642,36 +1788,82 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
     u64* offsets = n_pairs + n;
     uint32_t* hpix = reinterpret_cast<uint32_t*>(offsets + n + 1);
     uint32_t* resolved = hpix + n;
-    uint32_t* owner = resolved + n;
+    uint32_t* heads = resolved + n;
+    uint32_t* owner = heads + n;
     uint32_t* label_init = owner + nxy;
-    uint32_t* n_resolved = label_init + nxy;  // [0] rounds: resolved count; [1] queue head; [2] status
-    uintptr_t pa = reinterpret_cast<uintptr_t>(n_resolved + 4);
+    // [0] rounds: resolved count; [1] queue head; [2] status; [3] pool blocks
+    // taken; [4] pool ran out
+    uint32_t* words = label_init + nxy;
+    uintptr_t pa = reinterpret_cast<uintptr_t>(words + 8);
     pa = (pa + 15) & ~(uintptr_t)15;
     u64* scan_scratch = reinterpret_cast<u64*>(pa);
     uint8_t* stop = reinterpret_cast<uint8_t*>(scan_scratch + scan_scratch_words(n));
     pa = reinterpret_cast<uintptr_t>(stop + nxy);
     pa = (pa + 15) & ~(uintptr_t)15;
-    uint2* pairs = reinterpret_cast<uint2*>(pa);
+    uint2* pairs = reinterpret_cast<uint2*>(pa);  // the path store
     const u64 cap_pairs = (workspace_bytes - fixed) / sizeof(uint2);
     SLM_CUDA(cudaMemsetAsync(owner, 0xff, (size_t)nxy * sizeof(uint32_t), SS));
     SLM_CUDA(cudaMemsetAsync(resolved, 0, (size_t)n * sizeof(uint32_t), SS));
+    SLM_CUDA(cudaMemsetAsync(words, 0, 8 * sizeof(uint32_t), SS));
     SLM_CUDA(cudaMemcpyAsync(label_init, label, (size_t)nxy * sizeof(uint32_t), cudaMemcpyDeviceToDevice, SS));
     k_owner_map<<<blocks_for(n, 256), 256, 0, SS>>>(*p, n, F2(seed_point), owner, hpix);
     SLM_LAUNCHED("k_owner_map");
     k_flank_stop<<<(unsigned)(num_sms() * 8), 256, 0, SS>>>(nxy, mask, mapping, p->is_thinchannel, stop);
     SLM_LAUNCHED("k_flank_stop");
-    k_flank_paths<<<blocks_for(n, 128), 128, 0, SS>>>(*p, 0u, n, F2(seed_point), stop, F2(uv), n_pairs, nullptr,
-                                                     0ull, nullptr);
-    SLM_LAUNCHED("k_flank_paths");
+    if (required_bytes) *required_bytes = fixed;
+
+    // 1. Every walk traced once into linked blocks, then settled in one
+    //    persistent launch.  The rounds (k_flank_round) run instead when the
+    //    environment variable SLM_FLANK_ROUNDS is nonzero (for tests), and
+    //    from the initial labels if a settle wait ran out.
+    const char* force = std::getenv("SLM_FLANK_ROUNDS");
+    const bool rounds_only = force && force[0] && force[0] != '0';
+    const unsigned side = left ? 1u : 0u;
+    bool counted = false, settle = !rounds_only;
+    unsigned settle_grid = 0;
+    if (settle) {
+        int occ = 0;
+        SLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_flank_settle<LinkedPath>, 256, 0));
+        settle_grid = (unsigned)(num_sms() * (occ > 0 ? occ : 1));
+        const u64 cap_blocks = cap_pairs / FLANK_BLOCK;
+        k_flank_paths_linked<<<blocks_for(n, 128), 128, 0, SS>>>(
+            *p, n, F2(seed_point), stop, F2(uv), n_pairs, heads, pairs,
+            (uint32_t)(cap_blocks < 0xfffffffeull ? cap_blocks : 0xfffffffeull), words + 3);
+        SLM_LAUNCHED("k_flank_paths_linked");
+        counted = true;
+        uint32_t ran_out = 0;
+        SLM_CUDA(cudaMemcpyAsync(&ran_out, words + 4, sizeof(uint32_t), cudaMemcpyDeviceToHost, SS));
+        SLM_CUDA(cudaStreamSynchronize(SS));
+        if (!ran_out) {
+            k_flank_settle<LinkedPath><<<settle_grid, 256, 0, SS>>>(
+                *p, 0u, n, side, nullptr, 0ull, heads, n_pairs, pairs, hpix, stop, mapping, owner, label_init,
+                label, resolved, words + 1, words + 2);
+            SLM_LAUNCHED("k_flank_settle");
+            uint32_t st = 0;
+            SLM_CUDA(cudaMemcpyAsync(&st, words + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, SS));
+            SLM_CUDA(cudaStreamSynchronize(SS));
+            if (st == 0u) return SLM_OK;
+            rc = flank_restart(label, label_init, resolved, n, nxy, SS);
+            if (rc) return rc;
+            settle = false;
+        }
+    }
+
+    // 2. The paths did not fit the pool (or the rounds run): stored
+    //    contiguously, in index-ordered chunks when they do not all fit.  An
+    //    item reads only initial labels and the final labels of lower-index
+    //    owners, which earlier chunks have resolved.
+    if (!counted) {
+        k_flank_paths<<<blocks_for(n, 128), 128, 0, SS>>>(*p, 0u, n, F2(seed_point), stop, F2(uv), n_pairs,
+                                                         nullptr, 0ull, nullptr);
+        SLM_LAUNCHED("k_flank_paths");
+    }
     rc = exclusive_scan(n_pairs, n, offsets, scan_scratch, SS);
     if (rc) return rc;
     u64 total = 0;
     SLM_CUDA(cudaMemcpyAsync(&total, offsets + n, sizeof(u64), cudaMemcpyDeviceToHost, SS));
     SLM_CUDA(cudaStreamSynchronize(SS));
     if (required_bytes) *required_bytes = slm_fix_flanks_workspace(n, nxy, total);
-    // Items run in index order, chunk after chunk, each chunk's paths stored
-    // at once: an item reads only initial labels and the final labels of
-    // lower-index owners, which earlier chunks have resolved.
     std::vector<std::pair<uint32_t, uint32_t>> chunks;
     if (total <= cap_pairs) {
         chunks.emplace_back(0u, n);
@@ -1695,16 +1887,10 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
             a = b;
         }
     }
-    // Each chunk settled in one persistent launch (k_flank_settle); in rounds
-    // (k_flank_round) from the initial labels if a wait there ran out, or when
-    // the environment variable SLM_FLANK_ROUNDS is nonzero (for tests).
-    const char* force = std::getenv("SLM_FLANK_ROUNDS");
-    bool settle = !(force && force[0] && force[0] != '0');
     if (settle) {
         int occ = 0;
-        SLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_flank_settle, 256, 0));
+        SLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_flank_settle<ContigPath>, 256, 0));
         const unsigned grid = (unsigned)(num_sms() * (occ > 0 ? occ : 1));
-        SLM_CUDA(cudaMemsetAsync(n_resolved + 2, 0, sizeof(uint32_t), SS));
         for (const auto& c : chunks) {
             const uint32_t a = c.first, m = c.second - c.first;
             u64 base = 0;
@@ -1713,23 +1899,21 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
             k_flank_paths<<<blocks_for(m, 128), 128, 0, SS>>>(*p, a, m, F2(seed_point), stop, F2(uv), nullptr,
                                                              offsets, base, pairs);
             SLM_LAUNCHED("k_flank_paths");
-            SLM_CUDA(cudaMemsetAsync(n_resolved + 1, 0, sizeof(uint32_t), SS));
-            k_flank_settle<<<grid, 256, 0, SS>>>(*p, a, m, left ? 1u : 0u, offsets, base, pairs, hpix, stop,
-                                                 mapping, owner, label_init, label, resolved, n_resolved + 1,
-                                                 n_resolved + 2);
+            SLM_CUDA(cudaMemsetAsync(words + 1, 0, sizeof(uint32_t), SS));
+            k_flank_settle<ContigPath><<<grid, 256, 0, SS>>>(*p, a, m, side, offsets, base, nullptr, nullptr,
+                                                             pairs, hpix, stop, mapping, owner, label_init,
+                                                             label, resolved, words + 1, words + 2);
             SLM_LAUNCHED("k_flank_settle");
         }
         uint32_t st = 0;
-        SLM_CUDA(cudaMemcpyAsync(&st, n_resolved + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, SS));
+        SLM_CUDA(cudaMemcpyAsync(&st, words + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, SS));
         SLM_CUDA(cudaStreamSynchronize(SS));
         if (st == 0u) return SLM_OK;
-        // start over from the initial labels, in rounds
-        SLM_CUDA(cudaMemcpyAsync(label, label_init, (size_t)nxy * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
-                                 SS));
-        SLM_CUDA(cudaMemsetAsync(resolved, 0, (size_t)n * sizeof(uint32_t), SS));
+        rc = flank_restart(label, label_init, resolved, n, nxy, SS);
+        if (rc) return rc;
     }
-    // rounds keep counting across chunks, so owners of earlier chunks count
-    // as resolved before
+    // 3. Rounds; they keep counting across chunks, so owners of earlier
+    //    chunks count as resolved before.
     uint32_t round = 1;
     for (const auto& c : chunks) {
         const uint32_t a = c.first, m = c.second - c.first;
@@ -1745,13 +1929,13 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
                 set_error("fix flanks did not resolve within %u rounds", m + 1);
                 return SLM_ERR_ITERATION_CAP;
             }
-            SLM_CUDA(cudaMemsetAsync(n_resolved, 0, sizeof(uint32_t), SS));
-            k_flank_round<<<blocks_for(m, 256), 256, 0, SS>>>(*p, a, m, left ? 1u : 0u, round, offsets, base,
-                                                             pairs, hpix, mask, mapping, owner, label_init,
-                                                             label, resolved, n_resolved);
+            SLM_CUDA(cudaMemsetAsync(words, 0, sizeof(uint32_t), SS));
+            k_flank_round<<<blocks_for(m, 256), 256, 0, SS>>>(*p, a, m, side, round, offsets, base, pairs, hpix,
+                                                             mask, mapping, owner, label_init, label, resolved,
+                                                             words);
             SLM_LAUNCHED("k_flank_round");
             uint32_t newly = 0;
-            SLM_CUDA(cudaMemcpyAsync(&newly, n_resolved, sizeof(uint32_t), cudaMemcpyDeviceToHost, SS));
+            SLM_CUDA(cudaMemcpyAsync(&newly, words, sizeof(uint32_t), cudaMemcpyDeviceToHost, SS));
             SLM_CUDA(cudaStreamSynchronize(SS));
             if (newly == 0) {
                 set_error("fix flanks round %u resolved nothing", round);

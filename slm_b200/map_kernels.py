@@ -29,12 +29,12 @@ SPECS = {
     "hillslopes": ("slm_hillslopes", (4,), None),
     "hillslope_lengths": ("slm_hillslope_lengths", (4,), None),
 }
-# bytes of stored flank paths per chunk.  None: 1 KiB per item (at least
-# 1 GiB), at most half the device's free memory and FLANK_PATH_MAX -- one
-# chunk at 8192^2 holds ~40 GB of paths, and each extra chunk retraces its
-# walks and ends in a tail of waits
+# bytes of the flank path store.  None: 2 KiB per item (at least 1 GiB), at
+# most half the device's free memory and FLANK_PATH_MAX.  The walks are
+# traced once into it when they fit (~45 GB at 8192^2); otherwise they are
+# traced again into index-ordered chunks of it.
 FLANK_PATH_BUDGET = None
-FLANK_PATH_MAX = 64 << 30
+FLANK_PATH_MAX = 96 << 30
 _MIN_WS = {
     "count_downchannels": lambda L, p, n: L.slm_count_downchannels_workspace(n, 0),
     "flag_downchannels": lambda L, p, n: L.slm_flag_downchannels_workspace(n, p.nxy_padded),
@@ -74,7 +74,7 @@ def run_device(name, params, seeds_d, n, bufs, device=None, stream=None, status=
             budget = FLANK_PATH_BUDGET
             if budget is None:
                 free, _ = torch.cuda.mem_get_info(dev)
-                budget = min(max(1 << 30, int(n) << 10), FLANK_PATH_MAX, free // 2)
+                budget = min(max(1 << 30, int(n) << 11), FLANK_PATH_MAX, free // 2)
             size += int(budget)
         ws = torch.empty(size, dtype=torch.uint8, device=dev)
         rc = fn(*(args + [ptr(ws), size, ctypes.byref(need), st]))

@@ -114,10 +114,10 @@ def test_mapping_pipeline_incised_bit_exact(seed):
 @pytest.mark.parametrize("form", ["settle", "rounds"])
 @pytest.mark.parametrize("case", ["pipeline", "incised"])
 def test_flank_fix_forms_bit_exact(monkeypatch, form, case):
-    """fix_right/left_flanks in both forms -- the stored paths settled in one
-    persistent launch that waits on lower-index owners (the default), and
-    resolved in rounds (SLM_FLANK_ROUNDS=1, the fallback) -- give the
-    oracle's labels."""
+    """fix_right/left_flanks in both forms -- every walk traced once into
+    linked blocks and settled in one persistent launch that waits on
+    lower-index owners (the default), and resolved in rounds
+    (SLM_FLANK_ROUNDS=1, the fallback) -- give the oracle's labels."""
     if form == "rounds":
         monkeypatch.setenv("SLM_FLANK_ROUNDS", "1")
     else:
@@ -132,13 +132,18 @@ def test_flank_fix_forms_bit_exact(monkeypatch, form, case):
     assert [n for n, _ in run.calls].count("fix_right_flanks") == 1
 
 
-def test_flank_fix_in_chunks_bit_exact(monkeypatch):
-    """A path budget far below the total makes the rounds form of
-    fix_right/left_flanks run its items in many index-ordered chunks; labels
-    equal the oracle's."""
+@pytest.mark.parametrize("form", ["settle", "rounds"])
+def test_flank_fix_in_chunks_bit_exact(monkeypatch, form):
+    """A path budget far below the total: the single-pass store runs out, so
+    fix_right/left_flanks store the paths contiguously in many index-ordered
+    chunks and settle them chunk by chunk (or, with SLM_FLANK_ROUNDS=1,
+    resolve them in rounds); labels equal the oracle's."""
     from slm_b200 import map_kernels
     monkeypatch.setattr(map_kernels, "FLANK_PATH_BUDGET", 2048)
-    monkeypatch.setenv("SLM_FLANK_ROUNDS", "1")
+    if form == "rounds":
+        monkeypatch.setenv("SLM_FLANK_ROUNDS", "1")
+    else:
+        monkeypatch.delenv("SLM_FLANK_ROUNDS", raising=False)
     c, info, data = pipeline_case(nx=120, ny=96, seed=12)
     run = DeviceVsOracle()
     assert M.map_channels_segments(None, info, data, runner=run)
