@@ -56,6 +56,65 @@ def host_copy(src, min_bytes=8 << 20):
     return dst
 
 
+def _parallel_copy(dst, src):
+    """np.copyto of two same-size contiguous arrays, split over up to 8 threads."""
+    global _COPY_POOL
+    if _COPY_POOL is None:
+        from concurrent.futures import ThreadPoolExecutor
+        _COPY_POOL = ThreadPoolExecutor(max(1, min(8, os.cpu_count() or 1)))
+    f, g = src.reshape(-1), dst.reshape(-1)
+    n, k = f.size, _COPY_POOL._max_workers
+    list(_COPY_POOL.map(lambda i: np.copyto(g[i * n // k:(i + 1) * n // k], f[i * n // k:(i + 1) * n // k]),
+                        range(k)))
+
+
+_STAGING = {}
+
+
+def pinned_staging(slot, shape, dtype):
+    """A pinned host tensor of this shape and torch dtype, kept for reuse (one per slot)."""
+    key = (slot, tuple(shape), dtype)
+    st = _STAGING.get(key)
+    if st is None:
+        st = torch.empty(tuple(shape), dtype=dtype, pin_memory=True)
+        _STAGING[key] = st
+    return st
+
+
+def upload(array, device, slot, dtype=None):
+    """``to_device`` for large pageable arrays (any strides): gathered into a
+    pinned staging buffer by several threads, cast to ``dtype`` on the way,
+    then copied by DMA.  The caller synchronises the current stream before
+    reusing ``slot``."""
+    a = array.view(np.uint8) if array.dtype == np.bool_ else array
+    dt = np.dtype(dtype) if dtype is not None else a.dtype
+    if a.nbytes < (32 << 20) or a.ndim == 0:
+        return torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).to(device)
+    st = pinned_staging(slot, a.shape, torch.from_numpy(np.empty(0, dt)).dtype)
+    dst = st.numpy()
+    global _COPY_POOL
+    if _COPY_POOL is None:
+        from concurrent.futures import ThreadPoolExecutor
+        _COPY_POOL = ThreadPoolExecutor(max(1, min(8, os.cpu_count() or 1)))
+    n, k = a.shape[0], _COPY_POOL._max_workers
+    list(_COPY_POOL.map(lambda i: np.copyto(dst[i * n // k:(i + 1) * n // k], a[i * n // k:(i + 1) * n // k],
+                                            casting="unsafe"), range(k)))
+    return st.to(device, non_blocking=True)
+
+
+def download(tensors, slot):
+    """Fresh NumPy copies of device tensors: all go to pinned staging buffers
+    by DMA, one synchronisation, then out of them on several threads."""
+    stages = []
+    for i, t in enumerate(tensors):
+        st = pinned_staging((slot, i), t.shape, t.dtype)
+        st.copy_(t, non_blocking=True)
+        stages.append(st)
+    if stages:
+        torch.cuda.current_stream(tensors[0].device).synchronize()
+    return [host_copy(st.numpy()) for st in stages]
+
+
 def pinned_empty(shape, dtype):
     """A NumPy array backed by page-locked host memory (fast DMA both ways)."""
     tdt = {np.dtype(np.float32): torch.float32, np.dtype(np.uint8): torch.uint8,

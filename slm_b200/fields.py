@@ -29,7 +29,7 @@ import numpy as np
 import torch
 
 from . import kernels
-from .device import cuda_device, host_copy, low32, to_device, traced
+from .device import cuda_device, host_copy, low32, pinned_staging, to_device, traced
 from .distributed import allreduce_counts, shard_queue, shard_queue_params, sharded_field_pass
 from .params import kernel_params
 from .useful import create_seeds_device, create_seeds_device_state, vprint
@@ -52,17 +52,9 @@ def _slc_table(dev, dd, n):
     return t
 
 
-_STAGING = {}
-
-
 def _staging(slot, t):
     """Pinned host tensor shaped like device tensor ``t`` (kept for reuse, one per slot)."""
-    key = (slot, tuple(t.shape), t.dtype)
-    st = _STAGING.get(key)
-    if st is None:
-        st = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
-        _STAGING[key] = st
-    return st
+    return pinned_staging(slot, t.shape, t.dtype)
 
 
 _ROWS_POOL = None

@@ -19,7 +19,7 @@ import torch
 
 from . import _lib, map_kernels
 from ._lib import check, ptr
-from .device import cuda_device
+from .device import cuda_device, download, upload
 from .params import kernel_params
 
 
@@ -44,17 +44,20 @@ class DeviceMapping:
         self.shape = (nxp, nyp)
         self.n = nxp * nyp
 
-        def up(a, dt):
+        def up(a, dt, slot):
             if isinstance(a, torch.Tensor):
                 t = a if a.dtype != torch.bool else a.view(torch.uint8)
                 return t.to(dev, _TORCH[np.dtype(dt)]).contiguous()
-            return torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).to(dev)
+            return upload(a, dev, ("mapping", slot), dtype=np.dtype(dt))
         m = data.mask_array
-        self.mask = up(m.view(np.uint8) if isinstance(m, np.ndarray) and m.dtype == np.bool_ else m, np.uint8)
-        self.uv = up(data.uv_array, np.float32)
-        self.mapping = up(data.mapping_array, np.uint32).reshape(-1)
-        self.slt_dn = up(data.slt_array[:, :, 0], np.float32)
-        self.slc_dn = up(data.slc_array[:, :, 0], np.float64)
+        self.mask = up(m.view(np.uint8) if isinstance(m, np.ndarray) and m.dtype == np.bool_ else m, np.uint8,
+                       "mask")
+        self.uv = up(data.uv_array, np.float32, "uv")
+        self.mapping = up(data.mapping_array, np.uint32, "flags").reshape(-1)
+        self.slt_dn = up(data.slt_array[:, :, 0], np.float32, "slt")
+        self.slc_dn = up(data.slc_array[:, :, 0], np.float64, "slc")
+        # the staging buffers are free again once the copies have run
+        torch.cuda.current_stream(dev).synchronize()
         self.count = torch.zeros(self.n, dtype=torch.uint32, device=dev)
         self.link = torch.zeros(self.n, dtype=torch.uint32, device=dev)
         self.label = torch.zeros(self.n, dtype=torch.uint32, device=dev)
@@ -236,12 +239,16 @@ class DeviceMapping:
     def download(self):
         """Copy the grids back into ``data`` (the arrays the host sequence fills)."""
         d, shape = self.data, self.shape
-        d.mapping_array = self.mapping.cpu().numpy().reshape(shape)
-        d.count_array = self.count.cpu().numpy().reshape(shape)
-        d.link_array = self.link.cpu().numpy().reshape(shape)
-        d.label_array = self.label.cpu().numpy().view(np.int32).reshape(shape)
+        grids = [self.mapping, self.count, self.link, self.label]
         if self.channel_label is not None:
-            d.channel_label_array = self.channel_label.cpu().numpy().reshape(shape)
+            grids.append(self.channel_label)
+        out = download(grids, "mapping")
+        d.mapping_array = out[0].reshape(shape)
+        d.count_array = out[1].reshape(shape)
+        d.link_array = out[2].reshape(shape)
+        d.label_array = out[3].view(np.int32).reshape(shape)
+        if self.channel_label is not None:
+            d.channel_label_array = out[4].reshape(shape)
 
 
 def map_channels_segments_device(info, data, do_map_channels_from_scratch=True, do_map_segments=True,
