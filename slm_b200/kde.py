@@ -79,8 +79,18 @@ def estimate_univariate_pdf(distbn, do_detrend=False, logx_vec=None):
         kernels.pdf_univariate(kde_params(distbn, "pdf_univariate"), hist_d, pdf_d)
         pdf_array = pdf_d.cpu().numpy().reshape(npp, 1)
     vprint(verbose, "done")
-    return (pdf_array / (sum(pdf_array) * bin_dx),
-            histogram_array / (sum(histogram_array) * bin_dx))
+    # the reference normalises by Python's builtin sum over the rows: a
+    # left-to-right sum in the array's own dtype, which accumulate gives
+    return (pdf_array / (_row_sum(pdf_array) * bin_dx),
+            histogram_array / (_row_sum(histogram_array) * bin_dx))
+
+
+def _row_sum(a):
+    """``sum(a)`` (builtin) of an [n, 1] array: the rows added left to right in
+    a's dtype (kde.py:193-194)."""
+    if a.shape[0] == 0:
+        return 0
+    return np.add.accumulate(a, axis=0, dtype=a.dtype)[-1]
 
 
 def estimate_bivariate_pdf(distbn):
