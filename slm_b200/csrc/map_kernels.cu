@@ -954,17 +954,28 @@ __global__ void k_flank_round(const slm_params p, uint32_t g0, uint32_t n, uint3
 // one, with the running label there), and on later passes only polls the
 // owner's flag until it can go on.  The lowest unresolved item taken waits on
 // nothing unresolved, so some lane always advances.  A label is published
-// with a fence before its resolved flag.  The RK walks are traced in parallel
+// by a release store of its resolved flag, read with acquire.  The RK walks are traced in parallel
 // beforehand (k_flank_paths), so only the path scans lie on a chain of waits.
 //
 // Every wait is bounded: a lane that polls FLANK_WAIT_LIMIT times in a row
 // sets bit 0 of *status, and every warp stops; the caller then resolves the
 // items in rounds (k_flank_round) from the initial labels.
-#define FLANK_WAIT_LIMIT (1u << 22)
+#define FLANK_WAIT_LIMIT (1u << 24)
 
 // the label of pixel q as item g reads it (flank_read's rules, with the
-// owner's flag instead of its round); false and *wait_o when the owner has
-// not resolved.  Out of line, as flank_read.
+// owner's flag, read with acquire, instead of its round); false and *wait_o
+// when the owner has not resolved.  Out of line, as flank_read.
+// a flag read that orders the loads after it (acquire), and the flag write
+// that publishes the stores before it (release), at GPU scope
+__device__ __forceinline__ uint32_t load_acquire(const uint32_t* a) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(a) : "memory");
+    return v;
+}
+__device__ __forceinline__ void store_release(uint32_t* a, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(a), "r"(v) : "memory");
+}
+
 __device__ __noinline__ bool settle_read(uint32_t q, uint32_t g, uint32_t h, uint32_t lab_h,
                                         const uint32_t* __restrict__ owner,
                                         const uint32_t* __restrict__ label_init, const uint32_t* label,
@@ -972,8 +983,7 @@ __device__ __noinline__ bool settle_read(uint32_t q, uint32_t g, uint32_t h, uin
     if (q == h) { out = lab_h; return true; }
     const uint32_t o = owner[q];
     if (o == NO_OWNER || o > g) { out = label_init[q]; return true; }
-    if (((volatile const uint32_t*)resolved)[o] == 0u) { wait_o = o; return false; }
-    __threadfence();
+    if (load_acquire(resolved + o) == 0u) { wait_o = o; return false; }
     out = ((volatile const uint32_t*)label)[q];
     return true;
 }
@@ -1106,8 +1116,7 @@ __device__ int settle_scan(SettleLane<P>& w, uint32_t side, const slm_params& p,
         if (v & lfa) w.lab_h |= lfa;
     }
     label[w.h] = w.lab_h;
-    __threadfence();
-    ((volatile uint32_t*)resolved)[w.g] = 1u;
+    store_release(resolved + w.g, 1u);
     return 0;
 }
 
@@ -1177,22 +1186,32 @@ k_flank_settle(const slm_params p, uint32_t g0, uint32_t n, uint32_t side, const
             if (drained) break;
             continue;
         }
-        if (!w.alive) continue;
-        if (w.waiting) {
-            if (((volatile const uint32_t*)resolved)[w.wait_o] == 0u) {
-                if (++w.waited >= FLANK_WAIT_LIMIT) {
-                    atomicOr(status, 1u);
-                    w.alive = false;
+        bool idle_pass = true;  // this lane did nothing but wait this pass
+        if (w.alive) {
+            bool go = true;
+            if (w.waiting) {
+                if (load_acquire(resolved + w.wait_o) == 0u) {
+                    go = false;
+                    if (++w.waited >= FLANK_WAIT_LIMIT) {
+                        atomicOr(status, 1u);
+                        w.alive = false;
+                    }
+                } else {
+                    w.waiting = false;
+                    w.waited = 0;
                 }
-                continue;
             }
-            w.waiting = false;
-            w.waited = 0;
+            if (go) {
+                idle_pass = false;
+                if (settle_scan(w, side, p, stop, mapping, owner, label_init, label, resolved) == 2)
+                    w.waiting = true;
+                else
+                    w.alive = false;
+            }
         }
-        if (settle_scan(w, side, p, stop, mapping, owner, label_init, label, resolved) == 2)
-            w.waiting = true;
-        else
-            w.alive = false;
+        // a warp whose every lane only waited backs off, leaving the issue
+        // slots to warps that scan
+        if (__all_sync(FULL, idle_pass)) __nanosleep(256);
     }
 }
 
