@@ -977,12 +977,12 @@ __device__ __forceinline__ void store_release(uint32_t* a, uint32_t v) {
 }
 
 __device__ __noinline__ bool settle_read(uint32_t q, uint32_t g, uint32_t h, uint32_t lab_h,
-                                        const uint32_t* __restrict__ owner,
-                                        const uint32_t* __restrict__ label_init, const uint32_t* label,
+                                        const uint2* __restrict__ pix, const uint32_t* label,
                                         const uint32_t* resolved, uint32_t& out, uint32_t& wait_o) {
     if (q == h) { out = lab_h; return true; }
-    const uint32_t o = owner[q];
-    if (o == NO_OWNER || o > g) { out = label_init[q]; return true; }
+    const uint2 oi = pix[q];  // (owner, initial label) in one load
+    const uint32_t o = oi.x;
+    if (o == NO_OWNER || o > g) { out = oi.y; return true; }
     if (load_acquire(resolved + o) == 0u) { wait_o = o; return false; }
     out = ((volatile const uint32_t*)label)[q];
     return true;
@@ -1036,8 +1036,7 @@ struct SettleLane {
 template <class P>
 __device__ int settle_scan(SettleLane<P>& w, uint32_t side, const slm_params& p,
                            const uint8_t* __restrict__ stop, const uint32_t* __restrict__ mapping,
-                           const uint32_t* __restrict__ owner, const uint32_t* __restrict__ label_init,
-                           uint32_t* label, uint32_t* resolved) {
+                           const uint2* __restrict__ pix, uint32_t* label, uint32_t* resolved) {
     const uint32_t lfa = p.left_flank_addition, thin = p.is_thinchannel;
     uint32_t v = 0;
     // one pair of the walk's label scan: 0 go on, 1 the walk stops, 2 wait
@@ -1045,11 +1044,11 @@ __device__ int settle_scan(SettleLane<P>& w, uint32_t side, const slm_params& p,
     // current one its label is the one just read)
     auto scan = [&](uint2 e) -> int {
         if (stop[w.at]) return 1;
-        if (!settle_read(w.at, w.g, w.h, w.lab_h, owner, label_init, label, resolved, v, w.wait_o)) return 2;
+        if (!settle_read(w.at, w.g, w.h, w.lab_h, pix, label, resolved, v, w.wait_o)) return 2;
         const bool flank_ok = side ? (v & lfa) != 0u : ((~v) & lfa) != 0u;
         if (!flank_ok) return 1;
         if (e.x != w.at &&
-            !settle_read(e.x, w.g, w.h, w.lab_h, owner, label_init, label, resolved, v, w.wait_o))
+            !settle_read(e.x, w.g, w.h, w.lab_h, pix, label, resolved, v, w.wait_o))
             return 2;
         if ((w.lab_h & ~lfa) != (v & ~lfa)) w.lab_h = v;
         w.at = e.y;
@@ -1107,9 +1106,9 @@ __device__ int settle_scan(SettleLane<P>& w, uint32_t side, const slm_params& p,
         for (uint32_t i = 0; i < E; ++i) w.path.next();
     }
     // after the walk: the label at the last pixel, then the flank bit
-    if (!settle_read(w.at, w.g, w.h, w.lab_h, owner, label_init, label, resolved, v, w.wait_o)) return 2;
+    if (!settle_read(w.at, w.g, w.h, w.lab_h, pix, label, resolved, v, w.wait_o)) return 2;
     if ((w.lab_h & ~lfa) != (v & ~lfa)) w.lab_h = v;
-    settle_read(w.at, w.g, w.h, w.lab_h, owner, label_init, label, resolved, v, w.wait_o);
+    settle_read(w.at, w.g, w.h, w.lab_h, pix, label, resolved, v, w.wait_o);
     if (side) {
         if (((~v) & lfa) && !(mapping[w.at] & thin)) w.lab_h &= ~lfa;
     } else {
@@ -1118,6 +1117,13 @@ __device__ int settle_scan(SettleLane<P>& w, uint32_t side, const slm_params& p,
     label[w.h] = w.lab_h;
     store_release(resolved + w.g, 1u);
     return 0;
+}
+
+// pix[q] = (owner[q], label_init[q]), read together by the settle scan
+__global__ void k_flank_pix(uint32_t nxy, const uint32_t* __restrict__ owner,
+                            const uint32_t* __restrict__ label_init, uint2* __restrict__ pix) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nxy; q += gridDim.x * blockDim.x)
+        pix[q] = make_uint2(owner[q], label_init[q]);
 }
 
 // stop[q] = 1 where a flank walk's loop test ends regardless of labels
@@ -1136,8 +1142,8 @@ k_flank_settle(const slm_params p, uint32_t g0, uint32_t n, uint32_t side, const
                u64 base, const uint32_t* __restrict__ heads, const u64* __restrict__ n_pairs,
                const uint2* __restrict__ store, const uint32_t* __restrict__ hpix,
                const uint8_t* __restrict__ stop, const uint32_t* __restrict__ mapping,
-               const uint32_t* __restrict__ owner, const uint32_t* __restrict__ label_init, uint32_t* label,
-               uint32_t* resolved, uint32_t* queue_head, uint32_t* status) {
+               const uint2* __restrict__ pix, uint32_t* label, uint32_t* resolved, uint32_t* queue_head,
+               uint32_t* status) {
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
     SettleLane<P> w;
@@ -1174,7 +1180,7 @@ k_flank_settle(const slm_params p, uint32_t g0, uint32_t n, uint32_t side, const
                         }
                         w.h = hpix[w.g];
                         w.at = w.h;
-                        w.lab_h = label_init[w.h];
+                        w.lab_h = pix[w.h].y;
                         w.waited = 0;
                         w.waiting = false;
                         w.alive = true;
@@ -1203,7 +1209,7 @@ k_flank_settle(const slm_params p, uint32_t g0, uint32_t n, uint32_t side, const
             }
             if (go) {
                 idle_pass = false;
-                if (settle_scan(w, side, p, stop, mapping, owner, label_init, label, resolved) == 2)
+                if (settle_scan(w, side, p, stop, mapping, pix, label, resolved) == 2)
                     w.waiting = true;
                 else
                     w.alive = false;
@@ -1782,7 +1788,7 @@ size_t slm_fix_flanks_workspace(uint32_t n_seeds, uint32_t nxy_padded, uint64_t 
     return (size_t)(2 * (size_t)n_seeds + 1) * sizeof(u64) + (size_t)n_seeds * 3 * sizeof(uint32_t)
          + (size_t)nxy_padded * 2 * sizeof(uint32_t) + 8 * sizeof(uint32_t) + 256
          + scan_scratch_words(n_seeds) * sizeof(u64) + ((size_t)nxy_padded + 16)
-         + (size_t)n_pairs * sizeof(uint2);
+         + ((size_t)nxy_padded * sizeof(uint2) + 16) + (size_t)n_pairs * sizeof(uint2);
 }
 
 // restore the labels and flags before the rounds start over
@@ -1819,7 +1825,8 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
     uint8_t* stop = reinterpret_cast<uint8_t*>(scan_scratch + scan_scratch_words(n));
     pa = reinterpret_cast<uintptr_t>(stop + nxy);
     pa = (pa + 15) & ~(uintptr_t)15;
-    uint2* pairs = reinterpret_cast<uint2*>(pa);  // the path store
+    uint2* pix = reinterpret_cast<uint2*>(pa);
+    uint2* pairs = pix + nxy;  // the path store
     const u64 cap_pairs = (workspace_bytes - fixed) / sizeof(uint2);
     SLM_CUDA(cudaMemsetAsync(owner, 0xff, (size_t)nxy * sizeof(uint32_t), SS));
     SLM_CUDA(cudaMemsetAsync(resolved, 0, (size_t)n * sizeof(uint32_t), SS));
@@ -1829,6 +1836,8 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
     SLM_LAUNCHED("k_owner_map");
     k_flank_stop<<<(unsigned)(num_sms() * 8), 256, 0, SS>>>(nxy, mask, mapping, p->is_thinchannel, stop);
     SLM_LAUNCHED("k_flank_stop");
+    k_flank_pix<<<(unsigned)(num_sms() * 8), 256, 0, SS>>>(nxy, owner, label_init, pix);
+    SLM_LAUNCHED("k_flank_pix");
     if (required_bytes) *required_bytes = fixed;
 
     // 1. Every walk traced once into linked blocks, then settled in one
@@ -1855,8 +1864,8 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
         SLM_CUDA(cudaStreamSynchronize(SS));
         if (!ran_out) {
             k_flank_settle<LinkedPath><<<settle_grid, 256, 0, SS>>>(
-                *p, 0u, n, side, nullptr, 0ull, heads, n_pairs, pairs, hpix, stop, mapping, owner, label_init,
-                label, resolved, words + 1, words + 2);
+                *p, 0u, n, side, nullptr, 0ull, heads, n_pairs, pairs, hpix, stop, mapping, pix, label, resolved,
+                words + 1, words + 2);
             SLM_LAUNCHED("k_flank_settle");
             uint32_t st = 0;
             SLM_CUDA(cudaMemcpyAsync(&st, words + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, SS));
@@ -1920,8 +1929,8 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
             SLM_LAUNCHED("k_flank_paths");
             SLM_CUDA(cudaMemsetAsync(words + 1, 0, sizeof(uint32_t), SS));
             k_flank_settle<ContigPath><<<grid, 256, 0, SS>>>(*p, a, m, side, offsets, base, nullptr, nullptr,
-                                                             pairs, hpix, stop, mapping, owner, label_init,
-                                                             label, resolved, words + 1, words + 2);
+                                                             pairs, hpix, stop, mapping, pix, label, resolved,
+                                                             words + 1, words + 2);
             SLM_LAUNCHED("k_flank_settle");
         }
         uint32_t st = 0;
