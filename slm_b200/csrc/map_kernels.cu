@@ -961,7 +961,6 @@ __global__ void k_flank_round(const slm_params p, uint32_t g0, uint32_t n, uint3
 // sets bit 0 of *status, and every warp stops; the caller then resolves the
 // items in rounds (k_flank_round) from the initial labels.
 #define FLANK_WAIT_LIMIT (1u << 24)
-#define SETTLE_BATCH 8u
 
 // the label of pixel q as item g reads it (flank_read's rules, with the
 // owner's flag, read with acquire, instead of its round); false and *wait_o
@@ -1058,86 +1057,10 @@ __device__ int settle_scan(SettleLane<P>& w, uint32_t side, const slm_params& p,
     while (w.path.more()) {
         const uint2 e = w.path.get();
         if ((e.x & FLANK_PERIOD) == 0u) {
-            // up to SETTLE_BATCH plain pairs at once: every label they may
-            // read is loaded before any is used -- the pixel words, then the
-            // owners' flags (relaxed), one fence, then the labels whose flag
-            // was set -- and the pairs are then scanned in order as `scan`
-            // does.  A label whose owner had not resolved blocks the scan at
-            // its pair.
-            uint2 pr[SETTLE_BATCH];
-            P it = w.path;
-            int m = 0;
-            while (m < (int)SETTLE_BATCH && it.more()) {
-                const uint2 x = it.get();
-                if (x.x & FLANK_PERIOD) break;
-                pr[m++] = x;
-                it.next();
-            }
-            // values of the pixel each pair starts on (a) and of its compute
-            // pixel (c); state: 0 ready, 1 own pixel (running label), 2 owner
-            // not resolved
-            uint32_t va[SETTLE_BATCH], vc[SETTLE_BATCH], oa[SETTLE_BATCH], oc[SETTLE_BATCH];
-            uint8_t sa[SETTLE_BATCH], ka[SETTLE_BATCH], kc[SETTLE_BATCH];
-            bool any_lower = false;
-#pragma unroll
-            for (int i = 0; i < (int)SETTLE_BATCH; ++i) {
-                if (i >= m) break;
-                const uint32_t a = i == 0 ? w.at : pr[i - 1].y, c = pr[i].x;
-                sa[i] = stop[a];
-                ka[i] = 1;
-                kc[i] = 1;
-                if (a != w.h) {
-                    const uint2 oi = pix[a];
-                    oa[i] = oi.x;
-                    va[i] = oi.y;
-                    const bool lower = oi.x != NO_OWNER && oi.x < w.g;
-                    ka[i] = lower ? 2 : 0;
-                    any_lower |= lower;
-                }
-                if (c != w.h) {
-                    const uint2 oi = pix[c];
-                    oc[i] = oi.x;
-                    vc[i] = oi.y;
-                    const bool lower = oi.x != NO_OWNER && oi.x < w.g;
-                    kc[i] = lower ? 2 : 0;
-                    any_lower |= lower;
-                }
-            }
-            if (any_lower) {
-#pragma unroll
-                for (int i = 0; i < (int)SETTLE_BATCH; ++i) {
-                    if (i >= m) break;
-                    if (ka[i] == 2 && ((volatile const uint32_t*)resolved)[oa[i]] != 0u) ka[i] = 3;
-                    if (kc[i] == 2 && ((volatile const uint32_t*)resolved)[oc[i]] != 0u) kc[i] = 3;
-                }
-                __threadfence();
-#pragma unroll
-                for (int i = 0; i < (int)SETTLE_BATCH; ++i) {
-                    if (i >= m) break;
-                    const uint32_t a = i == 0 ? w.at : pr[i - 1].y;
-                    if (ka[i] == 3) { va[i] = ((volatile const uint32_t*)label)[a]; ka[i] = 0; }
-                    if (kc[i] == 3) { vc[i] = ((volatile const uint32_t*)label)[pr[i].x]; kc[i] = 0; }
-                }
-            }
-            int st = 0;
-#pragma unroll
-            for (int i = 0; i < (int)SETTLE_BATCH; ++i) {
-                if (i >= m) break;
-                if (sa[i]) { st = 1; break; }
-                if (ka[i] == 2) { w.wait_o = oa[i]; st = 2; break; }
-                uint32_t val = ka[i] == 1 ? w.lab_h : va[i];
-                const bool flank_ok = side ? (val & lfa) != 0u : ((~val) & lfa) != 0u;
-                if (!flank_ok) { st = 1; break; }
-                if (pr[i].x != w.at) {
-                    if (kc[i] == 2) { w.wait_o = oc[i]; st = 2; break; }
-                    val = kc[i] == 1 ? w.lab_h : vc[i];
-                }
-                if ((w.lab_h & ~lfa) != (val & ~lfa)) w.lab_h = val;
-                w.at = pr[i].y;
-                w.path.next();
-            }
+            const int st = scan(e);
             if (st == 2) return 2;
             if (st == 1) { w.path.end(); break; }
+            w.path.next();
             continue;
         }
         // a period record, as k_flank_round runs it (n pairs cycling through
