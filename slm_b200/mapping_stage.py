@@ -60,6 +60,9 @@ MAPPING_PARAMETERS = dict(vars(default_parameters().mapping))
 MAPPING_PARAMETERS.update(do_map_channels_segments=True, do_map_hsl=True, midslope_filter_sigma=5.0,
                           midslope_threshold=0.03, ridge_filter_sigma=2.0, ridge_threshold=0.8,
                           n_hsl_averaging_threshold=1, hsl_averaging_threshold=5.0)
+# this project's: threads (each with its own CUDA stream) pass 2 runs its
+# independent coarse subsegments on when the grids are on the GPU
+MAPPING_PARAMETERS.update(pass2_workers=6)
 
 HSL_COLUMNS = ("count", "mean [m]", "stddev [m]")
 
@@ -223,6 +226,36 @@ class DeviceEngine:
             return None
         with torch.cuda.device(self.dm.dev):
             return self.dm.hsl(False)
+
+
+def subsegment_order(coarse, base, labels, boxes, pad):
+    """The order constraints among pass 2's coarse subsegments: subsegment j
+    reads the flags of its window (the box of its own pixels grown by 1 or 2
+    px, within the frame, widened by ``pad``) and writes only its own
+    unmasked pixels.  For every pair whose writes fall in the other's window
+    the lower label goes first.  Returns (successor lists, predecessor
+    counts), by position in ``labels``."""
+    n = len(labels)
+    index = {int(lab): i for i, lab in enumerate(labels)}
+    nx, ny = coarse.shape
+    written = np.where(base, 0, coarse)
+    succ = [set() for _ in range(n)]
+    for j in range(n):
+        g = 2 if labels[j] < 0 else 1
+        x0, x1, y0, y1 = (int(v) for v in boxes[j])
+        x0, x1 = max(pad, x0 - g) - pad, min(nx - 1 - pad, x1 + g) + pad
+        y0, y1 = max(pad, y0 - g) - pad, min(ny - 1 - pad, y1 + g) + pad
+        for v in np.unique(written[max(0, x0):x1 + 1, max(0, y0):y1 + 1]):
+            i = index.get(int(v))
+            if i is None or i == j:
+                continue
+            a, b = (i, j) if i < j else (j, i)
+            succ[a].add(b)
+    indeg = [0] * n
+    for a in range(n):
+        for b in succ[a]:
+            indeg[b] += 1
+    return [sorted(x) for x in succ], indeg
 
 
 # ------------------------------------------------------------------ subsegment statistics
@@ -395,13 +428,18 @@ class Mapping:
         self.state.add_active_mask({"merged_coarse": self.merged_coarse_mask_array})
         frame = torch.ones_like(roi.base)
         frame[pad:-pad, pad:-pad] = False
-        means, tables = [], []
         roi.hsl.zero_()
         # the job's masks do not change inside the loop
         base = torch.from_numpy(self._base_mask()).to(roi.device)
         coarse_labels = self.coarse_subsegments_list_array
         nxp, nyp = roi.coarse.shape
-        for label, (x0, x1, y0, y1) in zip(coarse_labels, label_boxes(roi.coarse, coarse_labels)):
+        boxes = label_boxes(roi.coarse, coarse_labels)
+
+        def one(j, engine, analysis):
+            """Coarse subsegment j; returns (mean, table) or None.  It writes
+            the hillslope lengths and flags of its own unmasked pixels."""
+            label = coarse_labels[j]
+            x0, x1, y0, y1 = boxes[j]
             # the subsegment grown by 1 px (2 for a left flank), off the
             # frame, worked out on the crop its growth can reach
             g = 2 if label < 0 else 1
@@ -415,7 +453,7 @@ class Mapping:
             _paste(region, (win.sl[0].start, win.sl[1].start), region_c, (cx, cy))
             mask_w = win.of(base) | ~region
             own_w = win.of(roi.coarse) == int(label)
-            t = self.analysis.estimate_channel_threshold(types.SimpleNamespace(
+            t = analysis.estimate_channel_threshold(types.SimpleNamespace(
                 mask_array=mask_w.cpu().numpy(), slt_array=roi.slt_h[win.sl], sla_array=roi.sla_h[win.sl]),
                 verbose=quiet)
             if t is None or t > self.max_channel_threshold:
@@ -423,37 +461,101 @@ class Mapping:
             elif t < self.min_channel_threshold:
                 t = self.guess_channel_threshold / 2
             info.set_thresholds(channel_threshold=t, segmentation_threshold=self.fine_segmentation_threshold)
-            ok, flags, labels = self.engine.map(info, win, roi, mask_w, win.of(roi.mapping).clone())
+            ok, flags, labels = engine.map(info, win, roi, mask_w, win.of(roi.mapping).clone())
             if not ok:
-                continue
+                return None
             # this pass's channel heads are kept as WAS_CHANNELHEAD
             head = int(info.is_channelhead)
             flags = torch.where((flags & head) == head, flags | int(info.was_channelhead), flags)
             picked = ((flags & int(info.is_midslope)) > 0) & ~mask_w
             fine = labels[picked].cpu().numpy()
-            lengths = self.engine.lengths(info, flags, int(fine.shape[0]))
+            lengths = engine.lengths(info, flags, int(fine.shape[0]))
             if lengths is None:
-                continue
+                return None
             stats = length_statistics(fine, lengths, label)
             if stats is None:
-                continue
+                return None
             painted = paint_means(labels, stats, self.n_hsl_averaging_threshold, roi.device)
             kept = painted[~torch.isnan(painted)]
             kept = kept[kept >= self.hsl_averaging_threshold].cpu().numpy()
             if len(stats) == 0 or kept.shape[0] == 0:
-                continue
-            means.append(np.mean(kept))
-            tables.append(stats[(stats["count"] > 1) & (stats["mean [m]"] > 5.0)])
+                return None
             # only the subsegment's own unmasked pixels take the results
             take = own_w & ~win.of(base)
             win.of(roi.hsl)[take] = torch.nan_to_num(painted, nan=0.0)[take]
             target = win.of(roi.mapping)
             target[take] |= flags[take]
+            return np.mean(kept), stats[(stats["count"] > 1) & (stats["mean [m]"] > 5.0)]
+
+        results = self._run_subsegments(one, roi, base, coarse_labels, boxes)
+        means = [r[0] for r in results if r is not None]
+        tables = [r[1] for r in results if r is not None]
         roi.hsl.nan_to_num_(nan=0.0)
         self.hsl_mean_array = np.array(means, dtype=np.float32) if means else np.array([], dtype=np.float32)
         self.hsl_stats_df = pd.concat(tables) if tables else None
         self.state.reset_active_masks()
         self.print("\n**Pass#2 end**")
+
+    def _run_subsegments(self, one, roi, base, coarse_labels, boxes):
+        """``one(j, engine, analysis)`` for every coarse subsegment j; the
+        results in label order, identical to running them one after another
+        in that order.  With the grids on the GPU they run on
+        ``pass2_workers`` threads, each on its own CUDA stream with its own
+        engine and analysis: subsegment j reads the flags in its window and
+        writes flags and lengths only on its own unmasked pixels, so j waits
+        for every lower-label subsegment with such pixels in its window, and
+        a higher-label one with pixels in j's window waits for j."""
+        import copy
+        import heapq
+        import threading
+        from concurrent.futures import FIRST_COMPLETED, ThreadPoolExecutor, wait
+        n = len(coarse_labels)
+        workers = int(getattr(self, "pass2_workers", 1)) if isinstance(self.engine, DeviceEngine) else 1
+        if workers <= 1 or n <= 1:
+            return [one(j, self.engine, self.analysis) for j in range(n)]
+        succ, indeg = subsegment_order(roi.coarse.cpu().numpy(), base.cpu().numpy(), coarse_labels, boxes,
+                                       self.geodata.pad_width)
+        dev = roi.device
+        torch.cuda.current_stream(dev).synchronize()
+        local = threading.local()
+        engines, lock, last_pdf = [], threading.Lock(), []
+
+        def job(j):
+            if not hasattr(local, "stream"):
+                local.stream = torch.cuda.Stream(dev)
+                local.engine = DeviceEngine(self.device)
+                local.analysis = copy.copy(self.analysis)
+                with lock:
+                    engines.append(local.engine)
+            with torch.cuda.device(dev), torch.cuda.stream(local.stream):
+                r = one(j, local.engine, local.analysis)
+                local.stream.synchronize()
+            if j == n - 1 and hasattr(local.analysis, "mpdf_dslt"):
+                last_pdf.append(local.analysis.mpdf_dslt)
+            return r
+
+        results = [None] * n
+        ready = [j for j in range(n) if indeg[j] == 0]
+        heapq.heapify(ready)
+        with ThreadPoolExecutor(workers) as ex:
+            running = {}
+            while ready or running:
+                while ready and len(running) < 2 * workers:
+                    j = heapq.heappop(ready)
+                    running[ex.submit(job, j)] = j
+                done, _ = wait(running, return_when=FIRST_COMPLETED)
+                for f in done:
+                    j = running.pop(f)
+                    results[j] = f.result()
+                    for k in succ[j]:
+                        indeg[k] -= 1
+                        if indeg[k] == 0:
+                            heapq.heappush(ready, k)
+        for e in engines:
+            self.engine.status |= e.status
+        if last_pdf:  # the analysis ends with the last subsegment's pdf, as in order
+            self.analysis.mpdf_dslt = last_pdf[0]
+        return results
 
     def pass3(self):
         raise NotImplementedError("pass 3 smooths the hillslope lengths and the aspect with scikit-image's rank "

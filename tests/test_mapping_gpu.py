@@ -317,6 +317,55 @@ def test_mapping_stage_pass2_on_the_gpu():
     assert gpu.hsl_stats_df.equals(cpu.hsl_stats_df)
 
 
+def test_mapping_stage_pass2_threads_equal_order():
+    """Pass 2 with its independent coarse subsegments on six threads and
+    streams (the default on the GPU) equals pass 2 run one subsegment after
+    another in label order, on a grid with many subsegments."""
+    import types
+
+    from mapping_cases import incised_pipeline_case
+    from slm_b200 import analysis as A
+    from slm_b200.mapping_stage import Mapping
+    from slm_b200.skeleton import zhang_suen
+    from slm_b200.useful import default_parameters
+    from test_mapping_stage import ActiveMasks
+    n = 160
+    info0, data0 = incised_pipeline_case(n=n, seed=5, n_incisions=14, max_steps=300)
+    slt, slc = data0.slt_array, data0.slc_array
+    with np.errstate(divide="ignore", invalid="ignore"):
+        sla = np.where(slc > 0, np.sqrt(2.0) * slt / slc, 0.0).astype(np.float32)
+    d = default_parameters()
+    trace = types.SimpleNamespace(**vars(d.trace))
+    trace.subpixel_seed_point_density, trace.jitter_magnitude = 1, 0.0
+    trace.integrator_step_factor, trace.max_length = 0.1, 20.0
+    trace.slc_array, trace.slt_array, trace.sla_array = slc, slt, sla
+    geodata = types.SimpleNamespace(roi_nx=n, roi_ny=n, pad_width=2, roi_pixel_size=2.0)
+    preprocess = types.SimpleNamespace(uv_array=data0.uv_array)
+    analysis_params = {"analysis": dict(A.ANALYSIS_PARAMETERS, n_hist_bins=512, n_pdf_points=64,
+                                        pdf_slt_min=1e-3, pdf_sla_min=1e-3, pdf_slc_min=1e-3)}
+    out = []
+    for workers in (1, 6):
+        params = dict(vars(d.mapping))
+        params.update(coarse_channel_threshold=float(info0.channel_threshold), coarse_segmentation_threshold=12,
+                      fine_segmentation_threshold=6, midslope_filter_sigma=2.0, midslope_threshold=0.2,
+                      ridge_filter_sigma=2.0, ridge_threshold=0.3, do_measure_hsl_from_ridges=False,
+                      n_hsl_averaging_threshold=1, hsl_averaging_threshold=5.0, min_channel_threshold=1.0,
+                      max_channel_threshold=1000.0, guess_channel_threshold=30.0, pass2_workers=workers)
+        state = ActiveMasks(data0.mask_array, **vars(d.state))
+        m = Mapping(state, {"mapping": params}, geodata, preprocess, trace,
+                    analysis=A.Analysis(state, analysis_params, geodata, None, trace), thin=zhang_suen)
+        m.pass1()
+        m.pass2()
+        out.append(m)
+    seq, par = out
+    assert seq.n_coarse_subsegments == par.n_coarse_subsegments > 20
+    assert np.array_equal(seq.mapping_array, par.mapping_array)
+    assert np.array_equal(seq.hsl_array.view(np.uint32), par.hsl_array.view(np.uint32)) and seq.hsl_array.any()
+    assert np.array_equal(seq.hsl_mean_array, par.hsl_mean_array)
+    assert seq.hsl_stats_df.equals(par.hsl_stats_df)
+    assert seq.engine.status == par.engine.status
+
+
 @pytest.mark.parametrize("n", [0, 1, 1000, 65536, 65537, 300001, 10_000_000])
 def test_exclusive_scan_u64(n):
     """The tiled exclusive scan behind the stored flank paths (one block up
