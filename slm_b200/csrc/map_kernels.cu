@@ -573,27 +573,86 @@ __device__ __forceinline__ bool seg_move(const Step& s, Vec2& vec, uint32_t& idx
     return false;
 }
 
-__global__ void k_segment_hillslopes(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
-                                     const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
-                                     const uint32_t* __restrict__ mapping, uint32_t* label) {
-    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= n) return;
-    Vec2 vec = seed_vec(seeds, g);
-    uint32_t idx = pixel_of(vec, p), n_steps = 0;
-    const uint32_t h = idx;
-    float dt = p.dt_max;
+// Per-pixel walks with warp-local refill: warp w owns items
+// [w * WALK_PER_WARP, (w + 1) * WALK_PER_WARP); a lane whose walk ends takes
+// the warp's next item at once (a ballot, no global counter), so a warp's
+// lanes stay busy however uneven their walks are.  Each item's walk is the
+// one-thread-per-item walk, so results are unchanged.
+constexpr uint32_t WALK_PER_WARP = 256;
+
+template <class W>
+__global__ void __launch_bounds__(256) k_walks(W w, uint32_t n) {
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t lo = warp * WALK_PER_WARP;
+    const uint64_t hi = lo + WALK_PER_WARP < n ? lo + WALK_PER_WARP : n;
+    uint64_t next = lo;
+    bool alive = false;
+    while (true) {
+        const unsigned idle = __ballot_sync(FULL, !alive);
+        if (idle && next < hi) {
+            const uint64_t mine = next + __popc(idle & ((1u << lane) - 1u));
+            next += __popc(idle);
+            if (!alive && mine < hi) alive = w.start((uint32_t)mine);
+        }
+        if (!__any_sync(FULL, alive)) {
+            if (next >= hi) break;
+            continue;
+        }
+        if (alive) alive = w.step();
+    }
+}
+
+static unsigned walk_grid(uint32_t n) {
+    const uint64_t warps = ((uint64_t)n + WALK_PER_WARP - 1) / WALK_PER_WARP;
+    return (unsigned)((warps + 7) / 8);  // 8 warps per block of 256
+}
+
+// segment_hillslopes (segment.cl): from each hillslope pixel down to a thin
+// channel, whose label it takes
+struct SegHillWalk {
+    slm_params p;
+    const float2* seeds;
+    const uint8_t* mask;
+    const float2* uv;
+    const uint32_t* mapping;
+    uint32_t* label;
+    Vec2 vec;
+    float dt;
+    uint32_t idx, h, n_steps;
     StateCycle cyc;
-    cyc.init(vec, dt);
-    while (!mask[idx] && ((~mapping[idx]) & p.is_thinchannel) && n_steps < p.max_n_steps) {
+    __device__ bool start(uint32_t g) {
+        vec = seed_vec(seeds, g);
+        idx = pixel_of(vec, p);
+        h = idx;
+        n_steps = 0;
+        dt = p.dt_max;
+        cyc.init(vec, dt);
+        return step_test();
+    }
+    // the loop test; false ends the walk (and writes its label)
+    __device__ bool step_test() {
+        if (!mask[idx] && ((~mapping[idx]) & p.is_thinchannel) && n_steps < p.max_n_steps) return true;
+        finish();
+        return false;
+    }
+    __device__ void finish() {
+        if (mapping[idx] & p.is_thinchannel) label[h] = label[idx];
+    }
+    __device__ bool step() {
         const Step s = rk_plain(vec, dt, uv, p);
         idx = s.idx;
-        if (seg_move(s, vec, idx, dt, n_steps, p)) break;
+        if (seg_move(s, vec, idx, dt, n_steps, p)) {
+            finish();
+            return false;
+        }
         // a cycle of states that all continue the loop ends at the bound on a
         // pixel that is not a thin channel: no label
-        if (cyc.repeated(vec, dt)) return;
+        if (cyc.repeated(vec, dt)) return false;
+        return step_test();
     }
-    if (mapping[idx] & p.is_thinchannel) label[h] = label[idx];
-}
+};
 
 __device__ __forceinline__ uint32_t rotate_left(uint32_t px, uint32_t py, int8_t& dx, int8_t& dy,
                                                 uint32_t nyp) {
@@ -654,28 +713,51 @@ __global__ void k_subsegment_channel_edges(const slm_params p, uint32_t n,
     }
 }
 
-__global__ void k_subsegment_flanks(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
-                                    const uint8_t* __restrict__ mask, const float2* __restrict__ uv,
-                                    const uint32_t* __restrict__ mapping, uint32_t* label) {
-    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= n) return;
-    Vec2 vec = seed_vec(seeds, g);
-    uint32_t idx = pixel_of(vec, p), n_steps = 0;
-    const uint32_t h = idx;
-    float dt = p.dt_max;
+// subsegment_flanks (segment.cl:360-414): from each pixel down to a left
+// flank or thin channel; the left-flank bit when a left flank is reached
+struct SubsegFlankWalk {
+    slm_params p;
+    const float2* seeds;
+    const uint8_t* mask;
+    const float2* uv;
+    const uint32_t* mapping;
+    uint32_t* label;
+    Vec2 vec;
+    float dt;
+    uint32_t idx, h, n_steps;
     StateCycle cyc;
-    cyc.init(vec, dt);
-    while (!mask[idx] && ((~mapping[idx]) & p.is_leftflank) && ((~mapping[idx]) & p.is_thinchannel)
-           && n_steps < p.max_n_steps) {
+    __device__ bool start(uint32_t g) {
+        vec = seed_vec(seeds, g);
+        idx = pixel_of(vec, p);
+        h = idx;
+        n_steps = 0;
+        dt = p.dt_max;
+        cyc.init(vec, dt);
+        return step_test();
+    }
+    __device__ bool step_test() {
+        if (!mask[idx] && ((~mapping[idx]) & p.is_leftflank) && ((~mapping[idx]) & p.is_thinchannel)
+            && n_steps < p.max_n_steps)
+            return true;
+        finish();
+        return false;
+    }
+    __device__ void finish() {
+        if (mapping[idx] & p.is_leftflank) label[h] |= p.left_flank_addition;
+    }
+    __device__ bool step() {
         const Step s = rk_plain(vec, dt, uv, p);
         idx = s.idx;
-        if (seg_move(s, vec, idx, dt, n_steps, p)) break;
+        if (seg_move(s, vec, idx, dt, n_steps, p)) {
+            finish();
+            return false;
+        }
         // a cycle of states that all continue the loop ends at the bound on a
         // pixel that is not left flank: no flank bit
-        if (cyc.repeated(vec, dt)) return;
+        if (cyc.repeated(vec, dt)) return false;
+        return step_test();
     }
-    if (mapping[idx] & p.is_leftflank) label[h] |= p.left_flank_addition;
-}
+};
 
 // ------------------------------------------------------------------ fix flanks
 __global__ void k_owner_map(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
@@ -1734,9 +1816,9 @@ int slm_segment_hillslopes(const slm_params* p, uint32_t n, const float* seed_po
     int rc = map_checks(p, n, seed_point);
     if (rc) return rc;
     if (n == 0) return SLM_OK;
-    k_segment_hillslopes<<<blocks_for(n, 128), 128, 0, SS>>>(*p, n, F2(seed_point), mask, F2(uv), mapping,
-                                                            label);
-    SLM_LAUNCHED("k_segment_hillslopes");
+    SegHillWalk w{*p, F2(seed_point), mask, F2(uv), mapping, label};
+    k_walks<SegHillWalk><<<walk_grid(n), 256, 0, SS>>>(w, n);
+    SLM_LAUNCHED("k_walks<SegHillWalk>");
     return SLM_OK;
 }
 
@@ -1765,9 +1847,9 @@ int slm_subsegment_flanks(const slm_params* p, uint32_t n, const float* seed_poi
     int rc = map_checks(p, n, seed_point);
     if (rc) return rc;
     if (n == 0) return SLM_OK;
-    k_subsegment_flanks<<<blocks_for(n, 128), 128, 0, SS>>>(*p, n, F2(seed_point), mask, F2(uv), mapping,
-                                                           label);
-    SLM_LAUNCHED("k_subsegment_flanks");
+    SubsegFlankWalk w{*p, F2(seed_point), mask, F2(uv), mapping, label};
+    k_walks<SubsegFlankWalk><<<walk_grid(n), 256, 0, SS>>>(w, n);
+    SLM_LAUNCHED("k_walks<SubsegFlankWalk>");
     return SLM_OK;
 }
 
