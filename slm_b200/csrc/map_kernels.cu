@@ -28,7 +28,7 @@
 //       path.  One persistent launch (k_flank_resolve) takes items in
 //       ascending order and walks each once, waiting for the final label of a
 //       lower-index owner it reads.  Fallback (a bounded wait ran out): paths
-//       are traced in parallel (FlankPathWalk, compressed to the steps whose
+//       are traced in parallel (k_flank_paths, compressed to the steps whose
 //       (compute pixel, moved-to pixel) pair changes), then items are
 //       resolved in rounds (k_flank_round): an item resolves once every
 //       lower-index owner it reads has resolved in an earlier round.  The
@@ -830,65 +830,22 @@ struct LinkedSink {
 // equal pairs are stored once.  With pairs == nullptr only counts.
 // Items g0 .. g0+n-1; paths are stored at pairs[offsets[g] - base] (a chunk
 // of the item range at a time, so the stored paths fit the workspace).
-// The walk of a flank item up to its label-independent end (mask, thin
-// channel, step cap, stuck), as (compute pixel, moved-to pixel) pairs into
-// `sink`; consecutive equal pairs are stored once.  As in
-// count_downchannels: once (vec, dt) repeats bit for bit the per-step pairs
-// repeat with the period, so the rest of the walk is stored as one period
-// record {0x80000000|E, n} + the E pairs of a lap (after every step `last`
-// is that step's pair, so each lap merges alike).  Run by k_walks with
-// warp-local refill; the item's count goes to n_pairs[g] (only counted, or
-// into linked blocks; the contiguous store leaves n_pairs as it is).
+// The walk of item g into `sink`; returns its pair count.
 template <class Sink>
-struct FlankPathWalk {
-    slm_params p;
-    const float2* seeds;
-    const uint8_t* stop;
-    const float2* uv;
-    u64* n_pairs;
-    uint32_t g0;
-    const u64* offsets;  // contiguous store: pairs[offsets[g] - base ..]; NULL pairs: count only
-    u64 base;
-    uint2* pairs;
-    uint2* pool;  // linked store
-    uint32_t cap_blocks;
-    uint32_t* pool_ctr;
-    uint32_t* heads;
-    Sink sink;
-    Vec2 vec, tv;
-    float dt, tdt;
-    uint32_t g, idx, n_steps, power, lam;
-    uint2 last;
-
-    __device__ bool start(uint32_t t) {
-        g = g0 + t;
-        if constexpr (std::is_same<Sink, LinkedSink>::value) {
-            heads[g] = NO_BLOCK;
-            sink = LinkedSink{pool, pool_ctr, pool_ctr + 1, cap_blocks, NO_BLOCK, 0, heads + g, 0, true};
-        } else {
-            sink = ContigSink{pairs ? pairs + (offsets[g] - base) : nullptr, 0};
-        }
-        vec = seed_vec(seeds, g);
-        idx = pixel_of(vec, p);
-        n_steps = 0;
-        dt = p.dt_max;
-        last = make_uint2(NO_OWNER, NO_OWNER);
-        tv = vec;
-        tdt = dt;
-        power = 1;
-        lam = 0;
-        return test();
-    }
-    __device__ bool test() {
-        if (!stop[idx] && n_steps < p.max_n_steps) return true;
-        finish();
-        return false;
-    }
-    __device__ void finish() {
-        if constexpr (std::is_same<Sink, LinkedSink>::value) n_pairs[g] = sink.k;
-        else if (!pairs) n_pairs[g] = sink.k;
-    }
-    __device__ bool step() {
+__device__ u64 flank_walk(const slm_params& p, uint32_t g, const float2* __restrict__ seeds,
+                          const uint8_t* __restrict__ stop, const float2* __restrict__ uv, Sink& sink) {
+    Vec2 vec = seed_vec(seeds, g);
+    uint32_t idx = pixel_of(vec, p), n_steps = 0;
+    float dt = p.dt_max;
+    uint2 last = make_uint2(NO_OWNER, NO_OWNER);
+    // As in count_downchannels: once (vec, dt) repeats bit for bit the
+    // per-step pairs repeat with the period, so the rest of the walk is
+    // stored as one period record {0x80000000|E, n} + the E pairs of a lap
+    // (after every step `last` is that step's pair, so each lap merges alike).
+    Vec2 tv = vec;
+    float tdt = dt;
+    uint32_t power = 1, lam = 0;
+    while (!stop[idx] && n_steps < p.max_n_steps) {
         const Step s = rk_plain(vec, dt, uv, p);
         const uint32_t q = s.idx;
         idx = q;
@@ -897,10 +854,7 @@ struct FlankPathWalk {
             last = make_uint2(q, idx);
             sink.put(last);
         }
-        if (stuck) {
-            finish();
-            return false;
-        }
+        if (stuck) break;
         lam++;
         if (__float_as_uint(vec.x) == __float_as_uint(tv.x) && __float_as_uint(vec.y) == __float_as_uint(tv.y)
             && __float_as_uint(dt) == __float_as_uint(tdt) && n_steps < p.max_n_steps) {
@@ -932,8 +886,7 @@ struct FlankPathWalk {
                     }
                 }
             }
-            finish();
-            return false;
+            break;
         }
         if (lam == power) {
             tv = vec;
@@ -941,51 +894,37 @@ struct FlankPathWalk {
             power <<= 1;
             lam = 0;
         }
-        return test();
     }
-};
+    return sink.k;
+}
 
 // Items g0 .. g0+n-1: with pairs == NULL the pair counts into n_pairs[g],
 // else the pairs into pairs[offsets[g] - base ..].
-static int launch_flank_paths(const slm_params& p, uint32_t g0, uint32_t n, const float2* seeds,
-                               const uint8_t* stop, const float2* uv, u64* n_pairs, const u64* offsets, u64 base,
-                               uint2* pairs, cudaStream_t s) {
-    FlankPathWalk<ContigSink> w{};
-    w.p = p;
-    w.seeds = seeds;
-    w.stop = stop;
-    w.uv = uv;
-    w.n_pairs = n_pairs;
-    w.g0 = g0;
-    w.offsets = offsets;
-    w.base = base;
-    w.pairs = pairs;
-    k_walks<FlankPathWalk<ContigSink>><<<walk_grid(n), 256, 0, s>>>(w, n);
-    SLM_LAUNCHED("k_walks<FlankPathWalk<ContigSink>>");
-    return SLM_OK;
+__global__ void k_flank_paths(const slm_params p, uint32_t g0, uint32_t n, const float2* __restrict__ seeds,
+                              const uint8_t* __restrict__ stop, const float2* __restrict__ uv,
+                              u64* __restrict__ n_pairs, const u64* __restrict__ offsets, u64 base,
+                              uint2* __restrict__ pairs) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint32_t g = g0 + t;
+    ContigSink sink{pairs ? pairs + (offsets[g] - base) : nullptr, 0};
+    const u64 k = flank_walk(p, g, seeds, stop, uv, sink);
+    if (!pairs) n_pairs[g] = k;
 }
 
 // Items 0 .. n-1 in one pass: each path into linked blocks from the pool
 // (head block heads[g], NO_BLOCK for an empty path), its count into
 // n_pairs[g]; pool_ctr[0] counts the blocks taken, pool_ctr[1] is set when
 // the pool ran out (the counts are still exact).
-static int launch_flank_paths_linked(const slm_params& p, uint32_t n, const float2* seeds, const uint8_t* stop,
-                                      const float2* uv, u64* n_pairs, uint32_t* heads, uint2* pool,
-                                      uint32_t cap_blocks, uint32_t* pool_ctr, cudaStream_t s) {
-    FlankPathWalk<LinkedSink> w{};
-    w.p = p;
-    w.seeds = seeds;
-    w.stop = stop;
-    w.uv = uv;
-    w.n_pairs = n_pairs;
-    w.g0 = 0;
-    w.pool = pool;
-    w.cap_blocks = cap_blocks;
-    w.pool_ctr = pool_ctr;
-    w.heads = heads;
-    k_walks<FlankPathWalk<LinkedSink>><<<walk_grid(n), 256, 0, s>>>(w, n);
-    SLM_LAUNCHED("k_walks<FlankPathWalk<LinkedSink>>");
-    return SLM_OK;
+__global__ void k_flank_paths_linked(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
+                                     const uint8_t* __restrict__ stop, const float2* __restrict__ uv,
+                                     u64* __restrict__ n_pairs, uint32_t* __restrict__ heads,
+                                     uint2* __restrict__ pool, uint32_t cap_blocks, uint32_t* pool_ctr) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    heads[g] = NO_BLOCK;
+    LinkedSink sink{pool, pool_ctr, pool_ctr + 1, cap_blocks, NO_BLOCK, 0, heads + g, 0, true};
+    n_pairs[g] = flank_walk(p, g, seeds, stop, uv, sink);
 }
 
 // The label of pixel q as flank item g sees it: item g's own running value if
@@ -1098,7 +1037,7 @@ __global__ void k_flank_round(const slm_params p, uint32_t g0, uint32_t n, uint3
 // owner's flag until it can go on.  The lowest unresolved item taken waits on
 // nothing unresolved, so some lane always advances.  A label is published
 // by a release store of its resolved flag, read with acquire.  The RK walks are traced in parallel
-// beforehand (FlankPathWalk), so only the path scans lie on a chain of waits.
+// beforehand (k_flank_paths), so only the path scans lie on a chain of waits.
 //
 // Every wait is bounded: a lane that polls FLANK_WAIT_LIMIT times in a row
 // sets bit 0 of *status, and every warp stops; the caller then resolves the
@@ -1997,10 +1936,10 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
         SLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_flank_settle<LinkedPath>, 256, 0));
         settle_grid = (unsigned)(num_sms() * (occ > 0 ? occ : 1));
         const u64 cap_blocks = cap_pairs / FLANK_BLOCK;
-        rc = launch_flank_paths_linked(*p, n, F2(seed_point), stop, F2(uv), n_pairs, heads, pairs,
-                                       (uint32_t)(cap_blocks < 0xfffffffeull ? cap_blocks : 0xfffffffeull),
-                                       words + 3, SS);
-        if (rc) return rc;
+        k_flank_paths_linked<<<blocks_for(n, 128), 128, 0, SS>>>(
+            *p, n, F2(seed_point), stop, F2(uv), n_pairs, heads, pairs,
+            (uint32_t)(cap_blocks < 0xfffffffeull ? cap_blocks : 0xfffffffeull), words + 3);
+        SLM_LAUNCHED("k_flank_paths_linked");
         counted = true;
         uint32_t ran_out = 0;
         SLM_CUDA(cudaMemcpyAsync(&ran_out, words + 4, sizeof(uint32_t), cudaMemcpyDeviceToHost, SS));
@@ -2025,8 +1964,9 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
     //    item reads only initial labels and the final labels of lower-index
     //    owners, which earlier chunks have resolved.
     if (!counted) {
-        rc = launch_flank_paths(*p, 0u, n, F2(seed_point), stop, F2(uv), n_pairs, nullptr, 0ull, nullptr, SS);
-        if (rc) return rc;
+        k_flank_paths<<<blocks_for(n, 128), 128, 0, SS>>>(*p, 0u, n, F2(seed_point), stop, F2(uv), n_pairs,
+                                                         nullptr, 0ull, nullptr);
+        SLM_LAUNCHED("k_flank_paths");
     }
     rc = exclusive_scan(n_pairs, n, offsets, scan_scratch, SS);
     if (rc) return rc;
@@ -2066,8 +2006,9 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
             u64 base = 0;
             SLM_CUDA(cudaMemcpyAsync(&base, offsets + a, sizeof(u64), cudaMemcpyDeviceToHost, SS));
             SLM_CUDA(cudaStreamSynchronize(SS));
-            rc = launch_flank_paths(*p, a, m, F2(seed_point), stop, F2(uv), nullptr, offsets, base, pairs, SS);
-            if (rc) return rc;
+            k_flank_paths<<<blocks_for(m, 128), 128, 0, SS>>>(*p, a, m, F2(seed_point), stop, F2(uv), nullptr,
+                                                             offsets, base, pairs);
+            SLM_LAUNCHED("k_flank_paths");
             SLM_CUDA(cudaMemsetAsync(words + 1, 0, sizeof(uint32_t), SS));
             k_flank_settle<ContigPath><<<grid, 256, 0, SS>>>(*p, a, m, side, offsets, base, nullptr, nullptr,
                                                              pairs, hpix, stop, mapping, pix, label, resolved,
@@ -2089,8 +2030,9 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
         u64 base = 0;
         SLM_CUDA(cudaMemcpyAsync(&base, offsets + a, sizeof(u64), cudaMemcpyDeviceToHost, SS));
         SLM_CUDA(cudaStreamSynchronize(SS));
-        rc = launch_flank_paths(*p, a, m, F2(seed_point), stop, F2(uv), nullptr, offsets, base, pairs, SS);
-        if (rc) return rc;
+        k_flank_paths<<<blocks_for(m, 128), 128, 0, SS>>>(*p, a, m, F2(seed_point), stop, F2(uv), nullptr,
+                                                         offsets, base, pairs);
+        SLM_LAUNCHED("k_flank_paths");
         uint32_t done = 0;
         for (uint32_t r0 = round; done < m; ++round) {
             if (round - r0 > m + 1) {
