@@ -501,6 +501,136 @@ __global__ void k_count_replay(const slm_params p, uint32_t n, const float2* __r
 }
 
 
+// The same replay with one warp: runs of plain events (up to 32) are
+// decided together.  Event i of a run takes counter c + i + 1; the count it
+// compares with is the one an earlier event of the run wrote to the same
+// pixel (c + j + 1, always lower) or else the count loaded before the run,
+// so the first stopping event is a ballot.  Flags (an idempotent update),
+// links (the last writer per pixel wins: the highest lane of a match group
+// writes) and counts are then written in parallel, in the order the single
+// thread would leave them.  Repeat records are replayed by lane 0 as above.
+// __syncwarp orders each run's writes before the next run's loads.
+__global__ void __launch_bounds__(32) k_count_replay_warp(const slm_params p, uint32_t n,
+                                                          const float2* __restrict__ seeds,
+                                                          const u64* __restrict__ offsets,
+                                                          const uint32_t* __restrict__ events,
+                                                          const uint32_t* __restrict__ tail_idx, uint32_t* mapping,
+                                                          uint32_t* count, uint32_t* link) {
+    if (blockIdx.x != 0) return;
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x;
+    const uint32_t dummy = 0xFFFFFFE0u + lane;  // matches no pixel (nxy_padded < 2^32 - 32)
+    __shared__ uint32_t ring[CNT_PMAX];
+    for (uint32_t g = 0; g < n; ++g) {
+        const uint32_t head = pixel_of(seed_vec(seeds, g), p);
+        uint32_t counter = 1, prev = head, last = tail_idx[g], nd = 0;
+        if (lane == 0) count[head] = counter;
+        counter++;
+        bool stopped = false;
+        u64 k = offsets[g];
+        const u64 k_end = offsets[g + 1];
+        __syncwarp();
+        while (k < k_end && !stopped) {
+            const uint32_t wd0 = events[k];
+            if (wd0 & CNT_REPEAT) {
+                // a repeat record, by lane 0 as the single-thread replay does
+                if (lane == 0) {
+                    uint32_t pat_ring[CNT_PMAX];
+                    const uint32_t* pat;
+                    uint32_t P, reps;
+                    if ((wd0 & CNT_KIND) == CNT_PERIOD) {
+                        P = wd0 & ~CNT_KIND;
+                        pat = events + k + 1;
+                        k += P;
+                        reps = events[++k];
+                    } else {
+                        P = wd0 & ~CNT_REPEAT;
+                        reps = events[++k];
+                        for (uint32_t t = 0; t < P; ++t) pat_ring[t] = ring[(nd - P + t) % CNT_PMAX];
+                        pat = pat_ring;
+                    }
+                    ++k;
+                    const uint32_t lap = reps < P ? reps : P;
+                    for (uint32_t t = 0; t < lap; ++t) {
+                        const uint32_t e = pat[t];
+                        if (!count_event(p, e, counter, prev, mapping, count, link)) {
+                            last = e;
+                            stopped = true;
+                            break;
+                        }
+                        ring[nd % CNT_PMAX] = e;
+                        nd++;
+                    }
+                    const uint32_t r = reps - lap;
+                    if (!stopped && r > 0) {
+                        const uint32_t c0 = counter;
+                        const uint32_t start = r > P ? r - P : 0u;
+                        prev = pat[(start + P - 1) % P];
+                        for (uint32_t i = start; i < r; ++i) {
+                            const uint32_t e = pat[i % P];
+                            link[prev] = e;
+                            count[e] = c0 + 1 + i;
+                            prev = e;
+                            ring[nd % CNT_PMAX] = e;
+                            nd++;
+                        }
+                        counter = c0 + r;
+                    }
+                }
+                counter = __shfl_sync(FULL, counter, 0);
+                prev = __shfl_sync(FULL, prev, 0);
+                last = __shfl_sync(FULL, last, 0);
+                nd = __shfl_sync(FULL, nd, 0);
+                k = __shfl_sync(FULL, k, 0);
+                stopped = __shfl_sync(FULL, stopped ? 1 : 0, 0) != 0;
+                __syncwarp();
+                continue;
+            }
+            // a run of plain events: the prefix of events[k ..] up to a record
+            uint32_t e = dummy;
+            bool plain = false;
+            if (k + lane < k_end) {
+                const uint32_t w = events[k + lane];
+                plain = (w & CNT_REPEAT) == 0u;
+                if (plain) e = w;
+            }
+            const unsigned pm = __ballot_sync(FULL, plain);
+            const uint32_t m = (~pm == 0u) ? 32u : (uint32_t)(__ffs(~pm) - 1);
+            const bool in = lane < m;
+            if (!in) e = dummy;
+            const uint32_t c_loaded = in ? count[e] : 0u;
+            const unsigned same = __match_any_sync(FULL, e);
+            const unsigned earlier = same & ((1u << lane) - 1u);
+            const uint32_t mine = counter + lane + 1u;
+            const uint32_t seen = earlier ? counter + (uint32_t)(31 - __clz(earlier)) + 1u : c_loaded;
+            const unsigned stops = __ballot_sync(FULL, in && mine < seen);
+            const uint32_t s_at = stops ? (uint32_t)(__ffs(stops) - 1) : m;
+            const uint32_t n_proc = stops ? s_at + 1u : m;  // flags and links
+            const uint32_t n_pass = s_at;                   // counts, prev, ring
+            uint32_t prev_i = __shfl_up_sync(FULL, e, 1);
+            if (lane == 0) prev_i = prev;
+            if (lane < n_proc) mapping[e] = (mapping[e] & ~p.is_channelhead) | p.is_thinchannel;
+            const unsigned lm = __match_any_sync(FULL, lane < n_proc ? prev_i : dummy);
+            if (lane < n_proc && (uint32_t)(31 - __clz(lm)) == lane) link[prev_i] = e;
+            const unsigned cm = __match_any_sync(FULL, lane < n_pass ? e : dummy);
+            if (lane < n_pass && (uint32_t)(31 - __clz(cm)) == lane) count[e] = mine;
+            if (lane < n_pass && lane + CNT_PMAX >= n_pass) ring[(nd + lane) % CNT_PMAX] = e;
+            const uint32_t e_last_pass = __shfl_sync(FULL, e, n_pass > 0 ? n_pass - 1 : 0);
+            if (n_pass > 0) prev = e_last_pass;
+            nd += n_pass;
+            counter += n_pass;
+            if (stops) {
+                last = __shfl_sync(FULL, e, s_at);
+                stopped = true;
+            }
+            k += n_proc;
+            __syncwarp();
+        }
+        if (lane == 0) link[prev] = last;
+        __syncwarp();
+    }
+}
+
 // ------------------------------------------------------------------ label
 __global__ void k_label_confluences(const slm_params p, uint32_t n, const float2* __restrict__ seeds,
                                     const uint8_t* __restrict__ mask, const float* __restrict__ slt,
@@ -1730,8 +1860,9 @@ int slm_count_downchannels(const slm_params* p, uint32_t n, const float* seed_po
     k_count_paths<<<blocks_for(n, 128), 128, 0, SS>>>(*p, n, F2(seed_point), mask, F2(uv), nullptr,
                                                      offsets, events, tails);
     SLM_LAUNCHED("k_count_paths");
-    k_count_replay<<<1, 1, 0, SS>>>(*p, n, F2(seed_point), offsets, events, tails, mapping, count, link);
-    SLM_LAUNCHED("k_count_replay");
+    SLM_REQUIRE(p->nxy_padded < 0xFFFFFFE0u, "grid too large for the count replay");
+    k_count_replay_warp<<<1, 32, 0, SS>>>(*p, n, F2(seed_point), offsets, events, tails, mapping, count, link);
+    SLM_LAUNCHED("k_count_replay_warp");
     return SLM_OK;
 }
 
