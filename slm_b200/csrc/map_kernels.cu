@@ -1254,14 +1254,39 @@ __device__ int settle_scan(SettleLane<P>& w, uint32_t side, const slm_params& p,
     // one pair of the walk's label scan: 0 go on, 1 the walk stops, 2 wait
     // (stop[q]: mask or thin channel at q; when the compute pixel is the
     // current one its label is the one just read)
+    // The stop byte and both pixels' (owner, initial label) words are loaded
+    // together; each label is then settled as settle_read does.
     auto scan = [&](uint2 e) -> int {
-        if (stop[w.at]) return 1;
-        if (!settle_read(w.at, w.g, w.h, w.lab_h, pix, label, resolved, v, w.wait_o)) return 2;
+        const uint32_t a = w.at, c = e.x;
+        const bool own_a = a == w.h, own_c = c == w.h, same = c == a;
+        const uint8_t st_a = stop[a];
+        const uint2 oa = own_a ? make_uint2(NO_OWNER, 0u) : pix[a];
+        const uint2 oc = (own_c || same) ? make_uint2(NO_OWNER, 0u) : pix[c];
+        if (st_a) return 1;
+        if (own_a) {
+            v = w.lab_h;
+        } else if (oa.x == NO_OWNER || oa.x > w.g) {
+            v = oa.y;
+        } else if (load_acquire(resolved + oa.x) == 0u) {
+            w.wait_o = oa.x;
+            return 2;
+        } else {
+            v = ((volatile const uint32_t*)label)[a];
+        }
         const bool flank_ok = side ? (v & lfa) != 0u : ((~v) & lfa) != 0u;
         if (!flank_ok) return 1;
-        if (e.x != w.at &&
-            !settle_read(e.x, w.g, w.h, w.lab_h, pix, label, resolved, v, w.wait_o))
-            return 2;
+        if (!same) {
+            if (own_c) {
+                v = w.lab_h;
+            } else if (oc.x == NO_OWNER || oc.x > w.g) {
+                v = oc.y;
+            } else if (load_acquire(resolved + oc.x) == 0u) {
+                w.wait_o = oc.x;
+                return 2;
+            } else {
+                v = ((volatile const uint32_t*)label)[c];
+            }
+        }
         if ((w.lab_h & ~lfa) != (v & ~lfa)) w.lab_h = v;
         w.at = e.y;
         return 0;
