@@ -926,7 +926,6 @@ struct ContigSink {
         if (out) out[k] = e;
         ++k;
     }
-    __device__ void flush() {}
 };
 
 struct LinkedSink {
@@ -937,14 +936,6 @@ struct LinkedSink {
     uint32_t* head;
     u64 k;
     bool ok;
-    // entries (f & ~3) .. f - 1 of the current block, stored four at a time
-    // (two 16-byte stores of a 32-byte aligned group)
-    uint2 b0, b1, b2, b3;
-    __device__ void store_group(uint32_t at) {
-        uint4* q = reinterpret_cast<uint4*>(pool + (u64)cur * FLANK_BLOCK + at);
-        q[0] = make_uint4(b0.x, b0.y, b1.x, b1.y);
-        q[1] = make_uint4(b2.x, b2.y, b3.x, b3.y);
-    }
     __device__ void put(uint2 e) {
         ++k;
         if (!ok) return;
@@ -955,31 +946,12 @@ struct LinkedSink {
                 atomicOr(overflow, 1u);
                 return;
             }
-            if (cur == NO_BLOCK) {
-                *head = b;
-            } else {  // the block's last group: its last three pairs and the link
-                b3 = make_uint2(b, 0u);
-                store_group(FLANK_BLOCK - 4);
-            }
+            if (cur == NO_BLOCK) *head = b;
+            else pool[(u64)cur * FLANK_BLOCK + (FLANK_BLOCK - 1)] = make_uint2(b, 0u);
             cur = b;
             f = 0;
         }
-        switch (f & 3u) {
-            case 0: b0 = e; break;
-            case 1: b1 = e; break;
-            case 2: b2 = e; break;
-            default: b3 = e; break;
-        }
-        if ((++f & 3u) == 0u) store_group(f - 4);
-    }
-    // the entries still held, after the walk's last pair
-    __device__ void flush() {
-        if (!ok || cur == NO_BLOCK) return;
-        const uint32_t r = f & 3u;
-        uint2* q = pool + (u64)cur * FLANK_BLOCK + (f - r);
-        if (r > 0) q[0] = b0;
-        if (r > 1) q[1] = b1;
-        if (r > 2) q[2] = b2;
+        pool[(u64)cur * FLANK_BLOCK + f++] = e;
     }
 };
 
@@ -1081,9 +1053,8 @@ __global__ void k_flank_paths_linked(const slm_params p, uint32_t n, const float
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n) return;
     heads[g] = NO_BLOCK;
-    LinkedSink sink{pool, pool_ctr, pool_ctr + 1, cap_blocks, NO_BLOCK, 0, heads + g, 0, true, {}, {}, {}, {}};
+    LinkedSink sink{pool, pool_ctr, pool_ctr + 1, cap_blocks, NO_BLOCK, 0, heads + g, 0, true};
     n_pairs[g] = flank_walk(p, g, seeds, stop, uv, sink);
-    sink.flush();
 }
 
 // The label of pixel q as flank item g sees it: item g's own running value if
@@ -2055,7 +2026,7 @@ size_t slm_fix_flanks_workspace(uint32_t n_seeds, uint32_t nxy_padded, uint64_t 
     return (size_t)(2 * (size_t)n_seeds + 1) * sizeof(u64) + (size_t)n_seeds * 3 * sizeof(uint32_t)
          + (size_t)nxy_padded * 2 * sizeof(uint32_t) + 8 * sizeof(uint32_t) + 256
          + scan_scratch_words(n_seeds) * sizeof(u64) + ((size_t)nxy_padded + 16)
-         + ((size_t)nxy_padded * sizeof(uint2) + 48) + (size_t)n_pairs * sizeof(uint2);
+         + ((size_t)nxy_padded * sizeof(uint2) + 16) + (size_t)n_pairs * sizeof(uint2);
 }
 
 // restore the labels and flags before the rounds start over
@@ -2093,9 +2064,7 @@ static int fix_flanks(const slm_params* p, uint32_t n, const float* seed_point, 
     pa = reinterpret_cast<uintptr_t>(stop + nxy);
     pa = (pa + 15) & ~(uintptr_t)15;
     uint2* pix = reinterpret_cast<uint2*>(pa);
-    pa = reinterpret_cast<uintptr_t>(pix + nxy);
-    pa = (pa + 31) & ~(uintptr_t)31;  // the linked store writes 32-byte groups
-    uint2* pairs = reinterpret_cast<uint2*>(pa);  // the path store
+    uint2* pairs = pix + nxy;  // the path store
     const u64 cap_pairs = (workspace_bytes - fixed) / sizeof(uint2);
     SLM_CUDA(cudaMemsetAsync(owner, 0xff, (size_t)nxy * sizeof(uint32_t), SS));
     SLM_CUDA(cudaMemsetAsync(resolved, 0, (size_t)n * sizeof(uint32_t), SS));
