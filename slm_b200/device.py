@@ -38,19 +38,25 @@ _COPY_POOL = None
 
 
 def host_copy(src, min_bytes=8 << 20):
-    """A fresh NumPy copy of a host array, split over up to 8 threads when
-    large (np.copyto releases the GIL; the page faults of the new array are
-    taken in parallel too)."""
+    """A fresh C-ordered NumPy copy of a host array (any strides, as
+    ``src.copy()`` gives), split over up to 8 threads when large (np.copyto
+    releases the GIL; the page faults of the new array are taken in parallel
+    too)."""
     global _COPY_POOL
-    src = np.ascontiguousarray(src)
-    if src.nbytes < min_bytes:
+    src = np.asarray(src)
+    if src.nbytes < min_bytes or src.ndim == 0:
         return src.copy()
     if _COPY_POOL is None:
         from concurrent.futures import ThreadPoolExecutor
         _COPY_POOL = ThreadPoolExecutor(max(1, min(8, os.cpu_count() or 1)))
-    dst = np.empty_like(src)
-    f, g = src.reshape(-1), dst.reshape(-1)
-    n, k = f.size, _COPY_POOL._max_workers
+    dst = np.empty(src.shape, dtype=src.dtype)
+    k = _COPY_POOL._max_workers
+    if src.flags.c_contiguous:
+        f, g = src.reshape(-1), dst.reshape(-1)
+        n = f.size
+    else:  # rows of a strided view
+        f, g = src, dst
+        n = src.shape[0]
     list(_COPY_POOL.map(lambda i: np.copyto(g[i * n // k:(i + 1) * n // k], f[i * n // k:(i + 1) * n // k]),
                         range(k)))
     return dst

@@ -75,15 +75,17 @@ class Data:
         else:
             bounds_grid = np.index_exp[:, :]
             bounds_slx = np.index_exp[:, :, :]
-        self.mask_array = mask_array[bounds_grid].copy()
+        # copies, as the reference takes them (large ones on several threads)
+        from .device import host_copy
+        self.mask_array = host_copy(mask_array[bounds_grid])
         if mapping_array is not None:
-            self.mapping_array = mapping_array[bounds_grid].copy()
+            self.mapping_array = host_copy(mapping_array[bounds_grid])
         else:
             self.mapping_array = None
-        self.uv_array = uv_array[bounds_slx].copy() if uv_array is not None else None
-        self.sla_array = sla_array[bounds_slx].copy() if sla_array is not None else None
-        self.slc_array = slc_array[bounds_slx].copy() if slc_array is not None else None
-        self.slt_array = slt_array[bounds_slx].copy() if slt_array is not None else None
+        self.uv_array = host_copy(uv_array[bounds_slx]) if uv_array is not None else None
+        self.sla_array = host_copy(sla_array[bounds_slx]) if sla_array is not None else None
+        self.slc_array = host_copy(slc_array[bounds_slx]) if slc_array is not None else None
+        self.slt_array = host_copy(slt_array[bounds_slx]) if slt_array is not None else None
         self.traj_stats_df = traj_stats_df
         self.bounds_grid = bounds_grid
         self.bounds_slx = bounds_slx
@@ -96,7 +98,7 @@ class Data:
         self.traj_length_array = None
         self.subsegment_label_array = None
         self.subsegment_hsl_array = None
-        self.hsl_array = hsl_array[bounds_slx].copy() if hsl_array is not None else None
+        self.hsl_array = host_copy(hsl_array[bounds_slx]) if hsl_array is not None else None
 
 
 class Info:
