@@ -37,11 +37,13 @@ def to_device(array, device, dtype=None):
 _COPY_POOL = None
 
 
-def host_copy(src, min_bytes=8 << 20):
+def host_copy(src, min_bytes=8 << 20, pinned=False):
     """A fresh C-ordered NumPy copy of a host array (any strides, as
     ``src.copy()`` gives), split over up to 8 threads when large (np.copyto
     releases the GIL; the page faults of the new array are taken in parallel
-    too)."""
+    too).  ``pinned``: a large copy goes to page-locked memory when a GPU is
+    present (torch's caching host allocator reuses it once the array is
+    freed), so a later upload of it runs at DMA speed."""
     global _COPY_POOL
     src = np.asarray(src)
     if src.nbytes < min_bytes or src.ndim == 0:
@@ -49,7 +51,11 @@ def host_copy(src, min_bytes=8 << 20):
     if _COPY_POOL is None:
         from concurrent.futures import ThreadPoolExecutor
         _COPY_POOL = ThreadPoolExecutor(max(1, min(8, os.cpu_count() or 1)))
-    dst = np.empty(src.shape, dtype=src.dtype)
+    dst = None
+    if pinned and torch.cuda.is_available() and src.dtype in _PINNED_DTYPES:
+        dst = pinned_empty(src.shape, src.dtype)
+    if dst is None:
+        dst = np.empty(src.shape, dtype=src.dtype)
     k = _COPY_POOL._max_workers
     if src.flags.c_contiguous:
         f, g = src.reshape(-1), dst.reshape(-1)
@@ -121,13 +127,15 @@ def download(tensors, slot):
     return [host_copy(st.numpy()) for st in stages]
 
 
+_PINNED_DTYPES = {np.dtype(np.float32): torch.float32, np.dtype(np.uint8): torch.uint8,
+                  np.dtype(np.uint32): torch.uint32, np.dtype(np.uint16): torch.uint16,
+                  np.dtype(np.int8): torch.int8, np.dtype(np.uint64): torch.uint64,
+                  np.dtype(np.bool_): torch.bool}
+
+
 def pinned_empty(shape, dtype):
     """A NumPy array backed by page-locked host memory (fast DMA both ways)."""
-    tdt = {np.dtype(np.float32): torch.float32, np.dtype(np.uint8): torch.uint8,
-           np.dtype(np.uint32): torch.uint32, np.dtype(np.uint16): torch.uint16,
-           np.dtype(np.int8): torch.int8, np.dtype(np.uint64): torch.uint64,
-           np.dtype(np.bool_): torch.bool}[np.dtype(dtype)]
-    return torch.empty(shape, dtype=tdt, pin_memory=True).numpy()
+    return torch.empty(shape, dtype=_PINNED_DTYPES[np.dtype(dtype)], pin_memory=True).numpy()
 
 
 def low32(t_u64):

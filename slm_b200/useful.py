@@ -75,14 +75,15 @@ class Data:
         else:
             bounds_grid = np.index_exp[:, :]
             bounds_slx = np.index_exp[:, :, :]
-        # copies, as the reference takes them (large ones on several threads)
+        # copies, as the reference takes them (large ones on several threads;
+        # the grids the tracer uploads into page-locked memory)
         from .device import host_copy
-        self.mask_array = host_copy(mask_array[bounds_grid])
+        self.mask_array = host_copy(mask_array[bounds_grid], pinned=True)
         if mapping_array is not None:
             self.mapping_array = host_copy(mapping_array[bounds_grid])
         else:
             self.mapping_array = None
-        self.uv_array = host_copy(uv_array[bounds_slx]) if uv_array is not None else None
+        self.uv_array = host_copy(uv_array[bounds_slx], pinned=True) if uv_array is not None else None
         self.sla_array = host_copy(sla_array[bounds_slx]) if sla_array is not None else None
         self.slc_array = host_copy(slc_array[bounds_slx]) if slc_array is not None else None
         self.slt_array = host_copy(slt_array[bounds_slx]) if slt_array is not None else None
