@@ -192,13 +192,10 @@ int slm_integrate_fields_batched(const slm_params* p, const slm_launch* launch, 
  * counters) lives in a static device array of SLM_NOALLOC_SCRATCH_WORDS uint64
  * words inside this library, which every GPU that loads the library holds
  * until the process exits.  The caller still passes every input and output.
- * The first call on each device looks up the array's device address
- * (cudaGetSymbolAddress, with that device current); make that first call
- * before any stream capture.  The address is kept per device index and
- * belongs to the device's primary context, the one the CUDA runtime uses:
- * call this entry point only with that context current, and not after a
- * cudaDeviceReset in the same process (the kept address would then point
- * into a context that no longer exists).  All calls share the one array and each call
+ * Every call looks up the array's device address in the current context
+ * (cudaGetSymbolAddress), so a cudaDeviceReset or a change of context between
+ * calls is safe; the first call on a device may load the module there, so
+ * make it before any stream capture.  All calls share the one array and each call
  * clears the words it uses: calls that overlap on the GPU (several streams or
  * host threads) race on it, so the caller must serialise them.  The step and
  * trajectory counters are not returned.  Returns SLM_ERR_CAPACITY if the

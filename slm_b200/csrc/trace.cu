@@ -14,11 +14,9 @@
 // a pixel several times in a row) and adds the merged count and length sum
 // with one 64-bit atomic each when it moves to another pixel.
 #include <cstring>
-#include <mutex>
 #include "capi_util.cuh"
 #include "trace_common.cuh"
 
-#define SLM_MAX_DEVICES 64
 
 static_assert(sizeof(slm_tile) == 40, "slm_tile layout is part of the ABI");
 
@@ -832,27 +830,22 @@ namespace slm {
 
 static __device__ __align__(256) unsigned long long g_noalloc_scratch[SLM_NOALLOC_SCRATCH_WORDS];
 
-// Device address of g_noalloc_scratch per device.  In host code the array's
-// name is only a host-side stand-in, so the address comes from
-// cudaGetSymbolAddress, called once per device with that device current.
-static std::mutex g_noalloc_mutex;
-static u64* g_noalloc_addr[SLM_MAX_DEVICES] = {};
-
+// Device address of g_noalloc_scratch in the current context.  In host code
+// the array's name is only a host-side stand-in, so the address comes from
+// cudaGetSymbolAddress.  It is looked up on every call (a cheap query) rather
+// than cached: an address belongs to the context the module was loaded in, and
+// a cached one would go stale after cudaDeviceReset or in a caller's own
+// context.
 static int noalloc_scratch(u64** out) {
-    int dev = 0;
-    SLM_CUDA(cudaGetDevice(&dev));
-    SLM_REQUIRE(dev >= 0 && dev < SLM_MAX_DEVICES, "device %d beyond %d", dev, SLM_MAX_DEVICES);
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (g_noalloc_addr[dev] == nullptr) {
-        void* ptr = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-        if (e != cudaSuccess) {
-            set_error("cudaGetSymbolAddress(scratch) failed on device %d: %s", dev, cudaGetErrorString(e));
-            return SLM_ERR_CUDA;
-        }
-        g_noalloc_addr[dev] = static_cast<u64*>(ptr);
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+        int dev = -1;
+        cudaGetDevice(&dev);
+        set_error("cudaGetSymbolAddress(scratch) failed on device %d: %s", dev, cudaGetErrorString(e));
+        return SLM_ERR_CUDA;
     }
-    *out = g_noalloc_addr[dev];
+    *out = static_cast<u64*>(ptr);
     return SLM_OK;
 }
 

@@ -114,9 +114,19 @@ def upload(array, device, slot, dtype=None):
     return st.to(device, non_blocking=True)
 
 
-def download(tensors, slot):
+def download(tensors, slot, pinned=False):
     """Fresh NumPy copies of device tensors: all go to pinned staging buffers
-    by DMA, one synchronisation, then out of them on several threads."""
+    by DMA, one synchronisation, then out of them on several threads.  With
+    ``pinned`` the DMA writes straight into fresh page-locked arrays that the
+    caller keeps (torch's caching host allocator reuses their memory once
+    they are freed), and no host copy follows."""
+    if pinned and all(t.dtype in _PINNED_DTYPES.values() for t in tensors):
+        outs = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for t in tensors]
+        for o, t in zip(outs, tensors):
+            o.copy_(t, non_blocking=True)
+        if outs:
+            torch.cuda.current_stream(tensors[0].device).synchronize()
+        return [o.numpy() for o in outs]
     stages = []
     for i, t in enumerate(tensors):
         st = pinned_staging((slot, i), t.shape, t.dtype)
@@ -127,8 +137,8 @@ def download(tensors, slot):
     return [host_copy(st.numpy()) for st in stages]
 
 
-_PINNED_DTYPES = {np.dtype(np.float32): torch.float32, np.dtype(np.uint8): torch.uint8,
-                  np.dtype(np.uint32): torch.uint32, np.dtype(np.uint16): torch.uint16,
+_PINNED_DTYPES = {np.dtype(np.float32): torch.float32, np.dtype(np.float64): torch.float64,
+                  np.dtype(np.uint8): torch.uint8, np.dtype(np.uint32): torch.uint32, np.dtype(np.uint16): torch.uint16,
                   np.dtype(np.int8): torch.int8, np.dtype(np.uint64): torch.uint64,
                   np.dtype(np.bool_): torch.bool}
 

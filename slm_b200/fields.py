@@ -29,7 +29,7 @@ import numpy as np
 import torch
 
 from . import kernels
-from .device import cuda_device, host_copy, low32, pinned_staging, to_device, traced
+from .device import cuda_device, download, host_copy, low32, pinned_staging, to_device, traced
 from .distributed import allreduce_counts, shard_queue, shard_queue_params, sharded_field_pass
 from .params import kernel_params
 from .useful import create_seeds_device, create_seeds_device_state, vprint
@@ -61,16 +61,20 @@ _ROWS_POOL = None
 _SEEDS_POOL = None
 
 
-def _rows_to_host_behind(t, dev):
+def _rows_to_host_behind(t, dev, after=None):
     """A future of a fresh NumPy copy of device tensor ``t``: the copy to
-    pinned memory runs on a side stream behind the work queued so far, the copy
-    out of it on a worker thread, so both overlap what the caller queues next."""
+    pinned memory runs on a side stream behind the work queued so far (or
+    behind the CUDA event ``after`` alone), the copy out of it on a worker
+    thread, so both overlap what the caller queues next."""
     global _ROWS_POOL
     if _ROWS_POOL is None:
         from concurrent.futures import ThreadPoolExecutor
         _ROWS_POOL = ThreadPoolExecutor(1)
     side = torch.cuda.Stream(dev)
-    side.wait_stream(torch.cuda.current_stream(dev))
+    if after is None:
+        side.wait_stream(torch.cuda.current_stream(dev))
+    else:
+        side.wait_event(after)
     stage = _staging("seed rows", t)
     with torch.cuda.stream(side):
         stage.copy_(t, non_blocking=True)
@@ -140,8 +144,7 @@ class Fields:
                     acc = host_seeds = None
                     if trace:
                         info.n_seed_points, info.n_padded_seed_points = n, npad
-                        host_seeds = _rows_to_host_behind(seeds_d, dev)
-                        acc = self._trace(seeds_d, mask_d)
+                        acc, host_seeds = self._trace_and_rows(seeds_d, mask_d)
                     done = torch.cuda.Event()
                     done.record(side)
             return mask_d, seeds_d, n, npad, state, done, acc, host_seeds
@@ -189,11 +192,22 @@ class Fields:
                     mask_array, info.pad_width, info.n_work_items, dev, do_shuffle=info.do_shuffle,
                     rng_seed=info.shuffle_rng_seed, verbose=self.verbose, mask_d=mask_d)
             if acc is None:
-                host_seeds = _rows_to_host_behind(seeds_d, dev)
-                acc = self._trace(seeds_d, mask_d)
+                acc, host_seeds = self._trace_and_rows(seeds_d, mask_d)
             self._finish(acc, float(dds / pixel_size), float(uds / pixel_size), nxp, nyp)
             self.data.seed_point_array = host_seeds.result()
         vprint(self.verbose, "...done")
+
+    def _trace_and_rows(self, seeds_d, mask_d):
+        """``_trace`` of the seed list ``seeds_d``, with its copy to the host
+        (a future of it) queued once the first pass is: the copy runs beside
+        the passes and its host-side call does not delay their launch."""
+        dev = self.device
+        seeds_ready = torch.cuda.Event()
+        seeds_ready.record(torch.cuda.current_stream(dev))
+        rows = []
+        acc = self._trace(seeds_d, mask_d, on_launch=lambda: rows.append(
+            _rows_to_host_behind(seeds_d, dev, after=seeds_ready)))
+        return acc, rows[0]
 
     @traced("slm.Fields.finish")
     def _finish(self, acc, scale_down, scale_up, nxp, nyp):
@@ -217,20 +231,15 @@ class Fields:
             ptr(acc), nxy, int(info.subpixel_seed_point_density), scale_down, scale_up,
             1 if self.exact else 0, ptr(table_d), n_tab, ptr(slc), ptr(slt), ptr(sla),
             kernels._stream(None)))
-        # through pinned staging buffers (reused per shape), then into arrays
-        # the caller owns
-        out = []
-        for slot, t in enumerate((slc, slt, sla)):
-            st = _staging(slot, t)
-            st.copy_(t, non_blocking=True)
-            out.append(st)
-        torch.cuda.current_stream(dev).synchronize()
-        self.data.slc_array, self.data.slt_array, self.data.sla_array = (host_copy(o.numpy()) for o in out)
+        # by DMA straight into page-locked arrays the caller owns
+        self.data.slc_array, self.data.slt_array, self.data.sla_array = download(
+            (slc, slt, sla), "fields", pinned=True)
 
     @traced("slm.Fields.trace")
-    def _trace(self, seeds_d=None, mask_d=None):
+    def _trace(self, seeds_d=None, mask_d=None, on_launch=None):
         """Both passes on the device; returns the uint64 accumulators [2, 2, nxy].
-        The seeds and mask come from ``data`` unless given on the device."""
+        The seeds and mask come from ``data`` unless given on the device;
+        ``on_launch`` is called once the first pass is queued."""
         info = self.info
         dev = self.device
         mask_array = self.data.mask_array
@@ -264,12 +273,16 @@ class Fields:
                     prm = [shard_queue_params(p, queue) for p in prm]
                 kernels.integrate_fields_pair(prm[0], prm[1], seeds_d, mask_d, uv_d, acc[:, 0], acc[:, 1], work,
                                               integrator=self.integrator, order=queue)
+                if on_launch is not None:
+                    on_launch()
                 counts = work[1:4].view(torch.int64).clone()
                 if pg is not None:
                     allreduce_counts(acc, counts, group=pg)
                 counts = counts.cpu().tolist()
                 self.n_steps[0], self.n_steps[1] = counts[0] - counts[2], counts[2]
                 return acc
+            if on_launch is not None:
+                on_launch()
             for downup_idx, downup_sign in ((0, +1.0), (1, -1.0)):
                 info.downup_sign = downup_sign
                 prm = kernel_params(info, "INTEGRATE_FIELDS", downup_sign)

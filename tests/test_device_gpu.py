@@ -1,5 +1,6 @@
 """Host <-> device transfer helpers on the GPU: the pinned-staging upload of
-large strided arrays (with a dtype cast) and the batched download."""
+large strided arrays (with a dtype cast), the batched download (through
+staging, or straight into page-locked arrays) and the page-locked host copy."""
 import numpy as np
 import pytest
 import torch
@@ -37,3 +38,20 @@ def test_download_many():
         assert np.array_equal(o, t.cpu().numpy())
     out[1][0] = -5  # fresh copies, not views of the staging buffers
     assert D.download(ts, "test")[1][0] == 0
+
+
+def test_download_pinned_fresh_arrays():
+    ts = [torch.arange(n, dtype=dt, device=DEV) for n, dt in ((9_000_001, torch.float64), (5, torch.float32))]
+    a = D.download(ts, "test", pinned=True)
+    b = D.download(ts, "test", pinned=True)
+    for t, x, y in zip(ts, a, b):
+        assert np.array_equal(x, t.cpu().numpy()) and np.array_equal(y, x)
+        assert torch.from_numpy(x).is_pinned()
+    a[0][0] = -5  # each call's arrays are its own
+    assert b[0][0] == 0
+
+
+def test_host_copy_pinned_strided():
+    a = np.random.default_rng(3).random((3000, 2000, 2)).astype(np.float32)[:, :, 1]
+    c = D.host_copy(a, pinned=True)
+    assert np.array_equal(c, a) and c.flags.c_contiguous and torch.from_numpy(c).is_pinned()
