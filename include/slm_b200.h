@@ -350,6 +350,32 @@ size_t slm_exclusive_scan_u64_scratch(uint32_t n);
 int slm_exclusive_scan_u64(const uint64_t* in, uint32_t n, uint64_t* out, void* scratch, size_t scratch_bytes,
                            void* stream);
 
+/* slm_fmm_lengths -- the fast-marching distances behind pass 2's hillslope
+ * lengths (python/streamlines/mapping.py:841-900, Mapping.fmm_lengths, which
+ * calls scikit-fmm's skfmm.distance per fine subsegment).  One problem per
+ * subsegment[i] (an absolute label value): the window pixels with |label| ==
+ * subsegment[i], grown by one pixel (4-neighbour), are the domain; the
+ * domain's own-label pixels whose flags hold all of thin_bit take phi = -1,
+ * the rest +1; the signed distance from phi's zero contour is marched over
+ * the domain (second-order fast marching when order == 2, first-order when
+ * 1; unit grid, times dx).  Per problem: sum[i] and count[i] of the reached
+ * distances (the reference's mean is sum / count), n_phi[i] (own-label
+ * pixels), n_channel[i] (own-label thin-channel pixels) and status[i]: 0 ok,
+ * 1 no channel pixel (nothing marched), 2 no zero contour, 3 heap full
+ * (internal), 4 box or workspace out of range (the problem is skipped).
+ * box[4i..4i+3] = x0, x1, y0, y1 (inclusive) must hold the domain (the
+ * own-label pixels' box grown by one, clipped to the window); offset[i] is
+ * the problem's first pixel in the workspaces, which hold total pixels:
+ * val_ws [total] (on return the signed distance times dx on reached pixels,
+ * else 0), st_ws [total] (bits 0-1: 2 = reached, 3 = outside the domain;
+ * bit 2: phi < 0), hkey_ws [4 total], hidx_ws [4 total].
+ * label, flags [nx*ny] row-major; every pointer is DEVICE.  Asynchronous. */
+int slm_fmm_lengths(const int32_t* label, const uint32_t* flags, int nx, int ny, uint32_t thin_bit,
+                    const int32_t* subsegment, const int32_t* box, const int64_t* offset, int n, int64_t total,
+                    int order, double dx, double* val_ws, uint8_t* st_ws, double* hkey_ws, int32_t* hidx_ws,
+                    double* sum, int64_t* count, int64_t* n_phi, int64_t* n_channel, int32_t* status,
+                    void* stream);
+
 /* fix_right_flanks / fix_left_flanks (opencl/segment.cl:441-504, 530-594;
  * segment.py:210-232), with the result of the items run in ascending order.
  * The walks are traced in parallel, once, into linked blocks of the path

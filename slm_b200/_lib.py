@@ -98,6 +98,9 @@ SIGNATURES = {
     "slm_exclusive_scan_u64_scratch": (ctypes.c_size_t, [ctypes.c_uint32]),
     "slm_exclusive_scan_u64": (ctypes.c_int, [_P, ctypes.c_uint32, _P, _P, ctypes.c_size_t, _P]),
     "slm_selftest_cvt_i8": (ctypes.c_int, [_P, _P]),
+    "slm_fmm_lengths": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.c_int, _U, _P, _P, _P, ctypes.c_int,
+                                       ctypes.c_int64, ctypes.c_int, ctypes.c_double, _P, _P, _P, _P, _P, _P, _P,
+                                       _P, _P, _P]),
     "slm_create_seeds_device": (ctypes.c_int, [_P, _U, _U, _U, ctypes.c_int, _U, _P, ctypes.c_uint64, _P, _P,
                                                _P, ctypes.c_size_t, _P]),
     "slm_preprocess": (ctypes.c_int, [_P, ctypes.c_int, _U, _U, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),

@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libslm_b200.so")
 SOURCES = ["capi.cu", "trace.cu", "kde.cu", "map_kernels.cu", "scheduler.cu", "map_device.cu", "preprocess.cu",
-           "seeds.cpp", "seeds_device.cu", "gemm_tc.cu"]
+           "seeds.cpp", "seeds_device.cu", "gemm_tc.cu", "fmm.cu"]
 HEADERS = ["trace_common.cuh", "capi_util.cuh", "mt19937.hpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "nvcc")

@@ -39,10 +39,14 @@ How this implementation is organised:
   data selection runs on host copies of the window (the KDE itself runs on
   the GPU).
 
-The hillslope lengths are the ones traced along streamlines, the
-alternative the reference keeps beside its fast-marching measurement
-(skfmm, absent here).  Pass 3 (scikit-image's rank filters, absent) is not
-built.
+The hillslope lengths are measured as the reference's pass 2 measures
+them, by fast marching (``hsl_method="fmm"``, the default): every labelled
+subsegment of the window gets twice the mean eikonal distance of its grown
+region from its thin channel (``slm_b200.fmm``, the CUDA kernel
+``slm_fmm_lengths``), and each subsegment's value is painted on its pixels.
+``hsl_method="traced"`` takes instead the lengths traced along streamlines
+from the midslopes, the alternative the reference keeps beside it.  Pass 3
+(scikit-image's rank filters, absent) is not built.
 """
 from __future__ import annotations
 
@@ -65,6 +69,7 @@ MAPPING_PARAMETERS.update(do_map_channels_segments=True, do_map_hsl=True, midslo
 MAPPING_PARAMETERS.update(pass2_workers=6)
 
 HSL_COLUMNS = ("count", "mean [m]", "stddev [m]")
+FMM_ORDER = 2  # skfmm.distance's default order, which the reference's call takes
 
 
 # ------------------------------------------------------------------ grid helpers
@@ -185,6 +190,14 @@ class WrapperEngine:
         return (ok, torch.from_numpy(data.mapping_array.astype(np.int64)).to(roi.device),
                 torch.from_numpy(np.ascontiguousarray(lab, dtype=np.int32)).to(roi.device))
 
+    def fmm_lengths(self, info, flags, labels, selected, dx, order):
+        """The fast-marching length (int32) of each ``selected`` fine label
+        of the window, through the runner's ``fmm_solver`` when it has one
+        (the oracle's), else the CUDA kernel."""
+        from . import fmm
+        return fmm.fmm_lengths(labels, flags, int(info.is_thinchannel), selected, dx, order,
+                               solver=getattr(self.runner, "fmm_solver", None))
+
     def lengths(self, info, mapping, n):
         """The doubled hillslope lengths of the window's unmasked midslope
         pixels (row-major order), or None when there is none."""
@@ -219,6 +232,11 @@ class DeviceEngine:
         shape = mask.shape
         return (ok, self.dm.mapping.view(shape).to(torch.int64),
                 self.dm.label.view(shape).view(torch.int32).clone())
+
+    def fmm_lengths(self, info, flags, labels, selected, dx, order):
+        from . import fmm
+        with torch.cuda.device(labels.device):
+            return fmm.fmm_lengths(labels, flags, int(info.is_thinchannel), selected, dx, order)
 
     def lengths(self, info, mapping, n):
         self.dm.mapping.copy_(mapping.reshape(-1).to(torch.uint32))
@@ -267,7 +285,7 @@ def length_statistics(fine_labels, lengths, coarse_label):
     formed."""
     import pandas as pd
     fine_labels = np.asarray(fine_labels, dtype=np.int32)
-    lengths = np.asarray(lengths, dtype=np.float32)
+    lengths = np.asarray(lengths)  # float32 traced lengths, int32 fast-marching ones
     keep = fine_labels != 0
     try:
         rows = pd.Series(lengths[keep]).groupby(fine_labels[keep]).agg(["count", "mean", "std"])
@@ -410,19 +428,20 @@ class Mapping:
 
     # ---------------------------------------------------------------- pass 2
     @traced("slm.Mapping.pass2")
-    def pass2(self, hsl_method="traced"):
+    def pass2(self, hsl_method="fmm"):
         """Per coarse subsegment (pass 1's labels, ascending): see the module
-        docstring.  Needs ``pass1`` and an ``analysis``."""
+        docstring.  ``hsl_method``: "fmm" (the reference's measurement) or
+        "traced".  Needs ``pass1`` and an ``analysis``."""
         import pandas as pd
-        if hsl_method != "traced":
-            raise NotImplementedError("hsl_method {!r}: fast marching needs skfmm, which is not available "
-                                      "here; use 'traced'".format(hsl_method))
-        if self.do_measure_hsl_from_ridges:
+        if hsl_method not in ("fmm", "traced"):
+            raise ValueError("hsl_method {!r}: 'fmm' or 'traced'".format(hsl_method))
+        if hsl_method == "traced" and self.do_measure_hsl_from_ridges:
             raise NotImplementedError("traced hillslope lengths start from the midslopes; the reference's "
                                       "traced measurement selects no seeds when measuring from ridges")
         self.print("\n**Pass#2 begin**")
         roi = self._roi
         pad = self.geodata.pad_width
+        pixel_size = float(self.geodata.roi_pixel_size)
         quiet = getattr(self.state, "verbose", False)
         # the job's masks, without pass 1's mask of its coarse subsegments
         self.state.add_active_mask({"merged_coarse": self.merged_coarse_mask_array})
@@ -467,15 +486,27 @@ class Mapping:
             # this pass's channel heads are kept as WAS_CHANNELHEAD
             head = int(info.is_channelhead)
             flags = torch.where((flags & head) == head, flags | int(info.was_channelhead), flags)
-            picked = ((flags & int(info.is_midslope)) > 0) & ~mask_w
-            fine = labels[picked].cpu().numpy()
-            lengths = engine.lengths(info, flags, int(fine.shape[0]))
-            if lengths is None:
-                return None
+            if hsl_method == "fmm":
+                # every subsegment with an unmasked pixel, one length each;
+                # all are painted (no count threshold)
+                fine = torch.unique(labels[~mask_w])
+                fine = fine[fine != 0].cpu().numpy().astype(np.int32)
+                lengths = engine.fmm_lengths(info, flags, labels, fine, pixel_size, FMM_ORDER)
+                if not (lengths > 0).any():
+                    return None
+                min_count = 0
+            else:
+                picked = ((flags & int(info.is_midslope)) > 0) & ~mask_w
+                fine = labels[picked].cpu().numpy()
+                lengths = engine.lengths(info, flags, int(fine.shape[0]))
+                if lengths is None:
+                    return None
+                lengths = np.asarray(lengths, dtype=np.float32)
+                min_count = self.n_hsl_averaging_threshold
             stats = length_statistics(fine, lengths, label)
             if stats is None:
                 return None
-            painted = paint_means(labels, stats, self.n_hsl_averaging_threshold, roi.device)
+            painted = paint_means(labels, stats, min_count, roi.device)
             kept = painted[~torch.isnan(painted)]
             kept = kept[kept >= self.hsl_averaging_threshold].cpu().numpy()
             if len(stats) == 0 or kept.shape[0] == 0:

@@ -267,11 +267,13 @@ def test_mapping_stage_pass1_on_the_gpu():
 
 
 @pytest.mark.gpu
-def test_mapping_stage_pass2_on_the_gpu():
+@pytest.mark.parametrize("hsl_method", ["fmm", "traced"])
+def test_mapping_stage_pass2_on_the_gpu(hsl_method):
     """Passes 1 and 2 with the region's grids on the GPU (device engine: the
-    mapping sequence and the traced lengths with the windows resident there)
-    equal the same passes through the wrappers on the oracle; the channel
-    thresholds come from the device KDE on both sides."""
+    mapping sequence and the fast-marching or traced lengths with the
+    windows resident there) equal the same passes through the wrappers on
+    the oracle; the channel thresholds come from the device KDE on both
+    sides."""
     import types
 
     from mapping_cases import incised_pipeline_case
@@ -307,7 +309,7 @@ def test_mapping_stage_pass2_on_the_gpu():
                     analysis=A.Analysis(state, analysis_params, geodata, None, trace), runner=runner,
                     thin=zhang_suen)
         m.pass1()
-        m.pass2()
+        m.pass2(hsl_method=hsl_method)
         out.append(m)
     gpu, cpu = out
     assert gpu.n_coarse_subsegments == cpu.n_coarse_subsegments > 1
@@ -317,7 +319,8 @@ def test_mapping_stage_pass2_on_the_gpu():
     assert gpu.hsl_stats_df.equals(cpu.hsl_stats_df)
 
 
-def test_mapping_stage_pass2_threads_equal_order():
+@pytest.mark.parametrize("hsl_method", ["fmm", "traced"])
+def test_mapping_stage_pass2_threads_equal_order(hsl_method):
     """Pass 2 with its independent coarse subsegments on six threads and
     streams (the default on the GPU) equals pass 2 run one subsegment after
     another in label order, on a grid with many subsegments."""
@@ -355,7 +358,7 @@ def test_mapping_stage_pass2_threads_equal_order():
         m = Mapping(state, {"mapping": params}, geodata, preprocess, trace,
                     analysis=A.Analysis(state, analysis_params, geodata, None, trace), thin=zhang_suen)
         m.pass1()
-        m.pass2()
+        m.pass2(hsl_method=hsl_method)
         out.append(m)
     seq, par = out
     assert seq.n_coarse_subsegments == par.n_coarse_subsegments > 20

@@ -193,11 +193,10 @@ class ActiveMasks:
         return out
 
 
-def test_pass2_traced_matches_reference(reference_dir, monkeypatch):
-    """Pass 2 with the lengths traced along streamlines, against the
-    reference's pass2 with its fast-marching measurement swapped for its own
-    traced-length methods (the alternative it keeps switched off).  Kernels on
-    the oracle; channel thresholds from the same Analysis on a CPU stand-in KDE."""
+def _pass2_against_reference(reference_dir, monkeypatch, hsl_method):
+    """Runs the reference's pass1 + pass2 and this package's on the same
+    incised case (kernels on the oracle; channel thresholds from the same
+    Analysis on a CPU stand-in KDE); returns (reference, mine)."""
     import pandas as pd
 
     from slm_b200 import analysis as A
@@ -244,13 +243,17 @@ def test_pass2_traced_matches_reference(reference_dir, monkeypatch):
     ref.__dict__.update(state=ref_state, geodata=geodata, preprocess=preprocess, trace=trace, cl_state=None,
                         verbose=False, vprogress=False, vbackup=False, print=lambda *a, **k: None,
                         analysis=A.Analysis(ref_state, analysis_params, geodata, None, trace))
-    ref.select_subsegments = lambda info, data, do_restrict=True: R.Mapping.select_subsegments(ref, info, data)
+    if hsl_method == "traced":
+        ref.select_subsegments = lambda info, data, do_restrict=True: R.Mapping.select_subsegments(ref, info, data)
 
-    def traced(info, data):
-        data.fmm_mean_hsl = 0.0
-        return R.Mapping.measure_hsl_traced(ref, info, data)
-    ref.measure_hsl_fmm = traced
-    ref.remap_hsl = lambda info, data, n_hsl_averaging_threshold=None: R.Mapping.remap_hsl(ref, info, data)
+        def traced(info, data):
+            data.fmm_mean_hsl = 0.0
+            return R.Mapping.measure_hsl_traced(ref, info, data)
+        ref.measure_hsl_fmm = traced
+        ref.remap_hsl = lambda info, data, n_hsl_averaging_threshold=None: R.Mapping.remap_hsl(ref, info, data)
+    else:  # the reference's own fast-marching branch, skfmm's distance from the oracle
+        import eikonal
+        monkeypatch.setattr(R, "skfmm", types.SimpleNamespace(distance=eikonal.distance), raising=False)
     ref.pass1()
     ref.pass2()
 
@@ -259,9 +262,34 @@ def test_pass2_traced_matches_reference(reference_dir, monkeypatch):
                    analysis=A.Analysis(my_state, analysis_params, geodata, None, trace), runner=oracle_runner,
                    thin=zhang_suen)
     mine.pass1()
-    mine.pass2()
+    mine.pass2(hsl_method=hsl_method)
+    return ref, mine
+
+
+def _assert_same_pass2(ref, mine):
     assert mine.n_coarse_subsegments == ref.n_coarse_subsegments > 1
     assert np.array_equal(mine.mapping_array, ref.mapping_array)
     assert np.array_equal(mine.hsl_array, ref.hsl_array) and mine.hsl_array.any()
     assert np.array_equal(mine.hsl_mean_array, ref.hsl_mean_array) and mine.hsl_mean_array.size > 0
     assert mine.hsl_stats_df.equals(ref.hsl_stats_df)
+
+
+def test_pass2_traced_matches_reference(reference_dir, monkeypatch):
+    """Pass 2 with the lengths traced along streamlines, against the
+    reference's pass2 with its fast-marching measurement swapped for its own
+    traced-length methods (the alternative it keeps switched off)."""
+    _assert_same_pass2(*_pass2_against_reference(reference_dir, monkeypatch, "traced"))
+
+
+def test_pass2_fmm_matches_reference(reference_dir, monkeypatch):
+    """Pass 2 as the reference runs it: its own fast-marching branch
+    (select_subsegments without restriction, fmm_lengths, parse_hsl,
+    remap_hsl with no count threshold), skfmm.distance stood in by the
+    oracle's restatement, against this package's default pass 2 with the
+    oracle's solver.  Pins the call site: the grown regions, the channel
+    phi, the ratio test, the doubled mean and its int32 truncation, the
+    painting and the statistics."""
+    ref, mine = _pass2_against_reference(reference_dir, monkeypatch, "fmm")
+    _assert_same_pass2(ref, mine)
+    assert (mine.hsl_array > 0).sum() > 100
+
