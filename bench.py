@@ -990,8 +990,9 @@ def run_stages(args, wl, dev):
 
     # the Mapping stage's passes 1 and 2 with the grids on the GPU: the
     # coarse channels at the 94th-percentile threshold, then per coarse
-    # subsegment its KDE threshold, fine channels, traced hillslope lengths
-    # and their statistics
+    # subsegment its KDE threshold, fine channels, the hillslope lengths (by
+    # fast marching, the reference's measurement; then, on a fresh stage,
+    # traced along streamlines) and their statistics
     import types
 
     from slm_b200 import analysis as A
@@ -1005,14 +1006,22 @@ def run_stages(args, wl, dev):
     trace_ns = types.SimpleNamespace(**vars(wl.defaults.trace))
     trace_ns.slc_array, trace_ns.slt_array, trace_ns.sla_array = data2.slc_array, data2.slt_array, data2.sla_array
     geodata = types.SimpleNamespace(roi_nx=spec.n, roi_ny=spec.n, pad_width=2, roi_pixel_size=spec.pixel_size)
-    stage = Mapping(state, {"mapping": dict(coarse_channel_threshold=float(thr), coarse_segmentation_threshold=200)},
-                    geodata, types.SimpleNamespace(uv_array=wl.uv), trace_ns,
-                    analysis=A.Analysis(state, None, geodata, None, trace_ns), device=dev)
+    def new_stage():
+        return Mapping(state, {"mapping": dict(coarse_channel_threshold=float(thr),
+                                               coarse_segmentation_threshold=200)},
+                       geodata, types.SimpleNamespace(uv_array=wl.uv), trace_ns,
+                       analysis=A.Analysis(state, None, geodata, None, trace_ns), device=dev)
+    stage = new_stage()
     timed("mapping_pass1_s", stage.pass1)
-    timed("mapping_pass2_s", stage.pass2)
+    timed("mapping_pass2_s", lambda: stage.pass2(hsl_method="fmm"))
     out["mapping_coarse_subsegments"] = int(stage.n_coarse_subsegments)
     out["mapping_passes_status"] = int(stage.engine.status)
     out["mapping_pass2_subsegments_with_lengths"] = int(len(stage.hsl_mean_array))
+    out["mapping_pass2_hsl_pixels"] = int((stage.hsl_array > 0).sum())
+    traced = new_stage()
+    traced.pass1()
+    timed("mapping_pass2_traced_s", lambda: traced.pass2(hsl_method="traced"))
+    out["mapping_pass2_traced_subsegments_with_lengths"] = int(len(traced.hsl_mean_array))
     out["ok"] = bool(ok)
     return out
 

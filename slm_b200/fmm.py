@@ -19,6 +19,8 @@ skfmm's exception).
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 import torch
 
@@ -84,19 +86,29 @@ def device_solver(label, flags, thin_bit, subsegments, dx, order, fields=False):
         st = torch.empty(total, dtype=torch.uint8, device=dev)
         hkey = torch.empty(4 * total, dtype=torch.float64, device=dev)
         hidx = torch.empty(4 * total, dtype=torch.int32, device=dev)
-        sub_d = torch.from_numpy(keys[li].astype(np.int32)).to(dev)
-        box_d = torch.from_numpy(b.astype(np.int32).reshape(-1)).to(dev)
-        off_d = torch.from_numpy(offs).to(dev)
-        s_d = torch.empty(m, dtype=torch.float64, device=dev)
-        c_d, p_d, h_d = (torch.empty(m, dtype=torch.int64, device=dev) for _ in range(3))
-        st_d = torch.empty(m, dtype=torch.int32, device=dev)
+        # inputs up in one buffer (offsets int64, boxes and labels int32),
+        # outputs back in one (sum f64, count / n_phi / n_channel i64, status i32)
+        up = np.empty(8 * m + 16 * m + 4 * m, dtype=np.uint8)
+        up[:8 * m].view(np.int64)[:] = offs
+        up[8 * m:24 * m].view(np.int32)[:] = b.astype(np.int32).reshape(-1)
+        up[24 * m:].view(np.int32)[:] = keys[li].astype(np.int32)
+        up_d = torch.from_numpy(up).to(dev)
+        down_d = torch.empty(36 * m, dtype=torch.uint8, device=dev)
         P = _lib.ptr
+        u0, d0 = up_d.data_ptr(), down_d.data_ptr()
+
+        def at(base, byte):
+            return ctypes.c_void_p(base + byte)
         _lib.check(_lib.load().slm_fmm_lengths(
-            P(label), P(flags32), int(nx), int(ny), int(thin_bit) & 0xFFFFFFFF, P(sub_d), P(box_d), P(off_d),
-            int(m), total, int(order), float(dx), P(val), P(st), P(hkey), P(hidx), P(s_d), P(c_d), P(p_d),
-            P(h_d), P(st_d), torch.cuda.current_stream(dev).cuda_stream))
-        for k, t in enumerate((s_d, c_d, p_d, h_d, st_d)):
-            out[k][li] = t.cpu().numpy()
+            P(label), P(flags32), int(nx), int(ny), int(thin_bit) & 0xFFFFFFFF, at(u0, 24 * m), at(u0, 8 * m),
+            at(u0, 0), int(m), total, int(order), float(dx), P(val), P(st), P(hkey), P(hidx), at(d0, 0),
+            at(d0, 8 * m), at(d0, 16 * m), at(d0, 24 * m), at(d0, 32 * m),
+            torch.cuda.current_stream(dev).cuda_stream))
+        down = down_d.cpu().numpy()
+        out[0][li] = down[:8 * m].view(np.float64)
+        for k in range(3):
+            out[1 + k][li] = down[8 * m * (k + 1):8 * m * (k + 2)].view(np.int64)
+        out[4][li] = down[32 * m:].view(np.int32)
         if fields:
             vh, sh = val.cpu().numpy(), st.cpu().numpy()
             per = [None] * n

@@ -32,7 +32,9 @@ SPECS = {
 # bytes of the flank path store.  None: 2 KiB per item (at least 1 GiB), at
 # most half the device's free memory and FLANK_PATH_MAX.  The walks are
 # traced once into it when they fit (~45 GB at 8192^2); otherwise they are
-# traced again into index-ordered chunks of it.
+# traced again into index-ordered chunks of it.  The free memory is asked
+# for (cudaMemGetInfo, milliseconds a call) only above the 1 GiB floor, or
+# when the floor itself cannot be allocated: not per call of a small window.
 FLANK_PATH_BUDGET = None
 FLANK_PATH_MAX = 96 << 30
 _MIN_WS = {
@@ -73,10 +75,17 @@ def run_device(name, params, seeds_d, n, bufs, device=None, stream=None, status=
             # the flank fix stores paths chunk by chunk within this budget
             budget = FLANK_PATH_BUDGET
             if budget is None:
-                free, _ = torch.cuda.mem_get_info(dev)
-                budget = min(max(1 << 30, int(n) << 11), FLANK_PATH_MAX, free // 2)
+                budget = max(1 << 30, int(n) << 11)
+                if budget > 1 << 30:
+                    budget = min(budget, FLANK_PATH_MAX, torch.cuda.mem_get_info(dev)[0] // 2)
+            try:
+                ws = torch.empty(size + int(budget), dtype=torch.uint8, device=dev)
+            except torch.cuda.OutOfMemoryError:
+                budget = min(int(budget), torch.cuda.mem_get_info(dev)[0] // 2)
+                ws = torch.empty(size + int(budget), dtype=torch.uint8, device=dev)
             size += int(budget)
-        ws = torch.empty(size, dtype=torch.uint8, device=dev)
+        else:
+            ws = torch.empty(size, dtype=torch.uint8, device=dev)
         rc = fn(*(args + [ptr(ws), size, ctypes.byref(need), st]))
         if rc == _lib.SLM_ERR_CAPACITY:
             size = int(need.value)
