@@ -35,7 +35,8 @@ class DeviceMapping:
         ``device`` (used in place; ``mapping_array`` is then updated there):
         ``mask_array`` [nxp, nyp] bool/uint8, ``uv_array`` [nxp, nyp, 2],
         ``mapping_array`` uint32, ``slt_array`` / ``slc_array`` [nxp, nyp, 2]
-        (only the downstream half is read)."""
+        (only the downstream half is read).  Its kernels run on the CUDA
+        stream that is current when it is made."""
         self.info, self.data = info, data
         self.dev = device if device is not None else cuda_device(0, 0)
         self.L = _lib.load()
@@ -73,6 +74,8 @@ class DeviceMapping:
         self._n_slots = 0
         self._no_status = torch.zeros(1, dtype=torch.uint32, device=dev)
         self._prm = None
+        # its kernels run on the stream that was current when it was made
+        self._st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
 
     @property
     def status(self):
@@ -97,7 +100,7 @@ class DeviceMapping:
         return prm
 
     def _stream(self):
-        return ctypes.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
+        return self._st
 
     # ------------------------------------------------------------ host-step kernels
     def pick(self, mask=True, map=None, flag=0, invert=False):

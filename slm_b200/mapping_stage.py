@@ -297,17 +297,39 @@ def length_statistics(fine_labels, lengths, coarse_label):
     return rows
 
 
+_EMPTY_STATS = {}
+
+
+def empty_statistics(coarse_label):
+    """``length_statistics``' table with no rows (its columns, dtypes and
+    index levels), made once per dtype of the coarse label."""
+    key = np.asarray(coarse_label).dtype
+    if key not in _EMPTY_STATS:
+        _EMPTY_STATS[key] = length_statistics(np.array([1], np.int32), np.array([0], np.int32),
+                                              coarse_label).iloc[0:0]
+    return _EMPTY_STATS[key].copy()
+
+
 def paint_means(labels, stats, min_count, device):
     """Each listed fine subsegment's mean length on its pixels (0 when it has
     fewer than ``min_count`` lengths, and on unlisted pixels); float32."""
-    out = torch.zeros(labels.shape, dtype=torch.float32, device=device)
     if stats is None or len(stats) == 0:
-        return out
+        return torch.zeros(labels.shape, dtype=torch.float32, device=device)
     fine = stats.index.get_level_values("fine").to_numpy(np.int64)
     value = np.where(stats["count"].to_numpy() >= min_count, stats["mean [m]"].to_numpy(), 0.0)
+    return paint_values(labels, fine, value, device)
+
+
+def paint_values(labels, fine, value, device):
+    """``value[i]`` (rounded to float32) on the pixels labelled ``fine[i]``;
+    0 elsewhere."""
+    out = torch.zeros(labels.shape, dtype=torch.float32, device=device)
+    fine = np.asarray(fine, dtype=np.int64)
+    if fine.size == 0:
+        return out
     order = np.argsort(fine, kind="stable")
     keys = torch.from_numpy(fine[order]).to(device)
-    vals = torch.from_numpy(value[order].astype(np.float32)).to(device)
+    vals = torch.from_numpy(np.asarray(value)[order].astype(np.float32)).to(device)
     lab = labels.to(torch.int64)
     k = torch.searchsorted(keys, lab).clamp_(max=keys.numel() - 1)
     hit = keys[k] == lab
@@ -487,36 +509,38 @@ class Mapping:
             head = int(info.is_channelhead)
             flags = torch.where((flags & head) == head, flags | int(info.was_channelhead), flags)
             if hsl_method == "fmm":
-                # every subsegment with an unmasked pixel, one length each;
-                # all are painted (no count threshold)
+                # every subsegment with an unmasked pixel, one length each:
+                # its statistics row has count 1 and mean = the length, every
+                # row is painted (no count threshold), and none passes the
+                # count > 1 filter of the returned table
                 fine = torch.unique(labels[~mask_w])
                 fine = fine[fine != 0].cpu().numpy().astype(np.int32)
                 lengths = engine.fmm_lengths(info, flags, labels, fine, pixel_size, FMM_ORDER)
                 if not (lengths > 0).any():
                     return None
-                min_count = 0
+                painted = paint_values(labels, fine, lengths.astype(np.float64), roi.device)
+                table = empty_statistics(label)
             else:
                 picked = ((flags & int(info.is_midslope)) > 0) & ~mask_w
                 fine = labels[picked].cpu().numpy()
                 lengths = engine.lengths(info, flags, int(fine.shape[0]))
                 if lengths is None:
                     return None
-                lengths = np.asarray(lengths, dtype=np.float32)
-                min_count = self.n_hsl_averaging_threshold
-            stats = length_statistics(fine, lengths, label)
-            if stats is None:
-                return None
-            painted = paint_means(labels, stats, min_count, roi.device)
+                stats = length_statistics(fine, np.asarray(lengths, dtype=np.float32), label)
+                if stats is None or len(stats) == 0:
+                    return None
+                painted = paint_means(labels, stats, self.n_hsl_averaging_threshold, roi.device)
+                table = stats[(stats["count"] > 1) & (stats["mean [m]"] > 5.0)]
             kept = painted[~torch.isnan(painted)]
             kept = kept[kept >= self.hsl_averaging_threshold].cpu().numpy()
-            if len(stats) == 0 or kept.shape[0] == 0:
+            if kept.shape[0] == 0:
                 return None
             # only the subsegment's own unmasked pixels take the results
             take = own_w & ~win.of(base)
             win.of(roi.hsl)[take] = torch.nan_to_num(painted, nan=0.0)[take]
             target = win.of(roi.mapping)
             target[take] |= flags[take]
-            return np.mean(kept), stats[(stats["count"] > 1) & (stats["mean [m]"] > 5.0)]
+            return np.mean(kept), table
 
         results = self._run_subsegments(one, roi, base, coarse_labels, boxes)
         means = [r[0] for r in results if r is not None]
