@@ -225,6 +225,37 @@ def hsl(cl_state, info, data, do_use_ridges, verbose=False, runner=None):
     return True
 
 
+def fmm_lengths(cl_state, info, data, pixel_size, order=2, verbose=False, runner=None):
+    """``Mapping.fmm_lengths`` (mapping.py:841-900) on ``data``: the
+    fast-marching length of each of ``data.selected_subsegments_array`` from
+    ``data.label_array`` and the thin-channel flags of
+    ``data.mapping_array``, into ``data.subsegment_hsl_array`` (int32, as the
+    reference's array is) and ``data.fmm_mean_hsl`` (the mean of the positive
+    ones).  Returns False when none is positive.  The distances come from the
+    runner's ``fmm_solver`` when it has one (the oracle's), else from the
+    CUDA kernel ``slm_fmm_lengths`` on the runner's device."""
+    from . import fmm
+    r = _runner(runner)
+    solver = getattr(r, "fmm_solver", None)
+    label, flags = data.label_array, data.mapping_array
+    if solver is None:
+        import torch
+
+        from .device import cuda_device
+        dev = getattr(r, "device", None) or cuda_device(0, 0)
+        label = torch.from_numpy(np.ascontiguousarray(label, dtype=np.int32)).to(dev)
+        flags = torch.from_numpy(np.asarray(flags).astype(np.int64)).to(dev)
+    hsl = fmm.fmm_lengths(label, flags, int(info.is_thinchannel), data.selected_subsegments_array,
+                          float(pixel_size), order, solver=solver)
+    data.subsegment_hsl_array = hsl
+    positive = hsl[hsl > 0]
+    if positive.size == 0:
+        return False
+    data.fmm_mean_hsl = np.mean(positive)
+    vprint(verbose, "FMM mean HSL = {0:0.1f}m".format(data.fmm_mean_hsl))
+    return True
+
+
 # ------------------------------------------------------------------ sequence
 def map_channels(info, data):
     """Channel pixels from the downstream fields (mapping.py:695-702)."""

@@ -89,3 +89,22 @@ def test_fmm_lengths_gpu_equals_oracle_solver():
     a = fmm.fmm_lengths(lab_d, flg_d, thin, sel, 2.0)
     b = fmm.fmm_lengths(label, flags, thin, sel, 2.0, solver=E.solve_problems)
     assert a.dtype == np.int32 and np.array_equal(a, b) and (a > 0).any()
+
+
+def test_wrapper_fmm_lengths_device_runner_equals_oracle():
+    """The reference-shaped wrapper (slm_b200.mapping.fmm_lengths) on the
+    device runner equals it on the oracle runner, on mapped grids."""
+    import copy
+
+    from mapping_cases import incised_pipeline_case, oracle_runner
+    from slm_b200 import mapping as M
+    info, data = incised_pipeline_case(n=64, seed=3, n_incisions=6, max_steps=200)
+    assert M.map_channels_segments(None, info, data, runner=oracle_runner)
+    lab = data.label_array[~data.mask_array]
+    data.selected_subsegments_array = np.unique(lab[lab != 0]).astype(np.int32)
+    a, b = copy.deepcopy(data), copy.deepcopy(data)
+    ok_gpu = M.fmm_lengths(None, info, a, 2.0, runner=M.DeviceRunner(DEV))
+    ok_cpu = M.fmm_lengths(None, info, b, 2.0, runner=oracle_runner)
+    assert ok_gpu and ok_cpu
+    assert np.array_equal(a.subsegment_hsl_array, b.subsegment_hsl_array)
+    assert a.fmm_mean_hsl == b.fmm_mean_hsl

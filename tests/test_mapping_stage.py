@@ -163,6 +163,34 @@ def test_traced_hillslope_length_statistics_match_reference(reference_dir, seed)
     assert len(stats) > 3 and painted.any()
 
 
+@pytest.mark.parametrize("seed", [3, 5])
+def test_fmm_lengths_match_reference(reference_dir, seed, monkeypatch):
+    """The wrappers' fmm_lengths (the oracle's solver) against the reference's
+    own select_subsegments(do_restrict=False) + Mapping.fmm_lengths, with
+    skfmm.distance stood in by the oracle's restatement, on the same mapped
+    grids: the int32 lengths per selected subsegment and their mean."""
+    import copy
+
+    import eikonal
+    R = _reference_mapping_module(reference_dir)
+    monkeypatch.setattr(R, "skfmm", types.SimpleNamespace(distance=eikonal.distance), raising=False)
+    info, data = incised_pipeline_case(n=64, seed=seed, n_incisions=6, max_steps=200)
+    assert M.map_channels_segments(None, info, data, runner=oracle_runner)
+    ref = R.Mapping.__new__(R.Mapping)
+    ref.__dict__.update(do_measure_hsl_from_ridges=False, cl_state=None, verbose=False, print=lambda *a, **k: None,
+                        geodata=types.SimpleNamespace(roi_pixel_size=2.0))
+    rd = copy.deepcopy(data)
+    ref.select_subsegments(info, rd, do_restrict=False)
+    ok = ref.fmm_lengths(info, rd)
+    md = copy.deepcopy(data)
+    md.selected_subsegments_array = rd.selected_subsegments_array.copy()
+    assert M.fmm_lengths(None, info, md, 2.0, runner=oracle_runner) == ok
+    assert md.subsegment_hsl_array.dtype == rd.subsegment_hsl_array.dtype == np.int32
+    assert np.array_equal(md.subsegment_hsl_array, rd.subsegment_hsl_array)
+    assert ok and md.fmm_mean_hsl == rd.fmm_mean_hsl
+    assert (md.subsegment_hsl_array > 0).sum() > 3
+
+
 class ActiveMasks:
     """The reference State's active-mask bookkeeping (state.py:374-459)."""
 
