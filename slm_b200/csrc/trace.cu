@@ -40,15 +40,17 @@ __device__ __forceinline__ void acc_flush(Acc& a, u64* __restrict__ slc, u64* __
 __device__ __forceinline__ void acc_visit(Acc& a, uint32_t idx, float l, u64* __restrict__ slc,
                                           u64* __restrict__ slt) {
     const u64 v = __float2uint_rz(l + 0.5f);
-    if (idx == a.idx && a.cnt) {
-        a.cnt += 1;
-        a.sum += v;
-    } else {
-        acc_flush(a, slc, slt);
-        a.idx = idx;
-        a.cnt = 1;
-        a.sum = v;
+    // only the two atomics of a finished run branch; the bookkeeping is
+    // selects, so a warp whose lanes change pixel at different steps runs it
+    // once with every lane active
+    const bool same = (idx == a.idx) && a.cnt;
+    if (!same && a.cnt) {
+        atomicAdd(slt + a.idx, a.sum);
+        atomicAdd(slc + a.idx, (u64)a.cnt);
     }
+    a.cnt = same ? a.cnt + 1u : 1u;
+    a.sum = same ? a.sum + v : v;
+    a.idx = idx;
 }
 
 // State of one jittered field trajectory between steps.
