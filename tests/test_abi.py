@@ -89,3 +89,19 @@ def test_pair_and_preprocess_arguments_rejected_without_device():
     n = ctypes.c_uint64(0)
     rc = L.slm_create_seeds(mask.ctypes.data, 6, 5, 1, 1, 1, out.ctypes.data, 3, ctypes.byref(n), None)
     assert rc == _lib.SLM_ERR_CAPACITY and n.value == 30
+
+
+def test_fmm_lengths_arguments_rejected_without_device():
+    """slm_fmm_lengths' host checks (nothing reaches the device): an order
+    other than 1 or 2, an empty window, a null buffer; no problems is a
+    no-op that touches nothing."""
+    L = _lib.load()
+    fake = ctypes.c_void_p(4096)  # never dereferenced: the checks fail first
+
+    def call(nx=8, ny=8, n=1, order=2, val=fake):
+        return L.slm_fmm_lengths(fake, fake, nx, ny, 1, fake, fake, fake, n, 64, order, 1.0, val, fake, fake,
+                                 fake, fake, fake, fake, fake, fake, None)
+    assert call(order=3) == _lib.SLM_ERR_ARGS and b"order" in L.slm_last_error()
+    assert call(nx=0) == _lib.SLM_ERR_ARGS and b"window" in L.slm_last_error()
+    assert call(val=None) == _lib.SLM_ERR_ARGS and b"null" in L.slm_last_error()
+    assert call(n=0, val=None) == _lib.SLM_OK
